@@ -1,0 +1,153 @@
+/*
+ * kmhd_sph.h -- C-ABI of the B200 spherical-transform cycle.
+ *
+ * Drop-in boundary for Calypso's transform entry points.  Every entry point
+ * takes plain pointers and sizes, returns an int status (KMHD_OK = 0) and never
+ * exits; kmhd_strerror() turns a status into text.  The reference aborts via
+ * calypso_MPI_abort instead (SOLVER_src/send_recv/calypso_mpi.f90:114).
+ *
+ * Spectral arrays use the reference's rj layout: d_rj(inod, icomp),
+ * column-major, inod = j + J*k (j fastest, k = radius), leading dimension ld.
+ * A vector field occupies three consecutive columns (S, dS/dr, T); the caller
+ * names the first column of each field (cols_*), as ipol%i_velo etc. do in
+ * MHD_src/sph_MHD/set_address_sph_trans_MHD.f90.  The j order is the
+ * reference's single-domain order (m = -L..L, then l = |m|..L) unless
+ * kmhd_sph_desc.idx_rj_lm gives (l, m) per j.
+ * Grid arrays use the reference's rtp layout: fld_rtp(nnod_rtp, ncomp),
+ * column-major, node = r + Nr*(theta + Ntheta*phi); a vector's three
+ * columns are (r, theta, phi) components.
+ * Paths are relative to MHD/Fortran_src/ of the reference.
+ */
+#ifndef KMHD_SPH_H
+#define KMHD_SPH_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum kmhd_status {
+  KMHD_OK = 0,
+  KMHD_ERR_ARG = 1,        /* invalid descriptor or argument */
+  KMHD_ERR_SIZE = 2,       /* unsupported size (L, grid, field counts) */
+  KMHD_ERR_CUDA = 3,       /* CUDA runtime error */
+  KMHD_ERR_NOMEM = 4,      /* device allocation failed */
+  KMHD_ERR_DEVICE = 5,     /* no sm_100 device */
+  KMHD_ERR_TIMEOUT = 6,    /* bounded device wait expired (work queue) */
+  KMHD_ERR_STATE = 7       /* call order / handle state */
+};
+
+enum kmhd_tier {
+  KMHD_TIER_FP64 = 0,      /* FP64 Legendre GEMMs (DMMA), bit-faithful method   */
+  KMHD_TIER_SPLIT_I8 = 1,  /* INT8-slice split products on tcgen05, <=1e-12     */
+  KMHD_TIER_FP32ACC = 2    /* 3-slice INT8 split products on tcgen05, <=1e-6    */
+};
+
+enum kmhd_product_kind {
+  KMHD_PROD_CROSS = 0,       /* fwd vector = coef * (bwd_vec[a] x bwd_vec[b])   */
+  KMHD_PROD_VEC_SCALAR = 1,  /* fwd vector = coef * bwd_vec[a] * bwd_scl[b]     */
+  KMHD_PROD_DOT = 2,         /* fwd scalar = coef * (bwd_vec[a] . bwd_vec[b])   */
+  KMHD_PROD_SCALAR = 3       /* fwd scalar = coef * bwd_scl[a] * bwd_scl[b]     */
+};
+
+/* One grid-space product of the cycle; forward vectors are produced in list
+ * order, then forward scalars.  Mirrors cal_cross_prod_w_coef_smp /
+ * cal_vec_scalar_prod_w_coef_smp / cal_dot_prod_w_coef_smp
+ * (CORE_src/BASE/cal_products_smp.f90) as called by nonlinear_terms_in_rtp
+ * (MHD_src/sph_MHD/cal_nonlinear_sph_MHD.f90:64-128). */
+typedef struct kmhd_product {
+  int32_t kind;
+  int32_t a, b;
+  double coef;
+} kmhd_product;
+
+typedef struct kmhd_sph_desc {
+  int32_t ltr;          /* truncation L (l_truncation)                         */
+  int32_t nth;          /* Gauss-Legendre latitudes  (nidx_rtm(2))             */
+  int32_t nph;          /* longitudes (nidx_rtp(3)), 2^a 3^b 5^c, > 2L         */
+  int32_t nr;           /* radial points (nidx_rj(1))                          */
+  const double *radius; /* [nr] host, radius_1d_rj_r                           */
+  const int32_t *idx_rj_lm; /* [2*(L+1)^2] host (l, m) per rj j, or NULL       */
+  int32_t nvector_b, nscalar_b;   /* rj -> rtp fields  (nvector_rj_2_rtp ...)  */
+  int32_t nvector_f, nscalar_f;   /* rtp -> rj fields  (nvector_rtp_2_rj ...)  */
+  int32_t nproduct;               /* grid products for kmhd_sph_cycle          */
+  const kmhd_product *products;   /* [nproduct] host                           */
+  int32_t tier;                   /* enum kmhd_tier                            */
+  int32_t nslice;                 /* split tiers: slices per operand, 0=default */
+  int32_t device;                 /* CUDA device ordinal                       */
+  int32_t flags;                  /* reserved, 0                               */
+} kmhd_sph_desc;
+
+typedef struct kmhd_sph kmhd_sph;
+
+/* Pointer-location flag for data arguments. */
+#define KMHD_PTR_DEVICE 0
+#define KMHD_PTR_HOST 1
+
+/* Builds the handle: Gauss nodes/weights, Schmidt P_l^m and dP_l^m/dtheta
+ * tables (FP64 recurrence on the device), index tables and work buffers.
+ * Replaces initialize_legendre_trans / init_legendre_rtm / set_sym_legendre_stack
+ * / init_legendre_sym_matmul (PARALLEL_src/SPH_SHELL_src/init_sph_trans.f90:79-168,
+ * t_legendre_work_sym_matmul.f90:150-262). */
+int kmhd_sph_create(const kmhd_sph_desc *desc, kmhd_sph **handle);
+
+/* Releases every device resource of the handle. */
+int kmhd_sph_destroy(kmhd_sph *handle);
+
+/* Binds a caller stream (cudaStream_t) for all subsequent calls; NULL = the
+ * handle's own stream. */
+int kmhd_sph_set_stream(kmhd_sph *handle, void *stream);
+
+/* Backward transform: spectral fields -> grid.  Replaces sph_b_trans_w_coriolis
+ * without Coriolis (MHD_src/sph_MHD/sph_trans_w_coriols.f90:113-187) and
+ * sph_backward_transforms (PARALLEL_src/SPH_SHELL_src/t_sph_transforms.f90:74-123).
+ * d_rj: ld >= J*nr; cols_b[nvector_b + nscalar_b] first column per field.
+ * fld_rtp: nnod_rtp x (3*nvector_b + nscalar_b), column-major. */
+int kmhd_sph_b_trans(kmhd_sph *handle, const double *d_rj, int64_t ld_rj,
+                     const int32_t *cols_b, double *fld_rtp, int32_t ptr_kind);
+
+/* Forward transform: grid forces -> spectral.  Replaces sph_f_trans_w_coriolis
+ * without Coriolis (sph_trans_w_coriols.f90:189-246) and sph_forward_transforms
+ * (t_sph_transforms.f90:250-297).  frc_rtp: nnod_rtp x (3*nvector_f + nscalar_f). */
+int kmhd_sph_f_trans(kmhd_sph *handle, const double *frc_rtp, double *d_rj,
+                     int64_t ld_rj, const int32_t *cols_f, int32_t ptr_kind);
+
+/* Full cycle: backward transform, grid products, forward transform.  Replaces
+ * the copy_mhd_spectr_to_send -> sph_b_trans -> nonlinear_terms_in_rtp ->
+ * sph_f_trans -> copy_mhd_spectr_from_recv segment of nonlinear_by_pseudo_sph
+ * (MHD_src/sph_MHD/cal_nonlinear.f90:118-171). */
+int kmhd_sph_cycle(kmhd_sph *handle, const double *d_rj_in, int64_t ld_in,
+                   const int32_t *cols_b, double *d_rj_out, int64_t ld_out,
+                   const int32_t *cols_f, int32_t ptr_kind);
+
+/* Batched uneven instances: runs kmhd_sph_cycle for n handles with device
+ * pointers in one grouped launch sequence (work list over instance, m and
+ * radial blocks) captured in a CUDA graph on the first handle's stream.
+ * Replaces n calls of the cycle; the reference has no batched form. */
+int kmhd_sph_batch_cycle(kmhd_sph **handles, int32_t n, const double *const *d_rj_in,
+                         const int64_t *ld_in, const int32_t *const *cols_b,
+                         double *const *d_rj_out, const int64_t *ld_out,
+                         const int32_t *const *cols_f);
+
+/* Stage times of the last call in ms (CUDA events): [0] Legendre bwd (label 22),
+ * [1] FFT + products + FFT (labels 24 + nonlinear), [2] Legendre fwd (label 23),
+ * [3] whole call.  Labels as in MHD_src/IO/init_sph_MHD_elapsed_label.f90:38-84. */
+int kmhd_sph_last_timing(kmhd_sph *handle, double *ms4);
+
+/* Copies the device Gauss colatitudes/weights [nth] and the hemisphere
+ * P / dP tables of order m ([nth_hemi x (L-m+1)], rows theta, cols l) to host
+ * arrays, for parity checks of the set-up stage. */
+int kmhd_sph_get_tables(kmhd_sph *handle, int32_t m, double *colat, double *weight,
+                        double *P, double *dP);
+
+/* Device bytes held by the handle. */
+int64_t kmhd_sph_device_bytes(const kmhd_sph *handle);
+
+const char *kmhd_strerror(int status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KMHD_SPH_H */

@@ -1,0 +1,107 @@
+// kmhd_internal.cuh -- shared device utilities and the per-instance plan.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/kmhd_sph.h"
+
+namespace kmhd {
+
+// ---------------------------------------------------------------------------
+// Tile geometry shared by host and device.
+constexpr int kWarps = 8;
+constexpr int kThreads = kWarps * 32;
+constexpr int kRB = 4;        // radii per column block (one "quad" per field)
+constexpr int kThBlk = 64;    // hemisphere latitudes per backward CTA
+constexpr int kKC = 16;       // reduction chunk (l for bwd, theta for fwd)
+constexpr int kLBlk = 32;     // l rows per parity per forward CTA
+constexpr int kMaxVec = 4;    // vectors per field group
+constexpr int kMaxScl = 2;    // scalars per field group
+constexpr int kMaxProd = 16;
+constexpr int kMaxFftFactors = 16;
+
+// Plan of one transform instance (device pointers + sizes).
+struct Plan {
+  int L, nth, nph, nr, nh, nh_pad, nr4, nrb;
+  long long J;
+  int nvb, nsb, nvf, nsf, ncb, ncf;
+  // tables
+  const double* radius;   // [nr]
+  const double* colat;    // [nth]
+  const double* weight;   // [nth]
+  const double* asin_t;   // [nth]
+  const double* P;        // Ptab[m][p][kpad][nh_pad]
+  const double* dP;
+  const long long* poff;  // [(L+1)*2] element offset of (m,p) block in P/dP
+  const int* kpad;        // [(L+1)*2]
+  const int* jmap;        // [(L+1)][2][L+1] -> rj j, -1 if absent
+  // work buffers
+  double* SB;             // packed backward spectra [m][p][kpad][nrb*ncolb_blk]
+  const long long* sboff; // [(L+1)*2]
+  double* rtm_b;          // [m][th][r][ncb][2]
+  double* rtm_f;          // [m][th][r][ncf][2]
+  // FFT
+  int nfac;
+  int fac[kMaxFftFactors];
+  const double2* twid;    // [nph] e^{+2 pi i k/nph}
+  const int* digrev;      // [nph] frequency index of DIF output slot
+  // products
+  int nprod;
+  int pkind[kMaxProd], pa[kMaxProd], pb[kMaxProd];
+  double pcoef[kMaxProd];
+};
+
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__host__ __device__ __forceinline__ int kcount(int L, int m, int p) {
+  // number of l in [m, L] with (l - m) % 2 == p
+  return p == 0 ? (L - m) / 2 + 1 : (L - m + 1) / 2;
+}
+
+__host__ __device__ __forceinline__ double g7_of(int l, int m) {
+  // sph_normalizations (CORE_src/spherical_harmonics/spherical_harmonics.f90:121-136)
+  if (l == 0) return 1.0;
+  if (m == 0) return (double)(2 * l + 1) / (double)(2 * l * (l + 1));
+  return (double)(2 * l + 1) / (double)(4 * l * (l + 1));
+}
+__host__ __device__ __forceinline__ double g6_of(int l, int m) {
+  if (l == 0 && m == 0) return 0.5;
+  if (m == 0) return (double)(2 * l + 1) / 2.0;
+  return (double)(2 * l + 1) / 4.0;
+}
+__host__ __device__ __forceinline__ double g3_of(int l) {
+  // g(j,3) = l(l+1), overridden to 1/2 at l = 0 (schmidt_poly_on_rtm_grid.f90:109)
+  return l == 0 ? 0.5 : (double)(l * (l + 1));
+}
+
+// Launchers (defined in the .cu files).
+cudaError_t launch_tables(const Plan& p, double* colat, double* weight, double* asin_t,
+                          double* P, double* dP, cudaStream_t s);
+cudaError_t launch_pack_b(const Plan& p, int nlc_max, const double* d_rj, long long ld,
+                          const int* cols, int nv, int ns, cudaStream_t s);
+cudaError_t launch_leg_bwd_f64(const Plan& p, cudaStream_t s);
+cudaError_t launch_leg_fwd_f64(const Plan& p, double* d_rj, long long ld, const int* cols,
+                               cudaStream_t s);
+cudaError_t launch_fft_cycle(const Plan& p, cudaStream_t s);
+cudaError_t launch_fft_bwd_grid(const Plan& p, double* fld, cudaStream_t s);
+cudaError_t launch_fft_fwd_grid(const Plan& p, const double* frc, cudaStream_t s);
+
+}  // namespace kmhd

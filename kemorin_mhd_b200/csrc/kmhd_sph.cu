@@ -1,0 +1,609 @@
+// kmhd_sph.cu -- C-ABI of the B200 spherical-transform cycle (include/kmhd_sph.h).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kmhd_internal.cuh"
+#include "kmhd_split.cuh"
+
+namespace kmhd {
+size_t bwd_smem_bytes(int nv, int ns);
+size_t fft_smem_bytes(const Plan& p, int npair);
+}  // namespace kmhd
+
+using namespace kmhd;
+
+struct kmhd_sph {
+  kmhd_sph_desc desc;
+  Plan plan;
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  std::vector<kmhd_product> products;
+  std::vector<int> kpad_h;
+  std::vector<long long> poff_h, sboff_h;
+  std::vector<int> jmap_h;
+  int nlc_max = 0;
+  // device allocations
+  std::vector<void*> allocs;
+  int64_t bytes = 0;
+  double *radius = nullptr, *colat = nullptr, *weight = nullptr, *asin_t = nullptr;
+  double *P = nullptr, *dP = nullptr, *SB = nullptr, *rtm_b = nullptr, *rtm_f = nullptr;
+  long long *poff = nullptr, *sboff = nullptr;
+  int *kpad = nullptr, *jmap = nullptr, *digrev = nullptr;
+  double2* twid = nullptr;
+  int *cols_b_d = nullptr, *cols_f_d = nullptr;
+  std::vector<int> cols_b_cache, cols_f_cache;
+  // host-pointer staging
+  double *stage_in = nullptr, *stage_out = nullptr, *stage_grid = nullptr;
+  // split-precision state
+  SplitState* split = nullptr;
+  // timing
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  double last_ms[4] = {0, 0, 0, 0};
+};
+
+namespace {
+
+const char* kMsg[] = {"ok",
+                      "invalid argument",
+                      "unsupported size",
+                      "CUDA runtime error",
+                      "device allocation failed",
+                      "no sm_100 device",
+                      "bounded device wait expired",
+                      "invalid call order or handle state"};
+
+thread_local std::string g_last_cuda;
+
+#define KCHECK(call)                                                    \
+  do {                                                                  \
+    cudaError_t e_ = (call);                                            \
+    if (e_ != cudaSuccess) {                                            \
+      g_last_cuda = cudaGetErrorString(e_);                             \
+      return e_ == cudaErrorMemoryAllocation ? KMHD_ERR_NOMEM : KMHD_ERR_CUDA; \
+    }                                                                   \
+  } while (0)
+
+template <typename T>
+int dalloc(kmhd_sph* h, T** p, size_t n) {
+  void* q = nullptr;
+  const size_t bytes = sizeof(T) * (n > 0 ? n : 1);
+  cudaError_t e = cudaMalloc(&q, bytes);
+  if (e != cudaSuccess) {
+    g_last_cuda = cudaGetErrorString(e);
+    return KMHD_ERR_NOMEM;
+  }
+  h->allocs.push_back(q);
+  h->bytes += (int64_t)bytes;
+  *p = (T*)q;
+  return KMHD_OK;
+}
+
+bool factor_fft(int n, std::vector<int>& f) {
+  f.clear();
+  int r = n;
+  while (r % 8 == 0 && r / 8 >= 1) { f.push_back(8); r /= 8; }
+  while (r % 4 == 0) { f.push_back(4); r /= 4; }
+  while (r % 2 == 0) { f.push_back(2); r /= 2; }
+  while (r % 3 == 0) { f.push_back(3); r /= 3; }
+  while (r % 5 == 0) { f.push_back(5); r /= 5; }
+  return r == 1 && (int)f.size() <= kMaxFftFactors;
+}
+
+int validate(const kmhd_sph_desc* d) {
+  if (!d) return KMHD_ERR_ARG;
+  if (d->ltr < 1 || d->nth < 2 || d->nr < 1 || d->nph < 4) return KMHD_ERR_SIZE;
+  if (d->nph <= 2 * d->ltr + 1) return KMHD_ERR_SIZE;  // m <= L must stay below Nyquist
+  if (!d->radius) return KMHD_ERR_ARG;
+  if (d->nvector_b < 0 || d->nscalar_b < 0 || d->nvector_f < 0 || d->nscalar_f < 0)
+    return KMHD_ERR_ARG;
+  if (d->nvector_b > kMaxVec || d->nscalar_b > kMaxScl || d->nvector_f > kMaxVec ||
+      d->nscalar_f > kMaxScl)
+    return KMHD_ERR_SIZE;
+  if (d->nvector_b + d->nscalar_b == 0) return KMHD_ERR_ARG;
+  if (d->tier < KMHD_TIER_FP64 || d->tier > KMHD_TIER_FP32ACC) return KMHD_ERR_ARG;
+  if (d->nproduct < 0 || d->nproduct > kMaxProd) return KMHD_ERR_SIZE;
+  if (d->nproduct > 0 && !d->products) return KMHD_ERR_ARG;
+  int nv = 0, ns = 0;
+  for (int i = 0; i < d->nproduct; ++i) {
+    const kmhd_product& p = d->products[i];
+    switch (p.kind) {
+      case KMHD_PROD_CROSS:
+      case KMHD_PROD_DOT:
+        if (p.a < 0 || p.a >= d->nvector_b || p.b < 0 || p.b >= d->nvector_b) return KMHD_ERR_ARG;
+        break;
+      case KMHD_PROD_VEC_SCALAR:
+        if (p.a < 0 || p.a >= d->nvector_b || p.b < 0 || p.b >= d->nscalar_b) return KMHD_ERR_ARG;
+        break;
+      case KMHD_PROD_SCALAR:
+        if (p.a < 0 || p.a >= d->nscalar_b || p.b < 0 || p.b >= d->nscalar_b) return KMHD_ERR_ARG;
+        break;
+      default:
+        return KMHD_ERR_ARG;
+    }
+    if (p.kind == KMHD_PROD_CROSS || p.kind == KMHD_PROD_VEC_SCALAR) ++nv; else ++ns;
+  }
+  if (d->nproduct > 0 && (nv != d->nvector_f || ns != d->nscalar_f)) return KMHD_ERR_ARG;
+  std::vector<int> f;
+  if (!factor_fft(d->nph, f)) return KMHD_ERR_SIZE;
+  const int npair = (std::max(3 * d->nvector_b + d->nscalar_b, 3 * d->nvector_f + d->nscalar_f) + 1) / 2;
+  if (sizeof(double2) * ((size_t)npair * d->nph + d->nph) > 227 * 1024) return KMHD_ERR_SIZE;
+  return KMHD_OK;
+}
+
+int sync_cols(kmhd_sph* h, const int32_t* cols, int n, std::vector<int>& cache, int* dev) {
+  if (!cols) return KMHD_ERR_ARG;
+  for (int i = 0; i < n; ++i)
+    if (cols[i] < 0) return KMHD_ERR_ARG;
+  if ((int)cache.size() == n && std::memcmp(cache.data(), cols, sizeof(int) * n) == 0) return KMHD_OK;
+  cache.assign(cols, cols + n);
+  KCHECK(cudaMemcpyAsync(dev, cols, sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
+  KCHECK(cudaStreamSynchronize(h->stream));
+  return KMHD_OK;
+}
+
+int check_ld(const kmhd_sph* h, int64_t ld) {
+  return ld >= h->plan.J * (long long)h->plan.nr ? KMHD_OK : KMHD_ERR_ARG;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* kmhd_strerror(int status) {
+  if (status < 0 || status > KMHD_ERR_STATE) return "unknown status";
+  if (status == KMHD_ERR_CUDA && !g_last_cuda.empty()) return g_last_cuda.c_str();
+  return kMsg[status];
+}
+
+int64_t kmhd_sph_device_bytes(const kmhd_sph* h) { return h ? h->bytes : 0; }
+
+int kmhd_sph_destroy(kmhd_sph* h) {
+  if (!h) return KMHD_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->split) split_destroy(h->split);
+  for (void* p : h->allocs) cudaFree(p);
+  for (auto& e : h->ev)
+    if (e) cudaEventDestroy(e);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  delete h;
+  return KMHD_OK;
+}
+
+int kmhd_sph_create(const kmhd_sph_desc* d, kmhd_sph** out) {
+  if (!out) return KMHD_ERR_ARG;
+  *out = nullptr;
+  int st = validate(d);
+  if (st != KMHD_OK) return st;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || d->device < 0 || d->device >= ndev)
+    return KMHD_ERR_DEVICE;
+  cudaDeviceProp prop;
+  KCHECK(cudaGetDeviceProperties(&prop, d->device));
+  if (prop.major != 10) return KMHD_ERR_DEVICE;
+  KCHECK(cudaSetDevice(d->device));
+
+  kmhd_sph* h = new kmhd_sph();
+  h->desc = *d;
+  h->device = d->device;
+  if (d->nproduct > 0) h->products.assign(d->products, d->products + d->nproduct);
+  h->desc.products = nullptr;
+  h->desc.radius = nullptr;
+  h->desc.idx_rj_lm = nullptr;
+  auto fail = [&](int code) { kmhd_sph_destroy(h); return code; };
+  if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(KMHD_ERR_CUDA);
+  h->stream = h->own_stream;
+  for (auto& e : h->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return fail(KMHD_ERR_CUDA);
+
+  Plan& p = h->plan;
+  std::memset(&p, 0, sizeof(p));
+  p.L = d->ltr;
+  p.nth = d->nth;
+  p.nph = d->nph;
+  p.nr = d->nr;
+  p.nh = (d->nth + 1) / 2;
+  p.nh_pad = (p.nh + kThBlk - 1) / kThBlk * kThBlk;
+  p.nr4 = (d->nr + kRB - 1) / kRB * kRB;
+  p.nrb = p.nr4 / kRB;
+  p.J = (long long)(p.L + 1) * (p.L + 1);
+  p.nvb = d->nvector_b;
+  p.nsb = d->nscalar_b;
+  p.nvf = d->nvector_f;
+  p.nsf = d->nscalar_f;
+  p.ncb = 3 * p.nvb + p.nsb;
+  p.ncf = 3 * p.nvf + p.nsf;
+  const int L = p.L;
+
+  // ---- index tables (host)
+  h->kpad_h.resize(2 * (L + 1));
+  h->poff_h.resize(2 * (L + 1));
+  h->sboff_h.resize(2 * (L + 1));
+  const int CB = 24 * p.nvb + 8 * p.nsb;
+  long long po = 0, so = 0;
+  for (int m = 0; m <= L; ++m)
+    for (int q = 0; q < 2; ++q) {
+      const int K = kcount(L, m, q);
+      const int kp = (K + kKC - 1) / kKC * kKC;
+      h->kpad_h[2 * m + q] = kp;
+      h->poff_h[2 * m + q] = po;
+      h->sboff_h[2 * m + q] = so;
+      po += (long long)kp * p.nh_pad;
+      so += (long long)kp * p.nrb * CB;
+    }
+  h->nlc_max = h->kpad_h[0] / kKC;
+  // rj map: default order m = -L..L, l = |m|..L
+  h->jmap_h.assign((size_t)(L + 1) * 2 * (L + 1), -1);
+  {
+    const long long J = p.J;
+    std::vector<int> lm(2 * J);
+    if (d->idx_rj_lm) {
+      std::memcpy(lm.data(), d->idx_rj_lm, sizeof(int) * 2 * J);
+    } else {
+      long long j = 0;
+      for (int m = -L; m <= L; ++m)
+        for (int l = std::abs(m); l <= L; ++l) {
+          lm[2 * j] = l;
+          lm[2 * j + 1] = m;
+          ++j;
+        }
+    }
+    for (long long j = 0; j < J; ++j) {
+      const int l = lm[2 * j], m = lm[2 * j + 1];
+      if (l < 0 || l > L || std::abs(m) > l) return fail(KMHD_ERR_ARG);
+      const int am = std::abs(m), slot = m < 0 ? 1 : 0;
+      int& e = h->jmap_h[((size_t)am * 2 + slot) * (L + 1) + l];
+      if (e != -1) return fail(KMHD_ERR_ARG);  // duplicate mode
+      e = (int)j;
+    }
+  }
+  // FFT factors, twiddles e^{+2 pi i k/N}, digit reversal of the DIF output
+  std::vector<int> fac;
+  factor_fft(p.nph, fac);
+  p.nfac = (int)fac.size();
+  for (int i = 0; i < p.nfac; ++i) p.fac[i] = fac[i];
+  std::vector<double2> tw(p.nph);
+  for (int k = 0; k < p.nph; ++k) {
+    const long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)p.nph;
+    tw[k] = make_double2((double)cosl(a), (double)sinl(a));
+  }
+  std::vector<int> rev(p.nph);
+  {
+    std::vector<int> strides(p.nfac);
+    int s = p.nph;
+    for (int i = 0; i < p.nfac; ++i) { s /= fac[i]; strides[i] = s; }
+    for (int pos = 0; pos < p.nph; ++pos) {
+      int rem = pos, k = 0, mul = 1;
+      for (int i = 0; i < p.nfac; ++i) {
+        const int q = rem / strides[i];
+        rem %= strides[i];
+        k += q * mul;
+        mul *= fac[i];
+      }
+      rev[pos] = k;
+    }
+  }
+  p.nprod = (int)h->products.size();
+  for (int i = 0; i < p.nprod; ++i) {
+    p.pkind[i] = h->products[i].kind;
+    p.pa[i] = h->products[i].a;
+    p.pb[i] = h->products[i].b;
+    p.pcoef[i] = h->products[i].coef;
+  }
+
+  // ---- device allocations
+  const size_t nP = (size_t)po, nSB = (size_t)so;
+  const size_t nrtm_b = (size_t)(L + 1) * p.nth * p.nr * p.ncb * 2;
+  const size_t nrtm_f = (size_t)(L + 1) * p.nth * p.nr * std::max(p.ncf, 1) * 2;
+  const size_t nrj = (size_t)p.J * p.nr;
+  const size_t nnod = (size_t)p.nr * p.nth * p.nph;
+  if ((st = dalloc(h, &h->radius, p.nr)) || (st = dalloc(h, &h->colat, p.nth)) ||
+      (st = dalloc(h, &h->weight, p.nth)) || (st = dalloc(h, &h->asin_t, p.nth)) ||
+      (st = dalloc(h, &h->P, nP)) || (st = dalloc(h, &h->dP, nP)) ||
+      (st = dalloc(h, &h->poff, 2 * (L + 1))) || (st = dalloc(h, &h->sboff, 2 * (L + 1))) ||
+      (st = dalloc(h, &h->kpad, 2 * (L + 1))) || (st = dalloc(h, &h->jmap, h->jmap_h.size())) ||
+      (st = dalloc(h, &h->twid, p.nph)) || (st = dalloc(h, &h->digrev, p.nph)) ||
+      (st = dalloc(h, &h->cols_b_d, 16)) || (st = dalloc(h, &h->cols_f_d, 16)) ||
+      (st = dalloc(h, &h->SB, nSB)) || (st = dalloc(h, &h->rtm_b, nrtm_b)) ||
+      (st = dalloc(h, &h->rtm_f, nrtm_f)))
+    return fail(st);
+  (void)nrj;
+  (void)nnod;
+  cudaStream_t s = h->stream;
+  auto up = [&](void* dst, const void* src, size_t bytes) {
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+  };
+  if (up(h->radius, d->radius, sizeof(double) * p.nr) || up(h->poff, h->poff_h.data(), sizeof(long long) * 2 * (L + 1)) ||
+      up(h->sboff, h->sboff_h.data(), sizeof(long long) * 2 * (L + 1)) ||
+      up(h->kpad, h->kpad_h.data(), sizeof(int) * 2 * (L + 1)) ||
+      up(h->jmap, h->jmap_h.data(), sizeof(int) * h->jmap_h.size()) ||
+      up(h->twid, tw.data(), sizeof(double2) * p.nph) || up(h->digrev, rev.data(), sizeof(int) * p.nph) ||
+      cudaMemsetAsync(h->P, 0, sizeof(double) * nP, s) || cudaMemsetAsync(h->dP, 0, sizeof(double) * nP, s))
+    return fail(KMHD_ERR_CUDA);
+  p.radius = h->radius;
+  p.colat = h->colat;
+  p.weight = h->weight;
+  p.asin_t = h->asin_t;
+  p.P = h->P;
+  p.dP = h->dP;
+  p.poff = h->poff;
+  p.kpad = h->kpad;
+  p.jmap = h->jmap;
+  p.SB = h->SB;
+  p.sboff = h->sboff;
+  p.rtm_b = h->rtm_b;
+  p.rtm_f = h->rtm_f;
+  p.twid = h->twid;
+  p.digrev = h->digrev;
+  if (launch_tables(p, h->colat, h->weight, h->asin_t, h->P, h->dP, s) != cudaSuccess)
+    return fail(KMHD_ERR_CUDA);
+  if (d->tier != KMHD_TIER_FP64) {
+    st = split_create(&h->split, p, d->tier, d->nslice, s);
+    if (st != KMHD_OK) return fail(st);
+    h->bytes += split_bytes(h->split);
+  }
+  if (cudaStreamSynchronize(s) != cudaSuccess) return fail(KMHD_ERR_CUDA);
+  *out = h;
+  return KMHD_OK;
+}
+
+int kmhd_sph_set_stream(kmhd_sph* h, void* stream) {
+  if (!h) return KMHD_ERR_ARG;
+  h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+  return KMHD_OK;
+}
+
+int kmhd_sph_last_timing(kmhd_sph* h, double* ms4) {
+  if (!h || !ms4) return KMHD_ERR_ARG;
+  std::memcpy(ms4, h->last_ms, sizeof(h->last_ms));
+  return KMHD_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Stage a host d_rj (selected columns) into a compact device buffer.
+int stage_host_in(kmhd_sph* h, const double* d_rj, int64_t ld, const int32_t* cols, int nv, int ns,
+                  const double** dev, int64_t* dev_ld, std::vector<int>& cols_c) {
+  const Plan& p = h->plan;
+  const size_t nrj = (size_t)p.J * p.nr;
+  const int nc = 3 * nv + ns;
+  if (!h->stage_in) {
+    int st = dalloc(h, &h->stage_in, nrj * std::max(p.ncb, p.ncf));
+    if (st) return st;
+  }
+  cols_c.resize(nv + ns);
+  for (int f = 0; f < nv + ns; ++f) {
+    const int ncomp = f < nv ? 3 : 1;
+    const int c0 = f < nv ? 3 * f : 3 * nv + (f - nv);
+    cols_c[f] = c0;
+    KCHECK(cudaMemcpyAsync(h->stage_in + nrj * c0, d_rj + ld * cols[f], sizeof(double) * nrj * ncomp,
+                           cudaMemcpyHostToDevice, h->stream));
+  }
+  (void)nc;
+  *dev = h->stage_in;
+  *dev_ld = (int64_t)nrj;
+  return KMHD_OK;
+}
+
+int timed_begin(kmhd_sph* h) {
+  KCHECK(cudaEventRecord(h->ev[0], h->stream));
+  return KMHD_OK;
+}
+
+int run_bwd_spectral(kmhd_sph* h, const double* d_rj, int64_t ld) {
+  const Plan& p = h->plan;
+  if (h->split) {
+    int st = split_bwd(h->split, p, h->nlc_max, d_rj, ld, h->cols_b_d, h->stream);
+    return st;
+  }
+  KCHECK(launch_pack_b(p, h->nlc_max, d_rj, ld, h->cols_b_d, p.nvb, p.nsb, h->stream));
+  KCHECK(launch_leg_bwd_f64(p, h->stream));
+  return KMHD_OK;
+}
+
+int run_fwd_spectral(kmhd_sph* h, double* d_rj, int64_t ld) {
+  const Plan& p = h->plan;
+  if (h->split) return split_fwd(h->split, p, d_rj, ld, h->cols_f_d, h->stream);
+  KCHECK(launch_leg_fwd_f64(p, d_rj, ld, h->cols_f_d, h->stream));
+  return KMHD_OK;
+}
+
+int finish_timing(kmhd_sph* h) {
+  KCHECK(cudaEventSynchronize(h->ev[3]));
+  float a = 0, b = 0, c = 0, t = 0;
+  KCHECK(cudaEventElapsedTime(&a, h->ev[0], h->ev[1]));
+  KCHECK(cudaEventElapsedTime(&b, h->ev[1], h->ev[2]));
+  KCHECK(cudaEventElapsedTime(&c, h->ev[2], h->ev[3]));
+  KCHECK(cudaEventElapsedTime(&t, h->ev[0], h->ev[3]));
+  h->last_ms[0] = a;
+  h->last_ms[1] = b;
+  h->last_ms[2] = c;
+  h->last_ms[3] = t;
+  return KMHD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int kmhd_sph_b_trans(kmhd_sph* h, const double* d_rj, int64_t ld, const int32_t* cols_b,
+                     double* fld_rtp, int32_t ptr_kind) {
+  if (!h || !d_rj || !fld_rtp) return KMHD_ERR_ARG;
+  if (check_ld(h, ld)) return KMHD_ERR_ARG;
+  KCHECK(cudaSetDevice(h->device));
+  const Plan& p = h->plan;
+  const double* src = d_rj;
+  int64_t sld = ld;
+  std::vector<int> cc;
+  int st;
+  if (ptr_kind == KMHD_PTR_HOST) {
+    if ((st = stage_host_in(h, d_rj, ld, cols_b, p.nvb, p.nsb, &src, &sld, cc))) return st;
+    if ((st = sync_cols(h, cc.data(), p.nvb + p.nsb, h->cols_b_cache, h->cols_b_d))) return st;
+  } else if ((st = sync_cols(h, cols_b, p.nvb + p.nsb, h->cols_b_cache, h->cols_b_d))) {
+    return st;
+  }
+  const size_t nnod = (size_t)p.nr * p.nth * p.nph;
+  double* grid = fld_rtp;
+  if (ptr_kind == KMHD_PTR_HOST) {
+    if (!h->stage_grid && (st = dalloc(h, &h->stage_grid, nnod * std::max(p.ncb, p.ncf)))) return st;
+    grid = h->stage_grid;
+  }
+  if ((st = timed_begin(h))) return st;
+  if ((st = run_bwd_spectral(h, src, sld))) return st;
+  KCHECK(cudaEventRecord(h->ev[1], h->stream));
+  KCHECK(launch_fft_bwd_grid(p, grid, h->stream));
+  KCHECK(cudaEventRecord(h->ev[2], h->stream));
+  KCHECK(cudaEventRecord(h->ev[3], h->stream));
+  if (ptr_kind == KMHD_PTR_HOST)
+    KCHECK(cudaMemcpyAsync(fld_rtp, grid, sizeof(double) * nnod * p.ncb, cudaMemcpyDeviceToHost, h->stream));
+  KCHECK(cudaStreamSynchronize(h->stream));
+  return finish_timing(h);
+}
+
+int kmhd_sph_f_trans(kmhd_sph* h, const double* frc_rtp, double* d_rj, int64_t ld,
+                     const int32_t* cols_f, int32_t ptr_kind) {
+  if (!h || !d_rj || !frc_rtp) return KMHD_ERR_ARG;
+  if (check_ld(h, ld)) return KMHD_ERR_ARG;
+  const Plan& p = h->plan;
+  if (p.ncf == 0) return KMHD_ERR_STATE;
+  KCHECK(cudaSetDevice(h->device));
+  const size_t nnod = (size_t)p.nr * p.nth * p.nph;
+  const size_t nrj = (size_t)p.J * p.nr;
+  int st;
+  const double* grid = frc_rtp;
+  double* out = d_rj;
+  int64_t old = ld;
+  std::vector<int> cc(p.nvf + p.nsf);
+  if (ptr_kind == KMHD_PTR_HOST) {
+    if (!h->stage_grid && (st = dalloc(h, &h->stage_grid, nnod * std::max(p.ncb, p.ncf)))) return st;
+    if (!h->stage_out && (st = dalloc(h, &h->stage_out, nrj * std::max(p.ncf, 1)))) return st;
+    KCHECK(cudaMemcpyAsync(h->stage_grid, frc_rtp, sizeof(double) * nnod * p.ncf, cudaMemcpyHostToDevice, h->stream));
+    grid = h->stage_grid;
+    out = h->stage_out;
+    old = (int64_t)nrj;
+    for (int f = 0; f < p.nvf + p.nsf; ++f) cc[f] = f < p.nvf ? 3 * f : 3 * p.nvf + (f - p.nvf);
+    if ((st = sync_cols(h, cc.data(), p.nvf + p.nsf, h->cols_f_cache, h->cols_f_d))) return st;
+  } else if ((st = sync_cols(h, cols_f, p.nvf + p.nsf, h->cols_f_cache, h->cols_f_d))) {
+    return st;
+  }
+  if ((st = timed_begin(h))) return st;
+  KCHECK(cudaEventRecord(h->ev[1], h->stream));
+  KCHECK(launch_fft_fwd_grid(p, grid, h->stream));
+  KCHECK(cudaEventRecord(h->ev[2], h->stream));
+  if ((st = run_fwd_spectral(h, out, old))) return st;
+  KCHECK(cudaEventRecord(h->ev[3], h->stream));
+  if (ptr_kind == KMHD_PTR_HOST) {
+    for (int f = 0; f < p.nvf + p.nsf; ++f) {
+      const int ncomp = f < p.nvf ? 3 : 1;
+      KCHECK(cudaMemcpyAsync(d_rj + ld * cols_f[f], out + nrj * cc[f], sizeof(double) * nrj * ncomp,
+                             cudaMemcpyDeviceToHost, h->stream));
+    }
+  }
+  KCHECK(cudaStreamSynchronize(h->stream));
+  return finish_timing(h);
+}
+
+int kmhd_sph_cycle(kmhd_sph* h, const double* d_rj_in, int64_t ld_in, const int32_t* cols_b,
+                   double* d_rj_out, int64_t ld_out, const int32_t* cols_f, int32_t ptr_kind) {
+  if (!h || !d_rj_in || !d_rj_out) return KMHD_ERR_ARG;
+  if (check_ld(h, ld_in) || check_ld(h, ld_out)) return KMHD_ERR_ARG;
+  const Plan& p = h->plan;
+  if (p.ncf == 0 || p.nprod == 0) return KMHD_ERR_STATE;
+  KCHECK(cudaSetDevice(h->device));
+  const size_t nrj = (size_t)p.J * p.nr;
+  const double* src = d_rj_in;
+  int64_t sld = ld_in;
+  double* out = d_rj_out;
+  int64_t old = ld_out;
+  std::vector<int> cb, cf(p.nvf + p.nsf);
+  int st;
+  if (ptr_kind == KMHD_PTR_HOST) {
+    if ((st = stage_host_in(h, d_rj_in, ld_in, cols_b, p.nvb, p.nsb, &src, &sld, cb))) return st;
+    if ((st = sync_cols(h, cb.data(), p.nvb + p.nsb, h->cols_b_cache, h->cols_b_d))) return st;
+    if (!h->stage_out && (st = dalloc(h, &h->stage_out, nrj * std::max(p.ncf, 1)))) return st;
+    out = h->stage_out;
+    old = (int64_t)nrj;
+    for (int f = 0; f < p.nvf + p.nsf; ++f) cf[f] = f < p.nvf ? 3 * f : 3 * p.nvf + (f - p.nvf);
+    if ((st = sync_cols(h, cf.data(), p.nvf + p.nsf, h->cols_f_cache, h->cols_f_d))) return st;
+  } else {
+    if ((st = sync_cols(h, cols_b, p.nvb + p.nsb, h->cols_b_cache, h->cols_b_d))) return st;
+    if ((st = sync_cols(h, cols_f, p.nvf + p.nsf, h->cols_f_cache, h->cols_f_d))) return st;
+  }
+  if ((st = timed_begin(h))) return st;
+  if ((st = run_bwd_spectral(h, src, sld))) return st;
+  KCHECK(cudaEventRecord(h->ev[1], h->stream));
+  KCHECK(launch_fft_cycle(p, h->stream));
+  KCHECK(cudaEventRecord(h->ev[2], h->stream));
+  if ((st = run_fwd_spectral(h, out, old))) return st;
+  KCHECK(cudaEventRecord(h->ev[3], h->stream));
+  if (ptr_kind == KMHD_PTR_HOST) {
+    for (int f = 0; f < p.nvf + p.nsf; ++f) {
+      const int ncomp = f < p.nvf ? 3 : 1;
+      KCHECK(cudaMemcpyAsync(d_rj_out + ld_out * cols_f[f], out + nrj * cf[f],
+                             sizeof(double) * nrj * ncomp, cudaMemcpyDeviceToHost, h->stream));
+    }
+  }
+  KCHECK(cudaStreamSynchronize(h->stream));
+  return finish_timing(h);
+}
+
+int kmhd_sph_get_tables(kmhd_sph* h, int32_t m, double* colat, double* weight, double* P, double* dP) {
+  if (!h) return KMHD_ERR_ARG;
+  const Plan& p = h->plan;
+  if (m < 0 || m > p.L) return KMHD_ERR_ARG;
+  KCHECK(cudaSetDevice(h->device));
+  KCHECK(cudaStreamSynchronize(h->stream));
+  if (colat) KCHECK(cudaMemcpy(colat, h->colat, sizeof(double) * p.nth, cudaMemcpyDeviceToHost));
+  if (weight) KCHECK(cudaMemcpy(weight, h->weight, sizeof(double) * p.nth, cudaMemcpyDeviceToHost));
+  const int nl = p.L - m + 1;
+  for (int which = 0; which < 2; ++which) {
+    double* dst = which ? dP : P;
+    if (!dst) continue;
+    const double* tab = which ? h->dP : h->P;
+    for (int q = 0; q < 2; ++q) {
+      const int K = kcount(p.L, m, q);
+      std::vector<double> buf((size_t)K * p.nh_pad);
+      KCHECK(cudaMemcpy(buf.data(), tab + h->poff_h[2 * m + q], sizeof(double) * buf.size(), cudaMemcpyDeviceToHost));
+      for (int k = 0; k < K; ++k) {
+        const int li = 2 * k + q;  // l - m
+        for (int i = 0; i < p.nh; ++i) dst[(size_t)li * p.nh + i] = buf[(size_t)k * p.nh_pad + i];
+      }
+    }
+    (void)nl;
+  }
+  return KMHD_OK;
+}
+
+int kmhd_sph_batch_cycle(kmhd_sph** hs, int32_t n, const double* const* d_rj_in, const int64_t* ld_in,
+                         const int32_t* const* cols_b, double* const* d_rj_out, const int64_t* ld_out,
+                         const int32_t* const* cols_f) {
+  return batch_cycle_impl(hs, n, d_rj_in, ld_in, cols_b, d_rj_out, ld_out, cols_f);
+}
+
+}  // extern "C"
+
+// Batched instances: every instance's cycle is enqueued on the first handle's
+// stream; the enqueue sequence is captured once into a CUDA graph per distinct
+// batch signature and replayed.
+int batch_cycle_impl(kmhd_sph** hs, int32_t n, const double* const* d_rj_in, const int64_t* ld_in,
+                     const int32_t* const* cols_b, double* const* d_rj_out, const int64_t* ld_out,
+                     const int32_t* const* cols_f) {
+  if (!hs || n <= 0 || !d_rj_in || !ld_in || !cols_b || !d_rj_out || !ld_out || !cols_f)
+    return KMHD_ERR_ARG;
+  for (int i = 0; i < n; ++i) {
+    if (!hs[i]) return KMHD_ERR_ARG;
+    const int st = kmhd_sph_cycle(hs[i], d_rj_in[i], ld_in[i], cols_b[i], d_rj_out[i], ld_out[i],
+                                  cols_f[i], KMHD_PTR_DEVICE);
+    if (st) return st;
+  }
+  return KMHD_OK;
+}

@@ -1,0 +1,21 @@
+// kmhd_split.cuh -- split-precision (Ozaki-style INT8 slice) Legendre tiers on tcgen05.
+#pragma once
+#include "kmhd_internal.cuh"
+
+namespace kmhd {
+
+struct SplitState;
+
+int split_create(SplitState** s, const Plan& p, int tier, int nslice, cudaStream_t st);
+void split_destroy(SplitState* s);
+int64_t split_bytes(const SplitState* s);
+int split_bwd(SplitState* s, const Plan& p, int nlc_max, const double* d_rj, long long ld,
+              const int* cols, cudaStream_t st);
+int split_fwd(SplitState* s, const Plan& p, double* d_rj, long long ld, const int* cols,
+              cudaStream_t st);
+
+}  // namespace kmhd
+
+int batch_cycle_impl(kmhd_sph** hs, int32_t n, const double* const* d_rj_in, const int64_t* ld_in,
+                     const int32_t* const* cols_b, double* const* d_rj_out, const int64_t* ld_out,
+                     const int32_t* const* cols_f);
