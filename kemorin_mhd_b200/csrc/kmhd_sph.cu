@@ -385,8 +385,9 @@ int stage_host_in(kmhd_sph* h, const double* d_rj, int64_t ld, const int32_t* co
     const int ncomp = f < nv ? 3 : 1;
     const int c0 = f < nv ? 3 * f : 3 * nv + (f - nv);
     cols_c[f] = c0;
-    KCHECK(cudaMemcpyAsync(h->stage_in + nrj * c0, d_rj + ld * cols[f], sizeof(double) * nrj * ncomp,
-                           cudaMemcpyHostToDevice, h->stream));
+    for (int q = 0; q < ncomp; ++q)
+      KCHECK(cudaMemcpyAsync(h->stage_in + nrj * (c0 + q), d_rj + ld * (cols[f] + q), sizeof(double) * nrj,
+                             cudaMemcpyHostToDevice, h->stream));
   }
   (void)nc;
   *dev = h->stage_in;
@@ -504,8 +505,9 @@ int kmhd_sph_f_trans(kmhd_sph* h, const double* frc_rtp, double* d_rj, int64_t l
   if (ptr_kind == KMHD_PTR_HOST) {
     for (int f = 0; f < p.nvf + p.nsf; ++f) {
       const int ncomp = f < p.nvf ? 3 : 1;
-      KCHECK(cudaMemcpyAsync(d_rj + ld * cols_f[f], out + nrj * cc[f], sizeof(double) * nrj * ncomp,
-                             cudaMemcpyDeviceToHost, h->stream));
+      for (int q = 0; q < ncomp; ++q)
+        KCHECK(cudaMemcpyAsync(d_rj + ld * (cols_f[f] + q), out + nrj * (cc[f] + q), sizeof(double) * nrj,
+                               cudaMemcpyDeviceToHost, h->stream));
     }
   }
   KCHECK(cudaStreamSynchronize(h->stream));
@@ -548,8 +550,9 @@ int kmhd_sph_cycle(kmhd_sph* h, const double* d_rj_in, int64_t ld_in, const int3
   if (ptr_kind == KMHD_PTR_HOST) {
     for (int f = 0; f < p.nvf + p.nsf; ++f) {
       const int ncomp = f < p.nvf ? 3 : 1;
-      KCHECK(cudaMemcpyAsync(d_rj_out + ld_out * cols_f[f], out + nrj * cf[f],
-                             sizeof(double) * nrj * ncomp, cudaMemcpyDeviceToHost, h->stream));
+      for (int q = 0; q < ncomp; ++q)
+        KCHECK(cudaMemcpyAsync(d_rj_out + ld_out * (cols_f[f] + q), out + nrj * (cf[f] + q),
+                               sizeof(double) * nrj, cudaMemcpyDeviceToHost, h->stream));
     }
   }
   KCHECK(cudaStreamSynchronize(h->stream));
