@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""Throughput of the spherical-transform cycle on B200.
+
+One step = one full cycle (backward Legendre -> phi-FFT -> grid products ->
+phi-FFT -> forward Legendre) of one transform instance at L=511, Nr=257,
+Ntheta=768, Nphi=1536 with {u, omega, B} + {T} backward and
+{omega x u, u x B, u T} + {u . omega} forward (synthetic seeded spectra).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--tier split|fp64|fp32acc]
+
+Multi-GPU (torchrun, one rank per GPU): the cycle shards by radius with no
+collective inside the path; each rank runs its own full instance (weak scaling),
+value = all ranks' cycles / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "transform cycles/s at L=511 Nr=257: TC split-precision vs FP64 GPU, err≤1e-12"
+UNIT = "cycles/s"
+TIERS = {"fp64": 0, "split": 1, "fp32acc": 2}
+DTYPES = {"fp64": "f64", "split": "s8 slices (int32 accumulate) + f64 recombination",
+          "fp32acc": "s8 slices (int32 accumulate) + f64 recombination"}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax = float(parts[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_cycle_rate(cfg, seconds_target: float = 12.0, steps: int = 1, warmup: int = 0):
+    """Times the CPU FP64 oracle (reference sym_dgemm path restated, OpenBLAS
+    DGEMM, OpenMP over radial blocks) on a radial slab; returns cycles/s scaled
+    to the full radius count, the slab size, and the thread count."""
+    import numpy as np
+    from oracle import oracle as om
+    from kemorin_mhd_b200.config import SphConfig
+    from kemorin_mhd_b200.synthetic import make_d_rj
+    om.use_openblas()
+    threads = os.cpu_count() or 1
+    full_r = cfg.radius()
+
+    def slab(nr):
+        c = SphConfig(cfg.ltr, cfg.nth, cfg.nph, nr, cfg.nvb, cfg.nsb, cfg.nvf, cfg.nsf, cfg.products)
+        idx = np.linspace(0, cfg.nr - 1, nr).round().astype(int)
+        return c, full_r[idx]
+
+    c1, r1 = slab(2)
+    o = om.Oracle(c1, nthreads=threads, radius=r1)
+    d = make_d_rj(c1)
+    o.cycle(d)
+    t0 = time.perf_counter()
+    o.cycle(d)
+    t_per_radius = (time.perf_counter() - t0) / c1.nr
+    nr = int(max(2, min(cfg.nr, round(seconds_target / max(t_per_radius, 1e-6) / max(1, steps)))))
+    c, r = slab(nr)
+    o = om.Oracle(c, nthreads=threads, radius=r)
+    d = make_d_rj(c)
+    for _ in range(warmup):
+        o.cycle(d)
+    times = []
+    for _ in range(max(1, steps)):
+        t0 = time.perf_counter()
+        o.cycle(d)
+        times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    rate = 1.0 / (t * cfg.nr / nr)
+    return rate, nr, threads, o.last_timing()
+
+
+def run_reference(args, cfg):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    rate, nr, threads, stages = cpu_cycle_rate(cfg, seconds_target=max(4.0, 20.0 / max(1, args.steps)),
+                                              steps=args.steps, warmup=min(args.warmup, 1))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / rate,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded spectra N(0,1)(l+1)^-2 sin(pi(r-ri)/(ro-ri)))",
+        "config": {"workload": cfg.name, "L": cfg.ltr, "Nr": cfg.nr, "Ntheta": cfg.nth,
+                   "Nphi": cfg.nph, "fields_bwd": "u,omega,B + T", "fields_fwd": "omega x u, u x B, u T + u.omega"},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"radial slab of {nr}/{cfg.nr} radii per step, scaled x{cfg.nr / nr:.2f} (cost is linear in Nr)",
+                         "stages_ms": stages},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="cfg3")
+    ap.add_argument("--tier", default="auto", choices=["auto"] + list(TIERS))
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+
+    from kemorin_mhd_b200.config import NAMED
+    cfg = NAMED[args.config]
+    if args.impl == "reference":
+        return run_reference(args, cfg)
+
+    import numpy as np
+    import torch
+    from kemorin_mhd_b200 import sph_trans
+    from kemorin_mhd_b200.synthetic import make_d_rj_torch
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    tier = args.tier
+    if tier == "auto":
+        tier = "split"
+    lib = sph_trans.load_library()
+
+    def make(tier_name):
+        return sph_trans.SphTransform(cfg, tier=TIERS[tier_name], device=local)
+
+    try:
+        tr = make(tier)
+    except sph_trans.KmhdError:
+        if args.tier != "auto":
+            raise
+        tier = "fp64"
+        tr = make(tier)
+    stream = torch.cuda.current_stream()
+    tr.set_stream(stream.cuda_stream)
+    d_in = make_d_rj_torch(cfg, seed=1234 + rank)
+    d_out = torch.zeros((cfg.ncf, cfg.J * cfg.nr), dtype=torch.float64, device="cuda")
+
+    for _ in range(args.warmup):
+        tr.nonlinear_cycle(d_in, d_out)
+    torch.cuda.synchronize()
+
+    clocks = Clocks(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    stage = {"leg_bwd": 0.0, "fft_nl": 0.0, "leg_fwd": 0.0}
+    e0.record(stream)
+    for _ in range(args.steps):
+        tr.nonlinear_cycle(d_in, d_out)
+        t = tr.last_timing()
+        for k in stage:
+            stage[k] += t[k]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms_total = max_over_ranks(e0.elapsed_time(e1))
+    ms_step = ms_total / args.steps
+    value = ws * args.steps / (ms_total * 1e-3)
+    for k in stage:
+        stage[k] /= args.steps
+
+    # FP64 GPU cycle on the same input: the bar of the split tier (speed and error)
+    extra = {}
+    if tier != "fp64":
+        ref64 = make("fp64")
+        ref64.set_stream(stream.cuda_stream)
+        out64 = torch.zeros_like(d_out)
+        for _ in range(2):
+            ref64.nonlinear_cycle(d_in, out64)
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        n64 = max(2, args.steps // 2)
+        f0.record(stream)
+        for _ in range(n64):
+            ref64.nonlinear_cycle(d_in, out64)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        ms64 = max_over_ranks(f0.elapsed_time(f1) / n64)
+        den = out64.abs().amax(dim=1)
+        err = ((d_out - out64).abs().amax(dim=1) / den).tolist()
+        extra = {"fp64_gpu": {"value": ws * 1e3 / ms64, "unit": UNIT, "ms_per_step": ms64},
+                 "speedup_vs_fp64_gpu": ms64 / ms_step,
+                 "rel_err_vs_fp64_per_field": err, "rel_err_max": max(err)}
+        del ref64, out64
+
+    # roofline of the dominant kernel (the backward Legendre GEMM)
+    peaks, psrc = load_peaks()
+    flops_bwd = 2.0 * cfg.nh * cfg.J * cfg.nr * (5 * cfg.nvb + cfg.nsb)
+    if tier == "fp64":
+        pk = ctypes_probe(lib, local)
+        roof = {"bound": "tensor", "achieved": flops_bwd / (stage["leg_bwd"] * 1e-3) / 1e12,
+                "peak": pk, "unit": "TFLOP/s",
+                "peak_source": "FP64 tensor pipe measured in-process (DMMA chain probe); "
+                               "MEASURED_PEAKS.json carries no FP64 figure"}
+    else:
+        pk = 2.0 * peaks["bf16_tflops"]
+        roof = {"bound": "tensor", "achieved": flops_bwd / (stage["leg_bwd"] * 1e-3) / 1e12,
+                "peak": pk, "unit": "TFLOP/s",
+                "peak_source": f"2 x bf16 burst of {psrc} MEASURED_PEAKS.json (INT8:BF16 dense = 2:1)"}
+    roof["frac"] = roof["achieved"] / roof["peak"] if roof["peak"] else None
+    roof["traffic"] = read_traffic(tier)
+    roof["kernel"] = "Legendre backward GEMM"
+    roof["algorithmic_flops_per_launch"] = flops_bwd
+
+    # end to end through the public API with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        h_in = torch.empty((cfg.ncb, cfg.J * cfg.nr), dtype=torch.float64, pin_memory=True)
+        h_in.copy_(d_in)
+        h_out = torch.empty((cfg.ncf, cfg.J * cfg.nr), dtype=torch.float64, pin_memory=True)
+        tr.nonlinear_cycle(h_in, h_out)
+        ke = max(2, min(args.steps, 4))
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            tr.nonlinear_cycle(h_in, h_out)
+        torch.cuda.synchronize()
+        dt = max_over_ranks(time.perf_counter() - t0)
+        e2e = {"value": ws * ke / dt, "unit": UNIT, "h2d_bytes_per_step": h_in.numel() * 8,
+               "d2h_bytes_per_step": h_out.numel() * 8, "steps": ke,
+               "note": "host wall clock around kmhd_sph_cycle with pinned host d_rj in/out"}
+        del h_in, h_out
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        rate, nr, threads, stages = cpu_cycle_rate(cfg)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"one cycle of a radial slab of {nr}/{cfg.nr} radii, scaled x{cfg.nr / nr:.2f} "
+                         "(every stage is linear in Nr)",
+               "stages_ms": stages}
+
+    launches = {"fp64": 4, "split": 6, "fp32acc": 6}[tier]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": DTYPES[tier], "tier": tier,
+        "data": "synthetic (seeded spectra N(0,1)(l+1)^-2 sin(pi(r-ri)/(ro-ri)), Chebyshev radii)",
+        "config": {"workload": cfg.name, "L": cfg.ltr, "Nr": cfg.nr, "Ntheta": cfg.nth, "Nphi": cfg.nph,
+                   "fields_bwd": "u,omega,B + T", "fields_fwd": "omega x u, u x B, u T + u.omega",
+                   "parallelism": f"radial-instance x{ws} (no collective)",
+                   "l2": "inputs larger than L2 (d_rj 5.4 GB, rtm 16 GB per direction)"},
+        "stages_ms": stage, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": launches * args.steps, "clocks": clk,
+    }
+    line.update(extra)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    tr.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def ctypes_probe(lib, dev):
+    import ctypes
+    try:
+        f = lib.kmhd_probe_fp64_tflops
+    except AttributeError:
+        return None
+    f.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    v = ctypes.c_double()
+    return v.value if f(dev, ctypes.byref(v)) == 0 else None
+
+
+def read_traffic(tier):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", f"leg_bwd_{tier}_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_launch_full:"):
+            return float(line.split(":")[1])
+    return None
+
+
+if __name__ == "__main__":
+    sys.exit(main())

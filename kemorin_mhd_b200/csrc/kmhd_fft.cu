@@ -1,17 +1,18 @@
 // kmhd_fft.cu -- longitudinal real FFTs fused with the grid-space products.
 //
-// One CTA owns one (r, theta) line and keeps every component of it in shared
-// memory: inverse FFT -> products -> forward FFT never touch HBM.
+// Each (r, theta) line is handled by one CTA with every component of the line
+// in shared memory, so inverse FFT -> products -> forward FFT never touch HBM.
 // Convention (t_sph_single_FFTW.F90 normalisation with the FFTPACK slot order of
 // PARALLEL_src/SPH_SHELL_src/t_sph_FFTPACK5.f90:183-331):
 //   x_j = a_0 + sum_{k>=1} (a_k cos(2 pi jk/N) + b_k sin(2 pi jk/N)),
 //   a_0 = (1/N) sum x_j, a_k = (2/N) sum x_j cos, b_k = (2/N) sum x_j sin.
-// Two real components are carried as one complex sequence z = x_a + i x_b.
-// The inverse transform is an in-place mixed-radix decimation in frequency
+// Two real components travel as one complex sequence z = x_a + i x_b.  The
+// inverse transform is an in-place mixed-radix decimation in frequency
 // (natural spectrum in, digit-reversed grid out); the products are pointwise,
-// so they run on the digit-reversed grid; the forward transform is the exact
+// so they run on the digit-reversed grid; the forward transform is its exact
 // transpose (decimation in time, digit-reversed in, natural out).  No
-// reordering pass is needed.
+// reordering pass exists.  The first inverse pass reads the staged spectra
+// directly and skips the band L < k < N-L, which is zero.
 // Products: cal_cross_prod_w_coef_smp, cal_vec_scalar_prod_w_coef_smp,
 // cal_dot_prod_w_coef_smp (CORE_src/BASE/cal_products_smp.f90) as called by
 // nonlinear_terms_in_rtp (MHD_src/sph_MHD/cal_nonlinear_sph_MHD.f90:64-128).
@@ -20,125 +21,207 @@
 namespace kmhd {
 namespace {
 
+constexpr int kFftThreads = 256;
+
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-// multiply by (sign * i)
 template <int SIGN>
-__device__ __forceinline__ double2 mul_si(double2 a) {
+__device__ __forceinline__ double2 mul_si(double2 a) {  // a * (SIGN i)
   return SIGN > 0 ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
 }
 
-// In-place R-point DFT, y_q = sum_r x_r e^{SIGN 2 pi i r q / R}.
+// y_q = sum_r x_r e^{SIGN 2 pi i r q / R}, in place, compile-time R.
+template <int R, int SIGN>
+struct DFT;
 template <int SIGN>
-__device__ __forceinline__ void dft2(double2* x) {
-  const double2 a = x[0], b = x[1];
-  x[0] = cadd(a, b);
-  x[1] = csub(a, b);
-}
+struct DFT<2, SIGN> {
+  __device__ static void run(double2* x) {
+    const double2 a = x[0], b = x[1];
+    x[0] = cadd(a, b);
+    x[1] = csub(a, b);
+  }
+};
 template <int SIGN>
-__device__ __forceinline__ void dft4(double2* x) {
-  const double2 a = cadd(x[0], x[2]), b = csub(x[0], x[2]);
-  const double2 c = cadd(x[1], x[3]), d = mul_si<SIGN>(csub(x[1], x[3]));
-  x[0] = cadd(a, c);
-  x[1] = cadd(b, d);
-  x[2] = csub(a, c);
-  x[3] = csub(b, d);
-}
+struct DFT<4, SIGN> {
+  __device__ static void run(double2* x) {
+    const double2 a = cadd(x[0], x[2]), b = csub(x[0], x[2]);
+    const double2 c = cadd(x[1], x[3]), d = mul_si<SIGN>(csub(x[1], x[3]));
+    x[0] = cadd(a, c);
+    x[1] = cadd(b, d);
+    x[2] = csub(a, c);
+    x[3] = csub(b, d);
+  }
+};
 template <int SIGN>
-__device__ __forceinline__ void dft3(double2* x) {
-  const double s3 = 0.86602540378443864676 * (double)SIGN;
-  const double2 t = cadd(x[1], x[2]);
-  const double2 d = csub(x[1], x[2]);
-  const double2 u = make_double2(-d.y * s3, d.x * s3);
-  const double2 v = make_double2(x[0].x - 0.5 * t.x, x[0].y - 0.5 * t.y);
-  x[0] = cadd(x[0], t);
-  x[1] = cadd(v, u);
-  x[2] = csub(v, u);
-}
+struct DFT<3, SIGN> {
+  __device__ static void run(double2* x) {
+    const double s3 = 0.86602540378443864676 * (double)SIGN;
+    const double2 t = cadd(x[1], x[2]);
+    const double2 d = csub(x[1], x[2]);
+    const double2 u = make_double2(-d.y * s3, d.x * s3);
+    const double2 v = make_double2(x[0].x - 0.5 * t.x, x[0].y - 0.5 * t.y);
+    x[0] = cadd(x[0], t);
+    x[1] = cadd(v, u);
+    x[2] = csub(v, u);
+  }
+};
 template <int SIGN>
-__device__ __forceinline__ void dft5(double2* x) {
-  // direct 5-point DFT with exact-ish constants
-  const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
-  const double s1 = 0.95105651629515357212 * (double)SIGN, s2 = 0.58778525229247312917 * (double)SIGN;
-  const double2 a1 = cadd(x[1], x[4]), b1 = csub(x[1], x[4]);
-  const double2 a2 = cadd(x[2], x[3]), b2 = csub(x[2], x[3]);
-  const double2 x0 = x[0];
-  const double2 t1 = make_double2(x0.x + c1 * a1.x + c2 * a2.x, x0.y + c1 * a1.y + c2 * a2.y);
-  const double2 t2 = make_double2(x0.x + c2 * a1.x + c1 * a2.x, x0.y + c2 * a1.y + c1 * a2.y);
-  const double2 u1 = make_double2(-(s1 * b1.y + s2 * b2.y), s1 * b1.x + s2 * b2.x);
-  const double2 u2 = make_double2(-(s2 * b1.y - s1 * b2.y), s2 * b1.x - s1 * b2.x);
-  x[0] = make_double2(x0.x + a1.x + a2.x, x0.y + a1.y + a2.y);
-  x[1] = cadd(t1, u1);
-  x[4] = csub(t1, u1);
-  x[2] = cadd(t2, u2);
-  x[3] = csub(t2, u2);
-}
+struct DFT<5, SIGN> {
+  __device__ static void run(double2* x) {
+    const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
+    const double s1 = 0.95105651629515357212 * (double)SIGN, s2 = 0.58778525229247312917 * (double)SIGN;
+    const double2 a1 = cadd(x[1], x[4]), b1 = csub(x[1], x[4]);
+    const double2 a2 = cadd(x[2], x[3]), b2 = csub(x[2], x[3]);
+    const double2 x0 = x[0];
+    const double2 t1 = make_double2(x0.x + c1 * a1.x + c2 * a2.x, x0.y + c1 * a1.y + c2 * a2.y);
+    const double2 t2 = make_double2(x0.x + c2 * a1.x + c1 * a2.x, x0.y + c2 * a1.y + c1 * a2.y);
+    const double2 u1 = make_double2(-(s1 * b1.y + s2 * b2.y), s1 * b1.x + s2 * b2.x);
+    const double2 u2 = make_double2(-(s2 * b1.y - s1 * b2.y), s2 * b1.x - s1 * b2.x);
+    x[0] = make_double2(x0.x + a1.x + a2.x, x0.y + a1.y + a2.y);
+    x[1] = cadd(t1, u1);
+    x[4] = csub(t1, u1);
+    x[2] = cadd(t2, u2);
+    x[3] = csub(t2, u2);
+  }
+};
 template <int SIGN>
-__device__ __forceinline__ void dft8(double2* x) {
-  // radix-8 = 2 x 4 with internal twiddles e^{SIGN i pi k/4}
-  const double h = 0.70710678118654752440;
-  double2 e[4] = {x[0], x[2], x[4], x[6]}, o[4] = {x[1], x[3], x[5], x[7]};
-  dft4<SIGN>(e);
-  dft4<SIGN>(o);
-  // o[k] *= e^{SIGN 2 pi i k / 8}
-  o[1] = make_double2(h * (o[1].x - (double)SIGN * o[1].y), h * (o[1].y + (double)SIGN * o[1].x));
-  o[2] = mul_si<SIGN>(o[2]);
-  o[3] = make_double2(h * (-o[3].x - (double)SIGN * o[3].y), h * (-o[3].y + (double)SIGN * o[3].x));
+struct DFT<8, SIGN> {
+  __device__ static void run(double2* x) {
+    const double h = 0.70710678118654752440;
+    double2 e[4] = {x[0], x[2], x[4], x[6]}, o[4] = {x[1], x[3], x[5], x[7]};
+    DFT<4, SIGN>::run(e);
+    DFT<4, SIGN>::run(o);
+    o[1] = make_double2(h * (o[1].x - (double)SIGN * o[1].y), h * (o[1].y + (double)SIGN * o[1].x));
+    o[2] = mul_si<SIGN>(o[2]);
+    o[3] = make_double2(h * (-o[3].x - (double)SIGN * o[3].y), h * (-o[3].y + (double)SIGN * o[3].x));
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    x[k] = cadd(e[k], o[k]);
-    x[k + 4] = csub(e[k], o[k]);
+    for (int k = 0; k < 4; ++k) {
+      x[k] = cadd(e[k], o[k]);
+      x[k + 4] = csub(e[k], o[k]);
+    }
   }
-}
+};
 
 template <int SIGN>
-__device__ __forceinline__ void dft_r(double2* x, int R) {
-  switch (R) {
-    case 2: dft2<SIGN>(x); break;
-    case 3: dft3<SIGN>(x); break;
-    case 4: dft4<SIGN>(x); break;
-    case 5: dft5<SIGN>(x); break;
-    default: dft8<SIGN>(x); break;
-  }
-}
-
-// twiddle e^{SIGN 2 pi i idx / N} from the +sign table
-template <int SIGN>
-__device__ __forceinline__ double2 twd(const double2* tw, int idx) {
-  const double2 w = tw[idx];
+__device__ __forceinline__ double2 twd(const double2* __restrict__ tw, int idx) {
+  const double2 w = __ldg(tw + idx);
   return SIGN > 0 ? w : make_double2(w.x, -w.y);
 }
 
-// Inverse (+) DIF over all npair sequences z[p*N + .] in shared memory.
-__device__ void fft_dif_plus(double2* z, int npair, int N, const Plan& P, const double2* tw) {
-  int span = N;
-  for (int f = 0; f < P.nfac; ++f) {
-    const int R = P.fac[f];
-    const int s = span / R;
-    const int nbf = N / R;
-    const int stw = N / span;
-    for (int it = threadIdx.x; it < npair * nbf; it += blockDim.x) {
-      const int pp = it / nbf;
-      const int rem = it % nbf;
-      const int j = rem % s;
-      const int b = rem / s;
-      double2* base = z + (long long)pp * N + b * span + j;
-      double2 x[8];
-      for (int r = 0; r < R; ++r) x[r] = base[r * s];
-      dft_r<+1>(x, R);
-      base[0] = x[0];
-      for (int q = 1; q < R; ++q) base[q * s] = cmul(x[q], twd<+1>(tw, j * q * stw));
-    }
-    __syncthreads();
-    span = s;
+// One in-place DIF (+) pass over npair sequences: butterfly, then twiddle.
+template <int R>
+__device__ void dif_pass(double2* z, int npair, int N, int span, const double2* __restrict__ tw) {
+  const int s = span / R, nbf = N / R, stw = N / span;
+  for (int it = threadIdx.x; it < npair * nbf; it += blockDim.x) {
+    const int pp = it / nbf, rem = it % nbf;
+    const int j = rem % s, b = rem / s;
+    double2* base = z + pp * N + b * span + j;
+    double2 x[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) x[r] = base[r * s];
+    DFT<R, +1>::run(x);
+    base[0] = x[0];
+#pragma unroll
+    for (int q = 1; q < R; ++q) base[q * s] = cmul(x[q], twd<+1>(tw, j * q * stw));
   }
 }
 
-// Forward (-) DIT, the transpose of fft_dif_plus.
-__device__ void fft_dit_minus(double2* z, int npair, int N, const Plan& P, const double2* tw) {
+// One in-place DIT (-) pass, the transpose of dif_pass.
+template <int R>
+__device__ void dit_pass(double2* z, int npair, int N, int span, const double2* __restrict__ tw) {
+  const int s = span / R, nbf = N / R, stw = N / span;
+  for (int it = threadIdx.x; it < npair * nbf; it += blockDim.x) {
+    const int pp = it / nbf, rem = it % nbf;
+    const int j = rem % s, b = rem / s;
+    double2* base = z + pp * N + b * span + j;
+    double2 x[R];
+    x[0] = base[0];
+#pragma unroll
+    for (int q = 1; q < R; ++q) x[q] = cmul(base[q * s], twd<-1>(tw, j * q * stw));
+    DFT<R, -1>::run(x);
+#pragma unroll
+    for (int r = 0; r < R; ++r) base[r * s] = x[r];
+  }
+}
+
+__device__ void dif_dispatch(int R, double2* z, int npair, int N, int span, const double2* tw) {
+  switch (R) {
+    case 8: dif_pass<8>(z, npair, N, span, tw); break;
+    case 4: dif_pass<4>(z, npair, N, span, tw); break;
+    case 2: dif_pass<2>(z, npair, N, span, tw); break;
+    case 3: dif_pass<3>(z, npair, N, span, tw); break;
+    default: dif_pass<5>(z, npair, N, span, tw); break;
+  }
+}
+__device__ void dit_dispatch(int R, double2* z, int npair, int N, int span, const double2* tw) {
+  switch (R) {
+    case 8: dit_pass<8>(z, npair, N, span, tw); break;
+    case 4: dit_pass<4>(z, npair, N, span, tw); break;
+    case 2: dit_pass<2>(z, npair, N, span, tw); break;
+    case 3: dit_pass<3>(z, npair, N, span, tw); break;
+    default: dit_pass<5>(z, npair, N, span, tw); break;
+  }
+}
+
+// Complex spectrum of pair pp at frequency k from staged records
+// st[(m*nc + c)*2 + {0: a, 1: b}], m <= L.  z = X_{2pp} + i X_{2pp+1},
+// X_c[m] = (a - i b)/2 for m > 0, X_c[0] = a, X_c[N-m] = conj(X_c[m]).
+__device__ __forceinline__ double2 spec_at(const double* st, int nc, int pp, int k, int N, int L) {
+  int m;
+  bool mirror;
+  if (k <= L) { m = k; mirror = false; }
+  else if (k >= N - L) { m = N - k; mirror = true; }
+  else return make_double2(0.0, 0.0);
+  const double* r0 = st + (m * nc + 2 * pp) * 2;
+  const double a0 = r0[0], b0 = r0[1];
+  double a1 = 0.0, b1 = 0.0;
+  if (2 * pp + 1 < nc) { a1 = r0[2]; b1 = r0[3]; }
+  if (m == 0) return make_double2(a0, a1);
+  return mirror ? make_double2(0.5 * a0 - 0.5 * b1, 0.5 * b0 + 0.5 * a1)
+                : make_double2(0.5 * a0 + 0.5 * b1, 0.5 * a1 - 0.5 * b0);
+}
+
+// First DIF pass: input from the staged spectra, output into z.
+template <int R>
+__device__ void dif_first(const double* st, int nc, double2* z, int npair, int N, int L,
+                          const double2* __restrict__ tw) {
+  const int s = N / R, nbf = N / R;
+  for (int it = threadIdx.x; it < npair * nbf; it += blockDim.x) {
+    const int pp = it / nbf, j = it % nbf;
+    double2 x[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) x[r] = spec_at(st, nc, pp, j + r * s, N, L);
+    DFT<R, +1>::run(x);
+    double2* base = z + pp * N + j;
+    base[0] = x[0];
+#pragma unroll
+    for (int q = 1; q < R; ++q) base[q * s] = cmul(x[q], twd<+1>(tw, j * q));
+  }
+}
+__device__ void dif_first_dispatch(int R, const double* st, int nc, double2* z, int npair, int N,
+                                   int L, const double2* tw) {
+  switch (R) {
+    case 8: dif_first<8>(st, nc, z, npair, N, L, tw); break;
+    case 4: dif_first<4>(st, nc, z, npair, N, L, tw); break;
+    case 2: dif_first<2>(st, nc, z, npair, N, L, tw); break;
+    case 3: dif_first<3>(st, nc, z, npair, N, L, tw); break;
+    default: dif_first<5>(st, nc, z, npair, N, L, tw); break;
+  }
+}
+
+__device__ void dif_rest(double2* z, int npair, int N, const Plan& P, const double2* tw) {
+  int span = N / P.fac[0];
+  for (int f = 1; f < P.nfac; ++f) {
+    dif_dispatch(P.fac[f], z, npair, N, span, tw);
+    __syncthreads();
+    span /= P.fac[f];
+  }
+}
+
+__device__ void dit_all(double2* z, int npair, int N, const Plan& P, const double2* tw) {
   int spans[kMaxFftFactors];
   int span = N;
   for (int f = 0; f < P.nfac; ++f) {
@@ -146,77 +229,36 @@ __device__ void fft_dit_minus(double2* z, int npair, int N, const Plan& P, const
     span /= P.fac[f];
   }
   for (int f = P.nfac - 1; f >= 0; --f) {
-    const int R = P.fac[f];
-    span = spans[f];
-    const int s = span / R;
-    const int nbf = N / R;
-    const int stw = N / span;
-    for (int it = threadIdx.x; it < npair * nbf; it += blockDim.x) {
-      const int pp = it / nbf;
-      const int rem = it % nbf;
-      const int j = rem % s;
-      const int b = rem / s;
-      double2* base = z + (long long)pp * N + b * span + j;
-      double2 x[8];
-      x[0] = base[0];
-      for (int q = 1; q < R; ++q) x[q] = cmul(base[q * s], twd<-1>(tw, j * q * stw));
-      dft_r<-1>(x, R);
-      for (int r = 0; r < R; ++r) base[r * s] = x[r];
-    }
+    dit_dispatch(P.fac[f], z, npair, N, spans[f], tw);
     __syncthreads();
   }
 }
 
-// Load the spectra of line (r, theta) from rtm [m][th][r][nc][2] into z.
-__device__ void load_line_spectra(double2* z, int npair, const Plan& P, const double* rtm, int nc,
-                                  int th, int r) {
-  const int N = P.nph, L = P.L;
-  // zero the band L < k < N-L
-  for (int it = threadIdx.x; it < npair * (N - 2 * L - 1); it += blockDim.x) {
-    const int pp = it / (N - 2 * L - 1);
-    const int k = L + 1 + it % (N - 2 * L - 1);
-    z[(long long)pp * N + k] = make_double2(0.0, 0.0);
-  }
+// Stage the records of line (th, r) for all m into st via cp.async (16 B each).
+__device__ void prefetch_line(double* st, const double* rtm, int nc, const Plan& P, int th, int r) {
   const long long strideM = (long long)P.nth * P.nr * nc * 2;
   const double* base = rtm + ((long long)th * P.nr + r) * nc * 2;
-  for (int it = threadIdx.x; it < (L + 1) * npair; it += blockDim.x) {
-    const int m = it / npair, pp = it % npair;
-    const double* rec = base + m * strideM + 4 * pp;
-    const double a0 = rec[0], b0 = rec[1];
-    double a1 = 0.0, b1 = 0.0;
-    if (2 * pp + 1 < nc) {
-      a1 = rec[2];
-      b1 = rec[3];
-    }
-    double2* zp = z + (long long)pp * N;
-    if (m == 0) {
-      zp[0] = make_double2(a0, a1);
-    } else {
-      // X_c = (a_c - i b_c)/2 ; z = X_0 + i X_1 ; z[N-m] = conj(X_0) + i conj(X_1)
-      zp[m] = make_double2(0.5 * a0 + 0.5 * b1, 0.5 * a1 - 0.5 * b0);
-      zp[N - m] = make_double2(0.5 * a0 - 0.5 * b1, 0.5 * b0 + 0.5 * a1);
-    }
+  const int n = (P.L + 1) * nc;
+  for (int it = threadIdx.x; it < n; it += blockDim.x) {
+    const int m = it / nc, c = it % nc;
+    cp_async16(st + (m * nc + c) * 2, base + m * strideM + c * 2);
   }
+  cp_async_commit();
 }
 
-// Store (a_m, b_m), m <= L, of line (r, theta) from the natural-order forward
-// spectra in z into rtm [m][th][r][nc][2].
-__device__ void store_line_spectra(const double2* z, int npair, const Plan& P, double* rtm, int nc,
-                                   int th, int r) {
+// Natural-order forward spectra in z -> (a_m, b_m), m <= L, into rtm.
+__device__ void store_line(const double2* z, int npair, const Plan& P, double* rtm, int nc, int th, int r) {
   const int N = P.nph, L = P.L;
   const double aN = 1.0 / (double)N;
   const long long strideM = (long long)P.nth * P.nr * nc * 2;
   double* base = rtm + ((long long)th * P.nr + r) * nc * 2;
   for (int it = threadIdx.x; it < (L + 1) * npair; it += blockDim.x) {
     const int m = it / npair, pp = it % npair;
-    const double2* zp = z + (long long)pp * N;
+    const double2* zp = z + pp * N;
     const double2 zm = zp[m];
     double a0, b0, a1, b1;
     if (m == 0) {
-      a0 = zm.x * aN;
-      a1 = zm.y * aN;
-      b0 = 0.0;
-      b1 = 0.0;
+      a0 = zm.x * aN; a1 = zm.y * aN; b0 = 0.0; b1 = 0.0;
     } else {
       const double2 wm = zp[N - m];
       a0 = (zm.x + wm.x) * aN;
@@ -230,94 +272,169 @@ __device__ void store_line_spectra(const double2* z, int npair, const Plan& P, d
   }
 }
 
-__device__ __forceinline__ double zget(const double2* z, int N, int c, int pos) {
-  const double2 v = z[(long long)(c >> 1) * N + pos];
-  return (c & 1) ? v.y : v.x;
+// Vector a of the backward fields, selected without dynamic register indexing.
+template <int MV>
+__device__ __forceinline__ void selvec(const double* in, int a, double& x0, double& x1, double& x2) {
+  x0 = in[0]; x1 = in[1]; x2 = in[2];
+#pragma unroll
+  for (int v = 1; v < MV; ++v)
+    if (a == v) { x0 = in[3 * v]; x1 = in[3 * v + 1]; x2 = in[3 * v + 2]; }
+}
+template <int MS>
+__device__ __forceinline__ double selscl(const double* s, int b) {
+  double x = s[0];
+#pragma unroll
+  for (int q = 1; q < MS; ++q)
+    if (b == q) x = s[q];
+  return x;
 }
 
-__global__ void __launch_bounds__(512, 1) k_fft_cycle(Plan P) {
-  extern __shared__ double2 zs[];
+// Pointwise products on the digit-reversed grid.  MV*/MS* are compile-time
+// maxima; the plan's counts are <= them (products are ordered vectors first).
+template <int MVB, int MSB, int MVF, int MSF>
+__device__ void products(double2* z, int N, const Plan& P) {
+  constexpr int MCF = 3 * MVF + MSF;
+  const int nvb = P.nvb, nsb = P.nsb, nvf = P.nvf, nsf = P.nsf;
+  for (int pos = threadIdx.x; pos < N; pos += blockDim.x) {
+    double vin[3 * MVB > 0 ? 3 * MVB : 1], sin_[MSB > 0 ? MSB : 1];
+#pragma unroll
+    for (int c = 0; c < 3 * MVB; ++c)
+      if (c < 3 * nvb) {
+        const double2 v = z[(c >> 1) * N + pos];
+        vin[c] = (c & 1) ? v.y : v.x;
+      }
+#pragma unroll
+    for (int q = 0; q < MSB; ++q)
+      if (q < nsb) {
+        const int c = 3 * nvb + q;
+        const double2 v = z[(c >> 1) * N + pos];
+        sin_[q] = (c & 1) ? v.y : v.x;
+      }
+    double out[MCF > 0 ? MCF : 1];
+#pragma unroll
+    for (int i = 0; i < MVF; ++i) {
+      if (i < nvf) {
+        const int kind = P.pkind[i];
+        const double cf = P.pcoef[i];
+        double x0, x1, x2;
+        selvec<MVB>(vin, P.pa[i], x0, x1, x2);
+        if (kind == KMHD_PROD_CROSS) {
+          double y0, y1, y2;
+          selvec<MVB>(vin, P.pb[i], y0, y1, y2);
+          out[3 * i + 0] = (x1 * y2 - x2 * y1) * cf;
+          out[3 * i + 1] = (x2 * y0 - x0 * y2) * cf;
+          out[3 * i + 2] = (x0 * y1 - x1 * y0) * cf;
+        } else {
+          const double s = selscl<MSB>(sin_, P.pb[i]);
+          out[3 * i + 0] = x0 * s * cf;
+          out[3 * i + 1] = x1 * s * cf;
+          out[3 * i + 2] = x2 * s * cf;
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < MSF; ++j) {
+      if (j < nsf) {
+        const int q = nvf + j;
+        const int kind = P.pkind[q];
+        const double cf = P.pcoef[q];
+        double o;
+        if (kind == KMHD_PROD_DOT) {
+          double x0, x1, x2, y0, y1, y2;
+          selvec<MVB>(vin, P.pa[q], x0, x1, x2);
+          selvec<MVB>(vin, P.pb[q], y0, y1, y2);
+          o = (x0 * y0 + x1 * y1 + x2 * y2) * cf;
+        } else {
+          o = selscl<MSB>(sin_, P.pa[q]) * selscl<MSB>(sin_, P.pb[q]) * cf;
+        }
+        // output component 3*nvf + j: compile-time slot only when nvf == MVF
+        out[3 * MVF + j] = o;
+      }
+    }
+    // dense output order: vectors [0, 3*nvf), then scalars; compile-time slots
+    const int ncf = 3 * nvf + nsf;
+    double dense[MCF > 0 ? MCF : 1];
+#pragma unroll
+    for (int c = 0; c < MCF; ++c) {
+      double v = 0.0;
+      if (c < 3 * MVF) v = out[c < 3 * MVF ? c : 0];
+      if (c >= 3 * nvf) {
+        v = 0.0;
+#pragma unroll
+        for (int j = 0; j < MSF; ++j)
+          if (c == 3 * nvf + j) v = out[3 * MVF + j];
+      }
+      dense[c] = v;
+    }
+#pragma unroll
+    for (int c = 0; c < MCF; c += 2) {
+      if (c < ncf) {
+        const double hi = (c + 1 < MCF && c + 1 < ncf) ? dense[c + 1 < MCF ? c + 1 : c] : 0.0;
+        z[(c >> 1) * N + pos] = make_double2(dense[c], hi);
+      }
+    }
+  }
+}
+
+template <int MVB, int MSB, int MVF, int MSF>
+__global__ void __launch_bounds__(kFftThreads) k_fft_cycle(Plan P, int nlines) {
+  extern __shared__ double4 smraw[];
   const int N = P.nph;
   const int npb = (P.ncb + 1) / 2, npf = (P.ncf + 1) / 2;
   const int npair = npb > npf ? npb : npf;
-  double2* tw = zs + (long long)npair * N;
-  for (int k = threadIdx.x; k < N; k += blockDim.x) tw[k] = P.twid[k];
-  const int line = blockIdx.x;
-  const int r = line % P.nr, th = line / P.nr;
-  load_line_spectra(zs, npb, P, P.rtm_b, P.ncb, th, r);
-  __syncthreads();
-  fft_dif_plus(zs, npb, N, P, tw);
-  // products at every (digit-reversed) grid point
-  for (int pos = threadIdx.x; pos < N; pos += blockDim.x) {
-    double in[3 * kMaxVec + kMaxScl];
-    double out[3 * kMaxVec + kMaxScl];
-    for (int c = 0; c < P.ncb; ++c) in[c] = zget(zs, N, c, pos);
-    int iv = 0, is = 0;
-    for (int q = 0; q < P.nprod; ++q) {
-      const int kind = P.pkind[q];
-      const double cf = P.pcoef[q];
-      const int a = P.pa[q], b = P.pb[q];
-      if (kind == KMHD_PROD_CROSS) {
-        const double* x = in + 3 * a;
-        const double* y = in + 3 * b;
-        out[3 * iv + 0] = (x[1] * y[2] - x[2] * y[1]) * cf;
-        out[3 * iv + 1] = (x[2] * y[0] - x[0] * y[2]) * cf;
-        out[3 * iv + 2] = (x[0] * y[1] - x[1] * y[0]) * cf;
-        ++iv;
-      } else if (kind == KMHD_PROD_VEC_SCALAR) {
-        const double* x = in + 3 * a;
-        const double s = in[3 * P.nvb + b];
-        out[3 * iv + 0] = x[0] * s * cf;
-        out[3 * iv + 1] = x[1] * s * cf;
-        out[3 * iv + 2] = x[2] * s * cf;
-        ++iv;
-      } else if (kind == KMHD_PROD_DOT) {
-        const double* x = in + 3 * a;
-        const double* y = in + 3 * b;
-        out[3 * P.nvf + is] = (x[0] * y[0] + x[1] * y[1] + x[2] * y[2]) * cf;
-        ++is;
-      } else {
-        out[3 * P.nvf + is] = in[3 * P.nvb + a] * in[3 * P.nvb + b] * cf;
-        ++is;
-      }
-    }
-    for (int q = 0; q < npf; ++q) {
-      const double hi = (2 * q + 1 < P.ncf) ? out[2 * q + 1] : 0.0;
-      zs[(long long)q * N + pos] = make_double2(out[2 * q], hi);
-    }
+  double2* z = reinterpret_cast<double2*>(smraw);
+  double* st = reinterpret_cast<double*>(z + npair * N);
+  int line = blockIdx.x;
+  if (line >= nlines) return;
+  prefetch_line(st, P.rtm_b, P.ncb, P, line / P.nr, line % P.nr);
+  while (line < nlines) {
+    const int r = line % P.nr, th = line / P.nr;
+    cp_async_wait<0>();
+    __syncthreads();
+    dif_first_dispatch(P.fac[0], st, P.ncb, z, npb, N, P.L, P.twid);
+    __syncthreads();
+    const int next = line + gridDim.x;
+    if (next < nlines) prefetch_line(st, P.rtm_b, P.ncb, P, next / P.nr, next % P.nr);
+    dif_rest(z, npb, N, P, P.twid);
+    products<MVB, MSB, MVF, MSF>(z, N, P);
+    __syncthreads();
+    dit_all(z, npf, N, P, P.twid);
+    store_line(z, npf, P, P.rtm_f, P.ncf, th, r);
+    __syncthreads();
+    line = next;
   }
-  __syncthreads();
-  fft_dit_minus(zs, npf, N, P, tw);
-  store_line_spectra(zs, npf, P, P.rtm_f, P.ncf, th, r);
 }
 
 // Separable backward: spectra -> grid fld[node + nnod*c], node = r + nr*(th + nth*phi).
-__global__ void __launch_bounds__(512, 1) k_fft_bwd_grid(Plan P, double* __restrict__ fld) {
-  extern __shared__ double2 zs[];
+__global__ void __launch_bounds__(kFftThreads) k_fft_bwd_grid(Plan P, double* __restrict__ fld) {
+  extern __shared__ double4 smraw[];
   const int N = P.nph;
   const int npb = (P.ncb + 1) / 2;
-  double2* tw = zs + (long long)npb * N;
-  for (int k = threadIdx.x; k < N; k += blockDim.x) tw[k] = P.twid[k];
+  double2* z = reinterpret_cast<double2*>(smraw);
+  double* st = reinterpret_cast<double*>(z + npb * N);
   const int line = blockIdx.x;
   const int r = line % P.nr, th = line / P.nr;
-  load_line_spectra(zs, npb, P, P.rtm_b, P.ncb, th, r);
+  prefetch_line(st, P.rtm_b, P.ncb, P, th, r);
+  cp_async_wait<0>();
   __syncthreads();
-  fft_dif_plus(zs, npb, N, P, tw);
+  dif_first_dispatch(P.fac[0], st, P.ncb, z, npb, N, P.L, P.twid);
+  __syncthreads();
+  dif_rest(z, npb, N, P, P.twid);
   const long long nnod = (long long)P.nr * P.nth * N;
   for (int it = threadIdx.x; it < N * P.ncb; it += blockDim.x) {
     const int c = it / N, pos = it % N;
     const int phi = P.digrev[pos];
-    fld[(long long)r + (long long)P.nr * (th + (long long)P.nth * phi) + nnod * c] = zget(zs, N, c, pos);
+    const double2 v = z[(c >> 1) * N + pos];
+    fld[(long long)r + (long long)P.nr * (th + (long long)P.nth * phi) + nnod * c] = (c & 1) ? v.y : v.x;
   }
 }
 
 // Separable forward: grid frc -> spectra rtm_f.
-__global__ void __launch_bounds__(512, 1) k_fft_fwd_grid(Plan P, const double* __restrict__ frc) {
-  extern __shared__ double2 zs[];
+__global__ void __launch_bounds__(kFftThreads) k_fft_fwd_grid(Plan P, const double* __restrict__ frc) {
+  extern __shared__ double4 smraw[];
   const int N = P.nph;
   const int npf = (P.ncf + 1) / 2;
-  double2* tw = zs + (long long)npf * N;
-  for (int k = threadIdx.x; k < N; k += blockDim.x) tw[k] = P.twid[k];
+  double2* z = reinterpret_cast<double2*>(smraw);
   const int line = blockIdx.x;
   const int r = line % P.nr, th = line / P.nr;
   const long long nnod = (long long)P.nr * P.nth * N;
@@ -327,38 +444,65 @@ __global__ void __launch_bounds__(512, 1) k_fft_fwd_grid(Plan P, const double* _
     const long long node = (long long)r + (long long)P.nr * (th + (long long)P.nth * phi);
     const double lo = frc[node + nnod * (2 * q)];
     const double hi = (2 * q + 1 < P.ncf) ? frc[node + nnod * (2 * q + 1)] : 0.0;
-    zs[(long long)q * N + pos] = make_double2(lo, hi);
+    z[q * N + pos] = make_double2(lo, hi);
   }
   __syncthreads();
-  fft_dit_minus(zs, npf, N, P, tw);
-  store_line_spectra(zs, npf, P, P.rtm_f, P.ncf, th, r);
+  dit_all(z, npf, N, P, P.twid);
+  store_line(z, npf, P, P.rtm_f, P.ncf, th, r);
+}
+
+size_t smem_cycle(const Plan& p) {
+  const int npair = ((p.ncb > p.ncf ? p.ncb : p.ncf) + 1) / 2;
+  return sizeof(double2) * (size_t)npair * p.nph + sizeof(double) * 2 * (size_t)(p.L + 1) * p.ncb;
+}
+
+template <int MVB, int MSB, int MVF, int MSF>
+cudaError_t run_cycle(const Plan& p, cudaStream_t s) {
+  auto kern = k_fft_cycle<MVB, MSB, MVF, MSF>;
+  const size_t smem = smem_cycle(p);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, nsm = 0, occ = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kFftThreads, smem);
+  if (occ < 1) occ = 1;
+  const int nlines = p.nr * p.nth;
+  int grid = nsm * occ;
+  if (grid > nlines) grid = nlines;
+  kern<<<grid, kFftThreads, smem, s>>>(p, nlines);
+  return cudaGetLastError();
 }
 
 }  // namespace
 
 size_t fft_smem_bytes(const Plan& p, int npair) {
-  return sizeof(double2) * ((size_t)npair * p.nph + p.nph);
+  (void)npair;
+  return smem_cycle(p);
 }
 
 cudaError_t launch_fft_cycle(const Plan& p, cudaStream_t s) {
-  const int npair = ((p.ncb > p.ncf ? p.ncb : p.ncf) + 1) / 2;
-  const size_t smem = fft_smem_bytes(p, npair);
-  cudaFuncSetAttribute(k_fft_cycle, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_fft_cycle<<<p.nr * p.nth, 512, smem, s>>>(p);
-  return cudaGetLastError();
+  if (p.nvb == 3 && p.nsb == 1 && p.nvf == 3 && p.nsf == 1) return run_cycle<3, 1, 3, 1>(p, s);
+  if (p.nvb == 2 && p.nsb == 1 && p.nvf == 2 && p.nsf == 1) return run_cycle<2, 1, 2, 1>(p, s);
+  if (p.nvb == 1 && p.nsb == 1 && p.nvf == 1 && p.nsf == 0) return run_cycle<1, 1, 1, 0>(p, s);
+  return run_cycle<kMaxVec, kMaxScl, kMaxVec, kMaxScl>(p, s);
 }
 
 cudaError_t launch_fft_bwd_grid(const Plan& p, double* fld, cudaStream_t s) {
-  const size_t smem = fft_smem_bytes(p, (p.ncb + 1) / 2);
-  cudaFuncSetAttribute(k_fft_bwd_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_fft_bwd_grid<<<p.nr * p.nth, 512, smem, s>>>(p, fld);
+  const int npb = (p.ncb + 1) / 2;
+  const size_t smem = sizeof(double2) * (size_t)npb * p.nph + sizeof(double) * 2 * (size_t)(p.L + 1) * p.ncb;
+  cudaError_t e = cudaFuncSetAttribute(k_fft_bwd_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_fft_bwd_grid<<<p.nr * p.nth, kFftThreads, smem, s>>>(p, fld);
   return cudaGetLastError();
 }
 
 cudaError_t launch_fft_fwd_grid(const Plan& p, const double* frc, cudaStream_t s) {
-  const size_t smem = fft_smem_bytes(p, (p.ncf + 1) / 2);
-  cudaFuncSetAttribute(k_fft_fwd_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_fft_fwd_grid<<<p.nr * p.nth, 512, smem, s>>>(p, frc);
+  const int npf = (p.ncf + 1) / 2;
+  const size_t smem = sizeof(double2) * (size_t)npf * p.nph;
+  cudaError_t e = cudaFuncSetAttribute(k_fft_fwd_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_fft_fwd_grid<<<p.nr * p.nth, kFftThreads, smem, s>>>(p, frc);
   return cudaGetLastError();
 }
 

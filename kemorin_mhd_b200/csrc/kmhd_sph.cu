@@ -290,13 +290,19 @@ int kmhd_sph_create(const kmhd_sph_desc* d, kmhd_sph** out) {
       rev[pos] = k;
     }
   }
-  p.nprod = (int)h->products.size();
-  for (int i = 0; i < p.nprod; ++i) {
-    p.pkind[i] = h->products[i].kind;
-    p.pa[i] = h->products[i].a;
-    p.pb[i] = h->products[i].b;
-    p.pcoef[i] = h->products[i].coef;
-  }
+  // products: vector-valued first, then scalar-valued, each in list order (the
+  // forward field order); the grid kernel relies on this ordering
+  p.nprod = 0;
+  for (int pass = 0; pass < 2; ++pass)
+    for (const kmhd_product& q : h->products) {
+      const bool vec = q.kind == KMHD_PROD_CROSS || q.kind == KMHD_PROD_VEC_SCALAR;
+      if (vec != (pass == 0)) continue;
+      p.pkind[p.nprod] = q.kind;
+      p.pa[p.nprod] = q.a;
+      p.pb[p.nprod] = q.b;
+      p.pcoef[p.nprod] = q.coef;
+      ++p.nprod;
+    }
 
   // ---- device allocations
   const size_t nP = (size_t)po, nSB = (size_t)so;

@@ -112,7 +112,8 @@ void dgemm_nn(i64 m, i64 n, i64 k, const double* A, i64 lda, const double* B,
 struct CFFT {
   int n = 0;
   std::vector<int> radix;
-  std::vector<std::complex<double>> tw;  // e^{-2 pi i k / n}
+  // per stage: twiddles e^{-2 pi i j r / (l R)}, j < l, 1 <= r < R, laid out [j][r-1]
+  std::vector<std::vector<std::complex<double>>> stw;
   void init(int n_) {
     n = n_;
     radix.clear();
@@ -122,41 +123,46 @@ struct CFFT {
     while (r % 3 == 0) { radix.push_back(3); r /= 3; }
     while (r % 5 == 0) { radix.push_back(5); r /= 5; }
     if (r != 1) radix.push_back(r);  // generic DFT stage for any leftover prime
-    tw.resize(n);
-    for (int k = 0; k < n; ++k) {
-      const double a = -2.0 * M_PI * (double)k / (double)n;
-      tw[k] = std::complex<double>(std::cos(a), std::sin(a));
+    stw.clear();
+    int l = 1;
+    for (int R : radix) {
+      std::vector<std::complex<double>> t((size_t)l * (R - 1));
+      for (int j = 0; j < l; ++j)
+        for (int q = 1; q < R; ++q) {
+          const long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)j * q / (long double)(l * R);
+          t[(size_t)j * (R - 1) + (q - 1)] = std::complex<double>((double)cosl(a), (double)sinl(a));
+        }
+      stw.push_back(std::move(t));
+      l *= R;
     }
   }
   // sign = -1: forward e^{-i}, sign = +1: inverse e^{+i}; unnormalised.
+  // Stockham autosort: stage input viewed as [R][m][l], output as [m][R][l].
   void run(std::complex<double>* x, std::complex<double>* work, int sign) const {
     std::complex<double>* src = x;
     std::complex<double>* dst = work;
-    int l = 1;     // product of radices done
-    int m = n;     // remaining length
+    int l = 1, m = n;
     for (size_t s = 0; s < radix.size(); ++s) {
       const int R = radix[s];
       m /= R;
-      // Stockham: src viewed as [R][m][l], dst as [m][R][l]
-      for (int j = 0; j < l; ++j) {
-        for (int q = 0; q < m; ++q) {
-          std::complex<double> v[16];
-          std::complex<double> vv[64];
-          std::complex<double>* in = (R <= 16) ? v : vv;
-          for (int r = 0; r < R; ++r) in[r] = src[j + l * (q + m * r)];
-          // twiddle w^{j * q * ...}: stage twiddle e^{sign 2pi i j r / (l R)}
-          for (int r = 1; r < R; ++r) {
-            const long idx = (long)j * r * (n / (l * R)) % n;
-            std::complex<double> w = tw[idx];
-            if (sign > 0) w = std::conj(w);
-            in[r] *= w;
+      const std::complex<double>* tw = stw[s].data();
+      for (int q = 0; q < m; ++q) {
+        for (int j = 0; j < l; ++j) {
+          std::complex<double> in[64];
+          for (int r = 0; r < R; ++r) {
+            std::complex<double> v = src[j + l * (q + m * r)];
+            if (r > 0) {
+              std::complex<double> w = tw[(size_t)j * (R - 1) + (r - 1)];
+              if (sign > 0) w = std::conj(w);
+              v *= w;
+            }
+            in[r] = v;
           }
           std::complex<double>* out = dst + j + l * (R * q);
           if (R == 2) {
             out[0] = in[0] + in[1];
             out[l] = in[0] - in[1];
           } else if (R == 4) {
-            // X_p = sum_r x_r e^{sign 2 pi i p r / 4}; e^{sign i pi/2} = sign * i
             const std::complex<double> a = in[0] + in[2], b = in[0] - in[2];
             const std::complex<double> c = in[1] + in[3];
             const std::complex<double> d = (in[1] - in[3]) * std::complex<double>(0.0, (double)sign);
@@ -176,10 +182,8 @@ struct CFFT {
             for (int p = 0; p < R; ++p) {
               std::complex<double> acc = 0.0;
               for (int r = 0; r < R; ++r) {
-                const long idx = (long)((long)r * p % R) * (n / R);
-                std::complex<double> w = tw[idx];
-                if (sign > 0) w = std::conj(w);
-                acc += in[r] * w;
+                const long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)((r * p) % R) / R;
+                acc += in[r] * std::complex<double>((double)cosl(a), (double)(sign * sinl(a)));
               }
               out[p * l] = acc;
             }
@@ -743,38 +747,46 @@ void leg_fwd(const Oracle& o, const double* rtm, double* sp) {
 // rtm (slots m=-L..L: cos for m>=0, sin for -m) -> rtp grid, per (r, theta, comp).
 // Backward real FFT with the FFTPACK/FFTW-wrapper convention:
 //   x_j = a0 + sum_{k=1}^{N/2-1} (a_k cos(2 pi jk/N) + b_k sin(2 pi jk/N))
-// fld[(k + nr*(i + nth*p)) + nnod*comp]
+// fld[(k + nr*(i + nth*p)) + nnod*comp].  Work is blocked per latitude so the
+// grid is touched radius-contiguously, as FFTPACK's multiple-sequence RFFTMB
+// processes consecutive (r, theta) sequences together.
 void fft_bwd(const Oracle& o, const double* rtm, int nc, double* fld) {
-  const i64 N = o.nph, nrt = (i64)o.nr * o.nth, nnod = nrt * N;
+  const i64 N = o.nph, nnod = (i64)o.nr * o.nth * N;
+  const int np = (nc + 1) / 2;
 #pragma omp parallel num_threads(o.nthreads)
   {
-    std::vector<std::complex<double>> z(N), w(N);
+    std::vector<std::complex<double>> buf((size_t)o.nr * np * N), w(N);
 #pragma omp for schedule(static)
-    for (i64 jrt = 0; jrt < nrt; ++jrt) {
-      const i64 k = jrt % o.nr, i = jrt / o.nr;
-      for (int c0 = 0; c0 < nc; c0 += 2) {
-        const bool two = (c0 + 1 < nc);
-        for (i64 q = 0; q < N; ++q) z[q] = 0.0;
-        for (int m = 0; m <= o.L && m < N / 2; ++m) {
-          const i64 msp = o.L + m, msn = o.L - m;
-          for (int t = 0; t < (two ? 2 : 1); ++t) {
-            const int c = c0 + t;
-            const double a = rtm[((msp * o.nr + k) * o.nth + i) * nc + c];
-            const double b = (m == 0) ? 0.0 : rtm[((msn * o.nr + k) * o.nth + i) * nc + c];
-            // X[m] = (a - i b)/2 (m>0), X[0] = a; z = X_c0 + i X_c1
-            std::complex<double> X = (m == 0) ? std::complex<double>(a, 0.0)
-                                              : std::complex<double>(0.5 * a, -0.5 * b);
-            const std::complex<double> f = (t == 0) ? std::complex<double>(1, 0) : std::complex<double>(0, 1);
-            z[m] += f * X;
-            if (m > 0) z[N - m] += f * std::conj(X);
+    for (int i = 0; i < o.nth; ++i) {
+      for (int k = 0; k < o.nr; ++k)
+        for (int pp = 0; pp < np; ++pp) {
+          std::complex<double>* z = buf.data() + ((size_t)k * np + pp) * N;
+          for (i64 q = 0; q < N; ++q) z[q] = 0.0;
+          const int c0 = 2 * pp;
+          const bool two = (c0 + 1 < nc);
+          for (int m = 0; m <= o.L && m < N / 2; ++m) {
+            const i64 msp = o.L + m, msn = o.L - m;
+            for (int t = 0; t < (two ? 2 : 1); ++t) {
+              const int c = c0 + t;
+              const double a = rtm[((msp * o.nr + k) * o.nth + i) * nc + c];
+              const double b = (m == 0) ? 0.0 : rtm[((msn * o.nr + k) * o.nth + i) * nc + c];
+              std::complex<double> X = (m == 0) ? std::complex<double>(a, 0.0)
+                                                : std::complex<double>(0.5 * a, -0.5 * b);
+              const std::complex<double> f = (t == 0) ? std::complex<double>(1, 0) : std::complex<double>(0, 1);
+              z[m] += f * X;
+              if (m > 0) z[N - m] += f * std::conj(X);
+            }
+          }
+          o.fft.run(z, w.data(), +1);
+        }
+      for (int c = 0; c < nc; ++c)
+        for (i64 p = 0; p < N; ++p) {
+          double* dst = fld + (i64)o.nr * (i + (i64)o.nth * p) + nnod * c;
+          for (int k = 0; k < o.nr; ++k) {
+            const std::complex<double> v = buf[((size_t)k * np + c / 2) * N + p];
+            dst[k] = (c & 1) ? v.imag() : v.real();
           }
         }
-        o.fft.run(z.data(), w.data(), +1);
-        for (i64 p = 0; p < N; ++p) {
-          fld[(k + (i64)o.nr * (i + (i64)o.nth * p)) + nnod * c0] = z[p].real();
-          if (two) fld[(k + (i64)o.nr * (i + (i64)o.nth * p)) + nnod * (c0 + 1)] = z[p].imag();
-        }
-      }
     }
   }
 }
@@ -782,40 +794,46 @@ void fft_bwd(const Oracle& o, const double* rtm, int nc, double* fld) {
 // rtp grid -> rtm slots (m <= L kept).  a0 = (1/N) sum x, a_k = (2/N) sum x cos,
 // b_k = (2/N) sum x sin.
 void fft_fwd(const Oracle& o, const double* frc, int nc, double* rtm) {
-  const i64 N = o.nph, nrt = (i64)o.nr * o.nth, nnod = nrt * N;
+  const i64 N = o.nph, nnod = (i64)o.nr * o.nth * N;
+  const int np = (nc + 1) / 2;
   std::memset(rtm, 0, sizeof(double) * (i64)o.nth * o.nr * o.nmslot * nc);
 #pragma omp parallel num_threads(o.nthreads)
   {
-    std::vector<std::complex<double>> z(N), w(N);
+    std::vector<std::complex<double>> buf((size_t)o.nr * np * N), w(N);
 #pragma omp for schedule(static)
-    for (i64 jrt = 0; jrt < nrt; ++jrt) {
-      const i64 k = jrt % o.nr, i = jrt / o.nr;
-      for (int c0 = 0; c0 < nc; c0 += 2) {
-        const bool two = (c0 + 1 < nc);
+    for (int i = 0; i < o.nth; ++i) {
+      for (int pp = 0; pp < np; ++pp)
         for (i64 p = 0; p < N; ++p) {
-          const double x0 = frc[(k + (i64)o.nr * (i + (i64)o.nth * p)) + nnod * c0];
-          const double x1 = two ? frc[(k + (i64)o.nr * (i + (i64)o.nth * p)) + nnod * (c0 + 1)] : 0.0;
-          z[p] = std::complex<double>(x0, x1);
+          const double* s0 = frc + (i64)o.nr * (i + (i64)o.nth * p) + nnod * (2 * pp);
+          const double* s1 = s0 + nnod;
+          const bool two = (2 * pp + 1 < nc);
+          for (int k = 0; k < o.nr; ++k)
+            buf[((size_t)k * np + pp) * N + p] = std::complex<double>(s0[k], two ? s1[k] : 0.0);
         }
-        o.fft.run(z.data(), w.data(), -1);
-        const double aN = 1.0 / (double)N;
-        for (int m = 0; m <= o.L && m < N / 2; ++m) {
-          const std::complex<double> zp = z[m], zm = std::conj(z[(N - m) % N]);
-          const std::complex<double> X0 = 0.5 * (zp + zm);
-          const std::complex<double> X1 = std::complex<double>(0, -0.5) * (zp - zm);
-          for (int t = 0; t < (two ? 2 : 1); ++t) {
-            const std::complex<double> X = (t == 0) ? X0 : X1;
-            const int c = c0 + t;
-            const i64 msp = o.L + m, msn = o.L - m;
-            if (m == 0) {
-              rtm[((msp * o.nr + k) * o.nth + i) * nc + c] = aN * X.real();
-            } else {
-              rtm[((msp * o.nr + k) * o.nth + i) * nc + c] = 2.0 * aN * X.real();
-              rtm[((msn * o.nr + k) * o.nth + i) * nc + c] = -2.0 * aN * X.imag();
+      const double aN = 1.0 / (double)N;
+      for (int k = 0; k < o.nr; ++k)
+        for (int pp = 0; pp < np; ++pp) {
+          std::complex<double>* z = buf.data() + ((size_t)k * np + pp) * N;
+          o.fft.run(z, w.data(), -1);
+          const int c0 = 2 * pp;
+          const bool two = (c0 + 1 < nc);
+          for (int m = 0; m <= o.L && m < N / 2; ++m) {
+            const std::complex<double> zp = z[m], zm = std::conj(z[(N - m) % N]);
+            const std::complex<double> X0 = 0.5 * (zp + zm);
+            const std::complex<double> X1 = std::complex<double>(0, -0.5) * (zp - zm);
+            for (int t = 0; t < (two ? 2 : 1); ++t) {
+              const std::complex<double> X = (t == 0) ? X0 : X1;
+              const int c = c0 + t;
+              const i64 msp = o.L + m, msn = o.L - m;
+              if (m == 0) {
+                rtm[((msp * o.nr + k) * o.nth + i) * nc + c] = aN * X.real();
+              } else {
+                rtm[((msp * o.nr + k) * o.nth + i) * nc + c] = 2.0 * aN * X.real();
+                rtm[((msn * o.nr + k) * o.nth + i) * nc + c] = -2.0 * aN * X.imag();
+              }
             }
           }
         }
-      }
     }
   }
 }

@@ -9,8 +9,8 @@ from kemorin_mhd_b200 import sph_trans
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def declared_symbols():
-    src = open(os.path.join(ROOT, "include", "kmhd_sph.h")).read()
+def declared_symbols(header="kmhd_sph.h"):
+    src = open(os.path.join(ROOT, "include", header)).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     return sorted(set(re.findall(r"\b(kmhd_\w+)\s*\(", src)))
 
@@ -22,8 +22,10 @@ def test_header_matches_wrapper():
 def test_library_exports_all_symbols():
     kbuild.build()
     lib = ctypes.CDLL(kbuild.LIB)
-    for name in declared_symbols():
-        assert hasattr(lib, name), name
+    for hdr in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if hdr.endswith(".h"):
+            for name in declared_symbols(hdr):
+                assert hasattr(lib, name), (hdr, name)
 
 
 def test_strerror_without_gpu():
