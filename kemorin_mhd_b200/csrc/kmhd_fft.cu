@@ -169,16 +169,21 @@ __device__ void dit_dispatch(int R, double2* z, int npair, int N, int span, cons
 // Complex spectrum of pair pp at frequency k from staged records
 // st[(m*nc + c)*2 + {0: a, 1: b}], m <= L.  z = X_{2pp} + i X_{2pp+1},
 // X_c[m] = (a - i b)/2 for m > 0, X_c[0] = a, X_c[N-m] = conj(X_c[m]).
-__device__ __forceinline__ double2 spec_at(const double* st, int nc, int pp, int k, int N, int L) {
+__device__ __forceinline__ double2 spec_at(const double* st, int nc, int nv, int pp, int k, int N, int L) {
   int m;
   bool mirror;
   if (k <= L) { m = k; mirror = false; }
   else if (k >= N - L) { m = N - k; mirror = true; }
   else return make_double2(0.0, 0.0);
-  const double* r0 = st + (m * nc + 2 * pp) * 2;
+  const double* rec = st + m * nc * 2;
+  const double* r0 = rec + rec_off(2 * pp, nv);
   const double a0 = r0[0], b0 = r0[1];
   double a1 = 0.0, b1 = 0.0;
-  if (2 * pp + 1 < nc) { a1 = r0[2]; b1 = r0[3]; }
+  if (2 * pp + 1 < nc) {
+    const double* r1 = rec + rec_off(2 * pp + 1, nv);
+    a1 = r1[0];
+    b1 = r1[1];
+  }
   if (m == 0) return make_double2(a0, a1);
   return mirror ? make_double2(0.5 * a0 - 0.5 * b1, 0.5 * b0 + 0.5 * a1)
                 : make_double2(0.5 * a0 + 0.5 * b1, 0.5 * a1 - 0.5 * b0);
@@ -186,14 +191,14 @@ __device__ __forceinline__ double2 spec_at(const double* st, int nc, int pp, int
 
 // First DIF pass: input from the staged spectra, output into z.
 template <int R>
-__device__ void dif_first(const double* st, int nc, double2* z, int npair, int N, int L,
+__device__ void dif_first(const double* st, int nc, int nv, double2* z, int npair, int N, int L,
                           const double2* __restrict__ tw) {
   const int s = N / R, nbf = N / R;
   for (int it = threadIdx.x; it < npair * nbf; it += blockDim.x) {
     const int pp = it / nbf, j = it % nbf;
     double2 x[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) x[r] = spec_at(st, nc, pp, j + r * s, N, L);
+    for (int r = 0; r < R; ++r) x[r] = spec_at(st, nc, nv, pp, j + r * s, N, L);
     DFT<R, +1>::run(x);
     double2* base = z + pp * N + j;
     base[0] = x[0];
@@ -201,14 +206,14 @@ __device__ void dif_first(const double* st, int nc, double2* z, int npair, int N
     for (int q = 1; q < R; ++q) base[q * s] = cmul(x[q], twd<+1>(tw, j * q));
   }
 }
-__device__ void dif_first_dispatch(int R, const double* st, int nc, double2* z, int npair, int N,
-                                   int L, const double2* tw) {
+__device__ void dif_first_dispatch(int R, const double* st, int nc, int nv, double2* z, int npair,
+                                   int N, int L, const double2* tw) {
   switch (R) {
-    case 8: dif_first<8>(st, nc, z, npair, N, L, tw); break;
-    case 4: dif_first<4>(st, nc, z, npair, N, L, tw); break;
-    case 2: dif_first<2>(st, nc, z, npair, N, L, tw); break;
-    case 3: dif_first<3>(st, nc, z, npair, N, L, tw); break;
-    default: dif_first<5>(st, nc, z, npair, N, L, tw); break;
+    case 8: dif_first<8>(st, nc, nv, z, npair, N, L, tw); break;
+    case 4: dif_first<4>(st, nc, nv, z, npair, N, L, tw); break;
+    case 2: dif_first<2>(st, nc, nv, z, npair, N, L, tw); break;
+    case 3: dif_first<3>(st, nc, nv, z, npair, N, L, tw); break;
+    default: dif_first<5>(st, nc, nv, z, npair, N, L, tw); break;
   }
 }
 
@@ -247,7 +252,7 @@ __device__ void prefetch_line(double* st, const double* rtm, int nc, const Plan&
 }
 
 // Natural-order forward spectra in z -> (a_m, b_m), m <= L, into rtm.
-__device__ void store_line(const double2* z, int npair, const Plan& P, double* rtm, int nc, int th, int r) {
+__device__ void store_line(const double2* z, int npair, const Plan& P, double* rtm, int nc, int nv, int th, int r) {
   const int N = P.nph, L = P.L;
   const double aN = 1.0 / (double)N;
   const long long strideM = (long long)P.nth * P.nr * nc * 2;
@@ -266,9 +271,9 @@ __device__ void store_line(const double2* z, int npair, const Plan& P, double* r
       a1 = (zm.y + wm.y) * aN;
       b1 = (zm.x - wm.x) * aN;
     }
-    double* rec = base + m * strideM + 4 * pp;
-    *reinterpret_cast<double2*>(rec) = make_double2(a0, b0);
-    if (2 * pp + 1 < nc) *reinterpret_cast<double2*>(rec + 2) = make_double2(a1, b1);
+    double* rec = base + m * strideM;
+    *reinterpret_cast<double2*>(rec + rec_off(2 * pp, nv)) = make_double2(a0, b0);
+    if (2 * pp + 1 < nc) *reinterpret_cast<double2*>(rec + rec_off(2 * pp + 1, nv)) = make_double2(a1, b1);
   }
 }
 
@@ -391,7 +396,7 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_cycle(Plan P, int nlines) {
     const int r = line % P.nr, th = line / P.nr;
     cp_async_wait<0>();
     __syncthreads();
-    dif_first_dispatch(P.fac[0], st, P.ncb, z, npb, N, P.L, P.twid);
+    dif_first_dispatch(P.fac[0], st, P.ncb, P.nvb, z, npb, N, P.L, P.twid);
     __syncthreads();
     const int next = line + gridDim.x;
     if (next < nlines) prefetch_line(st, P.rtm_b, P.ncb, P, next / P.nr, next % P.nr);
@@ -399,7 +404,7 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_cycle(Plan P, int nlines) {
     products<MVB, MSB, MVF, MSF>(z, N, P);
     __syncthreads();
     dit_all(z, npf, N, P, P.twid);
-    store_line(z, npf, P, P.rtm_f, P.ncf, th, r);
+    store_line(z, npf, P, P.rtm_f, P.ncf, P.nvf, th, r);
     __syncthreads();
     line = next;
   }
@@ -417,7 +422,7 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_bwd_grid(Plan P, double* __
   prefetch_line(st, P.rtm_b, P.ncb, P, th, r);
   cp_async_wait<0>();
   __syncthreads();
-  dif_first_dispatch(P.fac[0], st, P.ncb, z, npb, N, P.L, P.twid);
+  dif_first_dispatch(P.fac[0], st, P.ncb, P.nvb, z, npb, N, P.L, P.twid);
   __syncthreads();
   dif_rest(z, npb, N, P, P.twid);
   const long long nnod = (long long)P.nr * P.nth * N;
@@ -448,7 +453,7 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_fwd_grid(Plan P, const doub
   }
   __syncthreads();
   dit_all(z, npf, N, P, P.twid);
-  store_line(z, npf, P, P.rtm_f, P.ncf, th, r);
+  store_line(z, npf, P, P.rtm_f, P.ncf, P.nvf, th, r);
 }
 
 size_t smem_cycle(const Plan& p) {

@@ -38,8 +38,8 @@ struct Plan {
   // work buffers
   double* SB;             // packed backward spectra [m][p][kpad][nrb*ncolb_blk]
   const long long* sboff; // [(L+1)*2]
-  double* rtm_b;          // [m][th][r][ncb][2]
-  double* rtm_f;          // [m][th][r][ncf][2]
+  double* rtm_b;          // [m][th][r][record of ncb (cos, sin) pairs, see rec_off]
+  double* rtm_f;          // [m][th][r][record of ncf pairs]
   // FFT
   int nfac;
   int fac[kMaxFftFactors];
@@ -69,6 +69,18 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// Offset (in doubles) of component c's (cos, sin) pair inside an rtm record of
+// one (m, theta, r): [theta/phi pairs of every vector: (th c, th s, ph c, ph s)]
+// [r pairs of every vector] [scalar pairs].  The theta/phi block of a vector is
+// one 32-byte sector, so tensor-core epilogues write whole sectors.
+__host__ __device__ __forceinline__ int rec_off(int c, int nv) {
+  if (c < 3 * nv) {
+    const int v = c / 3, q = c % 3;
+    return q == 0 ? 4 * nv + 2 * v : 4 * v + 2 * (q - 1);
+  }
+  return 6 * nv + 2 * (c - 3 * nv);
 }
 
 __host__ __device__ __forceinline__ int kcount(int L, int m, int p) {

@@ -240,12 +240,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_leg_bwd_f64(Plan p) {
         n.y = sym[2 * c + 1] + asym[2 * c + 1];
         s.x = sym[2 * c] - asym[2 * c];
         s.y = sym[2 * c + 1] - asym[2 * c + 1];
-        *reinterpret_cast<double2*>(outS + (3 * v + c) * 2) = s;
+        *reinterpret_cast<double2*>(outS + rec_off(3 * v + c, NV)) = s;
       } else {
         n.x = sym[2 * c];
         n.y = sym[2 * c + 1];
       }
-      *reinterpret_cast<double2*>(outN + (3 * v + c) * 2) = n;
+      *reinterpret_cast<double2*>(outN + rec_off(3 * v + c, NV)) = n;
     }
   }
 #pragma unroll
@@ -257,11 +257,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_leg_bwd_f64(Plan p) {
     if (pair) {
       n.x = sc + ac; n.y = ss + as;
       s.x = sc - ac; s.y = ss - as;
-      *reinterpret_cast<double2*>(outS + c * 2) = s;
+      *reinterpret_cast<double2*>(outS + rec_off(c, NV)) = s;
     } else {
       n.x = sc; n.y = ss;
     }
-    *reinterpret_cast<double2*>(outN + c * 2) = n;
+    *reinterpret_cast<double2*>(outN + rec_off(c, NV)) = n;
   }
 }
 
@@ -334,11 +334,12 @@ k_leg_fwd_f64(Plan p, double* __restrict__ d_rj, long long ld, const int* __rest
       double2 sy = make_double2(0.0, 0.0), as = sy, syn = sy, asn = sy;
       if (i < p.nh && r < p.nr) {
         const double wp = p.weight[i], ai = p.asin_t[i];
+        const int ro = rec_off(c, NV);
         const double2 nv = *reinterpret_cast<const double2*>(
-            p.rtm_f + ((long long)m * p.nth + i) * strideTh + ((long long)r * nc + c) * 2);
+            p.rtm_f + ((long long)m * p.nth + i) * strideTh + (long long)r * nc * 2 + ro);
         if (i < p.nth / 2) {
           const double2 sv = *reinterpret_cast<const double2*>(
-              p.rtm_f + ((long long)m * p.nth + (p.nth - 1 - i)) * strideTh + ((long long)r * nc + c) * 2);
+              p.rtm_f + ((long long)m * p.nth + (p.nth - 1 - i)) * strideTh + (long long)r * nc * 2 + ro);
           sy = make_double2((nv.x + sv.x) * wp, (nv.y + sv.y) * wp);
           as = make_double2((nv.x - sv.x) * wp, (nv.y - sv.y) * wp);
           syn = make_double2((nv.x + sv.x) * wp * ai, (nv.y + sv.y) * wp * ai);

@@ -426,6 +426,10 @@ int run_fwd_spectral(kmhd_sph* h, double* d_rj, int64_t ld) {
 
 int finish_timing(kmhd_sph* h) {
   KCHECK(cudaEventSynchronize(h->ev[3]));
+  if (h->split) {
+    const int e = split_check_error(h->split, h->stream);
+    if (e != KMHD_OK) return e;
+  }
   float a = 0, b = 0, c = 0, t = 0;
   KCHECK(cudaEventElapsedTime(&a, h->ev[0], h->ev[1]));
   KCHECK(cudaEventElapsedTime(&b, h->ev[1], h->ev[2]));

@@ -13,6 +13,8 @@ int split_bwd(SplitState* s, const Plan& p, int nlc_max, const double* d_rj, lon
               const int* cols, cudaStream_t st);
 int split_fwd(SplitState* s, const Plan& p, double* d_rj, long long ld, const int* cols,
               cudaStream_t st);
+// Reads and returns the device error word (KMHD_OK or KMHD_ERR_TIMEOUT); synchronises st.
+int split_check_error(SplitState* s, cudaStream_t st);
 
 }  // namespace kmhd
 

@@ -139,5 +139,7 @@ def test_scalar_product_single_mode():
     exp = np.zeros(J)
     exp[np.where((l == 0) & (m == 0))[0][0]] = 1.0 / 3.0
     exp[np.where((l == 2) & (m == 0))[0][0]] = 2.0 / 3.0
+    # the reference's Gauss weights carry ~1e-12 relative error (P'_n taken at
+    # the previous Newton iterate, gauss_integration.f90:111-116), hence 1e-11
     for k in range(cfg.nr):
-        assert np.abs(out[J * k:J * (k + 1), 0] - exp).max() < 1e-12
+        assert np.abs(out[J * k:J * (k + 1), 0] - exp).max() < 1e-11

@@ -1,0 +1,85 @@
+"""Split-precision tiers on the tcgen05 tensor cores vs the CPU FP64 oracle.
+
+Tolerances (max-norm relative error per field): tier "split" (6 INT8 slices,
+26 slice products) <= 1e-12; tier "fp32acc" (4 slices, 10 products) <= 1e-6.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from kemorin_mhd_b200.config import SphConfig, TIER_SPLIT_I8, TIER_FP32ACC
+from kemorin_mhd_b200.synthetic import make_d_rj
+from oracle.oracle import Oracle
+from tests.gpu_util import col_relerr, to_dev_fortran, from_dev_fortran
+
+TOL = {TIER_SPLIT_I8: 1e-12, TIER_FP32ACC: 1e-6}
+
+
+@pytest.mark.gpu
+def test_i8_mma_tile_layout():
+    from kemorin_mhd_b200.sph_trans import load_library
+    lib = load_library()
+    f = lib.kmhd_selftest_i8_mma
+    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    rng = np.random.default_rng(0)
+    A = rng.integers(-128, 128, (128, 32)).astype(np.int8)
+    B = rng.integers(-128, 128, (64, 32)).astype(np.int8)
+    D = np.zeros((128, 64), np.int32)
+    assert f(128, 256, A.ctypes.data, B.ctypes.data, D.ctypes.data) == 0
+    ref = A.astype(np.int64) @ B.astype(np.int64).T
+    assert np.array_equal(D.astype(np.int64), ref)
+
+
+CFGS = [
+    SphConfig(31, 48, 96, 9, name="L31"),
+    SphConfig(47, 73, 144, 6, name="L47_odd_nth"),
+    SphConfig(16, 26, 40, 5, nvb=1, nsb=2, nvf=1, nsf=1,
+              products=((1, 0, 1, 0.5), (3, 0, 1, 2.0)), name="L16_mixed"),
+    SphConfig(127, 192, 384, 17, name="L127"),
+]
+
+
+@pytest.fixture(scope="module", params=[(c, t) for c in CFGS for t in (TIER_SPLIT_I8, TIER_FP32ACC)],
+                ids=lambda p: f"{p[0].name}-tier{p[1]}")
+def case(request):
+    from kemorin_mhd_b200.sph_trans import SphTransform
+    cfg, tier = request.param
+    return cfg, tier, SphTransform(cfg, tier=tier), Oracle(cfg, nthreads=8)
+
+
+@pytest.mark.gpu
+def test_split_b_trans(case):
+    import torch
+    cfg, tier, tr, orc = case
+    d = make_d_rj(cfg, seed=21)
+    ref = orc.b_trans(d)
+    fld = torch.empty((cfg.ncb, cfg.nr * cfg.nth * cfg.nph), dtype=torch.float64, device="cuda")
+    tr.sph_b_trans(to_dev_fortran(d), fld)
+    err = col_relerr(from_dev_fortran(fld), ref)
+    assert err.max() <= TOL[tier], err
+
+
+@pytest.mark.gpu
+def test_split_f_trans(case):
+    import torch
+    cfg, tier, tr, orc = case
+    rng = np.random.default_rng(8)
+    frc = np.asfortranarray(rng.standard_normal((cfg.nr * cfg.nth * cfg.nph, cfg.ncf)))
+    ref = orc.f_trans(frc)
+    out = torch.zeros((cfg.ncf, cfg.J * cfg.nr), dtype=torch.float64, device="cuda")
+    tr.sph_f_trans(to_dev_fortran(frc), out)
+    err = col_relerr(from_dev_fortran(out), ref)
+    assert err.max() <= TOL[tier], err
+
+
+@pytest.mark.gpu
+def test_split_cycle(case):
+    import torch
+    cfg, tier, tr, orc = case
+    d = make_d_rj(cfg, seed=22)
+    ref = orc.cycle(d)
+    out = torch.zeros((cfg.ncf, cfg.J * cfg.nr), dtype=torch.float64, device="cuda")
+    tr.nonlinear_cycle(to_dev_fortran(d), out)
+    err = col_relerr(from_dev_fortran(out), ref)
+    assert err.max() <= TOL[tier], err
