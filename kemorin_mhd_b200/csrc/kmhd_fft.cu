@@ -456,6 +456,285 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_fwd_grid(Plan P, const doub
   store_line(z, npf, P, P.rtm_f, P.ncf, P.nvf, th, r);
 }
 
+// ---------------------------------------------------------------------------
+// Compile-time variant for the common N: factor list, spans and strides are
+// constants (no runtime division in the butterfly loops), 512 threads, and a
+// padded shared layout (one slot per 8 entries) that spreads the small-stride
+// passes over all banks.
+constexpr int kFftThreadsT = 512;
+
+__host__ __device__ constexpr int tfac_count(int n) {
+  int c = 0;
+  while (n % 8 == 0) { n /= 8; ++c; }
+  while (n % 4 == 0) { n /= 4; ++c; }
+  while (n % 2 == 0) { n /= 2; ++c; }
+  while (n % 3 == 0) { n /= 3; ++c; }
+  while (n % 5 == 0) { n /= 5; ++c; }
+  return c;
+}
+__host__ __device__ constexpr int tfac_at(int n, int i) {
+  int c = 0;
+  const int rs[5] = {8, 4, 2, 3, 5};
+  for (int q = 0; q < 5; ++q)
+    while (n % rs[q] == 0) {
+      if (c == i) return rs[q];
+      n /= rs[q];
+      ++c;
+    }
+  return 1;
+}
+__host__ __device__ constexpr int tspan_at(int n, int i) {
+  int sp = n;
+  for (int q = 0; q < i; ++q) sp /= tfac_at(n, q);
+  return sp;
+}
+__device__ __forceinline__ int ph(int i) { return i + (i >> 3); }
+
+template <int N, int I>
+__device__ __forceinline__ void tdif(double2* z, int npair, const double2* __restrict__ tw) {
+  if constexpr (I < tfac_count(N)) {
+    constexpr int R = tfac_at(N, I), span = tspan_at(N, I), s = span / R, nbf = N / R, stw = N / span;
+    constexpr int NP = N + N / 8;
+    for (int it = threadIdx.x; it < npair * nbf; it += blockDim.x) {
+      const int pp = it / nbf, rem = it - pp * nbf;
+      const int b = rem / s, j = rem - b * s;
+      double2* zp = z + pp * NP;
+      const int base = b * span + j;
+      double2 x[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) x[r] = zp[ph(base + r * s)];
+      DFT<R, +1>::run(x);
+      zp[ph(base)] = x[0];
+#pragma unroll
+      for (int q = 1; q < R; ++q) zp[ph(base + q * s)] = cmul(x[q], twd<+1>(tw, j * q * stw));
+    }
+    __syncthreads();
+    tdif<N, I + 1>(z, npair, tw);
+  }
+}
+
+template <int N, int I>
+__device__ __forceinline__ void tdit(double2* z, int npair, const double2* __restrict__ tw) {
+  if constexpr (I >= 0) {
+    constexpr int R = tfac_at(N, I), span = tspan_at(N, I), s = span / R, nbf = N / R, stw = N / span;
+    constexpr int NP = N + N / 8;
+    for (int it = threadIdx.x; it < npair * nbf; it += blockDim.x) {
+      const int pp = it / nbf, rem = it - pp * nbf;
+      const int b = rem / s, j = rem - b * s;
+      double2* zp = z + pp * NP;
+      const int base = b * span + j;
+      double2 x[R];
+      x[0] = zp[ph(base)];
+#pragma unroll
+      for (int q = 1; q < R; ++q) x[q] = cmul(zp[ph(base + q * s)], twd<-1>(tw, j * q * stw));
+      DFT<R, -1>::run(x);
+#pragma unroll
+      for (int r = 0; r < R; ++r) zp[ph(base + r * s)] = x[r];
+    }
+    __syncthreads();
+    tdit<N, I - 1>(z, npair, tw);
+  }
+}
+
+// first DIF pass from the staged spectra
+template <int N>
+__device__ __forceinline__ void tdif_first(const double* st, int nc, int nv, double2* z, int npair, int L,
+                                           const double2* __restrict__ tw) {
+  constexpr int R = tfac_at(N, 0), s = N / R, nbf = N / R;
+  constexpr int NP = N + N / 8;
+  for (int it = threadIdx.x; it < npair * nbf; it += blockDim.x) {
+    const int pp = it / nbf, j = it - pp * nbf;
+    double2 x[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) x[r] = spec_at(st, nc, nv, pp, j + r * s, N, L);
+    DFT<R, +1>::run(x);
+    double2* zp = z + pp * NP;
+    zp[ph(j)] = x[0];
+#pragma unroll
+    for (int q = 1; q < R; ++q) zp[ph(j + q * s)] = cmul(x[q], twd<+1>(tw, j * q));
+  }
+}
+
+template <int N>
+__device__ void tstore_line(const double2* z, int npair, const Plan& P, double* rtm, int nc, int nv, int th, int r) {
+  constexpr int NP = N + N / 8;
+  const int L = P.L;
+  const double aN = 1.0 / (double)N;
+  const long long strideM = (long long)P.nth * P.nr * nc * 2;
+  double* base = rtm + ((long long)th * P.nr + r) * nc * 2;
+  for (int it = threadIdx.x; it < (L + 1) * npair; it += blockDim.x) {
+    const int m = it / npair, pp = it - m * npair;
+    const double2* zp = z + pp * NP;
+    const double2 zm = zp[ph(m)];
+    double a0, b0, a1, b1;
+    if (m == 0) {
+      a0 = zm.x * aN; a1 = zm.y * aN; b0 = 0.0; b1 = 0.0;
+    } else {
+      const double2 wm = zp[ph(N - m)];
+      a0 = (zm.x + wm.x) * aN;
+      b0 = (wm.y - zm.y) * aN;
+      a1 = (zm.y + wm.y) * aN;
+      b1 = (zm.x - wm.x) * aN;
+    }
+    double* rec = base + m * strideM;
+    *reinterpret_cast<double2*>(rec + rec_off(2 * pp, nv)) = make_double2(a0, b0);
+    if (2 * pp + 1 < nc) *reinterpret_cast<double2*>(rec + rec_off(2 * pp + 1, nv)) = make_double2(a1, b1);
+  }
+}
+
+// products on the padded layout (same code as products(), addressing through ph)
+template <int N, int MVB, int MSB, int MVF, int MSF>
+__device__ void tproducts(double2* z, const Plan& P) {
+  constexpr int NP = N + N / 8;
+  constexpr int MCF = 3 * MVF + MSF;
+  const int nvb = P.nvb, nsb = P.nsb, nvf = P.nvf, nsf = P.nsf;
+  for (int pos = threadIdx.x; pos < N; pos += blockDim.x) {
+    const int pq = ph(pos);
+    double vin[3 * MVB > 0 ? 3 * MVB : 1], sin_[MSB > 0 ? MSB : 1];
+#pragma unroll
+    for (int c = 0; c < 3 * MVB; ++c)
+      if (c < 3 * nvb) {
+        const double2 v = z[(c >> 1) * NP + pq];
+        vin[c] = (c & 1) ? v.y : v.x;
+      }
+#pragma unroll
+    for (int q = 0; q < MSB; ++q)
+      if (q < nsb) {
+        const int c = 3 * nvb + q;
+        const double2 v = z[(c >> 1) * NP + pq];
+        sin_[q] = (c & 1) ? v.y : v.x;
+      }
+    double out[MCF > 0 ? MCF : 1];
+#pragma unroll
+    for (int i = 0; i < MVF; ++i) {
+      if (i < nvf) {
+        const double cf = P.pcoef[i];
+        double x0, x1, x2;
+        selvec<MVB>(vin, P.pa[i], x0, x1, x2);
+        if (P.pkind[i] == KMHD_PROD_CROSS) {
+          double y0, y1, y2;
+          selvec<MVB>(vin, P.pb[i], y0, y1, y2);
+          out[3 * i + 0] = (x1 * y2 - x2 * y1) * cf;
+          out[3 * i + 1] = (x2 * y0 - x0 * y2) * cf;
+          out[3 * i + 2] = (x0 * y1 - x1 * y0) * cf;
+        } else {
+          const double sv = selscl<MSB>(sin_, P.pb[i]);
+          out[3 * i + 0] = x0 * sv * cf;
+          out[3 * i + 1] = x1 * sv * cf;
+          out[3 * i + 2] = x2 * sv * cf;
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < MSF; ++j) {
+      if (j < nsf) {
+        const int q = nvf + j;
+        const double cf = P.pcoef[q];
+        double o;
+        if (P.pkind[q] == KMHD_PROD_DOT) {
+          double x0, x1, x2, y0, y1, y2;
+          selvec<MVB>(vin, P.pa[q], x0, x1, x2);
+          selvec<MVB>(vin, P.pb[q], y0, y1, y2);
+          o = (x0 * y0 + x1 * y1 + x2 * y2) * cf;
+        } else {
+          o = selscl<MSB>(sin_, P.pa[q]) * selscl<MSB>(sin_, P.pb[q]) * cf;
+        }
+        out[3 * MVF + j] = o;
+      }
+    }
+    const int ncf = 3 * nvf + nsf;
+    double dense[MCF > 0 ? MCF : 1];
+#pragma unroll
+    for (int c = 0; c < MCF; ++c) {
+      double v = 0.0;
+      if (c < 3 * MVF) v = out[c < 3 * MVF ? c : 0];
+      if (c >= 3 * nvf) {
+        v = 0.0;
+#pragma unroll
+        for (int j = 0; j < MSF; ++j)
+          if (c == 3 * nvf + j) v = out[3 * MVF + j];
+      }
+      dense[c] = v;
+    }
+#pragma unroll
+    for (int c = 0; c < MCF; c += 2) {
+      if (c < ncf) {
+        const double hi = (c + 1 < MCF && c + 1 < ncf) ? dense[c + 1 < MCF ? c + 1 : c] : 0.0;
+        z[(c >> 1) * NP + pq] = make_double2(dense[c], hi);
+      }
+    }
+  }
+}
+
+template <int N, int MVB, int MSB, int MVF, int MSF>
+__global__ void __launch_bounds__(kFftThreadsT, 1) k_fft_cycle_t(Plan P, int nlines) {
+  extern __shared__ double4 smraw[];
+  constexpr int NP = N + N / 8;
+  const int npb = (P.ncb + 1) / 2, npf = (P.ncf + 1) / 2;
+  const int npair = npb > npf ? npb : npf;
+  double2* z = reinterpret_cast<double2*>(smraw);
+  double* st = reinterpret_cast<double*>(z + npair * NP);
+  int line = blockIdx.x;
+  if (line >= nlines) return;
+  prefetch_line(st, P.rtm_b, P.ncb, P, line / P.nr, line % P.nr);
+  while (line < nlines) {
+    const int r = line % P.nr, th = line / P.nr;
+    cp_async_wait<0>();
+    __syncthreads();
+    tdif_first<N>(st, P.ncb, P.nvb, z, npb, P.L, P.twid);
+    __syncthreads();
+    const int next = line + gridDim.x;
+    if (next < nlines) prefetch_line(st, P.rtm_b, P.ncb, P, next / P.nr, next % P.nr);
+    tdif<N, 1>(z, npb, P.twid);
+    tproducts<N, MVB, MSB, MVF, MSF>(z, P);
+    __syncthreads();
+    tdit<N, tfac_count(N) - 1>(z, npf, P.twid);
+    tstore_line<N>(z, npf, P, P.rtm_f, P.ncf, P.nvf, th, r);
+    __syncthreads();
+    line = next;
+  }
+}
+
+size_t smem_cycle_t(const Plan& p) {
+  const int npair = ((p.ncb > p.ncf ? p.ncb : p.ncf) + 1) / 2;
+  return sizeof(double2) * (size_t)npair * (p.nph + p.nph / 8) + sizeof(double) * 2 * (size_t)(p.L + 1) * p.ncb;
+}
+
+template <int N, int MVB, int MSB, int MVF, int MSF>
+cudaError_t run_cycle_t(const Plan& p, cudaStream_t s) {
+  auto kern = k_fft_cycle_t<N, MVB, MSB, MVF, MSF>;
+  const size_t smem = smem_cycle_t(p);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, nsm = 0, occ = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kFftThreadsT, smem);
+  if (occ < 1) occ = 1;
+  const int nlines = p.nr * p.nth;
+  int grid = nsm * occ;
+  if (grid > nlines) grid = nlines;
+  kern<<<grid, kFftThreadsT, smem, s>>>(p, nlines);
+  return cudaGetLastError();
+}
+
+template <int MVB, int MSB, int MVF, int MSF>
+cudaError_t run_cycle_n(const Plan& p, cudaStream_t s, bool* handled) {
+  *handled = true;
+  if (smem_cycle_t(p) <= 227 * 1024) {
+    switch (p.nph) {
+      case 96: return run_cycle_t<96, MVB, MSB, MVF, MSF>(p, s);
+      case 192: return run_cycle_t<192, MVB, MSB, MVF, MSF>(p, s);
+      case 384: return run_cycle_t<384, MVB, MSB, MVF, MSF>(p, s);
+      case 768: return run_cycle_t<768, MVB, MSB, MVF, MSF>(p, s);
+      case 1536: return run_cycle_t<1536, MVB, MSB, MVF, MSF>(p, s);
+      default: break;
+    }
+  }
+  *handled = false;
+  return cudaSuccess;
+}
+
 size_t smem_cycle(const Plan& p) {
   const int npair = ((p.ncb > p.ncf ? p.ncb : p.ncf) + 1) / 2;
   return sizeof(double2) * (size_t)npair * p.nph + sizeof(double) * 2 * (size_t)(p.L + 1) * p.ncb;
@@ -487,7 +766,12 @@ size_t fft_smem_bytes(const Plan& p, int npair) {
 }
 
 cudaError_t launch_fft_cycle(const Plan& p, cudaStream_t s) {
-  if (p.nvb == 3 && p.nsb == 1 && p.nvf == 3 && p.nsf == 1) return run_cycle<3, 1, 3, 1>(p, s);
+  if (p.nvb == 3 && p.nsb == 1 && p.nvf == 3 && p.nsf == 1) {
+    bool handled = false;
+    const cudaError_t e = run_cycle_n<3, 1, 3, 1>(p, s, &handled);
+    if (handled) return e;
+    return run_cycle<3, 1, 3, 1>(p, s);
+  }
   if (p.nvb == 2 && p.nsb == 1 && p.nvf == 2 && p.nsf == 1) return run_cycle<2, 1, 2, 1>(p, s);
   if (p.nvb == 1 && p.nsb == 1 && p.nvf == 1 && p.nsf == 0) return run_cycle<1, 1, 1, 0>(p, s);
   return run_cycle<kMaxVec, kMaxScl, kMaxVec, kMaxScl>(p, s);

@@ -32,8 +32,9 @@ namespace {
 template <int NV, int NS>
 struct BwdGeo {
   static constexpr int CB = 24 * NV + 8 * NS;                       // columns per r-block
-  static constexpr int CBp = CB + ((8 - CB % 16) + 16) % 16;         // stride = 64 B mod 128
-  static constexpr int AS = kThBlk + 8;                              // A row stride (doubles)
+  // row strides = 32 B mod 128 B: a half warp (4 fragment rows x 32 B) spans all banks
+  static constexpr int CBp = CB + ((4 - CB % 16) + 16) % 16;
+  static constexpr int AS = kThBlk + 4;                              // A row stride (doubles)
   static constexpr int A_STAGE = 2 * kKC * AS;                       // P and dP
   static constexpr int B_STAGE = kKC * CBp;
   static constexpr size_t SMEM = sizeof(double) * 2 * (A_STAGE + B_STAGE);
@@ -269,7 +270,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_leg_bwd_f64(Plan p) {
 template <int NV, int NS>
 struct FwdGeo {
   static constexpr int CF = 40 * NV + 8 * NS;
-  static constexpr int CFp = CF + ((8 - CF % 16) + 16) % 16;
+  static constexpr int CFp = CF + ((4 - CF % 16) + 16) % 16;
   static constexpr int AS = kKC + 4;                      // 160 B rows
   static constexpr int A_TILE = kLBlk * AS;
   static constexpr int B_TILE = kKC * CFp;
@@ -304,6 +305,31 @@ k_leg_fwd_f64(Plan p, double* __restrict__ d_rj, long long ld, const int* __rest
   for (int s = 0; s < (NS > 0 ? NS : 1); ++s) accS[s][0] = accS[s][1] = 0.0;
 
   const long long strideTh = (long long)p.nr * nc * 2;
+  constexpr int kItems = (kKC * kRB * (3 * NV + NS) + kThreads - 1) / kThreads;
+  double2 pfN[kItems], pfS[kItems];
+  // global loads of one chunk's rtm_f values into registers (overlaps the MMAs)
+  auto prefetch = [&](int ch) {
+    const int th0 = ch * kKC;
+#pragma unroll
+    for (int q = 0; q < kItems; ++q) {
+      const int it = tid + q * kThreads;
+      pfN[q] = make_double2(0.0, 0.0);
+      pfS[q] = make_double2(0.0, 0.0);
+      if (it < kKC * kRB * nc) {
+        const int c = it % nc, rest = it / nc, u = rest % kRB, row = rest / kRB;
+        const int i = th0 + row, r = kRB * rb + u;
+        if (i < p.nh && r < p.nr) {
+          const int ro = rec_off(c, NV);
+          pfN[q] = *reinterpret_cast<const double2*>(p.rtm_f + ((long long)m * p.nth + i) * strideTh +
+                                                     (long long)r * nc * 2 + ro);
+          if (i < p.nth / 2)
+            pfS[q] = *reinterpret_cast<const double2*>(p.rtm_f + ((long long)m * p.nth + (p.nth - 1 - i)) * strideTh +
+                                                       (long long)r * nc * 2 + ro);
+        }
+      }
+    }
+  };
+  prefetch(0);
   for (int ch = 0; ch < nchunk; ++ch) {
     const int th0 = ch * kKC;
     // A: 4 tables x 32 k-rows x 16 theta
@@ -323,8 +349,11 @@ k_leg_fwd_f64(Plan p, double* __restrict__ d_rj, long long ld, const int* __rest
       }
     }
     cp_async_commit();
-    // B: (row, radius, comp) items, sym/asym with weights
-    for (int it = tid; it < kKC * kRB * nc; it += kThreads) {
+    // B: sym/asym with weights from the prefetched registers
+#pragma unroll
+    for (int q = 0; q < kItems; ++q) {
+      const int it = tid + q * kThreads;
+      if (it >= kKC * kRB * nc) continue;
       const int c = it % nc;
       const int rest = it / nc;
       const int u = rest % kRB;
@@ -334,12 +363,9 @@ k_leg_fwd_f64(Plan p, double* __restrict__ d_rj, long long ld, const int* __rest
       double2 sy = make_double2(0.0, 0.0), as = sy, syn = sy, asn = sy;
       if (i < p.nh && r < p.nr) {
         const double wp = p.weight[i], ai = p.asin_t[i];
-        const int ro = rec_off(c, NV);
-        const double2 nv = *reinterpret_cast<const double2*>(
-            p.rtm_f + ((long long)m * p.nth + i) * strideTh + (long long)r * nc * 2 + ro);
+        const double2 nv = pfN[q];
         if (i < p.nth / 2) {
-          const double2 sv = *reinterpret_cast<const double2*>(
-              p.rtm_f + ((long long)m * p.nth + (p.nth - 1 - i)) * strideTh + (long long)r * nc * 2 + ro);
+          const double2 sv = pfS[q];
           sy = make_double2((nv.x + sv.x) * wp, (nv.y + sv.y) * wp);
           as = make_double2((nv.x - sv.x) * wp, (nv.y - sv.y) * wp);
           syn = make_double2((nv.x + sv.x) * wp * ai, (nv.y + sv.y) * wp * ai);
@@ -352,29 +378,30 @@ k_leg_fwd_f64(Plan p, double* __restrict__ d_rj, long long ld, const int* __rest
       double* b0 = sB + row * G::CFp;               // parity 0
       double* b1 = sB + G::B_TILE + row * G::CFp;   // parity 1
       if (c < 3 * NV) {
-        const int v = c / 3, q = c % 3;
+        const int v = c / 3, qq = c % 3;
         const int base = 40 * v + 2 * u;
-        if (q == 0) {            // r: Zr tile (P)
+        if (qq == 0) {            // r: Zr tile (P)
           *reinterpret_cast<double2*>(b0 + base + 0) = sy;
           *reinterpret_cast<double2*>(b1 + base + 0) = as;
-        } else if (q == 1) {     // theta: U' tile (P, /sin), W tile (dP)
+        } else if (qq == 1) {     // theta: U' tile (P, /sin), W tile (dP)
           *reinterpret_cast<double2*>(b0 + base + 16) = syn;
           *reinterpret_cast<double2*>(b1 + base + 16) = asn;
           *reinterpret_cast<double2*>(b0 + base + 24) = as;
           *reinterpret_cast<double2*>(b1 + base + 24) = sy;
-        } else {                 // phi: U tile (P, /sin), W' tile (dP)
+        } else {                  // phi: U tile (P, /sin), W' tile (dP)
           *reinterpret_cast<double2*>(b0 + base + 8) = syn;
           *reinterpret_cast<double2*>(b1 + base + 8) = asn;
           *reinterpret_cast<double2*>(b0 + base + 32) = as;
           *reinterpret_cast<double2*>(b1 + base + 32) = sy;
         }
       } else {
-        const int s = c - 3 * NV;
-        const int base = 40 * NV + 8 * s + 2 * u;
+        const int sc = c - 3 * NV;
+        const int base = 40 * NV + 8 * sc + 2 * u;
         *reinterpret_cast<double2*>(b0 + base) = sy;
         *reinterpret_cast<double2*>(b1 + base) = as;
       }
     }
+    if (ch + 1 < nchunk) prefetch(ch + 1);
     cp_async_wait<0>();
     __syncthreads();
     const double* aP = sA + par * G::A_TILE + (rgi * 8 + g) * G::AS;
@@ -493,8 +520,8 @@ cudaError_t launch_leg_fwd_f64(const Plan& p, double* d_rj, long long ld, const 
 
 size_t bwd_smem_bytes(int nv, int ns) {
   const int CB = 24 * nv + 8 * ns;
-  const int CBp = CB + ((8 - CB % 16) + 16) % 16;
-  return sizeof(double) * 2 * (2 * kKC * (kThBlk + 8) + kKC * CBp);
+  const int CBp = CB + ((4 - CB % 16) + 16) % 16;
+  return sizeof(double) * 2 * (2 * kKC * (kThBlk + 4) + kKC * CBp);
 }
 
 }  // namespace kmhd

@@ -131,8 +131,12 @@ int validate(const kmhd_sph_desc* d) {
   if (d->nproduct > 0 && (nv != d->nvector_f || ns != d->nscalar_f)) return KMHD_ERR_ARG;
   std::vector<int> f;
   if (!factor_fft(d->nph, f)) return KMHD_ERR_SIZE;
-  const int npair = (std::max(3 * d->nvector_b + d->nscalar_b, 3 * d->nvector_f + d->nscalar_f) + 1) / 2;
-  if (sizeof(double2) * ((size_t)npair * d->nph + d->nph) > 227 * 1024) return KMHD_ERR_SIZE;
+  // one (r, theta) line of every component plus the staged spectra must fit in
+  // shared memory (fused FFT / products kernel)
+  const int ncb = 3 * d->nvector_b + d->nscalar_b, ncf = 3 * d->nvector_f + d->nscalar_f;
+  const int npair = (std::max(ncb, ncf) + 1) / 2;
+  if (sizeof(double2) * (size_t)npair * d->nph + sizeof(double) * 2 * (size_t)(d->ltr + 1) * ncb > 227 * 1024)
+    return KMHD_ERR_SIZE;
   return KMHD_OK;
 }
 
