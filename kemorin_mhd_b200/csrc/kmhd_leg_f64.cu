@@ -278,7 +278,7 @@ struct FwdGeo {
 };
 
 template <int NV, int NS>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, 2)
 k_leg_fwd_f64(Plan p, double* __restrict__ d_rj, long long ld, const int* __restrict__ cols) {
   using G = FwdGeo<NV, NS>;
   extern __shared__ double sm[];

@@ -251,167 +251,245 @@ __global__ void k_a_slices(Plan P, SliceTabs S, int t) {
 }
 
 // ---------------------------------------------------------------------------
-// B operand values.
-// Backward theta/phi column (v, r, q); K concatenation as the A type.
-__device__ inline double b_bwd_value(const Plan& P, const SliceTabs& S, const double* d_rj, long long ld,
-                                     const int* cols, int t, int m, int col, int k) {
-  const TypeGeo g = type_geo(t, P.L, m, P.nh);
+// Slicers, staged per (m, radius): every input value of that radius and order is
+// read once from HBM into shared memory; all derived columns of the four
+// operand types are then formed, scaled and digitised from there.
+//
+// Column list of one (m, r): backward: for each vector v: types 0/1 quantity q
+// (8 columns), for each field f < 4: types 2/3 slots (4 columns); forward: types
+// 4/5 (field f, slot) and types 6/7 (vector v, quantity q).
+constexpr int kMaxCols = 64;  // derived columns per (m, r): at most 48 with 4 fields
+
+struct ColRef {
+  int t, col;     // operand type and global column index
+  int f, q;       // field (vector or scalar slot) and quantity/slot selector
+};
+
+__device__ __forceinline__ int ncols_bwd(const Plan& P) { return 8 * P.nvb + 4 * (P.nvb + P.nsb); }
+__device__ __forceinline__ int ncols_fwd(const Plan& P) { return 4 * (P.nvf + P.nsf) + 8 * P.nvf; }
+
+__device__ __forceinline__ ColRef colref_bwd(const Plan& P, const SliceTabs& S, int r, int i) {
+  ColRef c;
+  if (i < 8 * P.nvb) {
+    const int v = i >> 3, t = (i >> 2) & 1, q = i & 3;
+    c.t = t; c.f = v; c.q = q; c.col = (v * S.nrT + r) * 4 + q;
+  } else {
+    const int j = i - 8 * P.nvb, f = j >> 2, t = 2 + ((j >> 1) & 1), slot = j & 1;
+    c.t = t; c.f = f; c.q = slot; c.col = (r * 4 + f) * 2 + slot;
+  }
+  return c;
+}
+__device__ __forceinline__ ColRef colref_fwd(const Plan& P, const SliceTabs& S, int r, int i) {
+  ColRef c;
+  const int nf1 = 4 * (P.nvf + P.nsf);
+  if (i < nf1) {
+    const int f = i >> 2, t = 4 + ((i >> 1) & 1), slot = i & 1;
+    c.t = t; c.f = f; c.q = slot; c.col = (r * 4 + f) * 2 + slot;
+  } else {
+    const int j = i - nf1, v = j >> 3, t = 6 + ((j >> 2) & 1), q = j & 3;
+    c.t = t; c.f = v; c.q = q; c.col = (v * S.nrT + r) * 4 + q;
+  }
+  return c;
+}
+
+// backward staged inputs: sm_in[(slot * nc + comp) * Kall + (l - m)]
+__device__ __forceinline__ double bval_staged(const Plan& P, const double* in, int Kall, const ColRef& c, int m,
+                                              int k, double ar) {
+  const TypeGeo g = type_geo(c.t, P.L, m, P.nh);
   const int Ke = kcount(P.L, m, 0), Ko = kcount(P.L, m, 1);
-  if (t <= 1) {
-    const int q = col & 3, r = (col >> 2) % S.nrT, v = (col >> 2) / S.nrT;
-    if (v >= P.nvb || r >= P.nr) return 0.0;
-    int par, kk;
+  const int nc = P.ncb;
+  if (c.t <= 1) {
     const bool first = k < g.kpart0;
-    kk = first ? k : k - g.kpart0;
-    // type 0: first part odd l (dP_o), second even l (msP_e); type 1 the reverse
-    par = (t == 0) ? (first ? 1 : 0) : (first ? 0 : 1);
+    const int kk = first ? k : k - g.kpart0;
+    const int par = (c.t == 0) ? (first ? 1 : 0) : (first ? 0 : 1);
     if (kk >= (par ? Ko : Ke)) return 0.0;
-    const int l = m + 2 * kk + par;
-    // quantity selection: first part uses dP columns, second the m/sin P columns
-    // q: 0 th cos, 1 th sin, 2 ph cos, 3 ph sin
-    // first part  : b+, b-, -c+, -c-
-    // second part : c-, -c+, b-, -b+
+    const int lo = 2 * kk + par;  // l - m
     int slot, comp;
     double sg = 1.0;
     if (first) {
-      comp = (q < 2) ? 1 : 2;  // b = dS/dr (col+1), c = T (col+2)
-      slot = q & 1;
-      if (q >= 2) sg = -1.0;
+      comp = (c.q < 2) ? 1 : 2;
+      slot = c.q & 1;
+      if (c.q >= 2) sg = -1.0;
     } else {
-      switch (q) {
+      switch (c.q) {
         case 0: comp = 2; slot = 1; break;
         case 1: comp = 2; slot = 0; sg = -1.0; break;
         case 2: comp = 1; slot = 1; break;
         default: comp = 1; slot = 0; sg = -1.0; break;
       }
     }
-    if (slot == 1 && m == 0) return 0.0;
-    const int j = P.jmap[((long long)m * 2 + slot) * (P.L + 1) + l];
-    const double x = d_rj[(long long)j + P.J * r + ld * (cols[v] + comp)];
-    return sg * (x * (1.0 / P.radius[r]));
+    return sg * (in[(slot * nc + 3 * c.f + comp) * Kall + lo] * ar);
   }
-  // r / scalar columns (r, f, slot), f < 4
-  const int slot = col & 1, f = (col >> 1) & 3, r = col >> 3;
-  if (r >= P.nr || f >= P.nvb + P.nsb) return 0.0;
-  const int par = t - 2;
-  if (k >= (par ? Ko : Ke)) return 0.0;
-  if (slot == 1 && m == 0) return 0.0;
-  const int l = m + 2 * k + par;
-  const int j = P.jmap[((long long)m * 2 + slot) * (P.L + 1) + l];
-  if (f < P.nvb) {
-    const double ar = 1.0 / P.radius[r];
-    return d_rj[(long long)j + P.J * r + ld * cols[f]] * (ar * ar) * g3_of(l);
-  }
-  return d_rj[(long long)j + P.J * r + ld * cols[f]];
+  const int par = c.t - 2;
+  if (k >= (par ? Ko : Ke) || c.f >= P.nvb + P.nsb) return 0.0;
+  const int lo = 2 * k + par;
+  if (c.f < P.nvb) return in[(c.q * nc + 3 * c.f) * Kall + lo] * (ar * ar) * g3_of(m + lo);
+  return in[(c.q * nc + 3 * P.nvb + (c.f - P.nvb)) * Kall + lo];
 }
 
-// Forward columns from the grid spectra rtm_f (sym / asym with weights).
-__device__ inline double b_fwd_value(const Plan& P, const SliceTabs& S, int t, int m, int col, int k) {
-  const TypeGeo g = type_geo(t, P.L, m, P.nh);
-  const int par = (t == 4 || t == 6) ? 0 : 1;
-  const long long strideTh = (long long)P.nr * P.ncf * 2;
-  auto sy = [&](int th, int r, int c, int slot, bool want_sym, bool overs) -> double {
-    // (N +- S) w [/ sin], equator: N w, asym 0
-    const int ro = rec_off(c, P.nvf) + slot;
+// forward staged inputs: sm_in[th * rec + rec_off(comp) + slot] (rec = 2 ncf), full theta range
+__device__ __forceinline__ double fval_staged(const Plan& P, const double* in, const ColRef& c, int m, int k) {
+  const TypeGeo g = type_geo(c.t, P.L, m, P.nh);
+  const int rec = 2 * P.ncf;
+  const int par = (c.t == 4 || c.t == 6) ? 0 : 1;
+  auto sy = [&](int th, int comp, int slot, bool want_sym, bool overs) -> double {
+    const int ro = rec_off(comp, P.nvf) + slot;
     const double wp = P.weight[th];
-    const double nval = P.rtm_f[((long long)m * P.nth + th) * strideTh + (long long)r * P.ncf * 2 + ro];
+    const double nv = in[th * rec + ro];
     double v;
     if (th < P.nth / 2) {
-      const double sval = P.rtm_f[((long long)m * P.nth + (P.nth - 1 - th)) * strideTh + (long long)r * P.ncf * 2 + ro];
-      v = want_sym ? (nval + sval) * wp : (nval - sval) * wp;
+      const double sv = in[(P.nth - 1 - th) * rec + ro];
+      v = want_sym ? (nv + sv) * wp : (nv - sv) * wp;
     } else {
-      v = want_sym ? nval * wp : 0.0;
+      v = want_sym ? nv * wp : 0.0;
     }
     return overs ? v * P.asin_t[th] : v;
   };
-  if (t <= 5) {
-    const int slot = col & 1, f = (col >> 1) & 3, r = col >> 3;
-    if (r >= P.nr || f >= P.nvf + P.nsf || k >= P.nh) return 0.0;
-    if (slot == 1 && m == 0) return 0.0;
-    const int c = f < P.nvf ? 3 * f : 3 * P.nvf + (f - P.nvf);
-    return sy(k, r, c, slot, par == 0, false);
+  if (c.t <= 5) {
+    if (c.f >= P.nvf + P.nsf || k >= P.nh) return 0.0;
+    if (c.q == 1 && m == 0) return 0.0;
+    const int comp = c.f < P.nvf ? 3 * c.f : 3 * P.nvf + (c.f - P.nvf);
+    return sy(k, comp, c.q, par == 0, false);
   }
-  const int q = col & 3, r = (col >> 2) % S.nrT, v = (col >> 2) / S.nrT;
-  if (v >= P.nvf || r >= P.nr) return 0.0;
   const bool first = k < g.kpart0;
   const int th = first ? k : k - g.kpart0;
   if (th >= P.nh) return 0.0;
   if (m == 0 && !first) return 0.0;
-  // W = [a]sym(F_theta) w, W' = [a]sym(F_phi) w      (dP part: asym for even l)
-  // U = [a]sym(F_phi) w/sin, U' = [a]sym(F_theta) w/sin (P part: sym for even l)
   const bool dP_sym = (par == 1), P_sym = (par == 0);
-  // q: 0 comp2+ = W.c - m U.s ; 1 comp2- = W.s + m U.c ; 2 comp3+ = -W'.c - m U'.s ; 3 comp3- = -W'.s + m U'.c
+  const int v = c.f;
   if (first) {
-    switch (q) {
-      case 0: return sy(th, r, 3 * v + 1, 0, dP_sym, false);
-      case 1: return sy(th, r, 3 * v + 1, 1, dP_sym, false);
-      case 2: return -sy(th, r, 3 * v + 2, 0, dP_sym, false);
-      default: return -sy(th, r, 3 * v + 2, 1, dP_sym, false);
+    switch (c.q) {
+      case 0: return sy(th, 3 * v + 1, 0, dP_sym, false);
+      case 1: return sy(th, 3 * v + 1, 1, dP_sym, false);
+      case 2: return -sy(th, 3 * v + 2, 0, dP_sym, false);
+      default: return -sy(th, 3 * v + 2, 1, dP_sym, false);
     }
   }
-  switch (q) {
-    case 0: return -sy(th, r, 3 * v + 2, 1, P_sym, true);
-    case 1: return sy(th, r, 3 * v + 2, 0, P_sym, true);
-    case 2: return -sy(th, r, 3 * v + 1, 1, P_sym, true);
-    default: return sy(th, r, 3 * v + 1, 0, P_sym, true);
+  switch (c.q) {
+    case 0: return -sy(th, 3 * v + 2, 1, P_sym, true);
+    case 1: return sy(th, 3 * v + 2, 0, P_sym, true);
+    case 2: return -sy(th, 3 * v + 1, 1, P_sym, true);
+    default: return sy(th, 3 * v + 1, 0, P_sym, true);
   }
 }
 
-// B slicer: one CTA per (m, type, n-tile).  Pass 1: column maxima of B' = B/D;
-// pass 2: digits, written as 16-byte rows of the tile layout.
-template <bool FWD>
-__global__ void k_b_slices(Plan P, SliceTabs S, int t, const double* __restrict__ d_rj, long long ld,
-                           const int* __restrict__ cols) {
-  __shared__ int colexp[kTN];
-  __shared__ double colmax[kTN];
-  const int m = blockIdx.y;
-  const int nt = blockIdx.x;
-  const TypeGeo g = type_geo(t, P.L, m, P.nh);
-  if (nt * kTN >= S.npadT[t]) return;
-  const int* dx = S.dexp + S.deoff[m * kNT + t];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  auto val = [&](int c, int k) -> double {
-    const int col = nt * kTN + c;
-    const double x = FWD ? b_fwd_value(P, S, t, m, col, k) : b_bwd_value(P, S, d_rj, ld, cols, t, m, col, k);
-    return ldexp(x, -dx[k]);
-  };
-  for (int c = warp; c < kTN; c += nw) {
-    double mx = 0.0;
-    for (int k = lane; k < g.kpad; k += 32) mx = fmax(mx, fabs(val(c, k)));
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if (lane == 0) {
-      colmax[c] = mx;
-      colexp[c] = mx > 0.0 ? exp_above(mx) : 0;
+template <int NS>
+__device__ __forceinline__ void digits_pack16(const double* v16, uint32_t (&w)[NS][4]) {
+#pragma unroll
+  for (int s = 0; s < NS; ++s)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) w[s][q] = 0u;
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    long long x = __double2ll_rn(v16[q]);
+#pragma unroll
+    for (int s = NS - 1; s >= 1; --s) {
+      const long long dd = ((x + 128) & 255) - 128;
+      w[s][q >> 2] |= ((uint32_t)dd & 0xFFu) << (8 * (q & 3));
+      x = (x - dd) >> 8;
+    }
+    w[0][q >> 2] |= ((uint32_t)x & 0xFFu) << (8 * (q & 3));
+  }
+}
+
+template <bool FWD, int NS>
+__global__ void __launch_bounds__(256) k_slice_mr(Plan P, SliceTabs S, const double* __restrict__ d_rj, long long ld,
+                                                   const int* __restrict__ cols) {
+  extern __shared__ double sin_[];
+  const int m = blockIdx.y, r = blockIdx.x;
+  const int L = P.L;
+  const int Kall = L - m + 1;
+  const int nc = FWD ? P.ncf : P.ncb;
+  // ---- stage inputs
+  if (!FWD) {
+    const int nrow = 2 * nc;
+    for (int it = threadIdx.x; it < nrow * Kall; it += blockDim.x) {
+      const int row = it / Kall, lo = it - row * Kall;
+      const int slot = row / nc, q = row - slot * nc;
+      double v = 0.0;
+      if (slot == 0 || m > 0) {
+        const int j = P.jmap[((long long)m * 2 + slot) * (L + 1) + m + lo];
+        const int col = q < 3 * P.nvb ? cols[q / 3] + q % 3 : cols[P.nvb + (q - 3 * P.nvb)];
+        v = d_rj[(long long)j + P.J * r + ld * col];
+      }
+      sin_[it] = v;
+    }
+  } else {
+    const int rec = 2 * nc;
+    const long long strideTh = (long long)P.nr * rec;
+    const double* base = P.rtm_f + (long long)m * P.nth * strideTh + (long long)r * rec;
+    for (int it = threadIdx.x; it < P.nth * (rec / 2); it += blockDim.x) {
+      const int th = it / (rec / 2), c2 = it - th * (rec / 2);
+      *reinterpret_cast<double2*>(sin_ + th * rec + 2 * c2) =
+          *reinterpret_cast<const double2*>(base + th * strideTh + 2 * c2);
     }
   }
   __syncthreads();
-  const int bits = 8 * S.ns - 2;
-  if (threadIdx.x < kTN) S.bexp[S.beoff[m * kNT + t] + nt * kTN + threadIdx.x] = colexp[threadIdx.x] - bits;
-  signed char* base = S.B + S.boff[m * kNT + t];
-  const int nkc = g.kpad / kTK;
-  const int n16 = g.kpad / 16;
-  for (int it = threadIdx.x; it < kTN * n16; it += blockDim.x) {
-    const int c = it % kTN, kb = it / kTN;
-    const bool nz = colmax[c] > 0.0;
-    const int sh = bits - colexp[c];
-    alignas(16) signed char row[8][16];
-    for (int q = 0; q < 16; ++q) {
-      signed char d[8];
-      const double v = nz ? ldexp(val(c, kb * 16 + q), sh) : 0.0;
-      digits(v, S.ns, d);
-      for (int s = 0; s < S.ns; ++s) row[s][q] = d[s];
+  const int ncol = FWD ? ncols_fwd(P) : ncols_bwd(P);
+  double* colmax = sin_ + (FWD ? P.nth * 2 * nc : 2 * nc * Kall);
+  int* colexp = reinterpret_cast<int*>(colmax + kMaxCols);
+  const double ar = 1.0 / P.radius[r];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // ---- column maxima of B' = B 2^-dexp
+  for (int i = warp; i < ncol; i += blockDim.x >> 5) {
+    const ColRef c = FWD ? colref_fwd(P, S, r, i) : colref_bwd(P, S, r, i);
+    const TypeGeo g = type_geo(c.t, L, m, P.nh);
+    const int* dx = S.dexp + S.deoff[m * kNT + c.t];
+    double mx = 0.0;
+    for (int k = lane; k < g.kpad; k += 32) {
+      const double x = FWD ? fval_staged(P, sin_, c, m, k) : bval_staged(P, sin_, Kall, c, m, k, ar);
+      mx = fmax(mx, fabs(ldexp(x, -__ldg(dx + k))));
     }
-    const int kc = kb >> 1;
-    for (int s = 0; s < S.ns; ++s) {
-      signed char* dst = base + ((long long)(nt * nkc + kc) * S.ns + s) * (kTN * kTK) + tile_off(c, (kb & 1) * 16);
-      *reinterpret_cast<int4*>(dst) = *reinterpret_cast<const int4*>(row[s]);
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) {
+      colmax[i] = mx;
+      colexp[i] = mx > 0.0 ? exp_above(mx) : 0;
+      S.bexp[S.beoff[m * kNT + c.t] + c.col] = (mx > 0.0 ? exp_above(mx) : 0) - (8 * NS - 2);
+    }
+  }
+  __syncthreads();
+  // ---- digits, 16 consecutive k per item
+  for (int i = warp; i < ncol; i += blockDim.x >> 5) {
+    const ColRef c = FWD ? colref_fwd(P, S, r, i) : colref_bwd(P, S, r, i);
+    const TypeGeo g = type_geo(c.t, L, m, P.nh);
+    const int n16 = g.kpad / 16;
+    const int nkc = g.kpad / kTK;
+    const bool nz = colmax[i] > 0.0;
+    const int sh = (8 * NS - 2) - colexp[i];
+    const int* dx = S.dexp + S.deoff[m * kNT + c.t];
+    signed char* base = S.B + S.boff[m * kNT + c.t];
+    const int nt = c.col / kTN, cr = c.col % kTN;
+    for (int kb = lane; kb < n16; kb += 32) {
+      double v16[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int k = kb * 16 + q;
+        const double x = FWD ? fval_staged(P, sin_, c, m, k) : bval_staged(P, sin_, Kall, c, m, k, ar);
+        v16[q] = nz ? ldexp(x, sh - __ldg(dx + k)) : 0.0;
+      }
+      uint32_t w[NS][4];
+      digits_pack16<NS>(v16, w);
+      const int kc = kb >> 1;
+#pragma unroll
+      for (int s2 = 0; s2 < NS; ++s2) {
+        signed char* dst = base + ((long long)(nt * nkc + kc) * NS + s2) * (kTN * kTK) + tile_off(cr, (kb & 1) * 16);
+        *reinterpret_cast<uint4*>(dst) = make_uint4(w[s2][0], w[s2][1], w[s2][2], w[s2][3]);
+      }
     }
   }
 }
 
 // ---------------------------------------------------------------------------
-// The split GEMM.  One CTA = (m, type, m-tile, n-tile); backward launches pair
-// the sym (rank 0) and asym (rank 1) CTAs of one output tile in a cluster.
+// The split GEMM: persistent, warp-specialised.
+//   warp 0 (one lane): issues the tcgen05.mma slice products into TMEM
+//   warp 1 (one lane): streams pre-laid-out slice tiles with bulk copies into a
+//                      stage ring, running ahead across tiles
+//   warps 2..5:        epilogue (TMEM -> FP64 recombination -> output)
+// One tile = (m, type, m-tile, n-tile).  The backward work list pairs the sym
+// (rank 0) and asym (rank 1) tiles of one output tile in a 2-CTA cluster; each
+// CTA sends its FP64 tile to the peer with remote shared-memory stores and a
+// remote mbarrier arrival, then emits N = sym + asym (rank 0) or S = sym - asym
+// (rank 1).
 struct Work {
   int m, t, mt, nt;
 };
@@ -428,33 +506,87 @@ struct GemmArgs {
   int* err;        // device error word
 };
 
+constexpr int kGemmWarps = 6;
+constexpr int kEpiThreads = 128;
+constexpr int kRing = 3;           // stage ring depth
+constexpr int kXS = kTN + 1;       // exchange row stride (doubles)
+
 __device__ __forceinline__ unsigned make_idesc() {
   // kind::i8: D s32 (2 << 4), A s8 (1 << 7), B s8 (1 << 10), K-major A/B, N = 64, M = 128
   return (2u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(kTN >> 3) << 17) | ((unsigned)(kTM >> 4) << 24);
 }
 
+// exact int32 -> double on the FP64 pipe (2^52 + 2^31 magic)
+__device__ __forceinline__ double i2d(int x) {
+  return __hiloint2double(0x43300000, (unsigned)x ^ 0x80000000u) - 4503601774854144.0;
+}
+// 2^e as a double, e in the normal range
+__device__ __forceinline__ double pow2(int e) {
+  if (e < -1022 || e > 1023) return ldexp(1.0, e);
+  return __longlong_as_double((long long)(e + 1023) << 52);
+}
+
+__device__ __forceinline__ unsigned mapa(const void* p, unsigned rank) {
+  unsigned a;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(a) : "r"(sptr(p)), "r"(rank));
+  return a;
+}
+__device__ __forceinline__ void st_remote_f64(unsigned addr, double v) {
+  asm volatile("st.shared::cluster.f64 [%0], %1;\n" ::"r"(addr), "d"(v) : "memory");
+}
+__device__ __forceinline__ void arrive_remote(unsigned bar_addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(bar_addr) : "memory");
+}
+__device__ __forceinline__ bool mbar_wait_cluster(unsigned long long* b, unsigned parity) {
+  for (long long it = 0; it < kSpinCap; ++it) {
+    unsigned ok;
+    asm volatile(
+        "{\n.reg .pred p;\nmbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+        "selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(sptr(b)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+template <int NS>
+__host__ __device__ constexpr size_t gemm_stage_bytes() { return (size_t)NS * (kTM + kTN) * kTK; }
+
 template <int NS, int TG>
-__global__ void __launch_bounds__(kGemmThreads, 1) k_split_gemm(GemmArgs args) {
+__global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args) {
   extern __shared__ __align__(1024) unsigned char sm[];
   constexpr int A_BYTES = NS * kTM * kTK, B_BYTES = NS * kTN * kTK;
   constexpr int STAGE = A_BYTES + B_BYTES;
-  unsigned long long* full = reinterpret_cast<unsigned long long*>(sm + kStages * STAGE);
-  unsigned long long* empty = full + kStages;
-  unsigned long long* done = empty + kStages;
-  unsigned* tmem_slot = reinterpret_cast<unsigned*>(done + 1);
+  double* recv = reinterpret_cast<double*>(sm + kRing * STAGE);   // [kTM][kXS], written by the peer
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(recv + kTM * kXS);
+  unsigned long long* full = bars;              // [kRing]
+  unsigned long long* empty = bars + kRing;     // [kRing]
+  unsigned long long* done = bars + 2 * kRing;  // accumulators ready
+  unsigned long long* tfree = done + 1;         // TMEM drained by the epilogue
+  unsigned long long* rfull = tfree + 1;        // peer wrote my recv buffer
+  unsigned long long* rempty = rfull + 1;       // peer consumed the buffer I wrote
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(rempty + 1);
+
   const Plan& P = args.P;
   const SliceTabs& S = args.S;
-  const Work w = args.work[blockIdx.x];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const TypeGeo g = type_geo(w.t, P.L, w.m, P.nh);
-  const int nk = g.rows > 0 ? g.kpad / kTK : 0;
+  const bool pair = args.pair != 0;
+  const unsigned rank = pair ? cluster_rank() : 0u;
+  const int nunits = pair ? args.nwork / 2 : args.nwork;
+  const int ustride = pair ? gridDim.x / 2 : gridDim.x;
+  const int ubase = pair ? blockIdx.x / 2 : blockIdx.x;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], 1);
+    for (int q = 0; q < kRing; ++q) {
+      mbar_init(&full[q], 1);
+      mbar_init(&empty[q], 1);
     }
     mbar_init(done, 1);
+    mbar_init(tfree, kEpiThreads);
+    mbar_init(rfull, kEpiThreads);
+    mbar_init(rempty, kEpiThreads);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 0) {
@@ -463,156 +595,199 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_split_gemm(GemmArgs args) {
   }
   tc_fence_before();
   __syncthreads();
+  if (pair) cluster_sync();  // peer barriers initialised before any remote arrival
   tc_fence_after();
   const unsigned tmem = *tmem_slot;
-  bool ok = true;
 
-  const signed char* Ag = S.A + S.aoff[w.m * kNT + w.t] + (long long)w.mt * nk * A_BYTES;
-  const signed char* Bg = S.B + S.boff[w.m * kNT + w.t] + (long long)w.nt * nk * B_BYTES;
+  auto item = [&](int u) -> Work { return args.work[pair ? 2 * u + (int)rank : u]; };
+  auto nk_of = [&](const Work& w) -> int {
+    const TypeGeo g = type_geo(w.t, P.L, w.m, P.nh);
+    return g.rows > 0 ? g.kpad / kTK : 0;
+  };
 
-  if (nk > 0) {
-    if (warp == 1 && lane == 0) {
-      // producer: bulk copies of pre-laid-out slice tiles
-      for (int kc = 0; kc < nk; ++kc) {
-        const int st = kc % kStages;
-        if (kc >= kStages && !mbar_wait(&empty[st], ((kc / kStages) - 1) & 1)) { ok = false; break; }
-        mbar_expect_tx(&full[st], STAGE);
-        bulk_g2s(sm + st * STAGE, Ag + (long long)kc * A_BYTES, A_BYTES, &full[st]);
-        bulk_g2s(sm + st * STAGE + A_BYTES, Bg + (long long)kc * B_BYTES, B_BYTES, &full[st]);
+  if (warp == 1) {
+    if (lane == 0) {
+      // ---- producer
+      long long gc = 0;
+      bool ok = true;
+      for (int u = ubase; u < nunits && ok; u += ustride) {
+        const Work w = item(u);
+        const int nk = nk_of(w);
+        const signed char* Ag = S.A + S.aoff[w.m * kNT + w.t] + (long long)w.mt * nk * A_BYTES;
+        const signed char* Bg = S.B + S.boff[w.m * kNT + w.t] + (long long)w.nt * nk * B_BYTES;
+        for (int kc = 0; kc < nk; ++kc, ++gc) {
+          const int st = (int)(gc % kRing);
+          if (gc >= kRing && !mbar_wait(&empty[st], (unsigned)(((gc / kRing) - 1) & 1))) { ok = false; break; }
+          mbar_expect_tx(&full[st], STAGE);
+          bulk_g2s(sm + st * STAGE, Ag + (long long)kc * A_BYTES, A_BYTES, &full[st]);
+          bulk_g2s(sm + st * STAGE + A_BYTES, Bg + (long long)kc * B_BYTES, B_BYTES, &full[st]);
+        }
       }
       if (!ok) atomicExch(args.err, KMHD_ERR_TIMEOUT);
-    } else if (warp == 0 && lane == 0) {
+    }
+  } else if (warp == 0) {
+    if (lane == 0) {
+      // ---- MMA issuer
       const unsigned idesc = make_idesc();
-      for (int kc = 0; kc < nk; ++kc) {
-        const int st = kc % kStages;
-        if (!mbar_wait(&full[st], (kc / kStages) & 1)) { ok = false; break; }
+      long long gc = 0;
+      int it = 0;
+      bool ok = true;
+      for (int u = ubase; u < nunits; u += ustride, ++it) {
+        const Work w = item(u);
+        const int nk = nk_of(w);
+        if (it > 0 && ok && !mbar_wait(tfree, (unsigned)((it - 1) & 1))) ok = false;
         tc_fence_after();
-        const unsigned char* As = sm + st * STAGE;
-        const unsigned char* Bs = As + A_BYTES;
+        for (int kc = 0; kc < nk && ok; ++kc, ++gc) {
+          const int st = (int)(gc % kRing);
+          if (!mbar_wait(&full[st], (unsigned)((gc / kRing) & 1))) { ok = false; break; }
+          tc_fence_after();
+          const unsigned char* As = sm + st * STAGE;
+          const unsigned char* Bs = As + A_BYTES;
 #pragma unroll
-        for (int u = 0; u < NS; ++u) {
+          for (int a = 0; a < NS; ++a) {
 #pragma unroll
-          for (int v = 0; v < NS; ++v) {
-            const int grp = u + v;
-            if (grp > TG) continue;
-            // the first product of group grp (smallest u) overwrites, the rest accumulate
-            const unsigned first_u = (grp < NS) ? 0 : grp - (NS - 1);
-            const unsigned acc = (kc > 0 || (unsigned)u > first_u) ? 1u : 0u;
-            mma_i8(tmem + (unsigned)(grp * kTN), smem_desc(As + u * (kTM * kTK), 128, 256),
-                   smem_desc(Bs + v * (kTN * kTK), 128, 256), idesc, acc);
+            for (int b = 0; b < NS; ++b) {
+              const int grp = a + b;
+              if (grp > TG) continue;
+              // the first product of group grp (smallest a) overwrites, the rest accumulate
+              const unsigned first_a = (grp < NS) ? 0 : grp - (NS - 1);
+              const unsigned acc = (kc > 0 || (unsigned)a > first_a) ? 1u : 0u;
+              mma_i8(tmem + (unsigned)(grp * kTN), smem_desc(As + a * (kTM * kTK), 128, 256),
+                     smem_desc(Bs + b * (kTN * kTK), 128, 256), idesc, acc);
+            }
           }
+          mma_commit(&empty[st]);
         }
-        mma_commit(&empty[st]);
+        mma_commit(done);
       }
-      mma_commit(done);
       if (!ok) atomicExch(args.err, KMHD_ERR_TIMEOUT);
     }
-    __syncwarp();
-    // every thread waits for the accumulators
-    if (!mbar_wait(done, 0)) {
-      ok = false;
-      atomicExch(args.err, KMHD_ERR_TIMEOUT);
-    }
-    tc_fence_after();
-  }
-
-  // ---- epilogue: combine groups, scale, and emit
-  const int row = warp * 32 + lane;  // TMEM lane
-  const int grow = w.mt * kTM + row;
-  const int eA = (grow < g.rows) ? S.aexp[S.aeoff[w.m * kNT + w.t] + grow] : 0;
-  const int* eBp = S.bexp + S.beoff[w.m * kNT + w.t] + w.nt * kTN;
-  const double wscale = ldexp(1.0, 8 * (2 * NS - 2 - TG));
-  double* xbuf = reinterpret_cast<double*>(sm);  // [kTM][kTN + 1] for the cluster exchange
-  for (int cb = 0; cb < kTN / 16; ++cb) {
-    double val[16];
-    if (nk > 0 && ok) {
-      int acc[TG + 1][16];
+  } else {
+    // ---- epilogue warps 2..5: TMEM lane quadrant = warp % 4
+    const int quad = warp & 3;
+    const int row = quad * 32 + lane;
+    const double wscale = pow2(8 * (2 * NS - 2 - TG));
+    const unsigned peer = rank ^ 1u;
+    const unsigned peer_recv = pair ? mapa(recv, peer) : 0u;
+    const unsigned peer_rfull = pair ? mapa(rfull, peer) : 0u;
+    const unsigned peer_rempty = pair ? mapa(rempty, peer) : 0u;
+    int it = 0;
+    bool ok = true;
+    for (int u = ubase; u < nunits; u += ustride, ++it) {
+      const Work w = item(u);
+      const int nk = nk_of(w);
+      const TypeGeo g = type_geo(w.t, P.L, w.m, P.nh);
+      const int grow = w.mt * kTM + row;
+      const int eA = (grow < g.rows) ? S.aexp[S.aeoff[w.m * kNT + w.t] + grow] : 0;
+      const int* eBp = S.bexp + S.beoff[w.m * kNT + w.t] + w.nt * kTN;
+      if (ok && !mbar_wait(done, (unsigned)(it & 1))) ok = false;
+      tc_fence_after();
+      double val[kTN];
+      if (nk > 0 && ok) {
 #pragma unroll
-      for (int gi = 0; gi <= TG; ++gi)
-        tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)(gi * kTN + cb * 16), acc[gi]);
-      tmem_wait_ld();
+        for (int cb = 0; cb < kTN / 16; ++cb) {
+          int acc[TG + 1][16];
 #pragma unroll
-      for (int c = 0; c < 16; ++c) {
-        double v = (double)acc[0][c];
+          for (int gi = 0; gi <= TG; ++gi)
+            tmem_ld16(tmem + ((unsigned)(quad * 32) << 16) + (unsigned)(gi * kTN + cb * 16), acc[gi]);
+          tmem_wait_ld();
 #pragma unroll
-        for (int gi = 1; gi <= TG; ++gi) v = v * 256.0 + (double)acc[gi][c];
-        val[c] = ldexp(v * wscale, eA + eBp[cb * 16 + c]);
-      }
-    } else {
+          for (int c = 0; c < 16; ++c) {
+            double v = i2d(acc[0][c]);
 #pragma unroll
-      for (int c = 0; c < 16; ++c) val[c] = 0.0;
-    }
-    if (args.pair) {
-#pragma unroll
-      for (int c = 0; c < 16; ++c) xbuf[row * (kTN + 1) + cb * 16 + c] = val[c];
-    } else {
-      // forward: scatter into d_rj with the r, r^2, g7, g6, m factors
-      const int par = (w.t == 4 || w.t == 6) ? 0 : 1;
-      const int l = w.m + 2 * grow + par;
-      if (grow < g.rows && l <= P.L) {
-        const double g7 = g7_of(l, w.m);
-#pragma unroll
-        for (int c = 0; c < 16; ++c) {
-          const int col = w.nt * kTN + cb * 16 + c;
-          if (w.t <= 5) {
-            const int slot = col & 1, f = (col >> 1) & 3, r = col >> 3;
-            if (r >= P.nr || f >= P.nvf + P.nsf || (slot == 1 && w.m == 0)) continue;
-            const long long j = P.jmap[((long long)w.m * 2 + slot) * (P.L + 1) + l] + P.J * r;
-            if (f < P.nvf) {
-              const double r1 = P.radius[r];
-              args.d_rj[j + args.ld * args.cols[f]] = val[c] * (r1 * r1) * g7;
-            } else {
-              args.d_rj[j + args.ld * args.cols[f]] = val[c] * g6_of(l, w.m);
-            }
-          } else {
-            const int q = col & 3, r = (col >> 2) % S.nrT, v = (col >> 2) / S.nrT;
-            if (v >= P.nvf || r >= P.nr) continue;
-            const int slot = q & 1;
-            if (slot == 1 && w.m == 0) continue;
-            const long long j = P.jmap[((long long)w.m * 2 + slot) * (P.L + 1) + l] + P.J * r;
-            args.d_rj[j + args.ld * (args.cols[v] + 1 + (q >> 1))] = val[c] * P.radius[r] * g7;
+            for (int gi = 1; gi <= TG; ++gi) v = fma(v, 256.0, i2d(acc[gi][c]));
+            val[cb * 16 + c] = v * (wscale * pow2(eA + __ldg(eBp + cb * 16 + c)));
           }
         }
+      } else {
+#pragma unroll
+        for (int c = 0; c < kTN; ++c) val[c] = 0.0;
+      }
+      tc_fence_before();
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(sptr(tfree)) : "memory");
+
+      if (!pair) {
+        // forward: scatter into d_rj with the r, r^2, g7, g6 factors
+        const int par = (w.t == 4 || w.t == 6) ? 0 : 1;
+        const int l = w.m + 2 * grow + par;
+        if (grow < g.rows && l <= P.L) {
+          const double g7 = g7_of(l, w.m);
+#pragma unroll
+          for (int c = 0; c < kTN; ++c) {
+            const int col = w.nt * kTN + c;
+            if (w.t <= 5) {
+              const int slot = col & 1, f = (col >> 1) & 3, r = col >> 3;
+              if (r >= P.nr || f >= P.nvf + P.nsf || (slot == 1 && w.m == 0)) continue;
+              const long long j = P.jmap[((long long)w.m * 2 + slot) * (P.L + 1) + l] + P.J * r;
+              if (f < P.nvf) {
+                const double r1 = P.radius[r];
+                args.d_rj[j + args.ld * args.cols[f]] = val[c] * (r1 * r1) * g7;
+              } else {
+                args.d_rj[j + args.ld * args.cols[f]] = val[c] * g6_of(l, w.m);
+              }
+            } else {
+              const int q = col & 3, r = (col >> 2) % S.nrT, v = (col >> 2) / S.nrT;
+              if (v >= P.nvf || r >= P.nr) continue;
+              const int slot = q & 1;
+              if (slot == 1 && w.m == 0) continue;
+              const long long j = P.jmap[((long long)w.m * 2 + slot) * (P.L + 1) + l] + P.J * r;
+              args.d_rj[j + args.ld * (args.cols[v] + 1 + (q >> 1))] = val[c] * P.radius[r] * g7;
+            }
+          }
+        }
+      } else {
+        // backward: send my tile to the peer, receive the peer's, emit N or S
+        if (it > 0 && ok && !mbar_wait_cluster(rempty, (unsigned)((it - 1) & 1))) ok = false;
+#pragma unroll
+        for (int c = 0; c < kTN; ++c) st_remote_f64(peer_recv + (unsigned)((row * kXS + c) * 8), val[c]);
+        arrive_remote(peer_rfull);
+        if (ok && !mbar_wait_cluster(rfull, (unsigned)(it & 1))) ok = false;
+        const int th = grow;
+        if (th < P.nh && ok) {
+          const bool pairrow = th < P.nth / 2;
+          const int thout = rank == 0 ? th : P.nth - 1 - th;
+          if (rank == 0 || pairrow) {
+            const long long recb = ((long long)w.m * P.nth + thout) * P.nr * P.ncb * 2;
+            const double* rv = recv + row * kXS;
+            if (w.t <= 1) {
+#pragma unroll
+              for (int c = 0; c < kTN; c += 4) {
+                const int col = w.nt * kTN + c;
+                const int r = (col >> 2) % S.nrT, vv = (col >> 2) / S.nrT;
+                if (vv >= P.nvb || r >= P.nr) continue;
+                double o[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                  o[q] = !pairrow ? val[c + q] : (rank == 0 ? val[c + q] + rv[c + q] : rv[c + q] - val[c + q]);
+                double* dst = P.rtm_b + recb + (long long)r * P.ncb * 2 + 4 * vv;
+                reinterpret_cast<double2*>(dst)[0] = make_double2(o[0], o[1]);
+                reinterpret_cast<double2*>(dst)[1] = make_double2(o[2], o[3]);
+              }
+            } else {
+#pragma unroll
+              for (int c = 0; c < kTN; c += 2) {
+                const int col = w.nt * kTN + c;
+                const int f = (col >> 1) & 3, r = col >> 3;
+                if (r >= P.nr || f >= P.nvb + P.nsb) continue;
+                double o[2];
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+                  o[q] = !pairrow ? val[c + q] : (rank == 0 ? val[c + q] + rv[c + q] : rv[c + q] - val[c + q]);
+                *reinterpret_cast<double2*>(P.rtm_b + recb + (long long)r * P.ncb * 2 + 4 * P.nvb + 2 * f) =
+                    make_double2(o[0], o[1]);
+              }
+            }
+          }
+        }
+        arrive_remote(peer_rempty);
       }
     }
+    if (!ok) atomicExch(args.err, KMHD_ERR_TIMEOUT);
   }
   tc_fence_before();
   __syncthreads();
+  if (pair) cluster_sync();  // no CTA leaves while its peer may still touch its shared memory
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;\n" ::"r"(tmem));
-
-  if (args.pair) {
-    // ---- backward: N = sym + asym (rank 0), S = sym - asym (rank 1)
-    cluster_sync();
-    const unsigned rank = cluster_rank();
-    const unsigned peer = rank ^ 1u;
-    const int th = grow;
-    if (th < P.nh) {
-      const bool pairrow = th < P.nth / 2;
-      const int thout = rank == 0 ? th : P.nth - 1 - th;
-      const bool write = rank == 0 || pairrow;
-      if (write) {
-        const long long recb = ((long long)w.m * P.nth + thout) * P.nr * P.ncb * 2;
-        for (int c = 0; c < kTN; ++c) {
-          const double own = xbuf[row * (kTN + 1) + c];
-          const double oth = ld_peer_f64(xbuf + row * (kTN + 1) + c, peer);
-          double v;
-          if (!pairrow) v = rank == 0 ? own : 0.0;            // equator: sym only
-          else v = rank == 0 ? own + oth : oth - own;          // rank 1 holds asym
-          const int col = w.nt * kTN + c;
-          if (w.t <= 1) {
-            const int q = col & 3, r = (col >> 2) % S.nrT, vv = (col >> 2) / S.nrT;
-            if (vv >= P.nvb || r >= P.nr) continue;
-            P.rtm_b[recb + (long long)r * P.ncb * 2 + 4 * vv + q] = v;
-          } else {
-            const int slot = col & 1, f = (col >> 1) & 3, r = col >> 3;
-            if (r >= P.nr || f >= P.nvb + P.nsb) continue;
-            P.rtm_b[recb + (long long)r * P.ncb * 2 + 4 * P.nvb + 2 * f + slot] = v;
-          }
-        }
-      }
-    }
-    cluster_sync();
-  }
 }
 
 }  // namespace
@@ -644,18 +819,29 @@ int salloc(SplitState* s, T** p, size_t n) {
 }
 
 size_t gemm_smem(int ns) {
-  return (size_t)kStages * ns * (kTM + kTN) * kTK + (2 * kStages + 2) * 8 + 64;
+  const size_t stage = (size_t)ns * (kTM + kTN) * kTK;
+  return kRing * stage + sizeof(double) * kTM * kXS + (2 * kRing + 6) * 8 + 64;
 }
 
 template <int NS, int TG>
-cudaError_t launch_gemm(const GemmArgs& a, int nblocks, bool cluster, cudaStream_t st) {
+cudaError_t launch_gemm(const GemmArgs& a, bool cluster, cudaStream_t st) {
   auto kern = k_split_gemm<NS, TG>;
-  const size_t smem = gemm_smem(NS) > (size_t)(kTM * (kTN + 1) * 8) ? gemm_smem(NS) : (size_t)(kTM * (kTN + 1) * 8) + 256;
+  const size_t smem = gemm_smem(NS);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  if (cluster) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 0);
+    (void)e;
+  }
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int units = cluster ? a.nwork / 2 : a.nwork;
+  int grid = cluster ? 2 * std::min(units, nsm / 2) : std::min(units, nsm);
+  if (grid <= 0) return cudaSuccess;
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(nblocks);
-  cfg.blockDim = dim3(kGemmThreads);
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kGemmWarps * 32);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
@@ -672,9 +858,9 @@ cudaError_t launch_gemm(const GemmArgs& a, int nblocks, bool cluster, cudaStream
   return cudaLaunchKernelEx(&cfg, kern, a);
 }
 
-cudaError_t run_gemm(const SplitState* s, const GemmArgs& a, int nblocks, bool cluster, cudaStream_t st) {
-  if (s->ns == 6) return launch_gemm<6, 6>(a, nblocks, cluster, st);
-  return launch_gemm<4, 3>(a, nblocks, cluster, st);
+cudaError_t run_gemm(const SplitState* s, const GemmArgs& a, bool cluster, cudaStream_t st) {
+  if (s->ns == 6) return launch_gemm<6, 6>(a, cluster, st);
+  return launch_gemm<4, 3>(a, cluster, st);
 }
 
 }  // namespace
@@ -781,7 +967,8 @@ int split_create(SplitState** out, const Plan& p, int tier, int nslice, cudaStre
       up(beoff_d, s->beoff.data(), sizeof(long long) * s->beoff.size()) ||
       (wb.size() && up(s->work_b, wb.data(), sizeof(Work) * wb.size())) ||
       (wf.size() && up(s->work_f, wf.data(), sizeof(Work) * wf.size())) ||
-      cudaMemsetAsync(s->err, 0, sizeof(int), st) || cudaMemsetAsync(S.B, 0, (size_t)bo, st)) {
+      cudaMemsetAsync(s->err, 0, sizeof(int), st) || cudaMemsetAsync(S.B, 0, (size_t)bo, st) ||
+      cudaMemsetAsync(S.bexp, 0, sizeof(int) * (size_t)beo, st)) {
     split_destroy(s);
     return KMHD_ERR_CUDA;
   }
@@ -806,11 +993,12 @@ int split_create(SplitState** out, const Plan& p, int tier, int nslice, cudaStre
 
 int split_bwd(SplitState* s, const Plan& p, int, const double* d_rj, long long ld, const int* cols, cudaStream_t st) {
   const SliceTabs& S = s->S;
-  int maxn = 0;
-  for (int t = 0; t < 4; ++t) maxn = std::max(maxn, S.npadT[t] / kTN);
-  for (int t = 0; t < 4; ++t) {
-    if (t <= 1 && p.nvb == 0) continue;
-    k_b_slices<false><<<dim3(maxn, p.L + 1), 256, 0, st>>>(p, S, t, d_rj, ld, cols);
+  {
+    const size_t smem = sizeof(double) * (2 * (size_t)p.ncb * (p.L + 1) + kMaxCols) + kMaxCols * sizeof(int);
+    auto kern = s->ns == 6 ? k_slice_mr<false, 6> : k_slice_mr<false, 4>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      return KMHD_ERR_CUDA;
+    kern<<<dim3(p.nr, p.L + 1), 256, smem, st>>>(p, S, d_rj, ld, cols);
   }
   if (cudaGetLastError() != cudaSuccess) return KMHD_ERR_CUDA;
   GemmArgs a;
@@ -823,17 +1011,18 @@ int split_bwd(SplitState* s, const Plan& p, int, const double* d_rj, long long l
   a.ld = 0;
   a.cols = nullptr;
   a.err = s->err;
-  if (s->nwork_b > 0 && run_gemm(s, a, s->nwork_b, true, st) != cudaSuccess) return KMHD_ERR_CUDA;
+  if (s->nwork_b > 0 && run_gemm(s, a, true, st) != cudaSuccess) return KMHD_ERR_CUDA;
   return KMHD_OK;
 }
 
 int split_fwd(SplitState* s, const Plan& p, double* d_rj, long long ld, const int* cols, cudaStream_t st) {
   const SliceTabs& S = s->S;
-  int maxn = 0;
-  for (int t = 4; t < 8; ++t) maxn = std::max(maxn, S.npadT[t] / kTN);
-  for (int t = 4; t < 8; ++t) {
-    if (t >= 6 && p.nvf == 0) continue;
-    k_b_slices<true><<<dim3(maxn, p.L + 1), 256, 0, st>>>(p, S, t, nullptr, 0, nullptr);
+  {
+    const size_t smem = sizeof(double) * (2 * (size_t)p.ncf * p.nth + kMaxCols) + kMaxCols * sizeof(int);
+    auto kern = s->ns == 6 ? k_slice_mr<true, 6> : k_slice_mr<true, 4>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      return KMHD_ERR_CUDA;
+    kern<<<dim3(p.nr, p.L + 1), 256, smem, st>>>(p, S, nullptr, 0, nullptr);
   }
   if (cudaGetLastError() != cudaSuccess) return KMHD_ERR_CUDA;
   GemmArgs a;
@@ -846,7 +1035,7 @@ int split_fwd(SplitState* s, const Plan& p, double* d_rj, long long ld, const in
   a.ld = ld;
   a.cols = cols;
   a.err = s->err;
-  if (s->nwork_f > 0 && run_gemm(s, a, s->nwork_f, false, st) != cudaSuccess) return KMHD_ERR_CUDA;
+  if (s->nwork_f > 0 && run_gemm(s, a, false, st) != cudaSuccess) return KMHD_ERR_CUDA;
   return KMHD_OK;
 }
 
