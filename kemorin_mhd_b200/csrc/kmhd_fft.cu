@@ -457,56 +457,73 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_fwd_grid(Plan P, const doub
 }
 
 // ---------------------------------------------------------------------------
-// Compile-time variant for the common N: factor list, spans and strides are
-// constants (no runtime division in the butterfly loops), 512 threads, and a
-// padded shared layout (one slot per 8 entries) that spreads the small-stride
-// passes over all banks.
+// Compile-time variant for the common N = 3 2^k: factor order (3, leftover 4 or
+// 2, then 8s), spans and strides are constants, 512 threads, and a bank-
+// conflict-free shared layout: inside each pair sequence the index is swizzled
+// i -> i ^ ((i >> 3) & 7) and pairs are N + 1 entries apart; passes with stride
+// >= 8 run the in-block index fastest across threads, the others the butterfly
+// block index, so every quarter warp (8 x 16 bytes) hits 8 distinct bank groups.
 constexpr int kFftThreadsT = 512;
 
 __host__ __device__ constexpr int tfac_count(int n) {
   int c = 0;
-  while (n % 8 == 0) { n /= 8; ++c; }
-  while (n % 4 == 0) { n /= 4; ++c; }
-  while (n % 2 == 0) { n /= 2; ++c; }
   while (n % 3 == 0) { n /= 3; ++c; }
   while (n % 5 == 0) { n /= 5; ++c; }
-  return c;
+  int e = 0;
+  while (n % 8 == 0) { n /= 8; ++e; }
+  if (n == 2 || n == 4) { ++c; n = 1; }
+  return c + e;
 }
 __host__ __device__ constexpr int tfac_at(int n, int i) {
   int c = 0;
-  const int rs[5] = {8, 4, 2, 3, 5};
-  for (int q = 0; q < 5; ++q)
-    while (n % rs[q] == 0) {
-      if (c == i) return rs[q];
-      n /= rs[q];
-      ++c;
-    }
-  return 1;
+  while (n % 3 == 0) { if (c == i) return 3; n /= 3; ++c; }
+  while (n % 5 == 0) { if (c == i) return 5; n /= 5; ++c; }
+  int r = n, e = 0;
+  while (r % 8 == 0) { r /= 8; ++e; }
+  if (r == 2 || r == 4) { if (c == i) return r; ++c; }
+  return 8;
 }
 __host__ __device__ constexpr int tspan_at(int n, int i) {
   int sp = n;
   for (int q = 0; q < i; ++q) sp /= tfac_at(n, q);
   return sp;
 }
-__device__ __forceinline__ int ph(int i) { return i + (i >> 3); }
+__device__ __forceinline__ int sw(int i) { return i ^ ((i >> 3) & 7); }
+
+// twiddles w^q, q = 1..R-1, from two table loads (w^1, w^2)
+template <int R, int SIGN>
+__device__ __forceinline__ void twiddles(const double2* __restrict__ tw, int base, int N, double2* w) {
+  if constexpr (R >= 2) w[1] = twd<SIGN>(tw, base);
+  if constexpr (R >= 3) w[2] = twd<SIGN>(tw, (2 * base) % N);
+  if constexpr (R >= 4) w[3] = cmul(w[1], w[2]);
+  if constexpr (R >= 5) w[4] = cmul(w[2], w[2]);
+  if constexpr (R >= 6) w[5] = cmul(w[4], w[1]);
+  if constexpr (R >= 7) w[6] = cmul(w[4], w[2]);
+  if constexpr (R >= 8) w[7] = cmul(w[4], w[3]);
+}
 
 template <int N, int I>
 __device__ __forceinline__ void tdif(double2* z, int npair, const double2* __restrict__ tw) {
   if constexpr (I < tfac_count(N)) {
     constexpr int R = tfac_at(N, I), span = tspan_at(N, I), s = span / R, nbf = N / R, stw = N / span;
-    constexpr int NP = N + N / 8;
+    constexpr int NB = N / span;  // butterfly blocks
+    constexpr int NP = N + 1;
     for (int it = threadIdx.x; it < npair * nbf; it += blockDim.x) {
       const int pp = it / nbf, rem = it - pp * nbf;
-      const int b = rem / s, j = rem - b * s;
+      int b, j;
+      if constexpr (s >= 8) { b = rem / s; j = rem - b * s; }
+      else { j = rem / NB; b = rem - j * NB; }
       double2* zp = z + pp * NP;
       const int base = b * span + j;
       double2 x[R];
 #pragma unroll
-      for (int r = 0; r < R; ++r) x[r] = zp[ph(base + r * s)];
+      for (int r = 0; r < R; ++r) x[r] = zp[sw(base + r * s)];
       DFT<R, +1>::run(x);
-      zp[ph(base)] = x[0];
+      double2 w[R];
+      twiddles<R, +1>(tw, j * stw, N, w);
+      zp[sw(base)] = x[0];
 #pragma unroll
-      for (int q = 1; q < R; ++q) zp[ph(base + q * s)] = cmul(x[q], twd<+1>(tw, j * q * stw));
+      for (int q = 1; q < R; ++q) zp[sw(base + q * s)] = cmul(x[q], w[q]);
     }
     __syncthreads();
     tdif<N, I + 1>(z, npair, tw);
@@ -517,60 +534,101 @@ template <int N, int I>
 __device__ __forceinline__ void tdit(double2* z, int npair, const double2* __restrict__ tw) {
   if constexpr (I >= 0) {
     constexpr int R = tfac_at(N, I), span = tspan_at(N, I), s = span / R, nbf = N / R, stw = N / span;
-    constexpr int NP = N + N / 8;
+    constexpr int NB = N / span;
+    constexpr int NP = N + 1;
     for (int it = threadIdx.x; it < npair * nbf; it += blockDim.x) {
       const int pp = it / nbf, rem = it - pp * nbf;
-      const int b = rem / s, j = rem - b * s;
+      int b, j;
+      if constexpr (s >= 8) { b = rem / s; j = rem - b * s; }
+      else { j = rem / NB; b = rem - j * NB; }
       double2* zp = z + pp * NP;
       const int base = b * span + j;
+      double2 w[R];
+      twiddles<R, -1>(tw, j * stw, N, w);
       double2 x[R];
-      x[0] = zp[ph(base)];
+      x[0] = zp[sw(base)];
 #pragma unroll
-      for (int q = 1; q < R; ++q) x[q] = cmul(zp[ph(base + q * s)], twd<-1>(tw, j * q * stw));
+      for (int q = 1; q < R; ++q) x[q] = cmul(zp[sw(base + q * s)], w[q]);
       DFT<R, -1>::run(x);
 #pragma unroll
-      for (int r = 0; r < R; ++r) zp[ph(base + r * s)] = x[r];
+      for (int r = 0; r < R; ++r) zp[sw(base + r * s)] = x[r];
     }
     __syncthreads();
     tdit<N, I - 1>(z, npair, tw);
   }
 }
 
-// first DIF pass from the staged spectra
+// staged records of one line: [m][ncs pairs], ncs = nc rounded up to odd
+__device__ __forceinline__ int ncs_of(int nc) { return nc | 1; }
+
+__device__ void prefetch_line_t(double* st, const double* rtm, int nc, const Plan& P, int th, int r) {
+  const long long strideM = (long long)P.nth * P.nr * nc * 2;
+  const double* base = rtm + ((long long)th * P.nr + r) * nc * 2;
+  const int ncs = ncs_of(nc);
+  const int n = (P.L + 1) * nc;
+  for (int it = threadIdx.x; it < n; it += blockDim.x) {
+    const int m = it / nc, c = it - m * nc;
+    cp_async16(st + (m * ncs + c) * 2, base + m * strideM + c * 2);
+  }
+  cp_async_commit();
+}
+
+__device__ __forceinline__ double2 spec_at_t(const double* st, int nc, int nv, int pp, int k, int N, int L) {
+  int m;
+  bool mirror;
+  if (k <= L) { m = k; mirror = false; }
+  else if (k >= N - L) { m = N - k; mirror = true; }
+  else return make_double2(0.0, 0.0);
+  const double* rec = st + m * ncs_of(nc) * 2;
+  const double* r0 = rec + rec_off(2 * pp, nv);
+  const double a0 = r0[0], b0 = r0[1];
+  double a1 = 0.0, b1 = 0.0;
+  if (2 * pp + 1 < nc) {
+    const double* r1 = rec + rec_off(2 * pp + 1, nv);
+    a1 = r1[0];
+    b1 = r1[1];
+  }
+  if (m == 0) return make_double2(a0, a1);
+  return mirror ? make_double2(0.5 * a0 - 0.5 * b1, 0.5 * b0 + 0.5 * a1)
+                : make_double2(0.5 * a0 + 0.5 * b1, 0.5 * a1 - 0.5 * b0);
+}
+
 template <int N>
 __device__ __forceinline__ void tdif_first(const double* st, int nc, int nv, double2* z, int npair, int L,
                                            const double2* __restrict__ tw) {
   constexpr int R = tfac_at(N, 0), s = N / R, nbf = N / R;
-  constexpr int NP = N + N / 8;
+  constexpr int NP = N + 1;
   for (int it = threadIdx.x; it < npair * nbf; it += blockDim.x) {
     const int pp = it / nbf, j = it - pp * nbf;
     double2 x[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) x[r] = spec_at(st, nc, nv, pp, j + r * s, N, L);
+    for (int r = 0; r < R; ++r) x[r] = spec_at_t(st, nc, nv, pp, j + r * s, N, L);
     DFT<R, +1>::run(x);
+    double2 w[R];
+    twiddles<R, +1>(tw, j, N, w);
     double2* zp = z + pp * NP;
-    zp[ph(j)] = x[0];
+    zp[sw(j)] = x[0];
 #pragma unroll
-    for (int q = 1; q < R; ++q) zp[ph(j + q * s)] = cmul(x[q], twd<+1>(tw, j * q));
+    for (int q = 1; q < R; ++q) zp[sw(j + q * s)] = cmul(x[q], w[q]);
   }
 }
 
 template <int N>
 __device__ void tstore_line(const double2* z, int npair, const Plan& P, double* rtm, int nc, int nv, int th, int r) {
-  constexpr int NP = N + N / 8;
+  constexpr int NP = N + 1;
   const int L = P.L;
   const double aN = 1.0 / (double)N;
   const long long strideM = (long long)P.nth * P.nr * nc * 2;
   double* base = rtm + ((long long)th * P.nr + r) * nc * 2;
   for (int it = threadIdx.x; it < (L + 1) * npair; it += blockDim.x) {
-    const int m = it / npair, pp = it - m * npair;
+    const int pp = it / (L + 1), m = it - pp * (L + 1);
     const double2* zp = z + pp * NP;
-    const double2 zm = zp[ph(m)];
+    const double2 zm = zp[sw(m)];
     double a0, b0, a1, b1;
     if (m == 0) {
       a0 = zm.x * aN; a1 = zm.y * aN; b0 = 0.0; b1 = 0.0;
     } else {
-      const double2 wm = zp[ph(N - m)];
+      const double2 wm = zp[sw(N - m)];
       a0 = (zm.x + wm.x) * aN;
       b0 = (wm.y - zm.y) * aN;
       a1 = (zm.y + wm.y) * aN;
@@ -582,14 +640,13 @@ __device__ void tstore_line(const double2* z, int npair, const Plan& P, double* 
   }
 }
 
-// products on the padded layout (same code as products(), addressing through ph)
 template <int N, int MVB, int MSB, int MVF, int MSF>
 __device__ void tproducts(double2* z, const Plan& P) {
-  constexpr int NP = N + N / 8;
+  constexpr int NP = N + 1;
   constexpr int MCF = 3 * MVF + MSF;
   const int nvb = P.nvb, nsb = P.nsb, nvf = P.nvf, nsf = P.nsf;
   for (int pos = threadIdx.x; pos < N; pos += blockDim.x) {
-    const int pq = ph(pos);
+    const int pq = sw(pos);
     double vin[3 * MVB > 0 ? 3 * MVB : 1], sin_[MSB > 0 ? MSB : 1];
 #pragma unroll
     for (int c = 0; c < 3 * MVB; ++c)
@@ -669,14 +726,14 @@ __device__ void tproducts(double2* z, const Plan& P) {
 template <int N, int MVB, int MSB, int MVF, int MSF>
 __global__ void __launch_bounds__(kFftThreadsT, 1) k_fft_cycle_t(Plan P, int nlines) {
   extern __shared__ double4 smraw[];
-  constexpr int NP = N + N / 8;
+  constexpr int NP = N + 1;
   const int npb = (P.ncb + 1) / 2, npf = (P.ncf + 1) / 2;
   const int npair = npb > npf ? npb : npf;
   double2* z = reinterpret_cast<double2*>(smraw);
-  double* st = reinterpret_cast<double*>(z + npair * NP);
+  double* st = reinterpret_cast<double*>(z + npair * NP + 1);  // keep 16-byte alignment
   int line = blockIdx.x;
   if (line >= nlines) return;
-  prefetch_line(st, P.rtm_b, P.ncb, P, line / P.nr, line % P.nr);
+  prefetch_line_t(st, P.rtm_b, P.ncb, P, line / P.nr, line % P.nr);
   while (line < nlines) {
     const int r = line % P.nr, th = line / P.nr;
     cp_async_wait<0>();
@@ -684,7 +741,7 @@ __global__ void __launch_bounds__(kFftThreadsT, 1) k_fft_cycle_t(Plan P, int nli
     tdif_first<N>(st, P.ncb, P.nvb, z, npb, P.L, P.twid);
     __syncthreads();
     const int next = line + gridDim.x;
-    if (next < nlines) prefetch_line(st, P.rtm_b, P.ncb, P, next / P.nr, next % P.nr);
+    if (next < nlines) prefetch_line_t(st, P.rtm_b, P.ncb, P, next / P.nr, next % P.nr);
     tdif<N, 1>(z, npb, P.twid);
     tproducts<N, MVB, MSB, MVF, MSF>(z, P);
     __syncthreads();
@@ -697,7 +754,7 @@ __global__ void __launch_bounds__(kFftThreadsT, 1) k_fft_cycle_t(Plan P, int nli
 
 size_t smem_cycle_t(const Plan& p) {
   const int npair = ((p.ncb > p.ncf ? p.ncb : p.ncf) + 1) / 2;
-  return sizeof(double2) * (size_t)npair * (p.nph + p.nph / 8) + sizeof(double) * 2 * (size_t)(p.L + 1) * p.ncb;
+  return sizeof(double2) * ((size_t)npair * (p.nph + 1) + 1) + sizeof(double) * 2 * (size_t)(p.L + 1) * (p.ncb | 1);
 }
 
 template <int N, int MVB, int MSB, int MVF, int MSF>
@@ -772,8 +829,18 @@ cudaError_t launch_fft_cycle(const Plan& p, cudaStream_t s) {
     if (handled) return e;
     return run_cycle<3, 1, 3, 1>(p, s);
   }
-  if (p.nvb == 2 && p.nsb == 1 && p.nvf == 2 && p.nsf == 1) return run_cycle<2, 1, 2, 1>(p, s);
-  if (p.nvb == 1 && p.nsb == 1 && p.nvf == 1 && p.nsf == 0) return run_cycle<1, 1, 1, 0>(p, s);
+  if (p.nvb == 2 && p.nsb == 1 && p.nvf == 2 && p.nsf == 1) {
+    bool handled = false;
+    const cudaError_t e = run_cycle_n<2, 1, 2, 1>(p, s, &handled);
+    if (handled) return e;
+    return run_cycle<2, 1, 2, 1>(p, s);
+  }
+  if (p.nvb == 1 && p.nsb == 1 && p.nvf == 1 && p.nsf == 0) {
+    bool handled = false;
+    const cudaError_t e = run_cycle_n<1, 1, 1, 0>(p, s, &handled);
+    if (handled) return e;
+    return run_cycle<1, 1, 1, 0>(p, s);
+  }
   return run_cycle<kMaxVec, kMaxScl, kMaxVec, kMaxScl>(p, s);
 }
 
