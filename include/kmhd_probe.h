@@ -23,6 +23,14 @@ int kmhd_selftest_i8_mma(int lbo, int sbo, const signed char *A, const signed ch
  * instructions. */
 int kmhd_probe_i8_mma(int device, int n, int iters, int group, double *tops);
 
+/* As kmhd_selftest_i8_mma for a 128B-swizzled K-major layout:
+ * D(128x64) = A(128x128) * B(64x128)^T, int8 row-major host inputs. */
+int kmhd_selftest_i8_mma_sw128(const signed char *A, const signed char *B, int *D);
+
+/* INT8 tensor-pipe rate for operand layout 0 (no swizzle, 8x16-byte core
+ * matrices) or 1 (128-byte swizzle), N = n, cycling nacc accumulators. */
+int kmhd_probe_i8_mma2(int device, int layout, int n, int nacc, int iters, double *tops);
+
 #ifdef __cplusplus
 }
 #endif

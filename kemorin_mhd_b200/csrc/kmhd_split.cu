@@ -121,6 +121,12 @@ __device__ __forceinline__ void digits(double v, int ns, signed char* d) {
   d[0] = (signed char)x;
 }
 
+// 2^e as a double, e in the normal range
+__device__ __forceinline__ double pow2(int e) {
+  if (e < -1022 || e > 1023) return ldexp(1.0, e);
+  return __longlong_as_double((long long)(e + 1023) << 52);
+}
+
 // frexp-style exponent: smallest e with |x| < 2^e (x > 0)
 __device__ __forceinline__ int exp_above(double x) {
   int e;
@@ -283,85 +289,143 @@ __device__ __forceinline__ ColRef colref_fwd(const Plan& P, const SliceTabs& S, 
   return c;
 }
 
-// backward staged inputs: sm_in[(slot * nc + comp) * Kall + (l - m)]
-__device__ __forceinline__ double bval_staged(const Plan& P, const double* in, int Kall, const ColRef& c, int m,
-                                              int k, double ar) {
+// A column resolved once: for each of the (at most two) concatenated K parts,
+// the staged row / record offset, parity, sign and flags.
+struct ColPar {
+  int kpart0, kpad;
+  int K0, K1;        // valid K per part
+  int par0, par1;    // parity of l - m per part (backward)
+  int off0, off1;    // backward: staged row * Kall; forward: record offset (comp pair + slot)
+  double sgn0, sgn1;
+  bool sym0, sym1;   // forward: (N + S) (true) or (N - S)
+  bool ovs0, ovs1;   // forward: times 1/sin(theta)
+  int kind;        // 0 theta/phi or F2 (two parts), 1 r vector (g3/r^2), 2 scalar, 3 zero
+};
+
+__device__ inline ColPar colpar_bwd(const Plan& P, const ColRef& c, int m, int Kall) {
+  ColPar cp;
   const TypeGeo g = type_geo(c.t, P.L, m, P.nh);
   const int Ke = kcount(P.L, m, 0), Ko = kcount(P.L, m, 1);
   const int nc = P.ncb;
+  cp.kpart0 = g.kpart0;
+  cp.kpad = g.kpad;
+  cp.sym0 = cp.sym1 = true;
+  cp.ovs0 = cp.ovs1 = false;
   if (c.t <= 1) {
-    const bool first = k < g.kpart0;
-    const int kk = first ? k : k - g.kpart0;
-    const int par = (c.t == 0) ? (first ? 1 : 0) : (first ? 0 : 1);
-    if (kk >= (par ? Ko : Ke)) return 0.0;
-    const int lo = 2 * kk + par;  // l - m
-    int slot, comp;
-    double sg = 1.0;
-    if (first) {
-      comp = (c.q < 2) ? 1 : 2;
-      slot = c.q & 1;
-      if (c.q >= 2) sg = -1.0;
-    } else {
-      switch (c.q) {
-        case 0: comp = 2; slot = 1; break;
-        case 1: comp = 2; slot = 0; sg = -1.0; break;
-        case 2: comp = 1; slot = 1; break;
-        default: comp = 1; slot = 0; sg = -1.0; break;
+    cp.kind = 0;
+    for (int part = 0; part < 2; ++part) {
+      const bool first = part == 0;
+      const int par = (c.t == 0) ? (first ? 1 : 0) : (first ? 0 : 1);
+      int slot, comp;
+      double sg = 1.0;
+      if (first) {
+        comp = (c.q < 2) ? 1 : 2;
+        slot = c.q & 1;
+        if (c.q >= 2) sg = -1.0;
+      } else {
+        switch (c.q) {
+          case 0: comp = 2; slot = 1; break;
+          case 1: comp = 2; slot = 0; sg = -1.0; break;
+          case 2: comp = 1; slot = 1; break;
+          default: comp = 1; slot = 0; sg = -1.0; break;
+        }
       }
+      (part ? cp.par1 : cp.par0) = par;
+      (part ? cp.K1 : cp.K0) = par ? Ko : Ke;
+      (part ? cp.off1 : cp.off0) = (slot * nc + 3 * c.f + comp) * Kall;
+      (part ? cp.sgn1 : cp.sgn0) = sg;
     }
-    return sg * (in[(slot * nc + 3 * c.f + comp) * Kall + lo] * ar);
+  } else {
+    const int par = c.t - 2;
+    cp.par0 = cp.par1 = par;
+    cp.K0 = cp.K1 = par ? Ko : Ke;
+    cp.sgn0 = cp.sgn1 = 1.0;
+    cp.kpart0 = g.kpad;  // single part
+    if (c.f < P.nvb) {
+      cp.kind = 1;
+      cp.off0 = cp.off1 = (c.q * nc + 3 * c.f) * Kall;
+    } else if (c.f < P.nvb + P.nsb) {
+      cp.kind = 2;
+      cp.off0 = cp.off1 = (c.q * nc + 3 * P.nvb + (c.f - P.nvb)) * Kall;
+    } else {
+      cp.kind = 3;
+      cp.off0 = cp.off1 = 0;
+    }
   }
-  const int par = c.t - 2;
-  if (k >= (par ? Ko : Ke) || c.f >= P.nvb + P.nsb) return 0.0;
-  const int lo = 2 * k + par;
-  if (c.f < P.nvb) return in[(c.q * nc + 3 * c.f) * Kall + lo] * (ar * ar) * g3_of(m + lo);
-  return in[(c.q * nc + 3 * P.nvb + (c.f - P.nvb)) * Kall + lo];
+  return cp;
 }
 
-// forward staged inputs: sm_in[th * rec + rec_off(comp) + slot] (rec = 2 ncf), full theta range
-__device__ __forceinline__ double fval_staged(const Plan& P, const double* in, const ColRef& c, int m, int k) {
+__device__ __forceinline__ double bval(const ColPar& cp, const double* in, int m, int k, double ar) {
+  if (cp.kind == 3) return 0.0;
+  const int part = k >= cp.kpart0 ? 1 : 0;
+  const int kk = k - (part ? cp.kpart0 : 0);
+  if (kk >= (part ? cp.K1 : cp.K0)) return 0.0;
+  const int lo = 2 * kk + (part ? cp.par1 : cp.par0);
+  const double x = in[(part ? cp.off1 : cp.off0) + lo];
+  if (cp.kind == 0) return (part ? cp.sgn1 : cp.sgn0) * (x * ar);
+  if (cp.kind == 1) return x * (ar * ar) * g3_of(m + lo);
+  return x;
+}
+
+__device__ inline ColPar colpar_fwd(const Plan& P, const ColRef& c, int m) {
+  ColPar cp;
   const TypeGeo g = type_geo(c.t, P.L, m, P.nh);
-  const int rec = 2 * P.ncf;
   const int par = (c.t == 4 || c.t == 6) ? 0 : 1;
-  auto sy = [&](int th, int comp, int slot, bool want_sym, bool overs) -> double {
-    const int ro = rec_off(comp, P.nvf) + slot;
-    const double wp = P.weight[th];
-    const double nv = in[th * rec + ro];
-    double v;
-    if (th < P.nth / 2) {
-      const double sv = in[(P.nth - 1 - th) * rec + ro];
-      v = want_sym ? (nv + sv) * wp : (nv - sv) * wp;
-    } else {
-      v = want_sym ? nv * wp : 0.0;
-    }
-    return overs ? v * P.asin_t[th] : v;
-  };
+  cp.kpart0 = g.kpart0;
+  cp.kpad = g.kpad;
+  cp.par0 = cp.par1 = par;
+  cp.K0 = cp.K1 = P.nh;
+  cp.ovs0 = cp.ovs1 = false;
   if (c.t <= 5) {
-    if (c.f >= P.nvf + P.nsf || k >= P.nh) return 0.0;
-    if (c.q == 1 && m == 0) return 0.0;
+    cp.kind = (c.f >= P.nvf + P.nsf || (c.q == 1 && m == 0)) ? 3 : 2;
     const int comp = c.f < P.nvf ? 3 * c.f : 3 * P.nvf + (c.f - P.nvf);
-    return sy(k, comp, c.q, par == 0, false);
+    cp.off0 = cp.off1 = cp.kind == 3 ? 0 : rec_off(comp, P.nvf) + c.q;
+    cp.sym0 = cp.sym1 = (par == 0);
+    cp.sgn0 = cp.sgn1 = 1.0;
+    cp.kpart0 = g.kpad;
+    return cp;
   }
-  const bool first = k < g.kpart0;
-  const int th = first ? k : k - g.kpart0;
-  if (th >= P.nh) return 0.0;
-  if (m == 0 && !first) return 0.0;
+  cp.kind = 0;
   const bool dP_sym = (par == 1), P_sym = (par == 0);
   const int v = c.f;
-  if (first) {
-    switch (c.q) {
-      case 0: return sy(th, 3 * v + 1, 0, dP_sym, false);
-      case 1: return sy(th, 3 * v + 1, 1, dP_sym, false);
-      case 2: return -sy(th, 3 * v + 2, 0, dP_sym, false);
-      default: return -sy(th, 3 * v + 2, 1, dP_sym, false);
-    }
-  }
+  // first part (dP columns) and second part (m P columns), see the A types 6/7
+  int comp0, slot0, comp1, slot1;
+  double s0, s1;
   switch (c.q) {
-    case 0: return -sy(th, 3 * v + 2, 1, P_sym, true);
-    case 1: return sy(th, 3 * v + 2, 0, P_sym, true);
-    case 2: return -sy(th, 3 * v + 1, 1, P_sym, true);
-    default: return sy(th, 3 * v + 1, 0, P_sym, true);
+    case 0: comp0 = 3 * v + 1; slot0 = 0; s0 = 1.0; comp1 = 3 * v + 2; slot1 = 1; s1 = -1.0; break;
+    case 1: comp0 = 3 * v + 1; slot0 = 1; s0 = 1.0; comp1 = 3 * v + 2; slot1 = 0; s1 = 1.0; break;
+    case 2: comp0 = 3 * v + 2; slot0 = 0; s0 = -1.0; comp1 = 3 * v + 1; slot1 = 1; s1 = -1.0; break;
+    default: comp0 = 3 * v + 2; slot0 = 1; s0 = -1.0; comp1 = 3 * v + 1; slot1 = 0; s1 = 1.0; break;
   }
+  cp.off0 = rec_off(comp0, P.nvf) + slot0;
+  cp.off1 = rec_off(comp1, P.nvf) + slot1;
+  cp.sgn0 = s0;
+  cp.sgn1 = s1;
+  cp.sym0 = dP_sym;
+  cp.sym1 = P_sym;
+  cp.ovs1 = true;
+  if (m == 0) cp.K1 = 0;
+  return cp;
+}
+
+// forward staged value: in = [theta][record], wts = [w, 1/sin] per hemisphere row
+__device__ __forceinline__ double fval(const ColPar& cp, const double* in, const double2* wts, int rec, int nth,
+                                       int k) {
+  if (cp.kind == 3) return 0.0;
+  const int part = k >= cp.kpart0 ? 1 : 0;
+  const int th = k - (part ? cp.kpart0 : 0);
+  if (th >= (part ? cp.K1 : cp.K0)) return 0.0;
+  const double2 wa = wts[th];
+  const double nv = in[th * rec + (part ? cp.off1 : cp.off0)];
+  double v;
+  if (th < nth / 2) {
+    const double sv = in[(nth - 1 - th) * rec + (part ? cp.off1 : cp.off0)];
+    v = (part ? cp.sym1 : cp.sym0) ? (nv + sv) * wa.x : (nv - sv) * wa.x;
+  } else {
+    v = (part ? cp.sym1 : cp.sym0) ? nv * wa.x : 0.0;
+  }
+  if ((part ? cp.ovs1 : cp.ovs0)) v = v * wa.y;
+  return (part ? cp.sgn1 : cp.sgn0) * v;
 }
 
 template <int NS>
@@ -391,7 +455,9 @@ __global__ void __launch_bounds__(256) k_slice_mr(Plan P, SliceTabs S, const dou
   const int L = P.L;
   const int Kall = L - m + 1;
   const int nc = FWD ? P.ncf : P.ncb;
+  const int rec = 2 * nc;
   // ---- stage inputs
+  double* tail;
   if (!FWD) {
     const int nrow = 2 * nc;
     for (int it = threadIdx.x; it < nrow * Kall; it += blockDim.x) {
@@ -405,8 +471,8 @@ __global__ void __launch_bounds__(256) k_slice_mr(Plan P, SliceTabs S, const dou
       }
       sin_[it] = v;
     }
+    tail = sin_ + 2 * nc * Kall;
   } else {
-    const int rec = 2 * nc;
     const long long strideTh = (long long)P.nr * rec;
     const double* base = P.rtm_f + (long long)m * P.nth * strideTh + (long long)r * rec;
     for (int it = threadIdx.x; it < P.nth * (rec / 2); it += blockDim.x) {
@@ -414,37 +480,42 @@ __global__ void __launch_bounds__(256) k_slice_mr(Plan P, SliceTabs S, const dou
       *reinterpret_cast<double2*>(sin_ + th * rec + 2 * c2) =
           *reinterpret_cast<const double2*>(base + th * strideTh + 2 * c2);
     }
+    double2* wts = reinterpret_cast<double2*>(sin_ + P.nth * rec);
+    for (int th = threadIdx.x; th < P.nh; th += blockDim.x) wts[th] = make_double2(P.weight[th], P.asin_t[th]);
+    tail = sin_ + P.nth * rec + 2 * P.nh;
   }
+  const double2* wts = reinterpret_cast<const double2*>(sin_ + P.nth * rec);
   __syncthreads();
   const int ncol = FWD ? ncols_fwd(P) : ncols_bwd(P);
-  double* colmax = sin_ + (FWD ? P.nth * 2 * nc : 2 * nc * Kall);
+  double* colmax = tail;
   int* colexp = reinterpret_cast<int*>(colmax + kMaxCols);
   const double ar = 1.0 / P.radius[r];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // ---- column maxima of B' = B 2^-dexp
   for (int i = warp; i < ncol; i += blockDim.x >> 5) {
     const ColRef c = FWD ? colref_fwd(P, S, r, i) : colref_bwd(P, S, r, i);
-    const TypeGeo g = type_geo(c.t, L, m, P.nh);
+    const ColPar cp = FWD ? colpar_fwd(P, c, m) : colpar_bwd(P, c, m, Kall);
     const int* dx = S.dexp + S.deoff[m * kNT + c.t];
     double mx = 0.0;
-    for (int k = lane; k < g.kpad; k += 32) {
-      const double x = FWD ? fval_staged(P, sin_, c, m, k) : bval_staged(P, sin_, Kall, c, m, k, ar);
-      mx = fmax(mx, fabs(ldexp(x, -__ldg(dx + k))));
+    for (int k = lane; k < cp.kpad; k += 32) {
+      const double x = FWD ? fval(cp, sin_, wts, rec, P.nth, k) : bval(cp, sin_, m, k, ar);
+      mx = fmax(mx, fabs(x * pow2(-__ldg(dx + k))));
     }
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     if (lane == 0) {
+      const int e = mx > 0.0 ? exp_above(mx) : 0;
       colmax[i] = mx;
-      colexp[i] = mx > 0.0 ? exp_above(mx) : 0;
-      S.bexp[S.beoff[m * kNT + c.t] + c.col] = (mx > 0.0 ? exp_above(mx) : 0) - (8 * NS - 2);
+      colexp[i] = e;
+      S.bexp[S.beoff[m * kNT + c.t] + c.col] = e - (8 * NS - 2);
     }
   }
   __syncthreads();
-  // ---- digits, 16 consecutive k per item
+  // ---- digits, 16 consecutive k per lane, one column per warp
   for (int i = warp; i < ncol; i += blockDim.x >> 5) {
     const ColRef c = FWD ? colref_fwd(P, S, r, i) : colref_bwd(P, S, r, i);
-    const TypeGeo g = type_geo(c.t, L, m, P.nh);
-    const int n16 = g.kpad / 16;
-    const int nkc = g.kpad / kTK;
+    const ColPar cp = FWD ? colpar_fwd(P, c, m) : colpar_bwd(P, c, m, Kall);
+    const int n16 = cp.kpad / 16;
+    const int nkc = cp.kpad / kTK;
     const bool nz = colmax[i] > 0.0;
     const int sh = (8 * NS - 2) - colexp[i];
     const int* dx = S.dexp + S.deoff[m * kNT + c.t];
@@ -455,8 +526,8 @@ __global__ void __launch_bounds__(256) k_slice_mr(Plan P, SliceTabs S, const dou
 #pragma unroll
       for (int q = 0; q < 16; ++q) {
         const int k = kb * 16 + q;
-        const double x = FWD ? fval_staged(P, sin_, c, m, k) : bval_staged(P, sin_, Kall, c, m, k, ar);
-        v16[q] = nz ? ldexp(x, sh - __ldg(dx + k)) : 0.0;
+        const double x = FWD ? fval(cp, sin_, wts, rec, P.nth, k) : bval(cp, sin_, m, k, ar);
+        v16[q] = nz ? x * pow2(sh - __ldg(dx + k)) : 0.0;
       }
       uint32_t w[NS][4];
       digits_pack16<NS>(v16, w);
@@ -511,12 +582,6 @@ __device__ __forceinline__ unsigned make_idesc() {
 __device__ __forceinline__ double i2d(int x) {
   return __hiloint2double(0x43300000, (unsigned)x ^ 0x80000000u) - 4503601774854144.0;
 }
-// 2^e as a double, e in the normal range
-__device__ __forceinline__ double pow2(int e) {
-  if (e < -1022 || e > 1023) return ldexp(1.0, e);
-  return __longlong_as_double((long long)(e + 1023) << 52);
-}
-
 __device__ __forceinline__ unsigned mapa(const void* p, unsigned rank) {
   unsigned a;
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(a) : "r"(sptr(p)), "r"(rank));
@@ -632,8 +697,9 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
           const int st = (int)(gc % kRing);
           if (!mbar_wait(&full[st], (unsigned)((gc / kRing) & 1))) { ok = false; break; }
           tc_fence_after();
-          const unsigned char* As = sm + st * STAGE;
-          const unsigned char* Bs = As + A_BYTES;
+          // descriptors of slice 0; slice s starts s tiles further (start address field, 16-byte units)
+          const uint64_t a0 = smem_desc(sm + st * STAGE, 128, 256);
+          const uint64_t b0 = smem_desc(sm + st * STAGE + A_BYTES, 128, 256);
 #pragma unroll
           for (int a = 0; a < NS; ++a) {
 #pragma unroll
@@ -643,8 +709,8 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
               // the first product of group grp (smallest a) overwrites, the rest accumulate
               const unsigned first_a = (grp < NS) ? 0 : grp - (NS - 1);
               const unsigned acc = (kc > 0 || (unsigned)a > first_a) ? 1u : 0u;
-              mma_i8(tmem + (unsigned)(grp * kTN), smem_desc(As + a * (kTM * kTK), 128, 256),
-                     smem_desc(Bs + b * (kTN * kTK), 128, 256), idesc, acc);
+              mma_i8(tmem + (unsigned)(grp * kTN), a0 + (uint64_t)(a * (kTM * kTK / 16)),
+                     b0 + (uint64_t)(b * (kTN * kTK / 16)), idesc, acc);
             }
           }
           mma_commit(&empty[st]);
@@ -1009,7 +1075,7 @@ int split_bwd(SplitState* s, const Plan& p, int, const double* d_rj, long long l
 int split_fwd(SplitState* s, const Plan& p, double* d_rj, long long ld, const int* cols, cudaStream_t st) {
   const SliceTabs& S = s->S;
   {
-    const size_t smem = sizeof(double) * (2 * (size_t)p.ncf * p.nth + kMaxCols) + kMaxCols * sizeof(int);
+    const size_t smem = sizeof(double) * (2 * (size_t)p.ncf * p.nth + 2 * (size_t)p.nh + kMaxCols) + kMaxCols * sizeof(int);
     auto kern = s->ns == 6 ? k_slice_mr<true, 6> : k_slice_mr<true, 4>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
       return KMHD_ERR_CUDA;
@@ -1193,5 +1259,161 @@ extern "C" int kmhd_probe_i8_mma(int device, int n, int iters, int group, double
   if (ce != cudaSuccess) return KMHD_ERR_CUDA;
   if (h) return h;
   *tops = 2.0 * kTM * n * kTK * (double)iters * nsm / (ms * 1e-3) / 1e12;
+  return KMHD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Layout study: SWIZZLE_128B K-major operands (128-byte rows, 16-byte chunk c
+// of row r stored at chunk c ^ (r & 7), 8-row atoms of 1024 bytes), k-steps of
+// 32 int8 advance the descriptor start address by 32 bytes.
+namespace kmhd {
+namespace {
+__host__ __device__ __forceinline__ int sw128_off(int row, int k) {
+  return row * 128 + ((((k >> 4) & 7) ^ (row & 7)) << 4) + (k & 15);
+}
+__device__ __forceinline__ uint64_t smem_desc_sw128(const void* p) {
+  const uint64_t a = (sptr(p) >> 4) & 0x3FFF;
+  return a | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) | (2ull << 61);
+}
+
+// D(128 x 64) = A(128 x 128) B(64 x 128)^T with SWIZZLE_128B tiles (4 k-steps)
+__global__ void __launch_bounds__(128, 1) k_selftest_mma_sw(const signed char* A, const signed char* B, int* D, int* err) {
+  __shared__ __align__(1024) unsigned char sa[128 * 128];
+  __shared__ __align__(1024) unsigned char sb[64 * 128];
+  __shared__ unsigned long long bar;
+  __shared__ unsigned slot;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int i = tid; i < 128 * 128; i += blockDim.x) sa[sw128_off(i / 128, i % 128)] = (unsigned char)A[i];
+  for (int i = tid; i < 64 * 128; i += blockDim.x) sb[sw128_off(i / 128, i % 128)] = (unsigned char)B[i];
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  if (tid == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;\n" ::"r"(sptr(&slot)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const unsigned tmem = slot;
+  if (tid == 0) {
+    const unsigned idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(64 >> 3) << 17) | ((unsigned)(128 >> 4) << 24);
+    const uint64_t ad = smem_desc_sw128(sa), bd = smem_desc_sw128(sb);
+    for (int ks = 0; ks < 4; ++ks) mma_i8(tmem, ad + (uint64_t)(ks * 2), bd + (uint64_t)(ks * 2), idesc, ks > 0 ? 1u : 0u);
+    mma_commit(&bar);
+  }
+  __syncwarp();
+  if (!mbar_wait(&bar, 0)) atomicExch(err, KMHD_ERR_TIMEOUT);
+  tc_fence_after();
+  for (int cb = 0; cb < 4; ++cb) {
+    int v[16];
+    tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)(cb * 16), v);
+    tmem_wait_ld();
+    for (int c = 0; c < 16; ++c) D[(warp * 32 + lane) * 64 + cb * 16 + c] = v[c];
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;\n" ::"r"(tmem));
+}
+
+// rate probe: layout 0 = SWIZZLE_NONE core matrices, 1 = SWIZZLE_128B; nacc accumulators cycled
+__global__ void __launch_bounds__(128, 1) k_probe_mma2(int layout, int n, int nacc, int iters, int* err) {
+  extern __shared__ __align__(1024) unsigned char smp[];
+  unsigned char* sa = smp;                 // 16 KB
+  unsigned char* sb = smp + 128 * 128;     // up to 32 KB
+  __shared__ unsigned long long bar;
+  __shared__ unsigned slot;
+  for (int i = threadIdx.x; i < (128 + 256) * 128; i += blockDim.x) smp[i] = (unsigned char)(i * 7);
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (threadIdx.x < 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;\n" ::"r"(sptr(&slot)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const unsigned tmem = slot;
+  if (threadIdx.x == 0) {
+    const unsigned idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(n >> 3) << 17) | ((unsigned)(128 >> 4) << 24);
+    const uint64_t ad = layout ? smem_desc_sw128(sa) : smem_desc(sa, 128, 256);
+    const uint64_t bd = layout ? smem_desc_sw128(sb) : smem_desc(sb, 128, 256);
+    for (int it = 0; it < iters; ++it) {
+      const int ks = it & 3;
+      const uint64_t koff = layout ? (uint64_t)(ks * 2) : 0;
+      mma_i8(tmem + (unsigned)((it % nacc) * n), ad + koff, bd + koff, idesc, it >= nacc ? 1u : 0u);
+    }
+    mma_commit(&bar);
+    if (!mbar_wait(&bar, 0)) atomicExch(err, KMHD_ERR_TIMEOUT);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (threadIdx.x < 32) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;\n" ::"r"(tmem));
+}
+}  // namespace
+}  // namespace kmhd
+
+extern "C" int kmhd_selftest_i8_mma_sw128(const signed char* A, const signed char* B, int* D) {
+  using namespace kmhd;
+  signed char *dA = nullptr, *dB = nullptr;
+  int *dD = nullptr, *err = nullptr;
+  int st = KMHD_OK;
+  if (cudaMalloc(&dA, 128 * 128) || cudaMalloc(&dB, 64 * 128) || cudaMalloc(&dD, sizeof(int) * 128 * 64) ||
+      cudaMalloc(&err, sizeof(int)))
+    st = KMHD_ERR_NOMEM;
+  if (!st) {
+    cudaMemcpy(dA, A, 128 * 128, cudaMemcpyHostToDevice);
+    cudaMemcpy(dB, B, 64 * 128, cudaMemcpyHostToDevice);
+    cudaMemset(err, 0, sizeof(int));
+    k_selftest_mma_sw<<<1, 128>>>(dA, dB, dD, err);
+    int h = 0;
+    if (cudaDeviceSynchronize() != cudaSuccess) st = KMHD_ERR_CUDA;
+    else {
+      cudaMemcpy(D, dD, sizeof(int) * 128 * 64, cudaMemcpyDeviceToHost);
+      cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost);
+      st = h;
+    }
+  }
+  cudaFree(dA);
+  cudaFree(dB);
+  cudaFree(dD);
+  cudaFree(err);
+  return st;
+}
+
+extern "C" int kmhd_probe_i8_mma2(int device, int layout, int n, int nacc, int iters, double* tops) {
+  using namespace kmhd;
+  if (!tops || n < 16 || n > 256 || n % 16 || nacc < 1 || nacc * n > 512) return KMHD_ERR_ARG;
+  if (cudaSetDevice(device) != cudaSuccess) return KMHD_ERR_DEVICE;
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  int* err = nullptr;
+  if (cudaMalloc(&err, sizeof(int)) != cudaSuccess) return KMHD_ERR_NOMEM;
+  cudaMemset(err, 0, sizeof(int));
+  const int smem = (128 + 256) * 128 + 1024;
+  cudaFuncSetAttribute(k_probe_mma2, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  k_probe_mma2<<<nsm, 128, smem>>>(layout, n, nacc, 64, err);
+  cudaEventRecord(e0);
+  k_probe_mma2<<<nsm, 128, smem>>>(layout, n, nacc, iters, err);
+  cudaEventRecord(e1);
+  cudaError_t ce = cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  int h = 0;
+  cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(err);
+  if (ce != cudaSuccess) return KMHD_ERR_CUDA;
+  if (h) return h;
+  *tops = 2.0 * 128 * n * 32 * (double)iters * nsm / (ms * 1e-3) / 1e12;
   return KMHD_OK;
 }
