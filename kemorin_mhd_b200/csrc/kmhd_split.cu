@@ -248,22 +248,16 @@ __global__ void k_a_slices(Plan P, SliceTabs S, int t) {
 }
 
 // ---------------------------------------------------------------------------
-// Slicers, staged per (m, radius): every input value of that radius and order is
-// read once from HBM into shared memory; all derived columns of the four
-// operand types are then formed, scaled and digitised from there.
-//
-// Column list of one (m, r): backward: for each vector v: types 0/1 quantity q
-// (8 columns), for each field f < 4: types 2/3 slots (4 columns); forward: types
-// 4/5 (field f, slot) and types 6/7 (vector v, quantity q).
-constexpr int kMaxCols = 64;  // derived columns per (m, r): at most 48 with 4 fields
+// Slicers.  Column list of one (m, r): backward: for each vector v: types 0/1
+// quantity q (8 columns), for each field f < 4: types 2/3 slots (4 columns);
+// forward: types 4/5 (field f, slot) and types 6/7 (vector v, quantity q).
+constexpr int kGrpCols = 16;  // derived columns of one slicer field group (at most 4 fields x 2 slots x 2 types)
+constexpr int kSlab = 288;    // per-slice staging bytes of one 256-byte tile block (k halves 144 apart)
 
 struct ColRef {
   int t, col;     // operand type and global column index
   int f, q;       // field (vector or scalar slot) and quantity/slot selector
 };
-
-__device__ __forceinline__ int ncols_bwd(const Plan& P) { return 8 * P.nvb + 4 * (P.nvb + P.nsb); }
-__device__ __forceinline__ int ncols_fwd(const Plan& P) { return 4 * (P.nvf + P.nsf) + 8 * P.nvf; }
 
 __device__ __forceinline__ ColRef colref_bwd(const Plan& P, const SliceTabs& S, int r, int i) {
   ColRef c;
@@ -289,255 +283,252 @@ __device__ __forceinline__ ColRef colref_fwd(const Plan& P, const SliceTabs& S, 
   return c;
 }
 
-// A column resolved once: for each of the (at most two) concatenated K parts,
-// the staged row / record offset, parity, sign and flags.
-struct ColPar {
-  int kpart0, kpad;
-  int K0, K1;        // valid K per part
-  int par0, par1;    // parity of l - m per part (backward)
-  int off0, off1;    // backward: staged row * Kall; forward: record offset (comp pair + slot)
-  double sgn0, sgn1;
-  bool sym0, sym1;   // forward: (N + S) (true) or (N - S)
-  bool ovs0, ovs1;   // forward: times 1/sin(theta)
-  int kind;        // 0 theta/phi or F2 (two parts), 1 r vector (g3/r^2), 2 scalar, 3 zero
-};
-
-__device__ inline ColPar colpar_bwd(const Plan& P, const ColRef& c, int m, int Kall) {
-  ColPar cp;
-  const TypeGeo g = type_geo(c.t, P.L, m, P.nh);
-  const int Ke = kcount(P.L, m, 0), Ko = kcount(P.L, m, 1);
-  const int nc = P.ncb;
-  cp.kpart0 = g.kpart0;
-  cp.kpad = g.kpad;
-  cp.sym0 = cp.sym1 = true;
-  cp.ovs0 = cp.ovs1 = false;
-  if (c.t <= 1) {
-    cp.kind = 0;
-    for (int part = 0; part < 2; ++part) {
-      const bool first = part == 0;
-      const int par = (c.t == 0) ? (first ? 1 : 0) : (first ? 0 : 1);
-      int slot, comp;
-      double sg = 1.0;
-      if (first) {
-        comp = (c.q < 2) ? 1 : 2;
-        slot = c.q & 1;
-        if (c.q >= 2) sg = -1.0;
-      } else {
-        switch (c.q) {
-          case 0: comp = 2; slot = 1; break;
-          case 1: comp = 2; slot = 0; sg = -1.0; break;
-          case 2: comp = 1; slot = 1; break;
-          default: comp = 1; slot = 0; sg = -1.0; break;
-        }
-      }
-      (part ? cp.par1 : cp.par0) = par;
-      (part ? cp.K1 : cp.K0) = par ? Ko : Ke;
-      (part ? cp.off1 : cp.off0) = (slot * nc + 3 * c.f + comp) * Kall;
-      (part ? cp.sgn1 : cp.sgn0) = sg;
-    }
-  } else {
-    const int par = c.t - 2;
-    cp.par0 = cp.par1 = par;
-    cp.K0 = cp.K1 = par ? Ko : Ke;
-    cp.sgn0 = cp.sgn1 = 1.0;
-    cp.kpart0 = g.kpad;  // single part
-    if (c.f < P.nvb) {
-      cp.kind = 1;
-      cp.off0 = cp.off1 = (c.q * nc + 3 * c.f) * Kall;
-    } else if (c.f < P.nvb + P.nsb) {
-      cp.kind = 2;
-      cp.off0 = cp.off1 = (c.q * nc + 3 * P.nvb + (c.f - P.nvb)) * Kall;
-    } else {
-      cp.kind = 3;
-      cp.off0 = cp.off1 = 0;
-    }
-  }
-  return cp;
-}
-
-__device__ __forceinline__ double bval(const ColPar& cp, const double* in, int m, int k, double ar) {
-  if (cp.kind == 3) return 0.0;
-  const int part = k >= cp.kpart0 ? 1 : 0;
-  const int kk = k - (part ? cp.kpart0 : 0);
-  if (kk >= (part ? cp.K1 : cp.K0)) return 0.0;
-  const int lo = 2 * kk + (part ? cp.par1 : cp.par0);
-  const double x = in[(part ? cp.off1 : cp.off0) + lo];
-  if (cp.kind == 0) return (part ? cp.sgn1 : cp.sgn0) * (x * ar);
-  if (cp.kind == 1) return x * (ar * ar) * g3_of(m + lo);
-  return x;
-}
-
-__device__ inline ColPar colpar_fwd(const Plan& P, const ColRef& c, int m) {
-  ColPar cp;
-  const TypeGeo g = type_geo(c.t, P.L, m, P.nh);
-  const int par = (c.t == 4 || c.t == 6) ? 0 : 1;
-  cp.kpart0 = g.kpart0;
-  cp.kpad = g.kpad;
-  cp.par0 = cp.par1 = par;
-  cp.K0 = cp.K1 = P.nh;
-  cp.ovs0 = cp.ovs1 = false;
-  if (c.t <= 5) {
-    cp.kind = (c.f >= P.nvf + P.nsf || (c.q == 1 && m == 0)) ? 3 : 2;
-    const int comp = c.f < P.nvf ? 3 * c.f : 3 * P.nvf + (c.f - P.nvf);
-    cp.off0 = cp.off1 = cp.kind == 3 ? 0 : rec_off(comp, P.nvf) + c.q;
-    cp.sym0 = cp.sym1 = (par == 0);
-    cp.sgn0 = cp.sgn1 = 1.0;
-    cp.kpart0 = g.kpad;
-    return cp;
-  }
-  cp.kind = 0;
-  const bool dP_sym = (par == 1), P_sym = (par == 0);
-  const int v = c.f;
-  // first part (dP columns) and second part (m P columns), see the A types 6/7
-  int comp0, slot0, comp1, slot1;
-  double s0, s1;
-  switch (c.q) {
-    case 0: comp0 = 3 * v + 1; slot0 = 0; s0 = 1.0; comp1 = 3 * v + 2; slot1 = 1; s1 = -1.0; break;
-    case 1: comp0 = 3 * v + 1; slot0 = 1; s0 = 1.0; comp1 = 3 * v + 2; slot1 = 0; s1 = 1.0; break;
-    case 2: comp0 = 3 * v + 2; slot0 = 0; s0 = -1.0; comp1 = 3 * v + 1; slot1 = 1; s1 = -1.0; break;
-    default: comp0 = 3 * v + 2; slot0 = 1; s0 = -1.0; comp1 = 3 * v + 1; slot1 = 0; s1 = 1.0; break;
-  }
-  cp.off0 = rec_off(comp0, P.nvf) + slot0;
-  cp.off1 = rec_off(comp1, P.nvf) + slot1;
-  cp.sgn0 = s0;
-  cp.sgn1 = s1;
-  cp.sym0 = dP_sym;
-  cp.sym1 = P_sym;
-  cp.ovs1 = true;
-  if (m == 0) cp.K1 = 0;
-  return cp;
-}
-
-// forward staged value: in = [theta][record], wts = [w, 1/sin] per hemisphere row
-__device__ __forceinline__ double fval(const ColPar& cp, const double* in, const double2* wts, int rec, int nth,
-                                       int k) {
-  if (cp.kind == 3) return 0.0;
-  const int part = k >= cp.kpart0 ? 1 : 0;
-  const int th = k - (part ? cp.kpart0 : 0);
-  if (th >= (part ? cp.K1 : cp.K0)) return 0.0;
-  const double2 wa = wts[th];
-  const double nv = in[th * rec + (part ? cp.off1 : cp.off0)];
-  double v;
-  if (th < nth / 2) {
-    const double sv = in[(nth - 1 - th) * rec + (part ? cp.off1 : cp.off0)];
-    v = (part ? cp.sym1 : cp.sym0) ? (nv + sv) * wa.x : (nv - sv) * wa.x;
-  } else {
-    v = (part ? cp.sym1 : cp.sym0) ? nv * wa.x : 0.0;
-  }
-  if ((part ? cp.ovs1 : cp.ovs0)) v = v * wa.y;
-  return (part ? cp.sgn1 : cp.sgn0) * v;
-}
-
+// Balanced base-256 digits of round(v), |round(v)| < 2^(8 NS - 2): d[NS-1] is
+// the least significant, every digit in [-128, 127] except d[0], which holds
+// the remaining high part (|d[0]| <= 64).  The value is split exactly into
+// hi 2^24 + lo with both halves in int32, so the digit loop runs on 32-bit
+// integers.
 template <int NS>
-__device__ __forceinline__ void digits_pack16(const double* v16, uint32_t (&w)[NS][4]) {
+__device__ __forceinline__ void split_digits(double v, int (&d)[NS]) {
+  const double x = rint(v);
+  const double hi = rint(x * 0x1p-24);
+  int lo = (int)fma(-hi, 0x1p24, x);
+  int h = (int)hi;
 #pragma unroll
-  for (int s = 0; s < NS; ++s)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) w[s][q] = 0u;
-#pragma unroll
-  for (int q = 0; q < 16; ++q) {
-    long long x = __double2ll_rn(v16[q]);
-#pragma unroll
-    for (int s = NS - 1; s >= 1; --s) {
-      const long long dd = ((x + 128) & 255) - 128;
-      w[s][q >> 2] |= ((uint32_t)dd & 0xFFu) << (8 * (q & 3));
-      x = (x - dd) >> 8;
-    }
-    w[0][q >> 2] |= ((uint32_t)x & 0xFFu) << (8 * (q & 3));
+  for (int s = NS - 1; s >= 1; --s) {
+    int& src = (s >= NS - 3) ? lo : h;
+    const int dd = (int)((unsigned)src << 24) >> 24;
+    d[s] = dd;
+    src = (src - dd) >> 8;
+    if (s == NS - 3) h += lo;
   }
+  d[0] = h;
 }
 
+// Slicer: one CTA per (field group z, radius r, order m).  Backward groups:
+// z < nvb is vector z (types 0/1 from its theta/phi components); z = nvb is
+// the radial components and scalars (types 2/3).  Forward groups: z = 0 is the
+// radial components and scalars (types 4/5, record words [4 nvf, rec));
+// z = 1 + v is vector v (types 6/7, record words [4v, 4v + 4)).
+//
+// Pass 1 builds the group's derived columns X[col][k] = B[k][col] 2^-dexp[k]
+// in shared memory, one thread per theta row (forward) or degree l
+// (backward), with the sym/asym combination, weights and factors of each
+// column written out explicitly (the same algebra as the FP64 tier's operand
+// loaders).  Pass 2 takes the column maxima, pass 3 cuts the digits.
 template <bool FWD, int NS>
 __global__ void __launch_bounds__(256) k_slice_mr(Plan P, SliceTabs S, const double* __restrict__ d_rj, long long ld,
                                                    const int* __restrict__ cols) {
-  extern __shared__ double sin_[];
-  const int m = blockIdx.y, r = blockIdx.x;
+  extern __shared__ double X[];
+  const int z = blockIdx.x, r = blockIdx.y, m = blockIdx.z;
   const int L = P.L;
   const int Kall = L - m + 1;
-  const int nc = FWD ? P.ncf : P.ncb;
-  const int rec = 2 * nc;
-  // ---- stage inputs
-  double* tail;
-  if (!FWD) {
-    const int nrow = 2 * nc;
-    for (int it = threadIdx.x; it < nrow * Kall; it += blockDim.x) {
-      const int row = it / Kall, lo = it - row * Kall;
-      const int slot = row / nc, q = row - slot * nc;
-      double v = 0.0;
-      if (slot == 0 || m > 0) {
-        const int j = P.jmap[((long long)m * 2 + slot) * (L + 1) + m + lo];
-        const int col = q < 3 * P.nvb ? cols[q / 3] + q % 3 : cols[P.nvb + (q - 3 * P.nvb)];
-        v = d_rj[(long long)j + P.J * r + ld * col];
-      }
-      sin_[it] = v;
-    }
-    tail = sin_ + 2 * nc * Kall;
-  } else {
-    const long long strideTh = (long long)P.nr * rec;
-    const double* base = P.rtm_f + (long long)m * P.nth * strideTh + (long long)r * rec;
-    for (int it = threadIdx.x; it < P.nth * (rec / 2); it += blockDim.x) {
-      const int th = it / (rec / 2), c2 = it - th * (rec / 2);
-      *reinterpret_cast<double2*>(sin_ + th * rec + 2 * c2) =
-          *reinterpret_cast<const double2*>(base + th * strideTh + 2 * c2);
-    }
-    double2* wts = reinterpret_cast<double2*>(sin_ + P.nth * rec);
-    for (int th = threadIdx.x; th < P.nh; th += blockDim.x) wts[th] = make_double2(P.weight[th], P.asin_t[th]);
-    tail = sin_ + P.nth * rec + 2 * P.nh;
-  }
-  const double2* wts = reinterpret_cast<const double2*>(sin_ + P.nth * rec);
+  const int nv = FWD ? P.nvf : P.nvb;
+  const int nF = FWD ? P.nvf + P.nsf : P.nvb + P.nsb;
+  const bool vgrp = FWD ? z > 0 : z < nv;  // vector (theta/phi) group
+  const int v = FWD ? z - 1 : z;
+  const int t0 = FWD ? (vgrp ? 6 : 4) : (vgrp ? 0 : 2);  // the group's two types: t0, t0 + 1
+  const int ncolg = vgrp ? 8 : 4 * nF;                    // local columns: 4 per (type) for vectors
+  int i0, g0;
+  if (!FWD) { i0 = vgrp ? 8 * v : 8 * nv; g0 = vgrp ? 2 * v : 2 * nv; }
+  else { i0 = vgrp ? 4 * nF + 8 * v : 0; g0 = vgrp ? 2 + 2 * v : 0; }
+  const TypeGeo ga = type_geo(t0, L, m, P.nh), gb = type_geo(t0 + 1, L, m, P.nh);
+  const int kst = max(ga.kpad, gb.kpad);  // X row stride
+  // local column c -> type: vectors 4 (t - t0) + q; radial/scalar 4 f + 2 (t - t0) + slot
+  auto ctype = [&](int c) { return t0 + (vgrp ? (c >> 2) : ((c >> 1) & 1)); };
+  const int* dxa = S.dexp + S.deoff[m * kNT + t0];
+  const int* dxb = S.dexp + S.deoff[m * kNT + t0 + 1];
+  const int nx = ncolg * kst;
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) X[i] = 0.0;
   __syncthreads();
-  const int ncol = FWD ? ncols_fwd(P) : ncols_bwd(P);
-  double* colmax = tail;
-  int* colexp = reinterpret_cast<int*>(colmax + kMaxCols);
   const double ar = 1.0 / P.radius[r];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // ---- column maxima of B' = B 2^-dexp
-  for (int i = warp; i < ncol; i += blockDim.x >> 5) {
-    const ColRef c = FWD ? colref_fwd(P, S, r, i) : colref_bwd(P, S, r, i);
-    const ColPar cp = FWD ? colpar_fwd(P, c, m) : colpar_bwd(P, c, m, Kall);
-    const int* dx = S.dexp + S.deoff[m * kNT + c.t];
-    double mx = 0.0;
-    for (int k = lane; k < cp.kpad; k += 32) {
-      const double x = FWD ? fval(cp, sin_, wts, rec, P.nth, k) : bval(cp, sin_, m, k, ar);
-      mx = fmax(mx, fabs(x * pow2(-__ldg(dx + k))));
+
+  // ---- pass 1: derived columns
+  if (FWD) {
+    const int rec = 2 * P.ncf;
+    const long long strideTh = (long long)P.nr * rec;
+    const double* base = P.rtm_f + (long long)m * P.nth * strideTh + (long long)r * rec + (vgrp ? 4 * v : 4 * nv);
+    for (int th = threadIdx.x; th < P.nh; th += blockDim.x) {
+      const bool hasS = th < P.nth / 2;
+      const double w = __ldg(P.weight + th);
+      const double* pn = base + th * strideTh;
+      const double* ps = base + (long long)(P.nth - 1 - th) * strideTh;
+      const double sa = pow2(-__ldg(dxa + th)), sb = pow2(-__ldg(dxb + th));
+      if (vgrp) {
+        // words (theta slot 0, theta slot 1, phi slot 0, phi slot 1)
+        const double2 n01 = __ldg(reinterpret_cast<const double2*>(pn));
+        const double2 n23 = __ldg(reinterpret_cast<const double2*>(pn + 2));
+        double2 s01 = make_double2(0.0, 0.0), s23 = s01;
+        if (hasS) {
+          s01 = __ldg(reinterpret_cast<const double2*>(ps));
+          s23 = __ldg(reinterpret_cast<const double2*>(ps + 2));
+        }
+        const double nn[4] = {n01.x, n01.y, n23.x, n23.y}, ss[4] = {s01.x, s01.y, s23.x, s23.y};
+        double sy[4], as[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          sy[c] = (nn[c] + ss[c]) * w;
+          as[c] = hasS ? (nn[c] - ss[c]) * w : 0.0;
+        }
+        const double ai = __ldg(P.asin_t + th);
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+          // type 6 + p: dP part takes (N + S) for p = 1, the m P part (N + S) / sin for p = 0
+          const double* A0 = p ? sy : as;
+          const double* A1 = p ? as : sy;
+          const TypeGeo& g = p ? gb : ga;
+          const double s0 = p ? sb : sa;
+          double* x = X + (4 * p) * kst;
+          x[0 * kst + th] = A0[0] * s0;
+          x[1 * kst + th] = A0[1] * s0;
+          x[2 * kst + th] = -A0[2] * s0;
+          x[3 * kst + th] = -A0[3] * s0;
+          if (m > 0) {
+            const int k1 = g.kpart0 + th;
+            const double s1 = pow2(-__ldg((p ? dxb : dxa) + k1)) * ai;
+            x[0 * kst + k1] = -A1[3] * s1;
+            x[1 * kst + k1] = A1[2] * s1;
+            x[2 * kst + k1] = -A1[1] * s1;
+            x[3 * kst + k1] = A1[0] * s1;
+          }
+        }
+      } else {
+        for (int f = 0; f < nF; ++f) {
+          const double2 nn = __ldg(reinterpret_cast<const double2*>(pn + 2 * f));
+          const double2 ss = hasS ? __ldg(reinterpret_cast<const double2*>(ps + 2 * f)) : make_double2(0.0, 0.0);
+          X[(4 * f + 0) * kst + th] = (nn.x + ss.x) * w * sa;
+          X[(4 * f + 2) * kst + th] = hasS ? (nn.x - ss.x) * w * sb : 0.0;
+          if (m > 0) {
+            X[(4 * f + 1) * kst + th] = (nn.y + ss.y) * w * sa;
+            X[(4 * f + 3) * kst + th] = hasS ? (nn.y - ss.y) * w * sb : 0.0;
+          }
+        }
+      }
     }
+  } else {
+    for (int kl = threadIdx.x; kl < Kall; kl += blockDim.x) {
+      const int l = m + kl, p = kl & 1, kk = kl >> 1;
+      const int j0 = __ldg(P.jmap + (long long)m * 2 * (L + 1) + l);
+      const int j1 = m > 0 ? __ldg(P.jmap + ((long long)m * 2 + 1) * (L + 1) + l) : 0;
+      const double* dr = d_rj + P.J * (long long)r;
+      if (vgrp) {
+        // x[c][slot], c = 0: dS/dr column (theta/phi source 1), c = 1: toroidal (source 2)
+        const double* d1 = dr + ld * (cols[v] + 1);
+        const double* d2 = dr + ld * (cols[v] + 2);
+        const double x10 = __ldg(d1 + j0) * ar, x20 = __ldg(d2 + j0) * ar;
+        const double x11 = m > 0 ? __ldg(d1 + j1) * ar : 0.0, x21 = m > 0 ? __ldg(d2 + j1) * ar : 0.0;
+        // type 0 takes odd l - m into part 0 (dP) and even into part 1 (m P); type 1 the reverse
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+          const bool part1 = (t == 0) ? (p == 0) : (p == 1);
+          const TypeGeo& g = t ? gb : ga;
+          const int k = (part1 ? g.kpart0 : 0) + kk;
+          const double sc = pow2(-__ldg((t ? dxb : dxa) + k));
+          double* x = X + (4 * t) * kst + k;
+          if (!part1) {
+            x[0 * kst] = x10 * sc;
+            x[1 * kst] = x11 * sc;
+            x[2 * kst] = -x20 * sc;
+            x[3 * kst] = -x21 * sc;
+          } else {
+            x[0 * kst] = x21 * sc;
+            x[1 * kst] = -x20 * sc;
+            x[2 * kst] = x11 * sc;
+            x[3 * kst] = -x10 * sc;
+          }
+        }
+      } else {
+        const int t = p;  // type 2 (even l - m) or 3 (odd)
+        const double sc = pow2(-__ldg((t ? dxb : dxa) + kk));
+        const double fr = ar * ar * g3_of(l);
+        for (int f = 0; f < nF; ++f) {
+          const double* d = dr + ld * cols[f];
+          const double fac = (f < nv ? fr : 1.0) * sc;
+          X[(4 * f + 2 * t) * kst + kk] = __ldg(d + j0) * fac;
+          if (m > 0) X[(4 * f + 2 * t + 1) * kst + kk] = __ldg(d + j1) * fac;
+        }
+      }
+    }
+  }
+  __syncthreads();
+
+  double* colmax = X + ((nx + 1) & ~1);
+  int* colexp = reinterpret_cast<int*>(colmax + kGrpCols);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nw = blockDim.x >> 5;
+  // ---- pass 2: column maxima
+  for (int c = warp; c < ncolg; c += nw) {
+    const int t = ctype(c);
+    const int kp = (t == t0) ? ga.kpad : gb.kpad;
+    double mx = 0.0;
+    for (int k = lane; k < kp; k += 32) mx = fmax(mx, fabs(X[c * kst + k]));
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     if (lane == 0) {
       const int e = mx > 0.0 ? exp_above(mx) : 0;
-      colmax[i] = mx;
-      colexp[i] = e;
-      S.bexp[S.beoff[m * kNT + c.t] + c.col] = e - (8 * NS - 2);
+      colmax[c] = mx;
+      colexp[c] = e;
+      const ColRef cr = FWD ? colref_fwd(P, S, r, i0 + c) : colref_bwd(P, S, r, i0 + c);
+      S.bexp[S.beoff[m * kNT + t] + cr.col] = e - (8 * NS - 2);
     }
   }
   __syncthreads();
-  // ---- digits, 16 consecutive k per lane, one column per warp
-  for (int i = warp; i < ncol; i += blockDim.x >> 5) {
-    const ColRef c = FWD ? colref_fwd(P, S, r, i) : colref_bwd(P, S, r, i);
-    const ColPar cp = FWD ? colpar_fwd(P, c, m) : colpar_bwd(P, c, m, Kall);
-    const int n16 = cp.kpad / 16;
-    const int nkc = cp.kpad / kTK;
-    const bool nz = colmax[i] > 0.0;
-    const int sh = (8 * NS - 2) - colexp[i];
-    const int* dx = S.dexp + S.deoff[m * kNT + c.t];
-    signed char* base = S.B + S.boff[m * kNT + c.t];
-    const int nt = c.col / kTN, cr = c.col % kTN;
-    for (int kb = lane; kb < n16; kb += 32) {
-      double v16[16];
+  // ---- pass 3: digits.  Work item = (column group, 32-wide K chunk), lane = k.
+  // A column group is the set of columns that share one 256-byte block of a
+  // core-matrix tile: 8 rows (one radius of types 2..5) or 4 rows (one radius
+  // and vector of types 0/1/6/7).  The warp assembles the block's NS slices
+  // in shared memory (k halves 144 bytes apart, so the byte stores of the two
+  // half-warps fall in different banks) and writes them out with 16-byte
+  // stores, 256 (or 2 x 64) contiguous bytes per slice.
+  unsigned char* wb = reinterpret_cast<unsigned char*>(
+                          (reinterpret_cast<uintptr_t>(colexp + kGrpCols) + 15) & ~static_cast<uintptr_t>(15)) +
+                      warp * (NS * kSlab);
+  int item0 = 0;
+  for (int gi = g0; gi < g0 + 2; ++gi) {
+    const int t = t0 + (gi - g0);
+    const bool eight = !vgrp;  // 8-row groups: radius blocks of types 2..5
+    const int gcol = eight ? r * 8 : (v * S.nrT + r) * 4;
+    const TypeGeo& geo = (t == t0) ? ga : gb;
+    const int nkc = geo.kpad / kTK;
+    const int nt = gcol / kTN, blk = (gcol % kTN) >> 3, rbase = gcol & 7;
+    signed char* base = S.B + S.boff[m * kNT + t];
+    for (int kc = ((warp - item0) % nw + nw) % nw; kc < nkc; kc += nw) {
+      const int k = kc * kTK + lane;
+      const int koff = (lane >> 4) * 144 + (lane & 15);
+      const int ncg = eight ? 8 : 4;
+      for (int q = 0; q < ncg; ++q) {
+        // local column of block row rbase + q
+        int c = -1;
+        if (!eight) c = 4 * (t - t0) + q;
+        else if ((q >> 1) < nF) c = 4 * (q >> 1) + 2 * (t - t0) + (q & 1);
+        int dg[NS];
+        if (c >= 0 && colmax[c] > 0.0) {
+          split_digits<NS>(X[c * kst + k] * pow2((8 * NS - 2) - colexp[c]), dg);
+        } else {
 #pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        const int k = kb * 16 + q;
-        const double x = FWD ? fval(cp, sin_, wts, rec, P.nth, k) : bval(cp, sin_, m, k, ar);
-        v16[q] = nz ? x * pow2(sh - __ldg(dx + k)) : 0.0;
-      }
-      uint32_t w[NS][4];
-      digits_pack16<NS>(v16, w);
-      const int kc = kb >> 1;
+          for (int s2 = 0; s2 < NS; ++s2) dg[s2] = 0;
+        }
+        const int o = koff + (rbase + q) * 16;
 #pragma unroll
-      for (int s2 = 0; s2 < NS; ++s2) {
-        signed char* dst = base + ((long long)(nt * nkc + kc) * NS + s2) * (kTN * kTK) + tile_off(cr, (kb & 1) * 16);
-        *reinterpret_cast<uint4*>(dst) = make_uint4(w[s2][0], w[s2][1], w[s2][2], w[s2][3]);
+        for (int s2 = 0; s2 < NS; ++s2) wb[s2 * kSlab + o] = (unsigned char)dg[s2];
       }
+      __syncwarp();
+      signed char* dst0 = base + (long long)(nt * nkc + kc) * NS * (kTN * kTK) + blk * 256;
+      if (eight) {
+        for (int u = lane; u < NS * 16; u += 32) {
+          const int s2 = u >> 4, h = (u >> 3) & 1, rr = u & 7;
+          *reinterpret_cast<uint4*>(dst0 + s2 * (kTN * kTK) + h * 128 + rr * 16) =
+              *reinterpret_cast<const uint4*>(wb + s2 * kSlab + h * 144 + rr * 16);
+        }
+      } else {
+        for (int u = lane; u < NS * 8; u += 32) {
+          const int s2 = u >> 3, h = (u >> 2) & 1, rr = rbase + (u & 3);
+          *reinterpret_cast<uint4*>(dst0 + s2 * (kTN * kTK) + h * 128 + rr * 16) =
+              *reinterpret_cast<const uint4*>(wb + s2 * kSlab + h * 144 + rr * 16);
+        }
+      }
+      __syncwarp();
     }
+    item0 += nkc;
   }
 }
 
@@ -570,13 +561,47 @@ struct GemmArgs {
 
 constexpr int kGemmWarps = 6;
 constexpr int kEpiThreads = 128;
-constexpr int kRing = 3;           // stage ring depth
-constexpr int kXS = kTN + 1;       // exchange row stride (doubles)
+constexpr int kRing = 4;           // stage ring depth
+constexpr int kXS = kTN + 2;       // exchange row stride (doubles): 16-byte rows, conflict-free v2 stores
 
-__device__ __forceinline__ unsigned make_idesc() {
-  // kind::i8: D s32 (2 << 4), A s8 (1 << 7), B s8 (1 << 10), K-major A/B, N = 64, M = 128
-  return (2u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(kTN >> 3) << 17) | ((unsigned)(kTM >> 4) << 24);
+__host__ __device__ constexpr unsigned make_idesc(int n) {
+  // kind::i8: D s32 (2 << 4), A s8 (1 << 7), B s8 (1 << 10), K-major A/B, N = n, M = 128
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(n >> 3) << 17) | ((unsigned)(kTM >> 4) << 24);
 }
+
+// MMA schedule of one K chunk.  The B slices of a stage are consecutive 64-row
+// core-matrix tiles (stride 256 B per 8 rows), so slices b .. b+nb-1 form one
+// N = 64·nb operand, and the product A_a·[B_b .. B_b+nb-1] lands in the
+// consecutive TMEM groups a+b .. a+b+nb-1.  This issues the 26 (10) slice
+// products of tier split (fp32acc) as 9 (4) MMAs of N up to 256.  In the first
+// chunk of a tile the entries flagged `init` run first without accumulation:
+// together they cover every group exactly once and touch no group written
+// before them.  Group g >= NS is first written by the single product
+// (g - NS + 2, NS - 2), which the a-row runs then skip.
+template <int NS, int TG>
+struct MmaSched {
+  int n = 0;
+  int a[24] = {}, b[24] = {}, nb[24] = {}, init[24] = {};
+  constexpr void push(int aa, int bb, int nn, int ii) {
+    a[n] = aa; b[n] = bb; nb[n] = nn; init[n] = ii; ++n;
+  }
+  static constexpr bool is_single(int aa, int bb) { return bb == NS - 2 && aa >= 2 && aa <= TG - NS + 2; }
+  constexpr MmaSched() {
+    const int top0 = (NS - 1 < TG) ? NS - 1 : TG;
+    for (int b0 = 0; b0 <= top0; b0 += 4) push(0, b0, (top0 - b0 + 1 < 4) ? top0 - b0 + 1 : 4, 1);
+    for (int g = NS; g <= TG; ++g) push(g - NS + 2, NS - 2, 1, 1);
+    for (int aa = 1; aa < NS; ++aa) {
+      const int top = (NS - 1 < TG - aa) ? NS - 1 : TG - aa;
+      int b0 = 0;
+      while (b0 <= top) {
+        int b1 = b0;  // run [b0, b1) avoiding the init singles
+        while (b1 <= top && b1 - b0 < 4 && !is_single(aa, b1)) ++b1;
+        if (b1 > b0) push(aa, b0, b1 - b0, 0);
+        b0 = (b1 > b0) ? b1 : b0 + 1;
+      }
+    }
+  }
+};
 
 // exact int32 -> double on the FP64 pipe (2^52 + 2^31 magic)
 __device__ __forceinline__ double i2d(int x) {
@@ -587,8 +612,8 @@ __device__ __forceinline__ unsigned mapa(const void* p, unsigned rank) {
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(a) : "r"(sptr(p)), "r"(rank));
   return a;
 }
-__device__ __forceinline__ void st_remote_f64(unsigned addr, double v) {
-  asm volatile("st.shared::cluster.f64 [%0], %1;\n" ::"r"(addr), "d"(v) : "memory");
+__device__ __forceinline__ void st_remote_f64x2(unsigned addr, double a, double b) {
+  asm volatile("st.shared::cluster.v2.f64 [%0], {%1, %2};\n" ::"r"(addr), "d"(a), "d"(b) : "memory");
 }
 __device__ __forceinline__ void arrive_remote(unsigned bar_addr) {
   asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(bar_addr) : "memory");
@@ -684,7 +709,7 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
   } else if (warp == 0) {
     if (lane == 0) {
       // ---- MMA issuer
-      const unsigned idesc = make_idesc();
+      constexpr MmaSched<NS, TG> sch{};
       long long gc = 0;
       int it = 0;
       bool ok = true;
@@ -701,17 +726,10 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
           const uint64_t a0 = smem_desc(sm + st * STAGE, 128, 256);
           const uint64_t b0 = smem_desc(sm + st * STAGE + A_BYTES, 128, 256);
 #pragma unroll
-          for (int a = 0; a < NS; ++a) {
-#pragma unroll
-            for (int b = 0; b < NS; ++b) {
-              const int grp = a + b;
-              if (grp > TG) continue;
-              // the first product of group grp (smallest a) overwrites, the rest accumulate
-              const unsigned first_a = (grp < NS) ? 0 : grp - (NS - 1);
-              const unsigned acc = (kc > 0 || (unsigned)a > first_a) ? 1u : 0u;
-              mma_i8(tmem + (unsigned)(grp * kTN), a0 + (uint64_t)(a * (kTM * kTK / 16)),
-                     b0 + (uint64_t)(b * (kTN * kTK / 16)), idesc, acc);
-            }
+          for (int q = 0; q < sch.n; ++q) {
+            const unsigned acc = (kc > 0 || !sch.init[q]) ? 1u : 0u;
+            mma_i8(tmem + (unsigned)((sch.a[q] + sch.b[q]) * kTN), a0 + (uint64_t)(sch.a[q] * (kTM * kTK / 16)),
+                   b0 + (uint64_t)(sch.b[q] * (kTN * kTK / 16)), make_idesc(kTN * sch.nb[q]), acc);
           }
           mma_commit(&empty[st]);
         }
@@ -736,8 +754,11 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
       const TypeGeo g = type_geo(w.t, P.L, w.m, P.nh);
       const int grow = w.mt * kTM + row;
       const int eA = (grow < g.rows) ? S.aexp[S.aeoff[w.m * kNT + w.t] + grow] : 0;
+      // column exponents: lane i holds columns i and 32 + i, broadcast by shuffles
       const int* eBp = S.bexp + S.beoff[w.m * kNT + w.t] + w.nt * kTN;
+      const int eb_lo = __ldg(eBp + lane), eb_hi = __ldg(eBp + 32 + lane);
       if (ok && !mbar_wait(done, (unsigned)(it & 1))) ok = false;
+      ok = __all_sync(0xffffffffu, ok);
       tc_fence_after();
       double val[kTN];
       if (nk > 0 && ok) {
@@ -753,7 +774,9 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
             double v = i2d(acc[0][c]);
 #pragma unroll
             for (int gi = 1; gi <= TG; ++gi) v = fma(v, 256.0, i2d(acc[gi][c]));
-            val[cb * 16 + c] = v * (wscale * pow2(eA + __ldg(eBp + cb * 16 + c)));
+            const int cc = cb * 16 + c;
+            const int eB = __shfl_sync(0xffffffffu, cc < 32 ? eb_lo : eb_hi, cc & 31);
+            val[cc] = v * (wscale * pow2(eA + eB));
           }
         }
       } else {
@@ -764,31 +787,52 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
       asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(sptr(tfree)) : "memory");
 
       if (!pair) {
-        // forward: scatter into d_rj with the r, r^2, g7, g6 factors
+        // forward: scatter into d_rj with the r, r^2, g7, g6 factors.  The
+        // column parameters (radius, field column) are warp-uniform; the two
+        // j offsets of this row's degree are loaded once per tile.
         const int par = (w.t == 4 || w.t == 6) ? 0 : 1;
         const int l = w.m + 2 * grow + par;
         if (grow < g.rows && l <= P.L) {
           const double g7 = g7_of(l, w.m);
+          const long long jm = (long long)w.m * 2 * (P.L + 1) + l;
+          const long long j0 = P.jmap[jm];
+          const long long j1 = w.m > 0 ? P.jmap[jm + P.L + 1] : 0;
+          const bool s1 = w.m > 0;
+          if (w.t <= 5) {
+            // column c = 8 (r - 8 nt) + 2 f + slot
+            const double g6 = g6_of(l, w.m);
 #pragma unroll
-          for (int c = 0; c < kTN; ++c) {
-            const int col = w.nt * kTN + c;
-            if (w.t <= 5) {
-              const int slot = col & 1, f = (col >> 1) & 3, r = col >> 3;
-              if (r >= P.nr || f >= P.nvf + P.nsf || (slot == 1 && w.m == 0)) continue;
-              const long long j = P.jmap[((long long)w.m * 2 + slot) * (P.L + 1) + l] + P.J * r;
-              if (f < P.nvf) {
-                const double r1 = P.radius[r];
-                args.d_rj[j + args.ld * args.cols[f]] = val[c] * (r1 * r1) * g7;
-              } else {
-                args.d_rj[j + args.ld * args.cols[f]] = val[c] * g6_of(l, w.m);
+            for (int rr = 0; rr < kTN / 8; ++rr) {
+              const int r = w.nt * (kTN / 8) + rr;
+              if (r >= P.nr) break;
+              const double r1 = P.radius[r];
+              const double fv = r1 * r1 * g7;
+              const long long jr = P.J * (long long)r;
+#pragma unroll
+              for (int f = 0; f < 4; ++f) {
+                if (f >= P.nvf + P.nsf) break;
+                const double fac = f < P.nvf ? fv : g6;
+                double* dst = args.d_rj + jr + args.ld * args.cols[f];
+                dst[j0] = val[8 * rr + 2 * f] * fac;
+                if (s1) dst[j1] = val[8 * rr + 2 * f + 1] * fac;
               }
-            } else {
-              const int q = col & 3, r = (col >> 2) % S.nrT, v = (col >> 2) / S.nrT;
-              if (v >= P.nvf || r >= P.nr) continue;
-              const int slot = q & 1;
-              if (slot == 1 && w.m == 0) continue;
-              const long long j = P.jmap[((long long)w.m * 2 + slot) * (P.L + 1) + l] + P.J * r;
-              args.d_rj[j + args.ld * (args.cols[v] + 1 + (q >> 1))] = val[c] * P.radius[r] * g7;
+            }
+          } else {
+            // column c = 4 (r + nrT v) + q, q = 2 (component - 1) + slot
+#pragma unroll
+            for (int c4 = 0; c4 < kTN / 4; ++c4) {
+              const int rv = w.nt * (kTN / 4) + c4;
+              const int r = rv % S.nrT, v = rv / S.nrT;
+              if (v >= P.nvf) break;
+              if (r >= P.nr) continue;
+              const double fac = P.radius[r] * g7;
+              double* dst = args.d_rj + P.J * (long long)r + args.ld * (args.cols[v] + 1);
+              dst[j0] = val[4 * c4] * fac;
+              dst[j0 + args.ld] = val[4 * c4 + 2] * fac;
+              if (s1) {
+                dst[j1] = val[4 * c4 + 1] * fac;
+                dst[j1 + args.ld] = val[4 * c4 + 3] * fac;
+              }
             }
           }
         }
@@ -796,7 +840,7 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
         // backward: send my tile to the peer, receive the peer's, emit N or S
         if (it > 0 && ok && !mbar_wait_cluster(rempty, (unsigned)((it - 1) & 1))) ok = false;
 #pragma unroll
-        for (int c = 0; c < kTN; ++c) st_remote_f64(peer_recv + (unsigned)((row * kXS + c) * 8), val[c]);
+        for (int c = 0; c < kTN; c += 2) st_remote_f64x2(peer_recv + (unsigned)((row * kXS + c) * 8), val[c], val[c + 1]);
         arrive_remote(peer_rfull);
         if (ok && !mbar_wait_cluster(rfull, (unsigned)(it & 1))) ok = false;
         const int th = grow;
@@ -1048,14 +1092,27 @@ int split_create(SplitState** out, const Plan& p, int tier, int nslice, cudaStre
   return KMHD_OK;
 }
 
+// dynamic shared memory of one slicer CTA (largest field group): the derived
+// columns X[col][k] (k up to the padded K of the group's types), the column
+// maxima and exponents, and eight per-warp slice staging blocks
+size_t slice_smem(const Plan& p, bool fwd, int ns) {
+  // K shrinks with m for the backward types and is m-independent forward: m = 0 is the largest
+  const int nF = fwd ? p.nvf + p.nsf : p.nvb + p.nsb;
+  const int tv = fwd ? 6 : 0, tr = fwd ? 4 : 2;
+  const size_t kv = std::max(type_geo(tv, p.L, 0, p.nh).kpad, type_geo(tv + 1, p.L, 0, p.nh).kpad);
+  const size_t kr = std::max(type_geo(tr, p.L, 0, p.nh).kpad, type_geo(tr + 1, p.L, 0, p.nh).kpad);
+  const size_t nx = std::max(8 * kv, 4 * (size_t)nF * kr);
+  return sizeof(double) * (nx + 1 + kGrpCols) + kGrpCols * sizeof(int) + 8 * (size_t)ns * kSlab + 16;
+}
+
 int split_bwd(SplitState* s, const Plan& p, int, const double* d_rj, long long ld, const int* cols, cudaStream_t st) {
   const SliceTabs& S = s->S;
   {
-    const size_t smem = sizeof(double) * (2 * (size_t)p.ncb * (p.L + 1) + kMaxCols) + kMaxCols * sizeof(int);
     auto kern = s->ns == 6 ? k_slice_mr<false, 6> : k_slice_mr<false, 4>;
+    const size_t smem = slice_smem(p, false, s->ns);
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
       return KMHD_ERR_CUDA;
-    kern<<<dim3(p.nr, p.L + 1), 256, smem, st>>>(p, S, d_rj, ld, cols);
+    kern<<<dim3(p.nvb + 1, p.nr, p.L + 1), 256, smem, st>>>(p, S, d_rj, ld, cols);
   }
   if (cudaGetLastError() != cudaSuccess) return KMHD_ERR_CUDA;
   GemmArgs a;
@@ -1075,11 +1132,11 @@ int split_bwd(SplitState* s, const Plan& p, int, const double* d_rj, long long l
 int split_fwd(SplitState* s, const Plan& p, double* d_rj, long long ld, const int* cols, cudaStream_t st) {
   const SliceTabs& S = s->S;
   {
-    const size_t smem = sizeof(double) * (2 * (size_t)p.ncf * p.nth + 2 * (size_t)p.nh + kMaxCols) + kMaxCols * sizeof(int);
+    const size_t smem = slice_smem(p, true, s->ns);
     auto kern = s->ns == 6 ? k_slice_mr<true, 6> : k_slice_mr<true, 4>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
       return KMHD_ERR_CUDA;
-    kern<<<dim3(p.nr, p.L + 1), 256, smem, st>>>(p, S, nullptr, 0, nullptr);
+    kern<<<dim3(p.nvf + 1, p.nr, p.L + 1), 256, smem, st>>>(p, S, nullptr, 0, nullptr);
   }
   if (cudaGetLastError() != cudaSuccess) return KMHD_ERR_CUDA;
   GemmArgs a;
@@ -1133,7 +1190,7 @@ __global__ void __launch_bounds__(128, 1) k_selftest_mma(const signed char* A, c
   tc_fence_after();
   const unsigned tmem = slot;
   if (tid == 0) {
-    mma_i8(tmem, smem_desc(sa, lbo, sbo), smem_desc(sb, lbo, sbo), make_idesc(), 0u);
+    mma_i8(tmem, smem_desc(sa, lbo, sbo), smem_desc(sb, lbo, sbo), make_idesc(kTN), 0u);
     mma_commit(&bar);
   }
   __syncwarp();
