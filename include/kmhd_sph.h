@@ -141,6 +141,27 @@ int kmhd_sph_last_timing(kmhd_sph *handle, double *ms4);
 int kmhd_sph_get_tables(kmhd_sph *handle, int32_t m, double *colat, double *weight,
                         double *P, double *dP);
 
+/* The FP64 cycle of kmhd_sph_cycle for callers that cannot allocate device
+ * memory: a solver whose host framework owns the whole device pool, or a
+ * time-step loop that must not call cudaMalloc/cudaFree (which can stall the
+ * device) once set-up is over.  No handle is built: every work buffer --
+ * Gauss/Schmidt tables, index maps, FFT twiddles, packed spectra and the
+ * (m, theta, r) records -- lives in one static 32 MiB device array that the
+ * library holds on every device it is loaded on until the process exits; the
+ * tables are recomputed on each call.  desc->tier must be KMHD_TIER_FP64;
+ * d_rj_in / d_rj_out are device pointers (cols_b / cols_f and desc's arrays
+ * stay on the host); stream is a cudaStream_t (NULL = default stream) and the
+ * call returns after it has been synchronised.  Returns KMHD_ERR_SIZE when the
+ * problem needs more than the 32 MiB (about L = 31, Ntheta = 48, Nphi = 96,
+ * Nr = 33 with four fields each way fits).  The first call on a device looks
+ * up the array's device address, so make it before any stream capture.  All
+ * calls share the one array: calls that overlap on the GPU (other host
+ * threads, other streams) race and corrupt each other's results.
+ * This entry point has no counterpart in the reference. */
+int kmhd_sph_cycle_noalloc(const kmhd_sph_desc *desc, const double *d_rj_in, int64_t ld_in,
+                           const int32_t *cols_b, double *d_rj_out, int64_t ld_out,
+                           const int32_t *cols_f, void *stream);
+
 /* Device bytes held by the handle. */
 int64_t kmhd_sph_device_bytes(const kmhd_sph *handle);
 

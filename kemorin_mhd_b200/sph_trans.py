@@ -53,7 +53,7 @@ class Desc(ctypes.Structure):
 
 EXPORTS = ["kmhd_sph_create", "kmhd_sph_destroy", "kmhd_sph_set_stream", "kmhd_sph_b_trans",
            "kmhd_sph_f_trans", "kmhd_sph_cycle", "kmhd_sph_batch_cycle", "kmhd_sph_last_timing",
-           "kmhd_sph_get_tables", "kmhd_sph_device_bytes", "kmhd_strerror"]
+           "kmhd_sph_get_tables", "kmhd_sph_device_bytes", "kmhd_strerror", "kmhd_sph_cycle_noalloc"]
 
 _lib = None
 
@@ -82,6 +82,7 @@ def load_library(path: str | None = None):
     lib.kmhd_sph_get_tables.argtypes = [vp, i32] + [ctypes.POINTER(ctypes.c_double)] * 4
     lib.kmhd_sph_device_bytes.restype = i64
     lib.kmhd_sph_device_bytes.argtypes = [vp]
+    lib.kmhd_sph_cycle_noalloc.argtypes = [ctypes.POINTER(Desc), vp, i64, ip, vp, i64, ip, vp]
     lib.kmhd_strerror.restype = ctypes.c_char_p
     lib.kmhd_strerror.argtypes = [ctypes.c_int]
     _lib = lib
