@@ -100,14 +100,6 @@ __device__ __forceinline__ void tmem_ld16(unsigned taddr, int* v) {
       : "r"(taddr));
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
-__device__ __forceinline__ unsigned cluster_rank() {
-  unsigned r;
-  asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ void cluster_sync() {
-  asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;\n" ::: "memory");
-}
 
 // ---------------------------------------------------------------------------
 // Digit extraction: v must satisfy |rint(v)| < 2^(8 ns - 2).
@@ -538,11 +530,10 @@ __global__ void __launch_bounds__(256) k_slice_mr(Plan P, SliceTabs S, const dou
 //   warp 1 (one lane): streams pre-laid-out slice tiles with bulk copies into a
 //                      stage ring, running ahead across tiles
 //   warps 2..5:        epilogue (TMEM -> FP64 recombination -> output)
-// One tile = (m, type, m-tile, n-tile).  The backward work list pairs the sym
-// (rank 0) and asym (rank 1) tiles of one output tile in a 2-CTA cluster; each
-// CTA sends its FP64 tile to the peer with remote shared-memory stores and a
-// remote mbarrier arrival, then emits N = sym + asym (rank 0) or S = sym - asym
-// (rank 1).
+// One tile = (m, type, m-tile, n-tile).  The backward work list pairs the two
+// parity tiles (types 0/1 or 2/3) of one output tile; one CTA runs them back to
+// back, keeps the first in shared memory and emits the north row
+// (first + second) and the south row (first - second) of the rtm records.
 struct Work {
   int m, t, mt, nt;
 };
@@ -552,7 +543,7 @@ struct GemmArgs {
   SliceTabs S;
   const Work* work;
   int nwork;
-  int pair;        // 1: backward cluster pairs
+  int pair;        // 1: backward tile pairs
   double* d_rj;    // forward output
   long long ld;
   const int* cols;
@@ -562,7 +553,7 @@ struct GemmArgs {
 constexpr int kGemmWarps = 6;
 constexpr int kEpiThreads = 128;
 constexpr int kRing = 4;           // stage ring depth
-constexpr int kXS = kTN + 2;       // exchange row stride (doubles): 16-byte rows, conflict-free v2 stores
+constexpr int kXS = kTN + 2;       // stash row stride (doubles): 16-byte rows, conflict-free v2 accesses
 
 __host__ __device__ constexpr unsigned make_idesc(int n) {
   // kind::i8: D s32 (2 << 4), A s8 (1 << 7), B s8 (1 << 10), K-major A/B, N = n, M = 128
@@ -607,57 +598,34 @@ struct MmaSched {
 __device__ __forceinline__ double i2d(int x) {
   return __hiloint2double(0x43300000, (unsigned)x ^ 0x80000000u) - 4503601774854144.0;
 }
-__device__ __forceinline__ unsigned mapa(const void* p, unsigned rank) {
-  unsigned a;
-  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(a) : "r"(sptr(p)), "r"(rank));
-  return a;
-}
-__device__ __forceinline__ void st_remote_f64x2(unsigned addr, double a, double b) {
-  asm volatile("st.shared::cluster.v2.f64 [%0], {%1, %2};\n" ::"r"(addr), "d"(a), "d"(b) : "memory");
-}
-__device__ __forceinline__ void arrive_remote(unsigned bar_addr) {
-  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(bar_addr) : "memory");
-}
-__device__ __forceinline__ bool mbar_wait_cluster(unsigned long long* b, unsigned parity) {
-  for (long long it = 0; it < kSpinCap; ++it) {
-    unsigned ok;
-    asm volatile(
-        "{\n.reg .pred p;\nmbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
-        "selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(sptr(b)), "r"(parity)
-        : "memory");
-    if (ok) return true;
-  }
-  return false;
-}
-
 template <int NS>
 __host__ __device__ constexpr size_t gemm_stage_bytes() { return (size_t)NS * (kTM + kTN) * kTK; }
+
+// 32-byte global store (sm_100 256-bit st.global); p must be 32-byte aligned
+__device__ __forceinline__ void st_global_v4(double* p, double a, double b, double c, double d) {
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};\n" ::"l"(p), "d"(a), "d"(b), "d"(c), "d"(d) : "memory");
+}
 
 template <int NS, int TG>
 __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args) {
   extern __shared__ __align__(1024) unsigned char sm[];
   constexpr int A_BYTES = NS * kTM * kTK, B_BYTES = NS * kTN * kTK;
   constexpr int STAGE = A_BYTES + B_BYTES;
-  double* recv = reinterpret_cast<double*>(sm + kRing * STAGE);   // [kTM][kXS], written by the peer
-  unsigned long long* bars = reinterpret_cast<unsigned long long*>(recv + kTM * kXS);
+  double* stash = reinterpret_cast<double*>(sm + kRing * STAGE);  // [kTM][kXS]: first tile of a backward pair
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(stash + kTM * kXS);
   unsigned long long* full = bars;              // [kRing]
   unsigned long long* empty = bars + kRing;     // [kRing]
   unsigned long long* done = bars + 2 * kRing;  // accumulators ready
   unsigned long long* tfree = done + 1;         // TMEM drained by the epilogue
-  unsigned long long* rfull = tfree + 1;        // peer wrote my recv buffer
-  unsigned long long* rempty = rfull + 1;       // peer consumed the buffer I wrote
-  unsigned* tmem_slot = reinterpret_cast<unsigned*>(rempty + 1);
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(tfree + 1);
 
   const Plan& P = args.P;
   const SliceTabs& S = args.S;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // backward units are (first, second) tile pairs run back to back by one CTA
   const bool pair = args.pair != 0;
-  const unsigned rank = pair ? cluster_rank() : 0u;
-  const int nunits = pair ? args.nwork / 2 : args.nwork;
-  const int ustride = pair ? gridDim.x / 2 : gridDim.x;
-  const int ubase = pair ? blockIdx.x / 2 : blockIdx.x;
+  const int per = pair ? 2 : 1;
+  const int nunits = args.nwork / per;
 
   if (threadIdx.x == 0) {
     for (int q = 0; q < kRing; ++q) {
@@ -666,8 +634,6 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
     }
     mbar_init(done, 1);
     mbar_init(tfree, kEpiThreads);
-    mbar_init(rfull, kEpiThreads);
-    mbar_init(rempty, kEpiThreads);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 0) {
@@ -676,11 +642,9 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
   }
   tc_fence_before();
   __syncthreads();
-  if (pair) cluster_sync();  // peer barriers initialised before any remote arrival
   tc_fence_after();
   const unsigned tmem = *tmem_slot;
 
-  auto item = [&](int u) -> Work { return args.work[pair ? 2 * u + (int)rank : u]; };
   auto nk_of = [&](const Work& w) -> int {
     const TypeGeo g = type_geo(w.t, P.L, w.m, P.nh);
     return g.rows > 0 ? g.kpad / kTK : 0;
@@ -691,17 +655,19 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
       // ---- producer
       long long gc = 0;
       bool ok = true;
-      for (int u = ubase; u < nunits && ok; u += ustride) {
-        const Work w = item(u);
-        const int nk = nk_of(w);
-        const signed char* Ag = S.A + S.aoff[w.m * kNT + w.t] + (long long)w.mt * nk * A_BYTES;
-        const signed char* Bg = S.B + S.boff[w.m * kNT + w.t] + (long long)w.nt * nk * B_BYTES;
-        for (int kc = 0; kc < nk; ++kc, ++gc) {
-          const int st = (int)(gc % kRing);
-          if (gc >= kRing && !mbar_wait(&empty[st], (unsigned)(((gc / kRing) - 1) & 1))) { ok = false; break; }
-          mbar_expect_tx(&full[st], STAGE);
-          bulk_g2s(sm + st * STAGE, Ag + (long long)kc * A_BYTES, A_BYTES, &full[st]);
-          bulk_g2s(sm + st * STAGE + A_BYTES, Bg + (long long)kc * B_BYTES, B_BYTES, &full[st]);
+      for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+        for (int h = 0; h < per && ok; ++h) {
+          const Work w = args.work[u * per + h];
+          const int nk = nk_of(w);
+          const signed char* Ag = S.A + S.aoff[w.m * kNT + w.t] + (long long)w.mt * nk * A_BYTES;
+          const signed char* Bg = S.B + S.boff[w.m * kNT + w.t] + (long long)w.nt * nk * B_BYTES;
+          for (int kc = 0; kc < nk; ++kc, ++gc) {
+            const int st = (int)(gc % kRing);
+            if (gc >= kRing && !mbar_wait(&empty[st], (unsigned)(((gc / kRing) - 1) & 1))) { ok = false; break; }
+            mbar_expect_tx(&full[st], STAGE);
+            bulk_g2s(sm + st * STAGE, Ag + (long long)kc * A_BYTES, A_BYTES, &full[st]);
+            bulk_g2s(sm + st * STAGE + A_BYTES, Bg + (long long)kc * B_BYTES, B_BYTES, &full[st]);
+          }
         }
       }
       if (!ok) atomicExch(args.err, KMHD_ERR_TIMEOUT);
@@ -713,27 +679,29 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
       long long gc = 0;
       int it = 0;
       bool ok = true;
-      for (int u = ubase; u < nunits; u += ustride, ++it) {
-        const Work w = item(u);
-        const int nk = nk_of(w);
-        if (it > 0 && ok && !mbar_wait(tfree, (unsigned)((it - 1) & 1))) ok = false;
-        tc_fence_after();
-        for (int kc = 0; kc < nk && ok; ++kc, ++gc) {
-          const int st = (int)(gc % kRing);
-          if (!mbar_wait(&full[st], (unsigned)((gc / kRing) & 1))) { ok = false; break; }
+      for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        for (int h = 0; h < per; ++h, ++it) {
+          const Work w = args.work[u * per + h];
+          const int nk = nk_of(w);
+          if (it > 0 && ok && !mbar_wait(tfree, (unsigned)((it - 1) & 1))) ok = false;
           tc_fence_after();
-          // descriptors of slice 0; slice s starts s tiles further (start address field, 16-byte units)
-          const uint64_t a0 = smem_desc(sm + st * STAGE, 128, 256);
-          const uint64_t b0 = smem_desc(sm + st * STAGE + A_BYTES, 128, 256);
+          for (int kc = 0; kc < nk && ok; ++kc, ++gc) {
+            const int st = (int)(gc % kRing);
+            if (!mbar_wait(&full[st], (unsigned)((gc / kRing) & 1))) { ok = false; break; }
+            tc_fence_after();
+            // descriptors of slice 0; slice s starts s tiles further (start address field, 16-byte units)
+            const uint64_t a0 = smem_desc(sm + st * STAGE, 128, 256);
+            const uint64_t b0 = smem_desc(sm + st * STAGE + A_BYTES, 128, 256);
 #pragma unroll
-          for (int q = 0; q < sch.n; ++q) {
-            const unsigned acc = (kc > 0 || !sch.init[q]) ? 1u : 0u;
-            mma_i8(tmem + (unsigned)((sch.a[q] + sch.b[q]) * kTN), a0 + (uint64_t)(sch.a[q] * (kTM * kTK / 16)),
-                   b0 + (uint64_t)(sch.b[q] * (kTN * kTK / 16)), make_idesc(kTN * sch.nb[q]), acc);
+            for (int q = 0; q < sch.n; ++q) {
+              const unsigned acc = (kc > 0 || !sch.init[q]) ? 1u : 0u;
+              mma_i8(tmem + (unsigned)((sch.a[q] + sch.b[q]) * kTN), a0 + (uint64_t)(sch.a[q] * (kTM * kTK / 16)),
+                     b0 + (uint64_t)(sch.b[q] * (kTN * kTK / 16)), make_idesc(kTN * sch.nb[q]), acc);
+            }
+            mma_commit(&empty[st]);
           }
-          mma_commit(&empty[st]);
+          mma_commit(done);
         }
-        mma_commit(done);
       }
       if (!ok) atomicExch(args.err, KMHD_ERR_TIMEOUT);
     }
@@ -742,152 +710,188 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
     const int quad = warp & 3;
     const int row = quad * 32 + lane;
     const double wscale = pow2(8 * (2 * NS - 2 - TG));
-    const unsigned peer = rank ^ 1u;
-    const unsigned peer_recv = pair ? mapa(recv, peer) : 0u;
-    const unsigned peer_rfull = pair ? mapa(rfull, peer) : 0u;
-    const unsigned peer_rempty = pair ? mapa(rempty, peer) : 0u;
+    // 32-byte stores into the rtm records need 32-byte aligned records
+    const bool v4ok = ((reinterpret_cast<uintptr_t>(P.rtm_b) | (uintptr_t)(P.ncb * 16)) & 31) == 0;
     int it = 0;
     bool ok = true;
-    for (int u = ubase; u < nunits; u += ustride, ++it) {
-      const Work w = item(u);
-      const int nk = nk_of(w);
-      const TypeGeo g = type_geo(w.t, P.L, w.m, P.nh);
-      const int grow = w.mt * kTM + row;
-      const int eA = (grow < g.rows) ? S.aexp[S.aeoff[w.m * kNT + w.t] + grow] : 0;
-      // column exponents: lane i holds columns i and 32 + i, broadcast by shuffles
-      const int* eBp = S.bexp + S.beoff[w.m * kNT + w.t] + w.nt * kTN;
-      const int eb_lo = __ldg(eBp + lane), eb_hi = __ldg(eBp + 32 + lane);
-      if (ok && !mbar_wait(done, (unsigned)(it & 1))) ok = false;
-      ok = __all_sync(0xffffffffu, ok);
-      tc_fence_after();
-      double val[kTN];
-      if (nk > 0 && ok) {
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+      for (int h = 0; h < per; ++h, ++it) {
+        const Work w = args.work[u * per + h];
+        const int nk = nk_of(w);
+        const TypeGeo g = type_geo(w.t, P.L, w.m, P.nh);
+        const int grow = w.mt * kTM + row;
+        const int eA = (grow < g.rows) ? S.aexp[S.aeoff[w.m * kNT + w.t] + grow] : 0;
+        // column exponents: lane i holds columns i and 32 + i, broadcast by shuffles
+        const int* eBp = S.bexp + S.beoff[w.m * kNT + w.t] + w.nt * kTN;
+        const int eb_lo = __ldg(eBp + lane), eb_hi = __ldg(eBp + 32 + lane);
+        if (ok && !mbar_wait(done, (unsigned)(it & 1))) ok = false;
+        ok = __all_sync(0xffffffffu, ok);
+        tc_fence_after();
+        double val[kTN];
+        if (nk > 0 && ok) {
 #pragma unroll
-        for (int cb = 0; cb < kTN / 16; ++cb) {
-          int acc[TG + 1][16];
+          for (int cb = 0; cb < kTN / 16; ++cb) {
+            int acc[TG + 1][16];
 #pragma unroll
-          for (int gi = 0; gi <= TG; ++gi)
-            tmem_ld16(tmem + ((unsigned)(quad * 32) << 16) + (unsigned)(gi * kTN + cb * 16), acc[gi]);
-          tmem_wait_ld();
+            for (int gi = 0; gi <= TG; ++gi)
+              tmem_ld16(tmem + ((unsigned)(quad * 32) << 16) + (unsigned)(gi * kTN + cb * 16), acc[gi]);
+            tmem_wait_ld();
 #pragma unroll
-          for (int c = 0; c < 16; ++c) {
-            double v = i2d(acc[0][c]);
+            for (int c = 0; c < 16; ++c) {
+              double v = i2d(acc[0][c]);
 #pragma unroll
-            for (int gi = 1; gi <= TG; ++gi) v = fma(v, 256.0, i2d(acc[gi][c]));
-            const int cc = cb * 16 + c;
-            const int eB = __shfl_sync(0xffffffffu, cc < 32 ? eb_lo : eb_hi, cc & 31);
-            val[cc] = v * (wscale * pow2(eA + eB));
+              for (int gi = 1; gi <= TG; ++gi) v = fma(v, 256.0, i2d(acc[gi][c]));
+              const int cc = cb * 16 + c;
+              const int eB = __shfl_sync(0xffffffffu, cc < 32 ? eb_lo : eb_hi, cc & 31);
+              val[cc] = v * (wscale * pow2(eA + eB));
+            }
           }
-        }
-      } else {
+        } else {
 #pragma unroll
-        for (int c = 0; c < kTN; ++c) val[c] = 0.0;
-      }
-      tc_fence_before();
-      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(sptr(tfree)) : "memory");
+          for (int c = 0; c < kTN; ++c) val[c] = 0.0;
+        }
+        tc_fence_before();
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(sptr(tfree)) : "memory");
 
-      if (!pair) {
-        // forward: scatter into d_rj with the r, r^2, g7, g6 factors.  The
-        // column parameters (radius, field column) are warp-uniform; the two
-        // j offsets of this row's degree are loaded once per tile.
-        const int par = (w.t == 4 || w.t == 6) ? 0 : 1;
-        const int l = w.m + 2 * grow + par;
-        if (grow < g.rows && l <= P.L) {
-          const double g7 = g7_of(l, w.m);
-          const long long jm = (long long)w.m * 2 * (P.L + 1) + l;
-          const long long j0 = P.jmap[jm];
-          const long long j1 = w.m > 0 ? P.jmap[jm + P.L + 1] : 0;
-          const bool s1 = w.m > 0;
-          if (w.t <= 5) {
-            // column c = 8 (r - 8 nt) + 2 f + slot
-            const double g6 = g6_of(l, w.m);
+        if (!pair) {
+          // forward: scatter into d_rj with the r, r^2, g7, g6 factors.  The
+          // column parameters (radius, field column) are warp-uniform; the two
+          // j offsets of this row's degree are loaded once per tile.
+          const int par = (w.t == 4 || w.t == 6) ? 0 : 1;
+          const int l = w.m + 2 * grow + par;
+          if (grow < g.rows && l <= P.L) {
+            const double g7 = g7_of(l, w.m);
+            const long long jm = (long long)w.m * 2 * (P.L + 1) + l;
+            const long long j0 = P.jmap[jm];
+            const long long j1 = w.m > 0 ? P.jmap[jm + P.L + 1] : 0;
+            const bool s1 = w.m > 0;
+            if (w.t <= 5) {
+              // column c = 8 (r - 8 nt) + 2 f + slot
+              const double g6 = g6_of(l, w.m);
 #pragma unroll
-            for (int rr = 0; rr < kTN / 8; ++rr) {
-              const int r = w.nt * (kTN / 8) + rr;
-              if (r >= P.nr) break;
-              const double r1 = P.radius[r];
-              const double fv = r1 * r1 * g7;
-              const long long jr = P.J * (long long)r;
+              for (int rr = 0; rr < kTN / 8; ++rr) {
+                const int r = w.nt * (kTN / 8) + rr;
+                if (r >= P.nr) break;
+                const double r1 = P.radius[r];
+                const double fv = r1 * r1 * g7;
+                const long long jr = P.J * (long long)r;
 #pragma unroll
-              for (int f = 0; f < 4; ++f) {
-                if (f >= P.nvf + P.nsf) break;
-                const double fac = f < P.nvf ? fv : g6;
-                double* dst = args.d_rj + jr + args.ld * args.cols[f];
-                dst[j0] = val[8 * rr + 2 * f] * fac;
-                if (s1) dst[j1] = val[8 * rr + 2 * f + 1] * fac;
+                for (int f = 0; f < 4; ++f) {
+                  if (f >= P.nvf + P.nsf) break;
+                  const double fac = f < P.nvf ? fv : g6;
+                  double* dst = args.d_rj + jr + args.ld * args.cols[f];
+                  dst[j0] = val[8 * rr + 2 * f] * fac;
+                  if (s1) dst[j1] = val[8 * rr + 2 * f + 1] * fac;
+                }
               }
-            }
-          } else {
-            // column c = 4 (r + nrT v) + q, q = 2 (component - 1) + slot
+            } else {
+              // column c = 4 (r + nrT v) + q, q = 2 (component - 1) + slot
 #pragma unroll
-            for (int c4 = 0; c4 < kTN / 4; ++c4) {
-              const int rv = w.nt * (kTN / 4) + c4;
-              const int r = rv % S.nrT, v = rv / S.nrT;
-              if (v >= P.nvf) break;
-              if (r >= P.nr) continue;
-              const double fac = P.radius[r] * g7;
-              double* dst = args.d_rj + P.J * (long long)r + args.ld * (args.cols[v] + 1);
-              dst[j0] = val[4 * c4] * fac;
-              dst[j0 + args.ld] = val[4 * c4 + 2] * fac;
-              if (s1) {
-                dst[j1] = val[4 * c4 + 1] * fac;
-                dst[j1 + args.ld] = val[4 * c4 + 3] * fac;
+              for (int c4 = 0; c4 < kTN / 4; ++c4) {
+                const int rv = w.nt * (kTN / 4) + c4;
+                const int r = rv % S.nrT, v = rv / S.nrT;
+                if (v >= P.nvf) break;
+                if (r >= P.nr) continue;
+                const double fac = P.radius[r] * g7;
+                double* dst = args.d_rj + P.J * (long long)r + args.ld * (args.cols[v] + 1);
+                dst[j0] = val[4 * c4] * fac;
+                dst[j0 + args.ld] = val[4 * c4 + 2] * fac;
+                if (s1) {
+                  dst[j1] = val[4 * c4 + 1] * fac;
+                  dst[j1 + args.ld] = val[4 * c4 + 3] * fac;
+                }
               }
             }
           }
-        }
-      } else {
-        // backward: send my tile to the peer, receive the peer's, emit N or S
-        if (it > 0 && ok && !mbar_wait_cluster(rempty, (unsigned)((it - 1) & 1))) ok = false;
+        } else if (h == 0) {
+          // first tile of a backward pair: keep this thread's row in shared memory
+          double* sr = stash + row * kXS;
 #pragma unroll
-        for (int c = 0; c < kTN; c += 2) st_remote_f64x2(peer_recv + (unsigned)((row * kXS + c) * 8), val[c], val[c + 1]);
-        arrive_remote(peer_rfull);
-        if (ok && !mbar_wait_cluster(rfull, (unsigned)(it & 1))) ok = false;
-        const int th = grow;
-        if (th < P.nh && ok) {
-          const bool pairrow = th < P.nth / 2;
-          const int thout = rank == 0 ? th : P.nth - 1 - th;
-          if (rank == 0 || pairrow) {
-            const long long recb = ((long long)w.m * P.nth + thout) * P.nr * P.ncb * 2;
-            const double* rv = recv + row * kXS;
+          for (int c = 0; c < kTN; c += 2) *reinterpret_cast<double2*>(sr + c) = make_double2(val[c], val[c + 1]);
+        } else {
+          // second tile: north row th gets first + second, south row nth-1-th
+          // first - second; an odd-Ntheta equator row gets the first alone
+          const int th = grow;
+          if (th < P.nh && ok) {
+            const bool pairrow = th < P.nth / 2;
+            const double* sr = stash + row * kXS;
+            const long long rec = (long long)P.ncb * 2;
+            double* baseN = P.rtm_b + ((long long)w.m * P.nth + th) * P.nr * rec;
+            double* baseS = P.rtm_b + ((long long)w.m * P.nth + (P.nth - 1 - th)) * P.nr * rec;
             if (w.t <= 1) {
+              // column c = 4 (r + nrT v) + q: one vector's (theta c, theta s, phi c, phi s)
 #pragma unroll
               for (int c = 0; c < kTN; c += 4) {
                 const int col = w.nt * kTN + c;
                 const int r = (col >> 2) % S.nrT, vv = (col >> 2) / S.nrT;
                 if (vv >= P.nvb || r >= P.nr) continue;
-                double o[4];
+                const double2 a01 = *reinterpret_cast<const double2*>(sr + c);
+                const double2 a23 = *reinterpret_cast<const double2*>(sr + c + 2);
+                double n[4], s_[4];
+                const double a[4] = {a01.x, a01.y, a23.x, a23.y};
 #pragma unroll
-                for (int q = 0; q < 4; ++q)
-                  o[q] = !pairrow ? val[c + q] : (rank == 0 ? val[c + q] + rv[c + q] : rv[c + q] - val[c + q]);
-                double* dst = P.rtm_b + recb + (long long)r * P.ncb * 2 + 4 * vv;
-                reinterpret_cast<double2*>(dst)[0] = make_double2(o[0], o[1]);
-                reinterpret_cast<double2*>(dst)[1] = make_double2(o[2], o[3]);
+                for (int q = 0; q < 4; ++q) {
+                  n[q] = pairrow ? a[q] + val[c + q] : a[q];
+                  s_[q] = a[q] - val[c + q];
+                }
+                double* dN = baseN + (long long)r * rec + 4 * vv;
+                double* dS = baseS + (long long)r * rec + 4 * vv;
+                if (v4ok) {
+                  st_global_v4(dN, n[0], n[1], n[2], n[3]);
+                  if (pairrow) st_global_v4(dS, s_[0], s_[1], s_[2], s_[3]);
+                } else {
+                  reinterpret_cast<double2*>(dN)[0] = make_double2(n[0], n[1]);
+                  reinterpret_cast<double2*>(dN)[1] = make_double2(n[2], n[3]);
+                  if (pairrow) {
+                    reinterpret_cast<double2*>(dS)[0] = make_double2(s_[0], s_[1]);
+                    reinterpret_cast<double2*>(dS)[1] = make_double2(s_[2], s_[3]);
+                  }
+                }
               }
             } else {
+              // column c = 8 (r - 8 nt) + 2 f + slot: radial components and scalars
+              const int nF = P.nvb + P.nsb;
 #pragma unroll
-              for (int c = 0; c < kTN; c += 2) {
-                const int col = w.nt * kTN + c;
-                const int f = (col >> 1) & 3, r = col >> 3;
-                if (r >= P.nr || f >= P.nvb + P.nsb) continue;
-                double o[2];
+              for (int rr = 0; rr < kTN / 8; ++rr) {
+                const int r = w.nt * (kTN / 8) + rr;
+                if (r >= P.nr) break;
+                double* dN = baseN + (long long)r * rec + 4 * P.nvb;
+                double* dS = baseS + (long long)r * rec + 4 * P.nvb;
 #pragma unroll
-                for (int q = 0; q < 2; ++q)
-                  o[q] = !pairrow ? val[c + q] : (rank == 0 ? val[c + q] + rv[c + q] : rv[c + q] - val[c + q]);
-                *reinterpret_cast<double2*>(P.rtm_b + recb + (long long)r * P.ncb * 2 + 4 * P.nvb + 2 * f) =
-                    make_double2(o[0], o[1]);
+                for (int fp = 0; fp < 2; ++fp) {
+                  const int c = 8 * rr + 4 * fp;
+                  if (2 * fp >= nF) break;
+                  const double2 a01 = *reinterpret_cast<const double2*>(sr + c);
+                  const double2 a23 = *reinterpret_cast<const double2*>(sr + c + 2);
+                  const double a[4] = {a01.x, a01.y, a23.x, a23.y};
+                  double n[4], s_[4];
+#pragma unroll
+                  for (int q = 0; q < 4; ++q) {
+                    n[q] = pairrow ? a[q] + val[c + q] : a[q];
+                    s_[q] = a[q] - val[c + q];
+                  }
+                  if (v4ok && 2 * fp + 1 < nF) {
+                    st_global_v4(dN + 4 * fp, n[0], n[1], n[2], n[3]);
+                    if (pairrow) st_global_v4(dS + 4 * fp, s_[0], s_[1], s_[2], s_[3]);
+                  } else {
+                    reinterpret_cast<double2*>(dN + 4 * fp)[0] = make_double2(n[0], n[1]);
+                    if (pairrow) reinterpret_cast<double2*>(dS + 4 * fp)[0] = make_double2(s_[0], s_[1]);
+                    if (2 * fp + 1 < nF) {
+                      reinterpret_cast<double2*>(dN + 4 * fp)[1] = make_double2(n[2], n[3]);
+                      if (pairrow) reinterpret_cast<double2*>(dS + 4 * fp)[1] = make_double2(s_[2], s_[3]);
+                    }
+                  }
+                }
               }
             }
           }
         }
-        arrive_remote(peer_rempty);
       }
     }
     if (!ok) atomicExch(args.err, KMHD_ERR_TIMEOUT);
   }
   tc_fence_before();
   __syncthreads();
-  if (pair) cluster_sync();  // no CTA leaves while its peer may still touch its shared memory
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;\n" ::"r"(tmem));
 }
 
@@ -925,43 +929,24 @@ size_t gemm_smem(int ns) {
 }
 
 template <int NS, int TG>
-cudaError_t launch_gemm(const GemmArgs& a, bool cluster, cudaStream_t st) {
+cudaError_t launch_gemm(const GemmArgs& a, cudaStream_t st) {
   auto kern = k_split_gemm<NS, TG>;
   const size_t smem = gemm_smem(NS);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  if (cluster) {
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 0);
-    (void)e;
-  }
   int dev = 0, nsm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const int units = cluster ? a.nwork / 2 : a.nwork;
-  int grid = cluster ? 2 * std::min(units, nsm / 2) : std::min(units, nsm);
+  const int units = a.pair ? a.nwork / 2 : a.nwork;
+  const int grid = std::min(units, nsm);
   if (grid <= 0) return cudaSuccess;
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(kGemmWarps * 32);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  int na = 0;
-  if (cluster) {
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = 2;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    na = 1;
-  }
-  cfg.attrs = attr;
-  cfg.numAttrs = na;
-  return cudaLaunchKernelEx(&cfg, kern, a);
+  kern<<<grid, kGemmWarps * 32, smem, st>>>(a);
+  return cudaGetLastError();
 }
 
-cudaError_t run_gemm(const SplitState* s, const GemmArgs& a, bool cluster, cudaStream_t st) {
-  if (s->ns == 6) return launch_gemm<6, 6>(a, cluster, st);
-  return launch_gemm<4, 3>(a, cluster, st);
+cudaError_t run_gemm(const SplitState* s, const GemmArgs& a, cudaStream_t st) {
+  if (s->ns == 6) return launch_gemm<6, 6>(a, st);
+  return launch_gemm<4, 3>(a, st);
 }
 
 }  // namespace
@@ -1125,7 +1110,7 @@ int split_bwd(SplitState* s, const Plan& p, int, const double* d_rj, long long l
   a.ld = 0;
   a.cols = nullptr;
   a.err = s->err;
-  if (s->nwork_b > 0 && run_gemm(s, a, true, st) != cudaSuccess) return KMHD_ERR_CUDA;
+  if (s->nwork_b > 0 && run_gemm(s, a, st) != cudaSuccess) return KMHD_ERR_CUDA;
   return KMHD_OK;
 }
 
@@ -1149,7 +1134,7 @@ int split_fwd(SplitState* s, const Plan& p, double* d_rj, long long ld, const in
   a.ld = ld;
   a.cols = cols;
   a.err = s->err;
-  if (s->nwork_f > 0 && run_gemm(s, a, false, st) != cudaSuccess) return KMHD_ERR_CUDA;
+  if (s->nwork_f > 0 && run_gemm(s, a, st) != cudaSuccess) return KMHD_ERR_CUDA;
   return KMHD_OK;
 }
 
