@@ -244,7 +244,7 @@ __global__ void k_a_slices(Plan P, SliceTabs S, int t) {
 // quantity q (8 columns), for each field f < 4: types 2/3 slots (4 columns);
 // forward: types 4/5 (field f, slot) and types 6/7 (vector v, quantity q).
 constexpr int kGrpCols = 16;  // derived columns of one slicer field group (at most 4 fields x 2 slots x 2 types)
-constexpr int kSlab = 288;    // per-slice staging bytes of one 256-byte tile block (k halves 144 apart)
+constexpr int kSlab = 320;    // per-slice staging bytes of one 256-byte tile block (k halves 192 apart)
 
 struct ColRef {
   int t, col;     // operand type and global column index
@@ -280,21 +280,42 @@ __device__ __forceinline__ ColRef colref_fwd(const Plan& P, const SliceTabs& S, 
 // the remaining high part (|d[0]| <= 64).  The value is split exactly into
 // hi 2^24 + lo with both halves in int32, so the digit loop runs on 32-bit
 // integers.
+// Balanced base-256 digits of round(v[i]), |round(v[i])| < 2^(8 NS - 2), for four
+// values, packed as bytes (value i in byte i) into one word per slice; w[NS-1]
+// holds the least significant digits.  A balanced digit's two's-complement
+// byte is the low byte of the running value x, and the next value is
+// (x + 128) >> 8.  Each value is split exactly into hi 2^24 + lo with both
+// halves in int32; the top digit (|d| <= 64) is what remains of hi.
+__device__ __forceinline__ uint32_t pack4(int b0, int b1, int b2, int b3) {
+  return __byte_perm(__byte_perm(b0, b1, 0x0040), __byte_perm(b2, b3, 0x0040), 0x5410);
+}
 template <int NS>
-__device__ __forceinline__ void split_digits(double v, int (&d)[NS]) {
-  const double x = rint(v);
-  const double hi = rint(x * 0x1p-24);
-  int lo = (int)fma(-hi, 0x1p24, x);
-  int h = (int)hi;
+__device__ __forceinline__ void digits4(const double (&v)[4], uint32_t (&w)[NS]) {
+  int lo[4], hi[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const double x = rint(v[i]);
+    const double h = rint(x * 0x1p-24);
+    lo[i] = (int)fma(-h, 0x1p24, x);
+    hi[i] = (int)h;
+  }
 #pragma unroll
   for (int s = NS - 1; s >= 1; --s) {
-    int& src = (s >= NS - 3) ? lo : h;
-    const int dd = (int)((unsigned)src << 24) >> 24;
-    d[s] = dd;
-    src = (src - dd) >> 8;
-    if (s == NS - 3) h += lo;
+    if (s >= NS - 3) {
+      w[s] = pack4(lo[0], lo[1], lo[2], lo[3]);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) lo[i] = (lo[i] + 128) >> 8;
+      if (s == NS - 3) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) hi[i] += lo[i];
+      }
+    } else {
+      w[s] = pack4(hi[0], hi[1], hi[2], hi[3]);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) hi[i] = (hi[i] + 128) >> 8;
+    }
   }
-  d[0] = h;
+  w[0] = pack4(hi[0], hi[1], hi[2], hi[3]);
 }
 
 // Slicer: one CTA per (field group z, radius r, order m).  Backward groups:
@@ -453,7 +474,10 @@ __global__ void __launch_bounds__(256) k_slice_mr(Plan P, SliceTabs S, const dou
     const int t = ctype(c);
     const int kp = (t == t0) ? ga.kpad : gb.kpad;
     double mx = 0.0;
-    for (int k = lane; k < kp; k += 32) mx = fmax(mx, fabs(X[c * kst + k]));
+    for (int k = 2 * lane; k < kp; k += 64) {
+      const double2 x2 = *reinterpret_cast<const double2*>(X + c * kst + k);
+      mx = fmax(mx, fmax(fabs(x2.x), fabs(x2.y)));
+    }
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     if (lane == 0) {
       const int e = mx > 0.0 ? exp_above(mx) : 0;
@@ -464,17 +488,19 @@ __global__ void __launch_bounds__(256) k_slice_mr(Plan P, SliceTabs S, const dou
     }
   }
   __syncthreads();
-  // ---- pass 3: digits.  Work item = (column group, 32-wide K chunk), lane = k.
-  // A column group is the set of columns that share one 256-byte block of a
+  // ---- pass 3: digits.  Work item = (column group, 32-wide K chunk).  A
+  // column group is the set of columns that share one 256-byte block of a
   // core-matrix tile: 8 rows (one radius of types 2..5) or 4 rows (one radius
-  // and vector of types 0/1/6/7).  The warp assembles the block's NS slices
-  // in shared memory (k halves 144 bytes apart, so the byte stores of the two
-  // half-warps fall in different banks) and writes them out with 16-byte
-  // stores, 256 (or 2 x 64) contiguous bytes per slice.
+  // and vector of types 0/1/6/7).  Lane l cuts 4 consecutive k (4 (l % 8) ..)
+  // of block row l / 8 (and l / 8 + 4 in 8-row groups) into one word per
+  // slice; the warp assembles the block's NS slices in shared memory (k halves
+  // 192 bytes apart, so the word stores hit 32 distinct banks) and writes them
+  // out with 16-byte stores, 256 (or 2 x 64) contiguous bytes per slice.
   unsigned char* wb = reinterpret_cast<unsigned char*>(
                           (reinterpret_cast<uintptr_t>(colexp + kGrpCols) + 15) & ~static_cast<uintptr_t>(15)) +
                       warp * (NS * kSlab);
   int item0 = 0;
+  const int q4 = lane >> 3, kq = 4 * (lane & 7);
   for (int gi = g0; gi < g0 + 2; ++gi) {
     const int t = t0 + (gi - g0);
     const bool eight = !vgrp;  // 8-row groups: radius blocks of types 2..5
@@ -484,24 +510,26 @@ __global__ void __launch_bounds__(256) k_slice_mr(Plan P, SliceTabs S, const dou
     const int nt = gcol / kTN, blk = (gcol % kTN) >> 3, rbase = gcol & 7;
     signed char* base = S.B + S.boff[m * kNT + t];
     for (int kc = ((warp - item0) % nw + nw) % nw; kc < nkc; kc += nw) {
-      const int k = kc * kTK + lane;
-      const int koff = (lane >> 4) * 144 + (lane & 15);
-      const int ncg = eight ? 8 : 4;
-      for (int q = 0; q < ncg; ++q) {
+      const int k = kc * kTK + kq;
+      for (int q = q4; q < (eight ? 8 : 4); q += 4) {
         // local column of block row rbase + q
         int c = -1;
         if (!eight) c = 4 * (t - t0) + q;
         else if ((q >> 1) < nF) c = 4 * (q >> 1) + 2 * (t - t0) + (q & 1);
-        int dg[NS];
+        uint32_t wd[NS];
         if (c >= 0 && colmax[c] > 0.0) {
-          split_digits<NS>(X[c * kst + k] * pow2((8 * NS - 2) - colexp[c]), dg);
+          const double sc = pow2((8 * NS - 2) - colexp[c]);
+          const double2 x01 = *reinterpret_cast<const double2*>(X + c * kst + k);
+          const double2 x23 = *reinterpret_cast<const double2*>(X + c * kst + k + 2);
+          const double xv[4] = {x01.x * sc, x01.y * sc, x23.x * sc, x23.y * sc};
+          digits4<NS>(xv, wd);
         } else {
 #pragma unroll
-          for (int s2 = 0; s2 < NS; ++s2) dg[s2] = 0;
+          for (int s2 = 0; s2 < NS; ++s2) wd[s2] = 0u;
         }
-        const int o = koff + (rbase + q) * 16;
+        const int o = (kq >> 4) * 192 + (rbase + q) * 16 + (kq & 15);
 #pragma unroll
-        for (int s2 = 0; s2 < NS; ++s2) wb[s2 * kSlab + o] = (unsigned char)dg[s2];
+        for (int s2 = 0; s2 < NS; ++s2) *reinterpret_cast<uint32_t*>(wb + s2 * kSlab + o) = wd[s2];
       }
       __syncwarp();
       signed char* dst0 = base + (long long)(nt * nkc + kc) * NS * (kTN * kTK) + blk * 256;
@@ -509,13 +537,13 @@ __global__ void __launch_bounds__(256) k_slice_mr(Plan P, SliceTabs S, const dou
         for (int u = lane; u < NS * 16; u += 32) {
           const int s2 = u >> 4, h = (u >> 3) & 1, rr = u & 7;
           *reinterpret_cast<uint4*>(dst0 + s2 * (kTN * kTK) + h * 128 + rr * 16) =
-              *reinterpret_cast<const uint4*>(wb + s2 * kSlab + h * 144 + rr * 16);
+              *reinterpret_cast<const uint4*>(wb + s2 * kSlab + h * 192 + rr * 16);
         }
       } else {
         for (int u = lane; u < NS * 8; u += 32) {
           const int s2 = u >> 3, h = (u >> 2) & 1, rr = rbase + (u & 3);
           *reinterpret_cast<uint4*>(dst0 + s2 * (kTN * kTK) + h * 128 + rr * 16) =
-              *reinterpret_cast<const uint4*>(wb + s2 * kSlab + h * 144 + rr * 16);
+              *reinterpret_cast<const uint4*>(wb + s2 * kSlab + h * 192 + rr * 16);
         }
       }
       __syncwarp();
