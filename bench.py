@@ -235,12 +235,16 @@ def main():
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     stage = {"leg_bwd": 0.0, "fft_nl": 0.0, "leg_fwd": 0.0}
+    kern = {"slice_bwd": 0.0, "gemm_bwd": 0.0, "fft_nl": 0.0, "slice_fwd": 0.0, "gemm_fwd": 0.0}
     e0.record(stream)
     for _ in range(args.steps):
         tr.nonlinear_cycle(d_in, d_out)
         t = tr.last_timing()
         for k in stage:
             stage[k] += t[k]
+        t = tr.kernel_timing()
+        for k in kern:
+            kern[k] += t[k]
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
@@ -250,6 +254,8 @@ def main():
     value = ws * args.steps / (ms_total * 1e-3)
     for k in stage:
         stage[k] /= args.steps
+    for k in kern:
+        kern[k] /= args.steps
 
     # FP64 GPU cycle on the same input: the bar of the split tier (speed and error)
     extra = {}
@@ -276,24 +282,34 @@ def main():
                  "rel_err_vs_fp64_per_field": err, "rel_err_max": max(err)}
         del ref64, out64
 
-    # roofline of the dominant kernel (the backward Legendre GEMM)
+    # roofline of the dominant kernel: the Legendre GEMM (split tiers: the one
+    # tcgen05 kernel, launched once per direction; FP64: the slower of the two
+    # DMMA kernels).  Durations are CUDA events on the launching stream.
     peaks, psrc = load_peaks()
-    flops_bwd = 2.0 * cfg.nh * cfg.J * cfg.nr * (5 * cfg.nvb + cfg.nsb)
+    flops = 2.0 * cfg.nh * cfg.J * cfg.nr * (5 * cfg.nvb + cfg.nsb)  # per direction (bwd = fwd here)
     if tier == "fp64":
+        which = "gemm_fwd" if kern["gemm_fwd"] >= kern["gemm_bwd"] else "gemm_bwd"
+        dur = kern[which]
         pk = ctypes_probe(lib, local)
-        roof = {"bound": "tensor", "achieved": flops_bwd / (stage["leg_bwd"] * 1e-3) / 1e12,
-                "peak": pk, "unit": "TFLOP/s",
+        roof = {"bound": "tensor", "achieved": flops / (dur * 1e-3) / 1e12, "peak": pk, "unit": "TFLOP/s",
                 "peak_source": "FP64 tensor pipe measured in-process (DMMA chain probe); "
-                               "MEASURED_PEAKS.json carries no FP64 figure"}
+                               "MEASURED_PEAKS.json carries no FP64 figure",
+                "kernel": "k_leg_fwd_f64" if which == "gemm_fwd" else "k_leg_bwd_f64"}
     else:
+        dur = 0.5 * (kern["gemm_bwd"] + kern["gemm_fwd"])
         pk = 2.0 * peaks["bf16_tflops"]
-        roof = {"bound": "tensor", "achieved": flops_bwd / (stage["leg_bwd"] * 1e-3) / 1e12,
-                "peak": pk, "unit": "TFLOP/s",
-                "peak_source": f"2 x bf16 burst of {psrc} MEASURED_PEAKS.json (INT8:BF16 dense = 2:1)"}
+        execd = split_executed_ops(cfg, 26 if tier == "split" else 10)
+        roof = {"bound": "tensor", "achieved": flops / (dur * 1e-3) / 1e12, "peak": pk, "unit": "TFLOP/s",
+                "peak_source": f"INT8 dense = 2 x bf16 burst of {psrc} MEASURED_PEAKS.json",
+                "kernel": "k_split_gemm",
+                "achieved_is": "useful FP64-equivalent flop/s (2*Nh*J*Nr*(5nv+ns) per launch)",
+                "executed_int8_tops": execd / (dur * 1e-3) / 1e12,
+                "executed_frac": execd / (dur * 1e-3) / 1e12 / pk,
+                "overhead_factor": execd / flops}
     roof["frac"] = roof["achieved"] / roof["peak"] if roof["peak"] else None
-    roof["traffic"] = read_traffic(tier)
-    roof["kernel"] = "Legendre backward GEMM"
-    roof["algorithmic_flops_per_launch"] = flops_bwd
+    roof["traffic"] = read_traffic(roof["kernel"], cfg.name)
+    roof["algorithmic_flops_per_launch"] = flops
+    roof["ms_per_launch"] = dur
 
     # end to end through the public API with pinned host buffers
     e2e = None
@@ -333,7 +349,7 @@ def main():
                    "fields_bwd": "u,omega,B + T", "fields_fwd": "omega x u, u x B, u T + u.omega",
                    "parallelism": f"radial-instance x{ws} (no collective)",
                    "l2": "inputs larger than L2 (d_rj 5.4 GB, rtm 16 GB per direction)"},
-        "stages_ms": stage, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+        "stages_ms": stage, "kernels_ms": kern, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": launches * args.steps, "clocks": clk,
     }
     line.update(extra)
@@ -356,15 +372,37 @@ def ctypes_probe(lib, dev):
     return v.value if f(dev, ctypes.byref(v)) == 0 else None
 
 
-def read_traffic(tier):
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", f"leg_bwd_{tier}_traffic.txt")
+def read_traffic(kernel, workload):
+    """DRAM bytes (read + write) per launch of the kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_{workload}_dram.txt")
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.startswith("traffic_bytes_per_launch_full:"):
+        if line.startswith("traffic_bytes_per_launch:"):
             return float(line.split(":")[1])
     return None
+
+
+def split_executed_ops(cfg, nprod):
+    """INT8 ops (2 per MAC) one launch of the split GEMM issues, averaged over
+    the two directions: every (m, type, 128-row tile, 64-column tile, 32-deep K
+    chunk) runs nprod slice products of 128 x 64 x 32."""
+    pad = lambda x, q: (x + q - 1) // q * q  # noqa: E731
+    L, nh, nr = cfg.ltr, cfg.nh, cfg.nr
+    nrT, nrR = pad(nr, 16), pad(nr, 8)
+    tot = 0
+    for m in range(L + 1):
+        ke, ko = (L - m) // 2 + 1, (L - m + 1) // 2
+        kep, kop, nhp = pad(ke, 32), pad(ko, 32), pad(nh, 32)
+        geo = {0: (nh, kop + kep, 4 * cfg.nvb * nrT), 1: (nh, kep + kop, 4 * cfg.nvb * nrT),
+               2: (nh, kep, 8 * nrR), 3: (nh, kop, 8 * nrR),
+               4: (ke, nhp, 8 * nrR), 5: (ko, nhp, 8 * nrR),
+               6: (ke, 2 * nhp, 4 * cfg.nvf * nrT), 7: (ko, 2 * nhp, 4 * cfg.nvf * nrT)}
+        for t, (rows, kp, ncol) in geo.items():
+            if rows == 0 or ncol == 0:
+                continue
+            tot += (pad(rows, 128) // 128) * (pad(ncol, 64) // 64) * (kp // 32)
+    return tot * nprod * 128 * 64 * 32 * 2 / 2.0
 
 
 if __name__ == "__main__":

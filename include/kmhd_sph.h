@@ -135,6 +135,14 @@ int kmhd_sph_batch_cycle(kmhd_sph **handles, int32_t n, const double *const *d_r
  * [3] whole call.  Labels as in MHD_src/IO/init_sph_MHD_elapsed_label.f90:38-84. */
 int kmhd_sph_last_timing(kmhd_sph *handle, double *ms4);
 
+/* Per-launch times in ms (CUDA events on the handle's stream) of the last
+ * kmhd_sph_cycle: [0] backward pack (FP64) or slicer (split tiers), [1]
+ * backward Legendre GEMM, [2] FFT + products + FFT, [3] forward slicer (0 for
+ * FP64), [4] forward Legendre GEMM.  KMHD_ERR_STATE if the last call was not
+ * a cycle.  Finer-grained than the reference's elapsed labels
+ * (MHD_src/IO/init_sph_MHD_elapsed_label.f90:38-84). */
+int kmhd_sph_last_kernel_timing(kmhd_sph *handle, double *ms5);
+
 /* Copies the device Gauss colatitudes/weights [nth] and the hemisphere
  * P / dP tables of order m ([nth_hemi x (L-m+1)], rows theta, cols l) to host
  * arrays, for parity checks of the set-up stage. */

@@ -44,7 +44,10 @@ struct kmhd_sph {
   SplitState* split = nullptr;
   // timing
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev_mid[2] = {nullptr, nullptr};  // after the bwd pack/slicer, after the fwd slicer
   double last_ms[4] = {0, 0, 0, 0};
+  double last_kernel_ms[5] = {0, 0, 0, 0, 0};
+  bool kernel_timed = false;
 };
 
 namespace {
@@ -175,6 +178,8 @@ int kmhd_sph_destroy(kmhd_sph* h) {
   for (void* p : h->allocs) cudaFree(p);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
+  for (auto& e : h->ev_mid)
+    if (e) cudaEventDestroy(e);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
   return KMHD_OK;
@@ -205,6 +210,8 @@ int kmhd_sph_create(const kmhd_sph_desc* d, kmhd_sph** out) {
     return fail(KMHD_ERR_CUDA);
   h->stream = h->own_stream;
   for (auto& e : h->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return fail(KMHD_ERR_CUDA);
+  for (auto& e : h->ev_mid)
     if (cudaEventCreate(&e) != cudaSuccess) return fail(KMHD_ERR_CUDA);
 
   Plan& p = h->plan;
@@ -413,17 +420,19 @@ int timed_begin(kmhd_sph* h) {
 int run_bwd_spectral(kmhd_sph* h, const double* d_rj, int64_t ld) {
   const Plan& p = h->plan;
   if (h->split) {
-    int st = split_bwd(h->split, p, h->nlc_max, d_rj, ld, h->cols_b_d, h->stream);
+    int st = split_bwd(h->split, p, h->nlc_max, d_rj, ld, h->cols_b_d, h->stream, h->ev_mid[0]);
     return st;
   }
   KCHECK(launch_pack_b(p, h->nlc_max, d_rj, ld, h->cols_b_d, p.nvb, p.nsb, h->stream));
+  KCHECK(cudaEventRecord(h->ev_mid[0], h->stream));
   KCHECK(launch_leg_bwd_f64(p, h->stream));
   return KMHD_OK;
 }
 
 int run_fwd_spectral(kmhd_sph* h, double* d_rj, int64_t ld) {
   const Plan& p = h->plan;
-  if (h->split) return split_fwd(h->split, p, d_rj, ld, h->cols_f_d, h->stream);
+  if (h->split) return split_fwd(h->split, p, d_rj, ld, h->cols_f_d, h->stream, h->ev_mid[1]);
+  KCHECK(cudaEventRecord(h->ev_mid[1], h->stream));  // the FP64 forward GEMM packs its operands itself
   KCHECK(launch_leg_fwd_f64(p, d_rj, ld, h->cols_f_d, h->stream));
   return KMHD_OK;
 }
@@ -443,6 +452,21 @@ int finish_timing(kmhd_sph* h) {
   h->last_ms[1] = b;
   h->last_ms[2] = c;
   h->last_ms[3] = t;
+  h->kernel_timed = false;
+  return KMHD_OK;
+}
+
+// Per-launch times of a full cycle: bwd pack/slicer, bwd GEMM, FFT + products,
+// fwd slicer (0 for the FP64 tier), fwd GEMM.
+int finish_kernel_timing(kmhd_sph* h) {
+  float k[5] = {0, 0, 0, 0, 0};
+  KCHECK(cudaEventElapsedTime(&k[0], h->ev[0], h->ev_mid[0]));
+  KCHECK(cudaEventElapsedTime(&k[1], h->ev_mid[0], h->ev[1]));
+  KCHECK(cudaEventElapsedTime(&k[2], h->ev[1], h->ev[2]));
+  KCHECK(cudaEventElapsedTime(&k[3], h->ev[2], h->ev_mid[1]));
+  KCHECK(cudaEventElapsedTime(&k[4], h->ev_mid[1], h->ev[3]));
+  for (int i = 0; i < 5; ++i) h->last_kernel_ms[i] = k[i];
+  h->kernel_timed = true;
   return KMHD_OK;
 }
 
@@ -570,7 +594,15 @@ int kmhd_sph_cycle(kmhd_sph* h, const double* d_rj_in, int64_t ld_in, const int3
     }
   }
   KCHECK(cudaStreamSynchronize(h->stream));
-  return finish_timing(h);
+  if ((st = finish_timing(h))) return st;
+  return finish_kernel_timing(h);
+}
+
+int kmhd_sph_last_kernel_timing(kmhd_sph* h, double* ms5) {
+  if (!h || !ms5) return KMHD_ERR_ARG;
+  if (!h->kernel_timed) return KMHD_ERR_STATE;
+  std::memcpy(ms5, h->last_kernel_ms, sizeof(h->last_kernel_ms));
+  return KMHD_OK;
 }
 
 int kmhd_sph_get_tables(kmhd_sph* h, int32_t m, double* colat, double* weight, double* P, double* dP) {

@@ -557,11 +557,12 @@ __global__ void __launch_bounds__(256) k_slice_mr(Plan P, SliceTabs S, const dou
 //   warp 0 (one lane): issues the tcgen05.mma slice products into TMEM
 //   warp 1 (one lane): streams pre-laid-out slice tiles with bulk copies into a
 //                      stage ring, running ahead across tiles
-//   warps 2..5:        epilogue (TMEM -> FP64 recombination -> output)
-// One tile = (m, type, m-tile, n-tile).  The backward work list pairs the two
-// parity tiles (types 0/1 or 2/3) of one output tile; one CTA runs them back to
-// back, keeps the first in shared memory and emits the north row
-// (first + second) and the south row (first - second) of the rtm records.
+//   warps 2..9:        epilogue (TMEM -> FP64 recombination -> output), two per TMEM lane quadrant
+// One tile = (m, type, m-tile, n-tile).  The work lists pair the two parity
+// tiles (types 0/1, 2/3, 4/5 or 6/7) of one output tile; one CTA runs them back
+// to back and keeps the first in shared memory.  Backward it then emits the
+// north row (first + second) and the south row (first - second) of the rtm
+// records; forward it scatters both degrees l and l + 1 of each row.
 struct Work {
   int m, t, mt, nt;
 };
@@ -571,15 +572,16 @@ struct GemmArgs {
   SliceTabs S;
   const Work* work;
   int nwork;
-  int pair;        // 1: backward tile pairs
+  int pair;        // 1: backward (rtm records out), 0: forward (d_rj out)
   double* d_rj;    // forward output
   long long ld;
   const int* cols;
   int* err;        // device error word
 };
 
-constexpr int kGemmWarps = 6;
-constexpr int kEpiThreads = 128;
+constexpr int kGemmWarps = 10;     // MMA issuer, bulk-copy producer, 8 epilogue warps
+constexpr int kEpiThreads = 256;
+constexpr int kHalf = kTN / 2;     // columns recombined by one epilogue warp
 constexpr int kRing = 4;           // stage ring depth
 constexpr int kXS = kTN + 2;       // stash row stride (doubles): 16-byte rows, conflict-free v2 accesses
 
@@ -639,7 +641,7 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
   extern __shared__ __align__(1024) unsigned char sm[];
   constexpr int A_BYTES = NS * kTM * kTK, B_BYTES = NS * kTN * kTK;
   constexpr int STAGE = A_BYTES + B_BYTES;
-  double* stash = reinterpret_cast<double*>(sm + kRing * STAGE);  // [kTM][kXS]: first tile of a backward pair
+  double* stash = reinterpret_cast<double*>(sm + kRing * STAGE);  // [kTM][kXS]: first tile of a pair
   unsigned long long* bars = reinterpret_cast<unsigned long long*>(stash + kTM * kXS);
   unsigned long long* full = bars;              // [kRing]
   unsigned long long* empty = bars + kRing;     // [kRing]
@@ -650,9 +652,9 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
   const Plan& P = args.P;
   const SliceTabs& S = args.S;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // backward units are (first, second) tile pairs run back to back by one CTA
-  const bool pair = args.pair != 0;
-  const int per = pair ? 2 : 1;
+  // units are (even, odd) parity tile pairs run back to back by one CTA
+  const bool bwd = args.pair != 0;
+  const int per = 2;
   const int nunits = args.nwork / per;
 
   if (threadIdx.x == 0) {
@@ -675,7 +677,7 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
 
   auto nk_of = [&](const Work& w) -> int {
     const TypeGeo g = type_geo(w.t, P.L, w.m, P.nh);
-    return g.rows > 0 ? g.kpad / kTK : 0;
+    return (g.rows > 0 && w.mt * kTM < g.rpad) ? g.kpad / kTK : 0;
   };
 
   if (warp == 1) {
@@ -734,8 +736,11 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
       if (!ok) atomicExch(args.err, KMHD_ERR_TIMEOUT);
     }
   } else {
-    // ---- epilogue warps 2..5: TMEM lane quadrant = warp % 4
+    // ---- epilogue warps 2..9: TMEM lane quadrant = warp % 4, two warps per
+    // quadrant, each recombining one 32-column half of the tile
     const int quad = warp & 3;
+    const int half = (warp - 2) >> 2;
+    const int cbase = kHalf * half;
     const int row = quad * 32 + lane;
     const double wscale = pow2(8 * (2 * NS - 2 - TG));
     // 32-byte stores into the rtm records need 32-byte aligned records
@@ -749,108 +754,137 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
         const TypeGeo g = type_geo(w.t, P.L, w.m, P.nh);
         const int grow = w.mt * kTM + row;
         const int eA = (grow < g.rows) ? S.aexp[S.aeoff[w.m * kNT + w.t] + grow] : 0;
-        // column exponents: lane i holds columns i and 32 + i, broadcast by shuffles
-        const int* eBp = S.bexp + S.beoff[w.m * kNT + w.t] + w.nt * kTN;
-        const int eb_lo = __ldg(eBp + lane), eb_hi = __ldg(eBp + 32 + lane);
+        // column exponents: lane i holds column cbase + i, broadcast by shuffles
+        const int eBl = __ldg(S.bexp + S.beoff[w.m * kNT + w.t] + w.nt * kTN + cbase + lane);
         if (ok && !mbar_wait(done, (unsigned)(it & 1))) ok = false;
         ok = __all_sync(0xffffffffu, ok);
         tc_fence_after();
-        double val[kTN];
+        double val[kHalf];  // columns cbase .. cbase + 31
         if (nk > 0 && ok) {
 #pragma unroll
-          for (int cb = 0; cb < kTN / 16; ++cb) {
+          for (int cb = 0; cb < kHalf / 16; ++cb) {
             int acc[TG + 1][16];
 #pragma unroll
             for (int gi = 0; gi <= TG; ++gi)
-              tmem_ld16(tmem + ((unsigned)(quad * 32) << 16) + (unsigned)(gi * kTN + cb * 16), acc[gi]);
+              tmem_ld16(tmem + ((unsigned)(quad * 32) << 16) + (unsigned)(gi * kTN + cbase + cb * 16), acc[gi]);
             tmem_wait_ld();
 #pragma unroll
             for (int c = 0; c < 16; ++c) {
-              double v = i2d(acc[0][c]);
+              // sum_g acc[g] 256^(TG-g): the four lowest groups combine exactly in
+              // int64 (< 2^51), the higher ones exactly in FP64 (< 2^43); one rounding
+              constexpr int G0 = TG >= 3 ? TG - 3 : 0;
+              long long lo = acc[G0][c];
 #pragma unroll
-              for (int gi = 1; gi <= TG; ++gi) v = fma(v, 256.0, i2d(acc[gi][c]));
-              const int cc = cb * 16 + c;
-              const int eB = __shfl_sync(0xffffffffu, cc < 32 ? eb_lo : eb_hi, cc & 31);
-              val[cc] = v * (wscale * pow2(eA + eB));
+              for (int gi = G0 + 1; gi <= TG; ++gi) lo = lo * 256 + acc[gi][c];
+              double v = (double)lo;
+              if constexpr (G0 > 0) {
+                double hi = i2d(acc[0][c]);
+#pragma unroll
+                for (int gi = 1; gi < G0; ++gi) hi = fma(hi, 256.0, i2d(acc[gi][c]));
+                v = fma(hi, pow2(8 * (TG - G0 + 1)), v);
+              }
+              const int eB = __shfl_sync(0xffffffffu, eBl, cb * 16 + c);
+              val[cb * 16 + c] = v * (wscale * pow2(eA + eB));
             }
           }
         } else {
 #pragma unroll
-          for (int c = 0; c < kTN; ++c) val[c] = 0.0;
+          for (int c = 0; c < kHalf; ++c) val[c] = 0.0;
         }
         tc_fence_before();
         asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(sptr(tfree)) : "memory");
 
-        if (!pair) {
-          // forward: scatter into d_rj with the r, r^2, g7, g6 factors.  The
-          // column parameters (radius, field column) are warp-uniform; the two
-          // j offsets of this row's degree are loaded once per tile.
-          const int par = (w.t == 4 || w.t == 6) ? 0 : 1;
-          const int l = w.m + 2 * grow + par;
-          if (grow < g.rows && l <= P.L) {
-            const double g7 = g7_of(l, w.m);
-            const long long jm = (long long)w.m * 2 * (P.L + 1) + l;
-            const long long j0 = P.jmap[jm];
-            const long long j1 = w.m > 0 ? P.jmap[jm + P.L + 1] : 0;
-            const bool s1 = w.m > 0;
-            if (w.t <= 5) {
-              // column c = 8 (r - 8 nt) + 2 f + slot
-              const double g6 = g6_of(l, w.m);
+        if (h == 0) {
+          // first tile of the pair: keep this thread's half row in shared memory
+          double* sr = stash + row * kXS + cbase;
 #pragma unroll
-              for (int rr = 0; rr < kTN / 8; ++rr) {
-                const int r = w.nt * (kTN / 8) + rr;
-                if (r >= P.nr) break;
-                const double r1 = P.radius[r];
-                const double fv = r1 * r1 * g7;
-                const long long jr = P.J * (long long)r;
+          for (int c = 0; c < kHalf; c += 2) *reinterpret_cast<double2*>(sr + c) = make_double2(val[c], val[c + 1]);
+        } else if (!bwd) {
+          // forward pair: row i carries degree l0 = m + 2 (128 mt + i) in the even
+          // tile (stash) and l0 + 1 in the odd tile (val).  Scatter both into d_rj
+          // with the r, r^2, g7, g6 factors; neighbouring lanes write neighbouring
+          // j, so every 32-byte sector is completed by this warp.  The column
+          // parameters (radius, field column) are warp-uniform.
+          const double* sr = stash + row * kXS + cbase;
+          const TypeGeo ge = type_geo(w.t - 1, P.L, w.m, P.nh);
+          const int l0 = w.m + 2 * grow, l1 = l0 + 1;
+          const bool ok0 = grow < ge.rows && l0 <= P.L, ok1 = grow < g.rows && l1 <= P.L;
+          const bool s1 = w.m > 0;
+          const long long jm = (long long)w.m * 2 * (P.L + 1);
+          const long long j00 = ok0 ? P.jmap[jm + l0] : 0, j01 = (ok0 && s1) ? P.jmap[jm + P.L + 1 + l0] : 0;
+          const long long j10 = ok1 ? P.jmap[jm + l1] : 0, j11 = (ok1 && s1) ? P.jmap[jm + P.L + 1 + l1] : 0;
+          const double g70 = g7_of(l0, w.m), g71 = g7_of(l1, w.m);
+          if (w.t == 5) {
+            // column c = 8 (r - 8 nt) + 2 f + slot
+            const double g60 = g6_of(l0, w.m), g61 = g6_of(l1, w.m);
 #pragma unroll
-                for (int f = 0; f < 4; ++f) {
-                  if (f >= P.nvf + P.nsf) break;
-                  const double fac = f < P.nvf ? fv : g6;
-                  double* dst = args.d_rj + jr + args.ld * args.cols[f];
-                  dst[j0] = val[8 * rr + 2 * f] * fac;
-                  if (s1) dst[j1] = val[8 * rr + 2 * f + 1] * fac;
+            for (int rr = 0; rr < kHalf / 8; ++rr) {
+              const int r = w.nt * (kTN / 8) + cbase / 8 + rr;
+              if (r >= P.nr) break;
+              const double r1 = P.radius[r];
+              const long long jr = P.J * (long long)r;
+#pragma unroll
+              for (int f = 0; f < 4; ++f) {
+                if (f >= P.nvf + P.nsf) break;
+                const bool vec = f < P.nvf;
+                const double fac0 = vec ? r1 * r1 * g70 : g60, fac1 = vec ? r1 * r1 * g71 : g61;
+                double* dst = args.d_rj + jr + args.ld * args.cols[f];
+                const int c = 8 * rr + 2 * f;
+                if (ok0) {
+                  dst[j00] = sr[c] * fac0;
+                  if (s1) dst[j01] = sr[c + 1] * fac0;
+                }
+                if (ok1) {
+                  dst[j10] = val[c] * fac1;
+                  if (s1) dst[j11] = val[c + 1] * fac1;
                 }
               }
-            } else {
-              // column c = 4 (r + nrT v) + q, q = 2 (component - 1) + slot
+            }
+          } else {
+            // column c = 4 (r + nrT v) + q, q = 2 (component - 1) + slot
 #pragma unroll
-              for (int c4 = 0; c4 < kTN / 4; ++c4) {
-                const int rv = w.nt * (kTN / 4) + c4;
-                const int r = rv % S.nrT, v = rv / S.nrT;
-                if (v >= P.nvf) break;
-                if (r >= P.nr) continue;
-                const double fac = P.radius[r] * g7;
-                double* dst = args.d_rj + P.J * (long long)r + args.ld * (args.cols[v] + 1);
-                dst[j0] = val[4 * c4] * fac;
-                dst[j0 + args.ld] = val[4 * c4 + 2] * fac;
+            for (int c4 = 0; c4 < kHalf / 4; ++c4) {
+              const int rv = w.nt * (kTN / 4) + cbase / 4 + c4;
+              const int r = rv % S.nrT, v = rv / S.nrT;
+              if (v >= P.nvf) break;
+              if (r >= P.nr) continue;
+              const double rr1 = P.radius[r];
+              const double fac0 = rr1 * g70, fac1 = rr1 * g71;
+              double* dst = args.d_rj + P.J * (long long)r + args.ld * (args.cols[v] + 1);
+              const int c = 4 * c4;
+              if (ok0) {
+                dst[j00] = sr[c] * fac0;
+                dst[j00 + args.ld] = sr[c + 2] * fac0;
                 if (s1) {
-                  dst[j1] = val[4 * c4 + 1] * fac;
-                  dst[j1 + args.ld] = val[4 * c4 + 3] * fac;
+                  dst[j01] = sr[c + 1] * fac0;
+                  dst[j01 + args.ld] = sr[c + 3] * fac0;
+                }
+              }
+              if (ok1) {
+                dst[j10] = val[c] * fac1;
+                dst[j10 + args.ld] = val[c + 2] * fac1;
+                if (s1) {
+                  dst[j11] = val[c + 1] * fac1;
+                  dst[j11 + args.ld] = val[c + 3] * fac1;
                 }
               }
             }
           }
-        } else if (h == 0) {
-          // first tile of a backward pair: keep this thread's row in shared memory
-          double* sr = stash + row * kXS;
-#pragma unroll
-          for (int c = 0; c < kTN; c += 2) *reinterpret_cast<double2*>(sr + c) = make_double2(val[c], val[c + 1]);
         } else {
-          // second tile: north row th gets first + second, south row nth-1-th
-          // first - second; an odd-Ntheta equator row gets the first alone
+          // second backward tile: north row th gets first + second, south row
+          // nth-1-th first - second; an odd-Ntheta equator row gets the first alone
           const int th = grow;
           if (th < P.nh && ok) {
             const bool pairrow = th < P.nth / 2;
-            const double* sr = stash + row * kXS;
+            const double* sr = stash + row * kXS + cbase;
             const long long rec = (long long)P.ncb * 2;
             double* baseN = P.rtm_b + ((long long)w.m * P.nth + th) * P.nr * rec;
             double* baseS = P.rtm_b + ((long long)w.m * P.nth + (P.nth - 1 - th)) * P.nr * rec;
             if (w.t <= 1) {
               // column c = 4 (r + nrT v) + q: one vector's (theta c, theta s, phi c, phi s)
 #pragma unroll
-              for (int c = 0; c < kTN; c += 4) {
-                const int col = w.nt * kTN + c;
+              for (int c = 0; c < kHalf; c += 4) {
+                const int col = w.nt * kTN + cbase + c;
                 const int r = (col >> 2) % S.nrT, vv = (col >> 2) / S.nrT;
                 if (vv >= P.nvb || r >= P.nr) continue;
                 const double2 a01 = *reinterpret_cast<const double2*>(sr + c);
@@ -880,8 +914,8 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
               // column c = 8 (r - 8 nt) + 2 f + slot: radial components and scalars
               const int nF = P.nvb + P.nsb;
 #pragma unroll
-              for (int rr = 0; rr < kTN / 8; ++rr) {
-                const int r = w.nt * (kTN / 8) + rr;
+              for (int rr = 0; rr < kHalf / 8; ++rr) {
+                const int r = w.nt * (kTN / 8) + cbase / 8 + rr;
                 if (r >= P.nr) break;
                 double* dN = baseN + (long long)r * rec + 4 * P.nvb;
                 double* dS = baseS + (long long)r * rec + 4 * P.nvb;
@@ -932,7 +966,7 @@ struct SplitState {
   std::vector<void*> allocs;
   int64_t bytes = 0;
   std::vector<long long> aoff, aeoff, deoff, boff, beoff;
-  Work* work_b = nullptr;  // backward work (cluster pairs)
+  Work* work_b = nullptr;  // backward work (parity tile pairs)
   Work* work_f = nullptr;  // forward work
   int nwork_b = 0, nwork_f = 0;
   int* err = nullptr;
@@ -965,7 +999,7 @@ cudaError_t launch_gemm(const GemmArgs& a, cudaStream_t st) {
   int dev = 0, nsm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const int units = a.pair ? a.nwork / 2 : a.nwork;
+  const int units = a.nwork / 2;
   const int grid = std::min(units, nsm);
   if (grid <= 0) return cudaSuccess;
   kern<<<grid, kGemmWarps * 32, smem, st>>>(a);
@@ -1033,25 +1067,32 @@ int split_create(SplitState** out, const Plan& p, int tier, int nslice, cudaStre
       bo += (long long)S.npadT[t] * g.kpad * s->ns;
       beo += S.npadT[t];
     }
-  // work lists: backward pairs (0,1) and (2,3) per (m, m-tile, n-tile); forward 4..7
+  // work lists: parity pairs (0,1), (2,3) backward and (4,5), (6,7) forward per
+  // (m, n-tile, m-tile), m-tile fastest: the units that read the same B panel
+  // are adjacent in the list, start together on neighbouring CTAs and share
+  // its chunks in L2.  A forward pair whose odd-parity type has one m-tile
+  // fewer keeps that tile as an empty partner (no K chunks).
   for (int m = 0; m <= L; ++m) {
     for (int tp = 0; tp < 4; tp += 2) {
       if ((tp == 0 && p.nvb == 0)) continue;
       const TypeGeo g = type_geo(tp, L, m, p.nh);
       const int nn = S.npadT[tp] / kTN;
-      for (int mt = 0; mt < g.rpad / kTM; ++mt)
-        for (int nt = 0; nt < nn; ++nt) {
+      for (int nt = 0; nt < nn; ++nt)
+        for (int mt = 0; mt < g.rpad / kTM; ++mt) {
           wb.push_back({m, tp, mt, nt});
           wb.push_back({m, tp + 1, mt, nt});
         }
     }
-    for (int t = 4; t < 8; ++t) {
-      if (t >= 6 && p.nvf == 0) continue;
-      const TypeGeo g = type_geo(t, L, m, p.nh);
+    for (int tp = 4; tp < 8; tp += 2) {
+      if (tp == 6 && p.nvf == 0) continue;
+      const TypeGeo g = type_geo(tp, L, m, p.nh);  // even parity: at least as many rows as odd
       if (g.rows <= 0) continue;
-      const int nn = S.npadT[t] / kTN;
-      for (int mt = 0; mt < g.rpad / kTM; ++mt)
-        for (int nt = 0; nt < nn; ++nt) wf.push_back({m, t, mt, nt});
+      const int nn = S.npadT[tp] / kTN;
+      for (int nt = 0; nt < nn; ++nt)
+        for (int mt = 0; mt < g.rpad / kTM; ++mt) {
+          wf.push_back({m, tp, mt, nt});
+          wf.push_back({m, tp + 1, mt, nt});
+        }
     }
   }
   int st_ = KMHD_OK;
@@ -1118,7 +1159,8 @@ size_t slice_smem(const Plan& p, bool fwd, int ns) {
   return sizeof(double) * (nx + 1 + kGrpCols) + kGrpCols * sizeof(int) + 8 * (size_t)ns * kSlab + 16;
 }
 
-int split_bwd(SplitState* s, const Plan& p, int, const double* d_rj, long long ld, const int* cols, cudaStream_t st) {
+int split_bwd(SplitState* s, const Plan& p, int, const double* d_rj, long long ld, const int* cols, cudaStream_t st,
+              cudaEvent_t mid) {
   const SliceTabs& S = s->S;
   {
     auto kern = s->ns == 6 ? k_slice_mr<false, 6> : k_slice_mr<false, 4>;
@@ -1128,6 +1170,7 @@ int split_bwd(SplitState* s, const Plan& p, int, const double* d_rj, long long l
     kern<<<dim3(p.nvb + 1, p.nr, p.L + 1), 256, smem, st>>>(p, S, d_rj, ld, cols);
   }
   if (cudaGetLastError() != cudaSuccess) return KMHD_ERR_CUDA;
+  if (mid && cudaEventRecord(mid, st) != cudaSuccess) return KMHD_ERR_CUDA;
   GemmArgs a;
   a.P = p;
   a.S = S;
@@ -1142,7 +1185,8 @@ int split_bwd(SplitState* s, const Plan& p, int, const double* d_rj, long long l
   return KMHD_OK;
 }
 
-int split_fwd(SplitState* s, const Plan& p, double* d_rj, long long ld, const int* cols, cudaStream_t st) {
+int split_fwd(SplitState* s, const Plan& p, double* d_rj, long long ld, const int* cols, cudaStream_t st,
+              cudaEvent_t mid) {
   const SliceTabs& S = s->S;
   {
     const size_t smem = slice_smem(p, true, s->ns);
@@ -1152,6 +1196,7 @@ int split_fwd(SplitState* s, const Plan& p, double* d_rj, long long ld, const in
     kern<<<dim3(p.nvf + 1, p.nr, p.L + 1), 256, smem, st>>>(p, S, nullptr, 0, nullptr);
   }
   if (cudaGetLastError() != cudaSuccess) return KMHD_ERR_CUDA;
+  if (mid && cudaEventRecord(mid, st) != cudaSuccess) return KMHD_ERR_CUDA;
   GemmArgs a;
   a.P = p;
   a.S = S;

@@ -9,10 +9,11 @@ struct SplitState;
 int split_create(SplitState** s, const Plan& p, int tier, int nslice, cudaStream_t st);
 void split_destroy(SplitState* s);
 int64_t split_bytes(const SplitState* s);
+// `mid` (optional) is recorded on st between the slicer and the GEMM launch.
 int split_bwd(SplitState* s, const Plan& p, int nlc_max, const double* d_rj, long long ld,
-              const int* cols, cudaStream_t st);
+              const int* cols, cudaStream_t st, cudaEvent_t mid = nullptr);
 int split_fwd(SplitState* s, const Plan& p, double* d_rj, long long ld, const int* cols,
-              cudaStream_t st);
+              cudaStream_t st, cudaEvent_t mid = nullptr);
 // Reads and returns the device error word (KMHD_OK or KMHD_ERR_TIMEOUT); synchronises st.
 int split_check_error(SplitState* s, cudaStream_t st);
 

@@ -53,7 +53,8 @@ class Desc(ctypes.Structure):
 
 EXPORTS = ["kmhd_sph_create", "kmhd_sph_destroy", "kmhd_sph_set_stream", "kmhd_sph_b_trans",
            "kmhd_sph_f_trans", "kmhd_sph_cycle", "kmhd_sph_batch_cycle", "kmhd_sph_last_timing",
-           "kmhd_sph_get_tables", "kmhd_sph_device_bytes", "kmhd_strerror", "kmhd_sph_cycle_noalloc"]
+           "kmhd_sph_get_tables", "kmhd_sph_device_bytes", "kmhd_strerror", "kmhd_sph_cycle_noalloc",
+           "kmhd_sph_last_kernel_timing"]
 
 _lib = None
 
@@ -79,6 +80,7 @@ def load_library(path: str | None = None):
                                          ctypes.POINTER(i64), ctypes.POINTER(ip),
                                          ctypes.POINTER(vp), ctypes.POINTER(i64), ctypes.POINTER(ip)]
     lib.kmhd_sph_last_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+    lib.kmhd_sph_last_kernel_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     lib.kmhd_sph_get_tables.argtypes = [vp, i32] + [ctypes.POINTER(ctypes.c_double)] * 4
     lib.kmhd_sph_device_bytes.restype = i64
     lib.kmhd_sph_device_bytes.argtypes = [vp]
@@ -175,6 +177,12 @@ class SphTransform:
         t = (ctypes.c_double * 4)()
         _check(load_library().kmhd_sph_last_timing(self._h, t), "last_timing")
         return dict(leg_bwd=t[0], fft_nl=t[1], leg_fwd=t[2], total=t[3])
+
+    def kernel_timing(self):
+        """Per-launch ms of the last cycle (CUDA events on the handle's stream)."""
+        t = (ctypes.c_double * 5)()
+        _check(load_library().kmhd_sph_last_kernel_timing(self._h, t), "last_kernel_timing")
+        return dict(slice_bwd=t[0], gemm_bwd=t[1], fft_nl=t[2], slice_fwd=t[3], gemm_fwd=t[4])
 
     def tables(self, m: int):
         c = self.cfg
