@@ -172,10 +172,15 @@ def main():
     ap.add_argument("--tier", default="auto", choices=["auto"] + list(TIERS))
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-tier comparison run")
+    ap.add_argument("--nr", type=int, default=0, help="override the radius count (small profiling cases)")
     args = ap.parse_args()
 
-    from kemorin_mhd_b200.config import NAMED
+    from kemorin_mhd_b200.config import NAMED, SphConfig
     cfg = NAMED[args.config]
+    if args.nr > 0:
+        cfg = SphConfig(cfg.ltr, cfg.nth, cfg.nph, args.nr, cfg.nvb, cfg.nsb, cfg.nvf, cfg.nsf, cfg.products,
+                        name=f"L{cfg.ltr}_Nr{args.nr}")
     if args.impl == "reference":
         return run_reference(args, cfg)
 
@@ -259,7 +264,7 @@ def main():
 
     # FP64 GPU cycle on the same input: the bar of the split tier (speed and error)
     extra = {}
-    if tier != "fp64":
+    if tier != "fp64" and not args.no_fp64:
         ref64 = make("fp64")
         ref64.set_stream(stream.cuda_stream)
         out64 = torch.zeros_like(d_out)
