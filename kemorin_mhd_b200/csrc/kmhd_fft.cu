@@ -16,6 +16,8 @@
 // Products: cal_cross_prod_w_coef_smp, cal_vec_scalar_prod_w_coef_smp,
 // cal_dot_prod_w_coef_smp (CORE_src/BASE/cal_products_smp.f90) as called by
 // nonlinear_terms_in_rtp (MHD_src/sph_MHD/cal_nonlinear_sph_MHD.f90:64-128).
+#include <utility>
+
 #include "kmhd_internal.cuh"
 
 namespace kmhd {
@@ -457,107 +459,6 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_fwd_grid(Plan P, const doub
 }
 
 // ---------------------------------------------------------------------------
-// Compile-time variant for the common N = 3 2^k: factor order (3, leftover 4 or
-// 2, then 8s), spans and strides are constants, 512 threads, and a bank-
-// conflict-free shared layout: inside each pair sequence the index is swizzled
-// i -> i ^ ((i >> 3) & 7) and pairs are N + 1 entries apart; passes with stride
-// >= 8 run the in-block index fastest across threads, the others the butterfly
-// block index, so every quarter warp (8 x 16 bytes) hits 8 distinct bank groups.
-constexpr int kFftThreadsT = 512;
-
-__host__ __device__ constexpr int tfac_count(int n) {
-  int c = 0;
-  while (n % 3 == 0) { n /= 3; ++c; }
-  while (n % 5 == 0) { n /= 5; ++c; }
-  int e = 0;
-  while (n % 8 == 0) { n /= 8; ++e; }
-  if (n == 2 || n == 4) { ++c; n = 1; }
-  return c + e;
-}
-__host__ __device__ constexpr int tfac_at(int n, int i) {
-  int c = 0;
-  while (n % 3 == 0) { if (c == i) return 3; n /= 3; ++c; }
-  while (n % 5 == 0) { if (c == i) return 5; n /= 5; ++c; }
-  int r = n, e = 0;
-  while (r % 8 == 0) { r /= 8; ++e; }
-  if (r == 2 || r == 4) { if (c == i) return r; ++c; }
-  return 8;
-}
-__host__ __device__ constexpr int tspan_at(int n, int i) {
-  int sp = n;
-  for (int q = 0; q < i; ++q) sp /= tfac_at(n, q);
-  return sp;
-}
-__device__ __forceinline__ int sw(int i) { return i ^ ((i >> 3) & 7); }
-
-// twiddles w^q, q = 1..R-1, from two table loads (w^1, w^2)
-template <int R, int SIGN>
-__device__ __forceinline__ void twiddles(const double2* __restrict__ tw, int base, int N, double2* w) {
-  if constexpr (R >= 2) w[1] = twd<SIGN>(tw, base);
-  if constexpr (R >= 3) w[2] = twd<SIGN>(tw, (2 * base) % N);
-  if constexpr (R >= 4) w[3] = cmul(w[1], w[2]);
-  if constexpr (R >= 5) w[4] = cmul(w[2], w[2]);
-  if constexpr (R >= 6) w[5] = cmul(w[4], w[1]);
-  if constexpr (R >= 7) w[6] = cmul(w[4], w[2]);
-  if constexpr (R >= 8) w[7] = cmul(w[4], w[3]);
-}
-
-template <int N, int I>
-__device__ __forceinline__ void tdif(double2* z, int npair, const double2* __restrict__ tw) {
-  if constexpr (I < tfac_count(N)) {
-    constexpr int R = tfac_at(N, I), span = tspan_at(N, I), s = span / R, nbf = N / R, stw = N / span;
-    constexpr int NB = N / span;  // butterfly blocks
-    constexpr int NP = N + 1;
-    for (int it = threadIdx.x; it < npair * nbf; it += blockDim.x) {
-      const int pp = it / nbf, rem = it - pp * nbf;
-      int b, j;
-      if constexpr (s >= 8) { b = rem / s; j = rem - b * s; }
-      else { j = rem / NB; b = rem - j * NB; }
-      double2* zp = z + pp * NP;
-      const int base = b * span + j;
-      double2 x[R];
-#pragma unroll
-      for (int r = 0; r < R; ++r) x[r] = zp[sw(base + r * s)];
-      DFT<R, +1>::run(x);
-      double2 w[R];
-      twiddles<R, +1>(tw, j * stw, N, w);
-      zp[sw(base)] = x[0];
-#pragma unroll
-      for (int q = 1; q < R; ++q) zp[sw(base + q * s)] = cmul(x[q], w[q]);
-    }
-    __syncthreads();
-    tdif<N, I + 1>(z, npair, tw);
-  }
-}
-
-template <int N, int I>
-__device__ __forceinline__ void tdit(double2* z, int npair, const double2* __restrict__ tw) {
-  if constexpr (I >= 0) {
-    constexpr int R = tfac_at(N, I), span = tspan_at(N, I), s = span / R, nbf = N / R, stw = N / span;
-    constexpr int NB = N / span;
-    constexpr int NP = N + 1;
-    for (int it = threadIdx.x; it < npair * nbf; it += blockDim.x) {
-      const int pp = it / nbf, rem = it - pp * nbf;
-      int b, j;
-      if constexpr (s >= 8) { b = rem / s; j = rem - b * s; }
-      else { j = rem / NB; b = rem - j * NB; }
-      double2* zp = z + pp * NP;
-      const int base = b * span + j;
-      double2 w[R];
-      twiddles<R, -1>(tw, j * stw, N, w);
-      double2 x[R];
-      x[0] = zp[sw(base)];
-#pragma unroll
-      for (int q = 1; q < R; ++q) x[q] = cmul(zp[sw(base + q * s)], w[q]);
-      DFT<R, -1>::run(x);
-#pragma unroll
-      for (int r = 0; r < R; ++r) zp[sw(base + r * s)] = x[r];
-    }
-    __syncthreads();
-    tdit<N, I - 1>(z, npair, tw);
-  }
-}
-
 // staged records of one line: [m][ncs pairs], ncs = nc rounded up to odd
 __device__ __forceinline__ int ncs_of(int nc) { return nc | 1; }
 
@@ -593,28 +494,395 @@ __device__ __forceinline__ double2 spec_at_t(const double* st, int nc, int nv, i
                 : make_double2(0.5 * a0 + 0.5 * b1, 0.5 * a1 - 0.5 * b0);
 }
 
-template <int N>
-__device__ __forceinline__ void tdif_first(const double* st, int nc, int nv, double2* z, int npair, int L,
-                                           const double2* __restrict__ tw) {
-  constexpr int R = tfac_at(N, 0), s = N / R, nbf = N / R;
+size_t smem_cycle_f(const Plan& p) {
+  const int npair = ((p.ncb > p.ncf ? p.ncb : p.ncf) + 1) / 2;
+  return sizeof(double2) * ((size_t)npair * (p.nph + 1) + 1) + sizeof(double) * 2 * (size_t)(p.L + 1) * (p.ncb | 1);
+}
+
+// ---------------------------------------------------------------------------
+// Fused-pass variant for N = F0 * M * 4 (F0 in {3, 6, 12, 24}, M in {4, 16}):
+// inverse passes radix F0 (reading the staged spectra), radix M, radix 4; the
+// last inverse radix-4 pass, the grid products and the first forward radix-4
+// pass share one item (4 grid points of every component in registers), so a
+// line takes five sweeps over shared memory instead of nine.  The radix-4
+// passes of span 4 carry no twiddles.  Swizzle i -> i ^ (((i >> 3) ^ (i >> 6))
+// & 7) inside each pair sequence (pairs N + 1 entries apart) keeps every
+// quarter warp on 8 distinct 16-byte bank groups in all passes at N = 1536.
+constexpr int kFftThreadsF = 384;
+
+__host__ __device__ constexpr int ff_mid(int n) { return (n % 64 == 0 && (n / 64 == 3 || n / 64 == 6 || n / 64 == 12 || n / 64 == 24)) ? 16 : 4; }
+__host__ __device__ constexpr int ff_first(int n) { return n / (4 * ff_mid(n)); }
+__device__ __forceinline__ int swf(int i) { return i ^ (((i >> 3) ^ (i >> 6)) & 7); }
+
+// e^{2 pi i k / 48}: cos and sin of the first quadrant, k = 0..11
+__host__ __device__ constexpr double c48q(int k) {
+  constexpr double c[12] = {1.0, 0.9914448613738104, 0.9659258262890683, 0.9238795325112867,
+                            0.8660254037844386, 0.7933533402912352, 0.7071067811865476, 0.6087614290087207,
+                            0.5, 0.3826834323650898, 0.25881904510252074, 0.1305261922200516};
+  return c[k];
+}
+// x * e^{SIGN 2 pi i e / R}, e and R compile-time, R | 48
+template <int R, int E, int SIGN>
+__device__ __forceinline__ double2 rot(double2 x) {
+  constexpr int k = (E * (48 / R)) % 48;
+  constexpr int q = k / 12, k0 = k % 12;
+  if constexpr (k0 == 0) {
+    // multiples of 90 degrees
+    if constexpr (q == 0) return x;
+    else if constexpr (q == 2) return make_double2(-x.x, -x.y);
+    else if constexpr ((q == 1) == (SIGN > 0)) return make_double2(-x.y, x.x);  // * i
+    else return make_double2(x.y, -x.x);                                        // * -i
+  } else {
+    // (c, s) of angle k * 7.5 degrees
+    constexpr double c0 = c48q(k0), s0 = c48q(12 - k0);
+    constexpr double c = q == 0 ? c0 : q == 1 ? -s0 : q == 2 ? -c0 : s0;
+    constexpr double sn = (q == 0 ? s0 : q == 1 ? c0 : q == 2 ? -s0 : -c0) * (double)SIGN;
+    return make_double2(x.x * c - x.y * sn, x.x * sn + x.y * c);
+  }
+}
+
+// DFT of length A*B (Cooley-Tukey, n = B n1 + n2, k = k1 + A k2), in place.
+template <int A, int B, int SIGN>
+struct DFT2F {
+  template <int N2, int K1>
+  __device__ static void tw_one(double2* y) {
+    y[N2 * A + K1] = rot<A * B, N2 * K1, SIGN>(y[N2 * A + K1]);
+  }
+  __device__ static void run(double2* x) {
+    double2 y[A * B];
+#pragma unroll
+    for (int n2 = 0; n2 < B; ++n2) {
+      double2 t[A];
+#pragma unroll
+      for (int n1 = 0; n1 < A; ++n1) t[n1] = x[B * n1 + n2];
+      DFT<A, SIGN>::run(t);
+#pragma unroll
+      for (int k1 = 0; k1 < A; ++k1) y[n2 * A + k1] = t[k1];
+    }
+    twiddle_all(y, std::make_integer_sequence<int, A * B>{});
+#pragma unroll
+    for (int k1 = 0; k1 < A; ++k1) {
+      double2 t[B];
+#pragma unroll
+      for (int n2 = 0; n2 < B; ++n2) t[n2] = y[n2 * A + k1];
+      DFT<B, SIGN>::run(t);
+#pragma unroll
+      for (int k2 = 0; k2 < B; ++k2) x[k1 + A * k2] = t[k2];
+    }
+  }
+  template <int... I>
+  __device__ static void twiddle_all(double2* y, std::integer_sequence<int, I...>) {
+    (tw_one<I / A, I % A>(y), ...);
+  }
+};
+template <int SIGN> struct DFT<6, SIGN> { __device__ static void run(double2* x) { DFT2F<3, 2, SIGN>::run(x); } };
+template <int SIGN> struct DFT<12, SIGN> { __device__ static void run(double2* x) { DFT2F<3, 4, SIGN>::run(x); } };
+template <int SIGN> struct DFT<16, SIGN> { __device__ static void run(double2* x) { DFT2F<4, 4, SIGN>::run(x); } };
+template <int SIGN> struct DFT<24, SIGN> { __device__ static void run(double2* x) { DFT2F<3, 8, SIGN>::run(x); } };
+template <int SIGN> struct DFT<1, SIGN> { __device__ static void run(double2*) {} };
+
+// DFT of length 3B whose middle third of inputs (n = B .. 2B-1) is zero: the
+// first-stage length-3 transforms see (x0, 0, x2).
+template <int A, int B, int SIGN>
+struct DFT2F_ZM;
+template <int B, int SIGN>
+struct DFT2F_ZM<3, B, SIGN> {
+  template <int N2, int K1>
+  __device__ static void tw_one(double2* y) {
+    y[N2 * 3 + K1] = rot<3 * B, N2 * K1, SIGN>(y[N2 * 3 + K1]);
+  }
+  template <int... I>
+  __device__ static void twiddle_all(double2* y, std::integer_sequence<int, I...>) {
+    (tw_one<I / 3, I % 3>(y), ...);
+  }
+  __device__ static void run(double2* x) {
+    const double s3 = 0.86602540378443864676 * (double)SIGN;
+    double2 y[3 * B];
+#pragma unroll
+    for (int n2 = 0; n2 < B; ++n2) {
+      const double2 a = x[n2], c = x[2 * B + n2];
+      const double2 v = make_double2(a.x - 0.5 * c.x, a.y - 0.5 * c.y);
+      const double2 u = make_double2(c.y * s3, -c.x * s3);  // -(SIGN i sqrt3/2) c
+      y[n2 * 3 + 0] = cadd(a, c);
+      y[n2 * 3 + 1] = cadd(v, u);
+      y[n2 * 3 + 2] = csub(v, u);
+    }
+    twiddle_all(y, std::make_integer_sequence<int, 3 * B>{});
+#pragma unroll
+    for (int k1 = 0; k1 < 3; ++k1) {
+      double2 t[B];
+#pragma unroll
+      for (int n2 = 0; n2 < B; ++n2) t[n2] = y[n2 * 3 + k1];
+      DFT<B, SIGN>::run(t);
+#pragma unroll
+      for (int k2 = 0; k2 < B; ++k2) x[k1 + 3 * k2] = t[k2];
+    }
+  }
+};
+
+// Shared-memory index of entry i of a pair sequence: swf(i).  The passes below
+// compute it with the bits that are compile-time constants folded out.
+//
+// First inverse pass: radix F0 over the whole line (span N, stride S1 = N/F0),
+// inputs from the staged spectra.  Twiddles w^(j q) are read straight from the
+// table (j q < N here).  When N = 3 (L + 1) (PR), the middle third of the
+// inputs (L < k < N - L) is zero and the outer thirds need no range checks.
+template <int N, bool PR>
+__device__ __forceinline__ void ff_dif_first(const double* st, int nc, int nv, double2* z, int npair, int L,
+                                             const double2* __restrict__ tw) {
+  constexpr int R = ff_first(N), S1 = N / R, NP = N + 1, T3 = R / 3;
+  for (int it = threadIdx.x; it < npair * S1; it += blockDim.x) {
+    const int pp = it / S1, j = it - pp * S1;
+    double2 x[R];
+    if constexpr (PR) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        if (r < T3) {
+          x[r] = spec_at_t(st, nc, nv, pp, j + r * S1, N, L);  // k <= L
+        } else if (r >= 2 * T3) {
+          x[r] = spec_at_t(st, nc, nv, pp, j + r * S1, N, L);  // k >= 2N/3
+        } else {
+          x[r] = make_double2(0.0, 0.0);
+        }
+      }
+      DFT2F_ZM<3, T3, +1>::run(x);
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) x[r] = spec_at_t(st, nc, nv, pp, j + r * S1, N, L);
+      DFT<R, +1>::run(x);
+    }
+    double2* zp = z + pp * NP;
+    if constexpr (S1 % 64 == 0) {
+      const int jj = j ^ ((j >> 3) & 7);
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const double2 v = q == 0 ? x[0] : cmul(x[q], twd<+1>(tw, j * q));
+        zp[(jj ^ (((q * S1) >> 6) & 7)) + q * S1] = v;
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < R; ++q) zp[swf(j + q * S1)] = q == 0 ? x[0] : cmul(x[q], twd<+1>(tw, j * q));
+    }
+  }
+}
+
+// Last forward pass (transpose of ff_dif_first): radix F0 over the whole line,
+// natural-order output.  With PR only the outer thirds of the output (the
+// orders 0..L and their mirrors) are stored.
+template <int N, bool PR>
+__device__ __forceinline__ void ff_dit_last(double2* z, int npair, const double2* __restrict__ tw) {
+  constexpr int R = ff_first(N), S1 = N / R, NP = N + 1, T3 = R / 3;
+  for (int it = threadIdx.x; it < npair * S1; it += blockDim.x) {
+    const int pp = it / S1, j = it - pp * S1;
+    double2* zp = z + pp * NP;
+    double2 x[R];
+    if constexpr (S1 % 64 == 0) {
+      const int jj = j ^ ((j >> 3) & 7);
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const double2 v = zp[(jj ^ (((q * S1) >> 6) & 7)) + q * S1];
+        x[q] = q == 0 ? v : cmul(v, twd<-1>(tw, j * q));
+      }
+      DFT<R, -1>::run(x);
+#pragma unroll
+      for (int q = 0; q < R; ++q)
+        if (!PR || q < T3 || q >= 2 * T3) zp[(jj ^ (((q * S1) >> 6) & 7)) + q * S1] = x[q];
+    } else {
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const double2 v = zp[swf(j + q * S1)];
+        x[q] = q == 0 ? v : cmul(v, twd<-1>(tw, j * q));
+      }
+      DFT<R, -1>::run(x);
+#pragma unroll
+      for (int q = 0; q < R; ++q)
+        if (!PR || q < T3 || q >= 2 * T3) zp[swf(j + q * S1)] = x[q];
+    }
+  }
+}
+
+// Middle pass of radix M over span SP = N/F0 (stride SP/M = 4): butterfly
+// block b fastest across threads.  For SP = 64 the swizzle of element r is
+// ((j + 4r) ^ (r/2) ^ (b % 8)) within the block, j < 4.
+template <int N, int SIGN>
+__device__ __forceinline__ void ff_mid_pass(double2* z, int npair, const double2* __restrict__ tw) {
+  constexpr int R = ff_mid(N), SP = N / ff_first(N), s = SP / R, nbf = N / R, NB = N / SP, stw = N / SP;
   constexpr int NP = N + 1;
   for (int it = threadIdx.x; it < npair * nbf; it += blockDim.x) {
-    const int pp = it / nbf, j = it - pp * nbf;
+    const int pp = it / nbf, rem = it - pp * nbf;
+    const int b = rem % NB, j = rem / NB;
+    double2* zp = z + pp * NP + b * SP;
     double2 x[R];
+    if constexpr (SP == 64 && s == 4) {
+      // element e = 4r + j (j < 4): e >> 3 = r / 2, so swf gives
+      // 8 (r / 2) + ((j ^ (b % 8)) ^ (r / 2) ^ 4 (r % 2))
+      const int jb = j ^ (b & 7);
+#define KMHD_MIDX(r) (8 * ((r) >> 1) + (jb ^ (((r) >> 1) ^ (4 * ((r) & 1)))))
+      if constexpr (SIGN > 0) {
 #pragma unroll
-    for (int r = 0; r < R; ++r) x[r] = spec_at_t(st, nc, nv, pp, j + r * s, N, L);
-    DFT<R, +1>::run(x);
-    double2 w[R];
-    twiddles<R, +1>(tw, j, N, w);
-    double2* zp = z + pp * NP;
-    zp[sw(j)] = x[0];
+        for (int r = 0; r < R; ++r) x[r] = zp[KMHD_MIDX(r)];
+        DFT<R, +1>::run(x);
 #pragma unroll
-    for (int q = 1; q < R; ++q) zp[sw(j + q * s)] = cmul(x[q], w[q]);
+        for (int q = 0; q < R; ++q) zp[KMHD_MIDX(q)] = q == 0 ? x[0] : cmul(x[q], twd<+1>(tw, j * q * stw));
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const double2 v = zp[KMHD_MIDX(r)];
+          x[r] = r == 0 ? v : cmul(v, twd<-1>(tw, j * r * stw));
+        }
+        DFT<R, -1>::run(x);
+#pragma unroll
+        for (int q = 0; q < R; ++q) zp[KMHD_MIDX(q)] = x[q];
+      }
+#undef KMHD_MIDX
+    } else {
+      if constexpr (SIGN > 0) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) x[r] = z[pp * NP + swf(b * SP + j + r * s)];
+        DFT<R, +1>::run(x);
+#pragma unroll
+        for (int q = 0; q < R; ++q)
+          z[pp * NP + swf(b * SP + j + q * s)] = q == 0 ? x[0] : cmul(x[q], twd<+1>(tw, j * q * stw));
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const double2 v = z[pp * NP + swf(b * SP + j + r * s)];
+          x[r] = r == 0 ? v : cmul(v, twd<-1>(tw, j * r * stw));
+        }
+        DFT<R, -1>::run(x);
+#pragma unroll
+        for (int q = 0; q < R; ++q) z[pp * NP + swf(b * SP + j + q * s)] = x[q];
+      }
+    }
+  }
+}
+
+// Grid products of one grid point: vin = backward components (3 MVB vector
+// components, then MSB scalars, as laid out in the pairs), out = forward
+// components in pair order.
+template <int MVB, int MSB, int MVF, int MSF>
+__device__ __forceinline__ void point_products(const double* vin_all, const Plan& P, double* dense) {
+  constexpr int MCF = 3 * MVF + MSF;
+  const int nvb = P.nvb, nvf = P.nvf, nsf = P.nsf;
+  double vin[3 * MVB > 0 ? 3 * MVB : 1], sin_[MSB > 0 ? MSB : 1];
+#pragma unroll
+  for (int c = 0; c < 3 * MVB; ++c) vin[c] = vin_all[c];
+#pragma unroll
+  for (int q = 0; q < MSB; ++q) sin_[q] = vin_all[3 * nvb + q < 3 * MVB + MSB ? 3 * nvb + q : 0];
+  double out[MCF > 0 ? MCF : 1];
+#pragma unroll
+  for (int i = 0; i < MVF; ++i) {
+    if (i < nvf) {
+      const double cf = P.pcoef[i];
+      double x0, x1, x2;
+      selvec<MVB>(vin, P.pa[i], x0, x1, x2);
+      if (P.pkind[i] == KMHD_PROD_CROSS) {
+        double y0, y1, y2;
+        selvec<MVB>(vin, P.pb[i], y0, y1, y2);
+        out[3 * i + 0] = (x1 * y2 - x2 * y1) * cf;
+        out[3 * i + 1] = (x2 * y0 - x0 * y2) * cf;
+        out[3 * i + 2] = (x0 * y1 - x1 * y0) * cf;
+      } else {
+        const double sv = selscl<MSB>(sin_, P.pb[i]);
+        out[3 * i + 0] = x0 * sv * cf;
+        out[3 * i + 1] = x1 * sv * cf;
+        out[3 * i + 2] = x2 * sv * cf;
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < MSF; ++j) {
+    if (j < nsf) {
+      const int q = nvf + j;
+      const double cf = P.pcoef[q];
+      double o;
+      if (P.pkind[q] == KMHD_PROD_DOT) {
+        double x0, x1, x2, y0, y1, y2;
+        selvec<MVB>(vin, P.pa[q], x0, x1, x2);
+        selvec<MVB>(vin, P.pb[q], y0, y1, y2);
+        o = (x0 * y0 + x1 * y1 + x2 * y2) * cf;
+      } else {
+        o = selscl<MSB>(sin_, P.pa[q]) * selscl<MSB>(sin_, P.pb[q]) * cf;
+      }
+      out[3 * MVF + j] = o;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < MCF; ++c) {
+    double v = 0.0;
+    if (c < 3 * MVF) v = out[c < 3 * MVF ? c : 0];
+    if (c >= 3 * nvf) {
+      v = 0.0;
+#pragma unroll
+      for (int j = 0; j < MSF; ++j)
+        if (c == 3 * nvf + j) v = out[3 * MVF + j];
+    }
+    dense[c] = v;
+  }
+}
+
+// Products of the standard MHD set at one grid point: backward (u, omega, B; T),
+// forward (omega x u, u x B, u T; u . omega), coefficients from the plan.
+__device__ __forceinline__ void point_products_mhd(const double* v, const Plan& P, double* o) {
+  const double u0 = v[0], u1 = v[1], u2 = v[2], w0 = v[3], w1 = v[4], w2 = v[5];
+  const double b0 = v[6], b1 = v[7], b2 = v[8], t = v[9];
+  const double c0 = P.pcoef[0], c1 = P.pcoef[1], c2 = P.pcoef[2], c3 = P.pcoef[3];
+  o[0] = (w1 * u2 - w2 * u1) * c0;
+  o[1] = (w2 * u0 - w0 * u2) * c0;
+  o[2] = (w0 * u1 - w1 * u0) * c0;
+  o[3] = (u1 * b2 - u2 * b1) * c1;
+  o[4] = (u2 * b0 - u0 * b2) * c1;
+  o[5] = (u0 * b1 - u1 * b0) * c1;
+  o[6] = u0 * t * c2;
+  o[7] = u1 * t * c2;
+  o[8] = u2 * t * c2;
+  o[9] = (u0 * w0 + u1 * w1 + u2 * w2) * c3;
+}
+
+// Last inverse radix-4 pass + products + first forward radix-4 pass, for the
+// grid points 4b .. 4b+3 of every pair.
+template <int N, int MVB, int MSB, int MVF, int MSF, int PK>
+__device__ __forceinline__ void ff_fused(double2* z, const Plan& P) {
+  constexpr int NP = N + 1;
+  constexpr int MCB = 3 * MVB + MSB, MCF = 3 * MVF + MSF;
+  constexpr int NPB = (MCB + 1) / 2, NPF = (MCF + 1) / 2;
+  constexpr int NPM = NPB > NPF ? NPB : NPF;
+  const int npb = (P.ncb + 1) / 2, npf = (P.ncf + 1) / 2, ncb = P.ncb, ncf = P.ncf;
+  for (int b = threadIdx.x; b < N / 4; b += blockDim.x) {
+    const int e0 = (4 * b) ^ (((b >> 1) ^ (b >> 4)) & 7);  // swf(4b + r) = e0 ^ r
+    double2 v[NPM][4];
+#pragma unroll
+    for (int pp = 0; pp < NPB; ++pp) {
+      if (pp < npb) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r) v[pp][r] = z[pp * NP + (e0 ^ r)];
+        DFT<4, +1>::run(v[pp]);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      double vin[MCB > 0 ? MCB : 1], dense[MCF > 0 ? MCF : 1];
+#pragma unroll
+      for (int c = 0; c < MCB; ++c) vin[c] = (c < ncb) ? ((c & 1) ? v[c >> 1][r].y : v[c >> 1][r].x) : 0.0;
+      if constexpr (PK == 1) point_products_mhd(vin, P, dense);
+      else point_products<MVB, MSB, MVF, MSF>(vin, P, dense);
+#pragma unroll
+      for (int q = 0; q < NPF; ++q)
+        v[q][r] = make_double2(2 * q < ncf ? dense[2 * q] : 0.0, 2 * q + 1 < ncf ? dense[2 * q + 1 < MCF ? 2 * q + 1 : 0] : 0.0);
+    }
+#pragma unroll
+    for (int q = 0; q < NPF; ++q) {
+      if (q < npf) {
+        DFT<4, -1>::run(v[q]);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) z[q * NP + (e0 ^ r)] = v[q][r];
+      }
+    }
   }
 }
 
 template <int N>
-__device__ void tstore_line(const double2* z, int npair, const Plan& P, double* rtm, int nc, int nv, int th, int r) {
+__device__ void ff_store_line(const double2* z, int npair, const Plan& P, double* rtm, int nc, int nv, int th, int r) {
   constexpr int NP = N + 1;
   const int L = P.L;
   const double aN = 1.0 / (double)N;
@@ -623,12 +891,12 @@ __device__ void tstore_line(const double2* z, int npair, const Plan& P, double* 
   for (int it = threadIdx.x; it < (L + 1) * npair; it += blockDim.x) {
     const int pp = it / (L + 1), m = it - pp * (L + 1);
     const double2* zp = z + pp * NP;
-    const double2 zm = zp[sw(m)];
+    const double2 zm = zp[swf(m)];
     double a0, b0, a1, b1;
     if (m == 0) {
       a0 = zm.x * aN; a1 = zm.y * aN; b0 = 0.0; b1 = 0.0;
     } else {
-      const double2 wm = zp[sw(N - m)];
+      const double2 wm = zp[swf(N - m)];
       a0 = (zm.x + wm.x) * aN;
       b0 = (wm.y - zm.y) * aN;
       a1 = (zm.y + wm.y) * aN;
@@ -640,91 +908,8 @@ __device__ void tstore_line(const double2* z, int npair, const Plan& P, double* 
   }
 }
 
-template <int N, int MVB, int MSB, int MVF, int MSF>
-__device__ void tproducts(double2* z, const Plan& P) {
-  constexpr int NP = N + 1;
-  constexpr int MCF = 3 * MVF + MSF;
-  const int nvb = P.nvb, nsb = P.nsb, nvf = P.nvf, nsf = P.nsf;
-  for (int pos = threadIdx.x; pos < N; pos += blockDim.x) {
-    const int pq = sw(pos);
-    double vin[3 * MVB > 0 ? 3 * MVB : 1], sin_[MSB > 0 ? MSB : 1];
-#pragma unroll
-    for (int c = 0; c < 3 * MVB; ++c)
-      if (c < 3 * nvb) {
-        const double2 v = z[(c >> 1) * NP + pq];
-        vin[c] = (c & 1) ? v.y : v.x;
-      }
-#pragma unroll
-    for (int q = 0; q < MSB; ++q)
-      if (q < nsb) {
-        const int c = 3 * nvb + q;
-        const double2 v = z[(c >> 1) * NP + pq];
-        sin_[q] = (c & 1) ? v.y : v.x;
-      }
-    double out[MCF > 0 ? MCF : 1];
-#pragma unroll
-    for (int i = 0; i < MVF; ++i) {
-      if (i < nvf) {
-        const double cf = P.pcoef[i];
-        double x0, x1, x2;
-        selvec<MVB>(vin, P.pa[i], x0, x1, x2);
-        if (P.pkind[i] == KMHD_PROD_CROSS) {
-          double y0, y1, y2;
-          selvec<MVB>(vin, P.pb[i], y0, y1, y2);
-          out[3 * i + 0] = (x1 * y2 - x2 * y1) * cf;
-          out[3 * i + 1] = (x2 * y0 - x0 * y2) * cf;
-          out[3 * i + 2] = (x0 * y1 - x1 * y0) * cf;
-        } else {
-          const double sv = selscl<MSB>(sin_, P.pb[i]);
-          out[3 * i + 0] = x0 * sv * cf;
-          out[3 * i + 1] = x1 * sv * cf;
-          out[3 * i + 2] = x2 * sv * cf;
-        }
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < MSF; ++j) {
-      if (j < nsf) {
-        const int q = nvf + j;
-        const double cf = P.pcoef[q];
-        double o;
-        if (P.pkind[q] == KMHD_PROD_DOT) {
-          double x0, x1, x2, y0, y1, y2;
-          selvec<MVB>(vin, P.pa[q], x0, x1, x2);
-          selvec<MVB>(vin, P.pb[q], y0, y1, y2);
-          o = (x0 * y0 + x1 * y1 + x2 * y2) * cf;
-        } else {
-          o = selscl<MSB>(sin_, P.pa[q]) * selscl<MSB>(sin_, P.pb[q]) * cf;
-        }
-        out[3 * MVF + j] = o;
-      }
-    }
-    const int ncf = 3 * nvf + nsf;
-    double dense[MCF > 0 ? MCF : 1];
-#pragma unroll
-    for (int c = 0; c < MCF; ++c) {
-      double v = 0.0;
-      if (c < 3 * MVF) v = out[c < 3 * MVF ? c : 0];
-      if (c >= 3 * nvf) {
-        v = 0.0;
-#pragma unroll
-        for (int j = 0; j < MSF; ++j)
-          if (c == 3 * nvf + j) v = out[3 * MVF + j];
-      }
-      dense[c] = v;
-    }
-#pragma unroll
-    for (int c = 0; c < MCF; c += 2) {
-      if (c < ncf) {
-        const double hi = (c + 1 < MCF && c + 1 < ncf) ? dense[c + 1 < MCF ? c + 1 : c] : 0.0;
-        z[(c >> 1) * NP + pq] = make_double2(dense[c], hi);
-      }
-    }
-  }
-}
-
-template <int N, int MVB, int MSB, int MVF, int MSF>
-__global__ void __launch_bounds__(kFftThreadsT, 1) k_fft_cycle_t(Plan P, int nlines) {
+template <int N, int MVB, int MSB, int MVF, int MSF, bool PR, int PK>
+__global__ void __launch_bounds__(kFftThreadsF, 1) k_fft_cycle_f(Plan P, int nlines) {
   extern __shared__ double4 smraw[];
   constexpr int NP = N + 1;
   const int npb = (P.ncb + 1) / 2, npf = (P.ncf + 1) / 2;
@@ -738,53 +923,72 @@ __global__ void __launch_bounds__(kFftThreadsT, 1) k_fft_cycle_t(Plan P, int nli
     const int r = line % P.nr, th = line / P.nr;
     cp_async_wait<0>();
     __syncthreads();
-    tdif_first<N>(st, P.ncb, P.nvb, z, npb, P.L, P.twid);
+    ff_dif_first<N, PR>(st, P.ncb, P.nvb, z, npb, P.L, P.twid);
     __syncthreads();
     const int next = line + gridDim.x;
     if (next < nlines) prefetch_line_t(st, P.rtm_b, P.ncb, P, next / P.nr, next % P.nr);
-    tdif<N, 1>(z, npb, P.twid);
-    tproducts<N, MVB, MSB, MVF, MSF>(z, P);
+    ff_mid_pass<N, +1>(z, npb, P.twid);
     __syncthreads();
-    tdit<N, tfac_count(N) - 1>(z, npf, P.twid);
-    tstore_line<N>(z, npf, P, P.rtm_f, P.ncf, P.nvf, th, r);
+    ff_fused<N, MVB, MSB, MVF, MSF, PK>(z, P);
+    __syncthreads();
+    ff_mid_pass<N, -1>(z, npf, P.twid);
+    __syncthreads();
+    ff_dit_last<N, PR>(z, npf, P.twid);
+    __syncthreads();
+    ff_store_line<N>(z, npf, P, P.rtm_f, P.ncf, P.nvf, th, r);
     __syncthreads();
     line = next;
   }
 }
 
-size_t smem_cycle_t(const Plan& p) {
-  const int npair = ((p.ncb > p.ncf ? p.ncb : p.ncf) + 1) / 2;
-  return sizeof(double2) * ((size_t)npair * (p.nph + 1) + 1) + sizeof(double) * 2 * (size_t)(p.L + 1) * (p.ncb | 1);
-}
-
-template <int N, int MVB, int MSB, int MVF, int MSF>
-cudaError_t run_cycle_t(const Plan& p, cudaStream_t s) {
-  auto kern = k_fft_cycle_t<N, MVB, MSB, MVF, MSF>;
-  const size_t smem = smem_cycle_t(p);
+template <int N, int MVB, int MSB, int MVF, int MSF, bool PR, int PK>
+cudaError_t run_cycle_fk(const Plan& p, cudaStream_t s) {
+  auto kern = k_fft_cycle_f<N, MVB, MSB, MVF, MSF, PR, PK>;
+  const size_t smem = smem_cycle_f(p);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int dev = 0, nsm = 0, occ = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kFftThreadsT, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kFftThreadsF, smem);
   if (occ < 1) occ = 1;
   const int nlines = p.nr * p.nth;
   int grid = nsm * occ;
   if (grid > nlines) grid = nlines;
-  kern<<<grid, kFftThreadsT, smem, s>>>(p, nlines);
+  kern<<<grid, kFftThreadsF, smem, s>>>(p, nlines);
   return cudaGetLastError();
+}
+
+// the standard MHD product list, after the vectors-first reordering
+inline bool is_mhd_products(const Plan& p) {
+  if (p.nvb != 3 || p.nsb != 1 || p.nvf != 3 || p.nsf != 1 || p.nprod != 4) return false;
+  const int k[4] = {KMHD_PROD_CROSS, KMHD_PROD_CROSS, KMHD_PROD_VEC_SCALAR, KMHD_PROD_DOT};
+  const int a[4] = {1, 0, 0, 0}, b[4] = {0, 2, 0, 1};
+  for (int i = 0; i < 4; ++i)
+    if (p.pkind[i] != k[i] || p.pa[i] != a[i] || p.pb[i] != b[i]) return false;
+  return true;
+}
+
+template <int N, int MVB, int MSB, int MVF, int MSF>
+cudaError_t run_cycle_f(const Plan& p, cudaStream_t s) {
+  const bool pr = p.nph == 3 * (p.L + 1);
+  if constexpr (MVB == 3 && MSB == 1 && MVF == 3 && MSF == 1) {
+    if (is_mhd_products(p))
+      return pr ? run_cycle_fk<N, MVB, MSB, MVF, MSF, true, 1>(p, s) : run_cycle_fk<N, MVB, MSB, MVF, MSF, false, 1>(p, s);
+  }
+  return pr ? run_cycle_fk<N, MVB, MSB, MVF, MSF, true, 0>(p, s) : run_cycle_fk<N, MVB, MSB, MVF, MSF, false, 0>(p, s);
 }
 
 template <int MVB, int MSB, int MVF, int MSF>
 cudaError_t run_cycle_n(const Plan& p, cudaStream_t s, bool* handled) {
   *handled = true;
-  if (smem_cycle_t(p) <= 227 * 1024) {
+  if (smem_cycle_f(p) <= 227 * 1024) {
     switch (p.nph) {
-      case 96: return run_cycle_t<96, MVB, MSB, MVF, MSF>(p, s);
-      case 192: return run_cycle_t<192, MVB, MSB, MVF, MSF>(p, s);
-      case 384: return run_cycle_t<384, MVB, MSB, MVF, MSF>(p, s);
-      case 768: return run_cycle_t<768, MVB, MSB, MVF, MSF>(p, s);
-      case 1536: return run_cycle_t<1536, MVB, MSB, MVF, MSF>(p, s);
+      case 96: return run_cycle_f<96, MVB, MSB, MVF, MSF>(p, s);
+      case 192: return run_cycle_f<192, MVB, MSB, MVF, MSF>(p, s);
+      case 384: return run_cycle_f<384, MVB, MSB, MVF, MSF>(p, s);
+      case 768: return run_cycle_f<768, MVB, MSB, MVF, MSF>(p, s);
+      case 1536: return run_cycle_f<1536, MVB, MSB, MVF, MSF>(p, s);
       default: break;
     }
   }

@@ -143,3 +143,34 @@ def test_scalar_product_single_mode():
     # the previous Newton iterate, gauss_integration.f90:111-116), hence 1e-11
     for k in range(cfg.nr):
         assert np.abs(out[J * k:J * (k + 1), 0] - exp).max() < 1e-11
+
+
+# Grid/field shapes that select each variant of the fused FFT + products kernel:
+# N = 3 (L + 1) (zero band of the spectrum pruned) or a wider grid, the standard
+# MHD product list or a generic one, and the other compiled field counts.
+# (Nr >= 3: with two radii the synthetic spectra vanish at both ends of the
+# shell and the relative error of the degenerate output columns is noise.)
+FFT_CFGS = [
+    SphConfig(31, 48, 192, 5, name="L31_nph192"),                      # N > 3(L+1): no pruning
+    SphConfig(31, 48, 96, 4, products=((0, 0, 1, 0.5), (0, 2, 0, 2.0), (1, 1, 0, -1.0), (2, 2, 2, 1.5)),
+              name="L31_generic_products"),                            # generic product code
+    SphConfig(63, 96, 192, 3, nvb=2, nsb=1, nvf=2, nsf=1,
+              products=((0, 1, 0, 1.0), (1, 0, 0, 1.0), (2, 0, 1, 1.0)), name="L63_2v1s"),
+    SphConfig(255, 384, 768, 3, nvb=1, nsb=1, nvf=1, nsf=0, products=((1, 0, 0, 1.0),), name="L255_1v1s"),
+    SphConfig(511, 768, 1536, 3, name="L511_Nr3"),                     # the benchmark's angular grid
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cfg", FFT_CFGS, ids=lambda c: c.name)
+def test_cycle_fft_variants(cfg):
+    import torch
+    from kemorin_mhd_b200.sph_trans import SphTransform
+    tr = SphTransform(cfg)
+    orc = Oracle(cfg, nthreads=8)
+    d = make_d_rj(cfg, seed=13)
+    ref = orc.cycle(d)
+    out = torch.zeros((cfg.ncf, cfg.J * cfg.nr), dtype=torch.float64, device="cuda")
+    tr.nonlinear_cycle(to_dev_fortran(d), out)
+    err = col_relerr(from_dev_fortran(out), ref)
+    assert err.max() <= TOL, err
