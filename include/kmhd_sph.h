@@ -122,8 +122,7 @@ int kmhd_sph_cycle(kmhd_sph *handle, const double *d_rj_in, int64_t ld_in,
                    const int32_t *cols_f, int32_t ptr_kind);
 
 /* Batched uneven instances: runs kmhd_sph_cycle for n handles with device
- * pointers in one grouped launch sequence (work list over instance, m and
- * radial blocks) captured in a CUDA graph on the first handle's stream.
+ * pointers, one instance after the other (each on its handle's stream).
  * Replaces n calls of the cycle; the reference has no batched form. */
 int kmhd_sph_batch_cycle(kmhd_sph **handles, int32_t n, const double *const *d_rj_in,
                          const int64_t *ld_in, const int32_t *const *cols_b,

@@ -640,9 +640,8 @@ int kmhd_sph_batch_cycle(kmhd_sph** hs, int32_t n, const double* const* d_rj_in,
 
 }  // extern "C"
 
-// Batched instances: every instance's cycle is enqueued on the first handle's
-// stream; the enqueue sequence is captured once into a CUDA graph per distinct
-// batch signature and replayed.
+// Batched instances: the cycles run one after the other, each on its own
+// handle's stream.
 int batch_cycle_impl(kmhd_sph** hs, int32_t n, const double* const* d_rj_in, const int64_t* ld_in,
                      const int32_t* const* cols_b, double* const* d_rj_out, const int64_t* ld_out,
                      const int32_t* const* cols_f) {
