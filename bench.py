@@ -344,7 +344,7 @@ def main():
                          "(every stage is linear in Nr)",
                "stages_ms": stages}
 
-    launches = {"fp64": 4, "split": 5, "fp32acc": 5}[tier]
+    launches = {"fp64": 4, "split": 6, "fp32acc": 6}[tier]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",

@@ -110,8 +110,9 @@ cudaError_t launch_tables(const Plan& p, double* colat, double* weight, double* 
 cudaError_t launch_pack_b(const Plan& p, int nlc_max, const double* d_rj, long long ld,
                           const int* cols, int nv, int ns, cudaStream_t s);
 cudaError_t launch_leg_bwd_f64(const Plan& p, cudaStream_t s);
+// m_count: run orders m < m_count only (0 = all orders)
 cudaError_t launch_leg_fwd_f64(const Plan& p, double* d_rj, long long ld, const int* cols,
-                               cudaStream_t s);
+                               cudaStream_t s, int m_count = 0);
 cudaError_t launch_fft_cycle(const Plan& p, cudaStream_t s);
 cudaError_t launch_fft_bwd_grid(const Plan& p, double* fld, cudaStream_t s);
 cudaError_t launch_fft_fwd_grid(const Plan& p, const double* frc, cudaStream_t s);

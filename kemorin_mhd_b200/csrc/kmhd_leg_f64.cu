@@ -467,12 +467,12 @@ cudaError_t run_bwd(const Plan& p, cudaStream_t s) {
 }
 
 template <int NV, int NS>
-cudaError_t run_fwd(const Plan& p, double* d_rj, long long ld, const int* cols, cudaStream_t s) {
+cudaError_t run_fwd(const Plan& p, double* d_rj, long long ld, const int* cols, cudaStream_t s, int m_count) {
   using G = FwdGeo<NV, NS>;
   auto kern = k_leg_fwd_f64<NV, NS>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
   const int nkb = (kcount(p.L, 0, 0) + kLBlk - 1) / kLBlk;
-  dim3 grid(nkb * p.nrb, p.L + 1);
+  dim3 grid(nkb * p.nrb, m_count);
   kern<<<grid, kThreads, G::SMEM, s>>>(p, d_rj, ld, cols);
   return cudaGetLastError();
 }
@@ -514,8 +514,9 @@ cudaError_t launch_leg_bwd_f64(const Plan& p, cudaStream_t s) {
 }
 
 cudaError_t launch_leg_fwd_f64(const Plan& p, double* d_rj, long long ld, const int* cols,
-                               cudaStream_t s) {
-  KMHD_DISPATCH(p.nvf, p.nsf, run_fwd, p, d_rj, ld, cols, s);
+                               cudaStream_t s, int m_count) {
+  if (m_count <= 0 || m_count > p.L + 1) m_count = p.L + 1;
+  KMHD_DISPATCH(p.nvf, p.nsf, run_fwd, p, d_rj, ld, cols, s, m_count);
 }
 
 size_t bwd_smem_bytes(int nv, int ns) {

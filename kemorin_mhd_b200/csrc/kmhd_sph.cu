@@ -431,7 +431,14 @@ int run_bwd_spectral(kmhd_sph* h, const double* d_rj, int64_t ld) {
 
 int run_fwd_spectral(kmhd_sph* h, double* d_rj, int64_t ld) {
   const Plan& p = h->plan;
-  if (h->split) return split_fwd(h->split, p, d_rj, ld, h->cols_f_d, h->stream, h->ev_mid[1]);
+  if (h->split) {
+    // split tiers: slicer + INT8 GEMM for every mode, then the dipole (l <= 2)
+    // modes are accumulated again in FP64 by the DMMA kernel over orders m <= 2
+    const int st = split_fwd(h->split, p, d_rj, ld, h->cols_f_d, h->stream, h->ev_mid[1]);
+    if (st != KMHD_OK) return st;
+    KCHECK(launch_leg_fwd_f64(p, d_rj, ld, h->cols_f_d, h->stream, std::min(3, p.L + 1)));
+    return KMHD_OK;
+  }
   KCHECK(cudaEventRecord(h->ev_mid[1], h->stream));  // the FP64 forward GEMM packs its operands itself
   KCHECK(launch_leg_fwd_f64(p, d_rj, ld, h->cols_f_d, h->stream));
   return KMHD_OK;

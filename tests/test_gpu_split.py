@@ -83,3 +83,29 @@ def test_split_cycle(case):
     tr.nonlinear_cycle(to_dev_fortran(d), out)
     err = col_relerr(from_dev_fortran(out), ref)
     assert err.max() <= TOL[tier], err
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tier", [TIER_SPLIT_I8, TIER_FP32ACC])
+def test_split_dipole_modes_fp64(tier):
+    """The orders m <= 2 (all dipole l <= 2 modes among them) of the forward
+    transform are accumulated in FP64 in both split tiers: FP64 tolerance 1e-13
+    on those rows of sph_f_trans, whatever the tier's bound on the others."""
+    import torch
+    from kemorin_mhd_b200.config import rj_order
+    from kemorin_mhd_b200.sph_trans import SphTransform
+    cfg = SphConfig(31, 48, 96, 5, name="L31_dipole")
+    tr = SphTransform(cfg, tier=tier)
+    orc = Oracle(cfg, nthreads=8)
+    rng = np.random.default_rng(17)
+    nnod = cfg.nr * cfg.nth * cfg.nph
+    frc = np.asfortranarray(rng.standard_normal((nnod, cfg.ncf)))
+    ref = orc.f_trans(frc)
+    out = torch.zeros((cfg.ncf, cfg.J * cfg.nr), dtype=torch.float64, device="cuda")
+    tr.sph_f_trans(to_dev_fortran(frc), out)
+    got = from_dev_fortran(out)
+    l, m = rj_order(cfg.ltr)
+    rows = np.concatenate([np.where(np.abs(m) <= 2)[0] + cfg.J * k for k in range(cfg.nr)])
+    den = np.abs(ref).max(axis=0)
+    err = (np.abs(got[rows] - ref[rows]).max(axis=0) / den).max()
+    assert err <= 1e-13, err
