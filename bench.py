@@ -176,6 +176,8 @@ def main():
     ap.add_argument("--nr", type=int, default=0, help="override the radius count (small profiling cases)")
     args = ap.parse_args()
 
+    if args.config == "cfg4":
+        return run_batch(args)
     from kemorin_mhd_b200.config import NAMED, SphConfig
     cfg = NAMED[args.config]
     if args.nr > 0:
@@ -363,6 +365,77 @@ def main():
     tr.close()
     if dist is not None:
         dist.destroy_process_group()
+    return 0
+
+
+def run_batch(args):
+    """cfg4: 64 uneven instances.  Baseline: the 64 plain FP64 cycles run one
+    after the other (each a synchronous call); then the split tier with the
+    path autotuner as one batched call (captured CUDA graph, every instance on
+    its own stream).  Host wall clock around whole synchronous calls."""
+    import torch
+    from kemorin_mhd_b200 import sph_trans
+    from kemorin_mhd_b200.config import batch_configs
+    from kemorin_mhd_b200.synthetic import make_d_rj_torch
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    cfgs = batch_configs()
+    n = len(cfgs)
+    d_in = [make_d_rj_torch(c, seed=500 + i) for i, c in enumerate(cfgs)]
+
+    def outs():
+        return [torch.zeros((c.ncf, c.J * c.nr), dtype=torch.float64, device="cuda") for c in cfgs]
+
+    # baseline: sequential plain FP64 cycles
+    trs = [sph_trans.SphTransform(c, tier=0, device=local) for c in cfgs]
+    o64 = outs()
+    for _ in range(max(1, args.warmup)):
+        for tr, d, o in zip(trs, d_in, o64):
+            tr.nonlinear_cycle(d, o)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for tr, d, o in zip(trs, d_in, o64):
+            tr.nonlinear_cycle(d, o)
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    for tr in trs:
+        tr.close()
+    del trs
+    torch.cuda.empty_cache()
+    # batched split tier with the path autotuner
+    trs = [sph_trans.SphTransform(c, tier=TIERS["split"], device=local, autotune=True) for c in cfgs]
+    ob = outs()
+    for _ in range(max(1, args.warmup)):
+        sph_trans.batch_cycle(trs, d_in, ob)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sph_trans.batch_cycle(trs, d_in, ob)
+    torch.cuda.synchronize()
+    t_b = time.perf_counter() - t0
+    clk = clocks.stop()
+    err = max(float(((a - b).abs().amax(dim=1) / b.abs().amax(dim=1)).max()) for a, b in zip(ob, o64))
+    nsplit = sum(1 for tr in trs if tr.uses_split())
+    value = n * args.steps / t_b
+    line = {
+        "metric": "batched uneven instance cycles/s (cfg4: 64 instances, L in {63,127,255}, Nr in {33,65,129}, 2-4 fields)",
+        "value": value, "unit": "instance cycles/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t_b / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": DTYPES["split"], "data": "synthetic (seeded spectra, as cfg3)",
+        "config": {"workload": "cfg4_batch64", "instances": n, "timing": "host wall clock around synchronous calls"},
+        "fp64_sequential": {"value": n * args.steps / t_seq, "unit": "instance cycles/s",
+                            "ms_per_step": 1e3 * t_seq / args.steps},
+        "speedup_vs_fp64_sequential": t_seq / t_b,
+        "autotuned_split_instances": nsplit, "autotuned_fp64_instances": n - nsplit,
+        "rel_err_vs_fp64_max": err, "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for tr in trs:
+        tr.close()
     return 0
 
 

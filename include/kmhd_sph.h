@@ -76,10 +76,15 @@ typedef struct kmhd_sph_desc {
   int32_t tier;                   /* enum kmhd_tier                            */
   int32_t nslice;                 /* split tiers: slices per operand, 0=default */
   int32_t device;                 /* CUDA device ordinal                       */
-  int32_t flags;                  /* reserved, 0                               */
+  int32_t flags;                  /* KMHD_FLAG_* bits, 0 = none                */
 } kmhd_sph_desc;
 
 typedef struct kmhd_sph kmhd_sph;
+
+/* kmhd_sph_desc.flags: for the split tiers, time the FP64 DMMA path against
+ * the split path on the first kmhd_sph_batch_cycle call and keep the faster
+ * (both meet the tier's error bound).  The reference has no counterpart. */
+#define KMHD_FLAG_AUTOTUNE 1
 
 /* Pointer-location flag for data arguments. */
 #define KMHD_PTR_DEVICE 0
@@ -121,9 +126,14 @@ int kmhd_sph_cycle(kmhd_sph *handle, const double *d_rj_in, int64_t ld_in,
                    const int32_t *cols_b, double *d_rj_out, int64_t ld_out,
                    const int32_t *cols_f, int32_t ptr_kind);
 
-/* Batched uneven instances: runs kmhd_sph_cycle for n handles with device
- * pointers, one instance after the other (each on its handle's stream).
- * Replaces n calls of the cycle; the reference has no batched form. */
+/* Batched uneven instances: n cycles (device pointers) of possibly different
+ * L, Nr and field counts.  Every instance runs on its own handle's stream; one
+ * CUDA graph, captured on the first call and replayed while handles, pointers
+ * and leading dimensions stay the same, forks them all and joins them, so small
+ * instances fill the GPU together.  Handles created with KMHD_FLAG_AUTOTUNE
+ * pick their Legendre path by timing on the first call.  Returns after all
+ * instances finished.  Replaces n calls of the cycle; the reference has no
+ * batched form. */
 int kmhd_sph_batch_cycle(kmhd_sph **handles, int32_t n, const double *const *d_rj_in,
                          const int64_t *ld_in, const int32_t *const *cols_b,
                          double *const *d_rj_out, const int64_t *ld_out,
@@ -168,6 +178,10 @@ int kmhd_sph_get_tables(kmhd_sph *handle, int32_t m, double *colat, double *weig
 int kmhd_sph_cycle_noalloc(const kmhd_sph_desc *desc, const double *d_rj_in, int64_t ld_in,
                            const int32_t *cols_b, double *d_rj_out, int64_t ld_out,
                            const int32_t *cols_f, void *stream);
+
+/* Legendre path the handle runs: 1 = the tier's split path, 0 = FP64 DMMA
+ * (FP64 tier, or a split-tier handle the autotuner moved to FP64). */
+int kmhd_sph_get_path(const kmhd_sph *handle, int32_t *path);
 
 /* Device bytes held by the handle. */
 int64_t kmhd_sph_device_bytes(const kmhd_sph *handle);

@@ -17,6 +17,15 @@ size_t fft_smem_bytes(const Plan& p, int npair);
 
 using namespace kmhd;
 
+struct BatchGraph {
+  std::vector<const void*> sig;  // per instance: handle, in, out, lds, path
+  std::vector<int64_t> sig_ld;
+  cudaStream_t s0 = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+};
+
 struct kmhd_sph {
   kmhd_sph_desc desc;
   Plan plan;
@@ -42,6 +51,11 @@ struct kmhd_sph {
   double *stage_in = nullptr, *stage_out = nullptr, *stage_grid = nullptr;
   // split-precision state
   SplitState* split = nullptr;
+  bool use_split = true;   // split tiers: run the split path (false: the FP64 DMMA path)
+  bool autotune = false;   // choose use_split by timing on the first batch call
+  bool tuned = false;
+  // batched cycles whose first handle this is: captured graph and its signature
+  struct BatchGraph* batch = nullptr;
   // timing
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t ev_mid[2] = {nullptr, nullptr};  // after the bwd pack/slicer, after the fwd slicer
@@ -170,11 +184,24 @@ const char* kmhd_strerror(int status) {
 
 int64_t kmhd_sph_device_bytes(const kmhd_sph* h) { return h ? h->bytes : 0; }
 
+int kmhd_sph_get_path(const kmhd_sph* h, int32_t* path) {
+  if (!h || !path) return KMHD_ERR_ARG;
+  *path = (h->split && h->use_split) ? 1 : 0;
+  return KMHD_OK;
+}
+
 int kmhd_sph_destroy(kmhd_sph* h) {
   if (!h) return KMHD_ERR_ARG;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->split) split_destroy(h->split);
+  if (h->batch) {
+    if (h->batch->exec) cudaGraphExecDestroy(h->batch->exec);
+    if (h->batch->fork) cudaEventDestroy(h->batch->fork);
+    for (cudaEvent_t e : h->batch->join) cudaEventDestroy(e);
+    if (h->batch->s0) cudaStreamDestroy(h->batch->s0);
+    delete h->batch;
+  }
   for (void* p : h->allocs) cudaFree(p);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
@@ -361,6 +388,7 @@ int kmhd_sph_create(const kmhd_sph_desc* d, kmhd_sph** out) {
   p.digrev = h->digrev;
   if (launch_tables(p, h->colat, h->weight, h->asin_t, h->P, h->dP, s) != cudaSuccess)
     return fail(KMHD_ERR_CUDA);
+  h->autotune = (d->flags & KMHD_FLAG_AUTOTUNE) != 0 && d->tier != KMHD_TIER_FP64;
   if (d->tier != KMHD_TIER_FP64) {
     st = split_create(&h->split, p, d->tier, d->nslice, s);
     if (st != KMHD_OK) return fail(st);
@@ -417,31 +445,40 @@ int timed_begin(kmhd_sph* h) {
   return KMHD_OK;
 }
 
-int run_bwd_spectral(kmhd_sph* h, const double* d_rj, int64_t ld) {
+int run_bwd_spectral(kmhd_sph* h, const double* d_rj, int64_t ld, bool timed = true) {
   const Plan& p = h->plan;
-  if (h->split) {
-    int st = split_bwd(h->split, p, h->nlc_max, d_rj, ld, h->cols_b_d, h->stream, h->ev_mid[0]);
+  if (h->split && h->use_split) {
+    int st = split_bwd(h->split, p, h->nlc_max, d_rj, ld, h->cols_b_d, h->stream, timed ? h->ev_mid[0] : nullptr);
     return st;
   }
   KCHECK(launch_pack_b(p, h->nlc_max, d_rj, ld, h->cols_b_d, p.nvb, p.nsb, h->stream));
-  KCHECK(cudaEventRecord(h->ev_mid[0], h->stream));
+  if (timed) KCHECK(cudaEventRecord(h->ev_mid[0], h->stream));
   KCHECK(launch_leg_bwd_f64(p, h->stream));
   return KMHD_OK;
 }
 
-int run_fwd_spectral(kmhd_sph* h, double* d_rj, int64_t ld) {
+int run_fwd_spectral(kmhd_sph* h, double* d_rj, int64_t ld, bool timed = true) {
   const Plan& p = h->plan;
-  if (h->split) {
+  if (h->split && h->use_split) {
     // split tiers: slicer + INT8 GEMM for every mode, then the dipole (l <= 2)
     // modes are accumulated again in FP64 by the DMMA kernel over orders m <= 2
-    const int st = split_fwd(h->split, p, d_rj, ld, h->cols_f_d, h->stream, h->ev_mid[1]);
+    const int st = split_fwd(h->split, p, d_rj, ld, h->cols_f_d, h->stream, timed ? h->ev_mid[1] : nullptr);
     if (st != KMHD_OK) return st;
     KCHECK(launch_leg_fwd_f64(p, d_rj, ld, h->cols_f_d, h->stream, std::min(3, p.L + 1)));
     return KMHD_OK;
   }
-  KCHECK(cudaEventRecord(h->ev_mid[1], h->stream));  // the FP64 forward GEMM packs its operands itself
+  if (timed) KCHECK(cudaEventRecord(h->ev_mid[1], h->stream));  // the FP64 forward GEMM packs its operands itself
   KCHECK(launch_leg_fwd_f64(p, d_rj, ld, h->cols_f_d, h->stream));
   return KMHD_OK;
+}
+
+// One cycle with device pointers on the handle's stream, columns already on
+// the device; no host synchronisation (safe inside stream capture).
+int enqueue_cycle(kmhd_sph* h, const double* in, int64_t ld_in, double* out, int64_t ld_out) {
+  int st;
+  if ((st = run_bwd_spectral(h, in, ld_in, false))) return st;
+  KCHECK(launch_fft_cycle(h->plan, h->stream));
+  return run_fwd_spectral(h, out, ld_out, false);
 }
 
 int finish_timing(kmhd_sph* h) {
@@ -647,18 +684,136 @@ int kmhd_sph_batch_cycle(kmhd_sph** hs, int32_t n, const double* const* d_rj_in,
 
 }  // extern "C"
 
-// Batched instances: the cycles run one after the other, each on its own
-// handle's stream.
+// Batched instances.  Every instance runs on its own handle's stream; one
+// captured CUDA graph forks them all from an internal stream and joins them,
+// so small instances fill the GPU together.  The graph is kept in the first
+// handle and replayed while the batch (handles, pointers, leading dimensions,
+// paths) stays the same.  Handles created with KMHD_FLAG_AUTOTUNE first time
+// the FP64 DMMA path and their split path on the call's own data and keep the
+// faster one (both meet the tier's error bound).
+namespace {
+
+int autotune_path(kmhd_sph* h, const double* in, int64_t ld_in, double* out, int64_t ld_out) {
+  float ms[2] = {0, 0};
+  for (int rep = 0; rep < 2; ++rep) {  // first round warms up
+    for (int path = 0; path < 2; ++path) {
+      h->use_split = path == 1;
+      KCHECK(cudaEventRecord(h->ev[0], h->stream));
+      const int st = enqueue_cycle(h, in, ld_in, out, ld_out);
+      if (st) return st;
+      KCHECK(cudaEventRecord(h->ev[3], h->stream));
+      KCHECK(cudaEventSynchronize(h->ev[3]));
+      KCHECK(cudaEventElapsedTime(&ms[path], h->ev[0], h->ev[3]));
+    }
+  }
+  h->use_split = ms[1] < ms[0];
+  h->tuned = true;
+  return KMHD_OK;
+}
+
+int batch_direct(kmhd_sph** hs, int32_t n, const double* const* in, const int64_t* ld_in, double* const* out,
+                 const int64_t* ld_out) {
+  for (int i = 0; i < n; ++i) {
+    const int st = enqueue_cycle(hs[i], in[i], ld_in[i], out[i], ld_out[i]);
+    if (st) return st;
+  }
+  for (int i = 0; i < n; ++i) KCHECK(cudaStreamSynchronize(hs[i]->stream));
+  return KMHD_OK;
+}
+
+}  // namespace
+
 int batch_cycle_impl(kmhd_sph** hs, int32_t n, const double* const* d_rj_in, const int64_t* ld_in,
                      const int32_t* const* cols_b, double* const* d_rj_out, const int64_t* ld_out,
                      const int32_t* const* cols_f) {
   if (!hs || n <= 0 || !d_rj_in || !ld_in || !cols_b || !d_rj_out || !ld_out || !cols_f)
     return KMHD_ERR_ARG;
+  int st;
   for (int i = 0; i < n; ++i) {
-    if (!hs[i]) return KMHD_ERR_ARG;
-    const int st = kmhd_sph_cycle(hs[i], d_rj_in[i], ld_in[i], cols_b[i], d_rj_out[i], ld_out[i],
-                                  cols_f[i], KMHD_PTR_DEVICE);
-    if (st) return st;
+    kmhd_sph* h = hs[i];
+    if (!h || !d_rj_in[i] || !d_rj_out[i]) return KMHD_ERR_ARG;
+    if (h->device != hs[0]->device) return KMHD_ERR_ARG;
+    if (check_ld(h, ld_in[i]) || check_ld(h, ld_out[i])) return KMHD_ERR_ARG;
+    if (h->plan.ncf == 0 || h->plan.nprod == 0) return KMHD_ERR_STATE;
   }
+  KCHECK(cudaSetDevice(hs[0]->device));
+  // column tables to the device (may synchronise: before any capture)
+  for (int i = 0; i < n; ++i) {
+    kmhd_sph* h = hs[i];
+    const Plan& p = h->plan;
+    if ((st = sync_cols(h, cols_b[i], p.nvb + p.nsb, h->cols_b_cache, h->cols_b_d))) return st;
+    if ((st = sync_cols(h, cols_f[i], p.nvf + p.nsf, h->cols_f_cache, h->cols_f_d))) return st;
+  }
+  for (int i = 0; i < n; ++i)
+    if (hs[i]->autotune && !hs[i]->tuned && (st = autotune_path(hs[i], d_rj_in[i], ld_in[i], d_rj_out[i], ld_out[i])))
+      return st;
+  for (int i = 0; i < n; ++i) hs[i]->kernel_timed = false;
+  // graph capture needs every instance on a capturable (non-legacy) stream
+  bool capturable = true;
+  for (int i = 0; i < n; ++i)
+    if (hs[i]->stream == nullptr || hs[i]->stream == cudaStreamLegacy) capturable = false;
+  if (!capturable) {
+    if ((st = batch_direct(hs, n, d_rj_in, ld_in, d_rj_out, ld_out))) return st;
+  } else {
+    std::vector<const void*> sig;
+    std::vector<int64_t> sig_ld;
+    for (int i = 0; i < n; ++i) {
+      sig.push_back(hs[i]);
+      sig.push_back(d_rj_in[i]);
+      sig.push_back(d_rj_out[i]);
+      sig.push_back(hs[i]->use_split ? hs[i] : nullptr);
+      sig.push_back(hs[i]->stream);
+      sig_ld.push_back(ld_in[i]);
+      sig_ld.push_back(ld_out[i]);
+    }
+    kmhd_sph* h0 = hs[0];
+    if (!h0->batch) h0->batch = new BatchGraph();
+    BatchGraph* bg = h0->batch;
+    if (!bg->exec || bg->sig != sig || bg->sig_ld != sig_ld) {
+      if (bg->exec) {
+        cudaGraphExecDestroy(bg->exec);
+        bg->exec = nullptr;
+      }
+      if (!bg->s0) KCHECK(cudaStreamCreateWithFlags(&bg->s0, cudaStreamNonBlocking));
+      if (!bg->fork) KCHECK(cudaEventCreateWithFlags(&bg->fork, cudaEventDisableTiming));
+      while ((int)bg->join.size() < n) {
+        cudaEvent_t e;
+        KCHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        bg->join.push_back(e);
+      }
+      cudaGraph_t graph = nullptr;
+      KCHECK(cudaStreamBeginCapture(bg->s0, cudaStreamCaptureModeRelaxed));
+      int cst = KMHD_OK;
+      if (cudaEventRecord(bg->fork, bg->s0) != cudaSuccess) cst = KMHD_ERR_CUDA;
+      for (int i = 0; i < n && cst == KMHD_OK; ++i) {
+        if (cudaStreamWaitEvent(hs[i]->stream, bg->fork, 0) != cudaSuccess) { cst = KMHD_ERR_CUDA; break; }
+        cst = enqueue_cycle(hs[i], d_rj_in[i], ld_in[i], d_rj_out[i], ld_out[i]);
+        if (cst) break;
+        if (cudaEventRecord(bg->join[i], hs[i]->stream) != cudaSuccess ||
+            cudaStreamWaitEvent(bg->s0, bg->join[i], 0) != cudaSuccess)
+          cst = KMHD_ERR_CUDA;
+      }
+      const cudaError_t ec = cudaStreamEndCapture(bg->s0, &graph);
+      if (cst == KMHD_OK && ec == cudaSuccess && graph) {
+        if (cudaGraphInstantiate(&bg->exec, graph, 0) != cudaSuccess) bg->exec = nullptr;
+      }
+      if (graph) cudaGraphDestroy(graph);
+      cudaGetLastError();  // clear a failed capture's error state
+      bg->sig = sig;
+      bg->sig_ld = sig_ld;
+      if (!bg->exec) bg->sig.clear();
+    }
+    if (bg->exec) {
+      KCHECK(cudaGraphLaunch(bg->exec, bg->s0));
+      KCHECK(cudaStreamSynchronize(bg->s0));
+    } else if ((st = batch_direct(hs, n, d_rj_in, ld_in, d_rj_out, ld_out))) {
+      return st;
+    }
+  }
+  for (int i = 0; i < n; ++i)
+    if (hs[i]->split) {
+      const int e = split_check_error(hs[i]->split, hs[i]->stream);
+      if (e != KMHD_OK) return e;
+    }
   return KMHD_OK;
 }

@@ -54,7 +54,7 @@ class Desc(ctypes.Structure):
 EXPORTS = ["kmhd_sph_create", "kmhd_sph_destroy", "kmhd_sph_set_stream", "kmhd_sph_b_trans",
            "kmhd_sph_f_trans", "kmhd_sph_cycle", "kmhd_sph_batch_cycle", "kmhd_sph_last_timing",
            "kmhd_sph_get_tables", "kmhd_sph_device_bytes", "kmhd_strerror", "kmhd_sph_cycle_noalloc",
-           "kmhd_sph_last_kernel_timing"]
+           "kmhd_sph_last_kernel_timing", "kmhd_sph_get_path"]
 
 _lib = None
 
@@ -81,6 +81,7 @@ def load_library(path: str | None = None):
                                          ctypes.POINTER(vp), ctypes.POINTER(i64), ctypes.POINTER(ip)]
     lib.kmhd_sph_last_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     lib.kmhd_sph_last_kernel_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+    lib.kmhd_sph_get_path.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
     lib.kmhd_sph_get_tables.argtypes = [vp, i32] + [ctypes.POINTER(ctypes.c_double)] * 4
     lib.kmhd_sph_device_bytes.restype = i64
     lib.kmhd_sph_device_bytes.argtypes = [vp]
@@ -126,7 +127,7 @@ class SphTransform:
     """One transform instance on one GPU (handle of the C-ABI)."""
 
     def __init__(self, cfg: SphConfig, tier: int = 0, nslice: int = 0, device: int = 0,
-                 radius=None, idx_rj_lm=None):
+                 radius=None, idx_rj_lm=None, autotune: bool = False):
         lib = load_library()
         self.cfg = cfg
         self.tier = tier
@@ -144,7 +145,7 @@ class SphTransform:
         d.nvector_b, d.nscalar_b, d.nvector_f, d.nscalar_f = cfg.nvb, cfg.nsb, cfg.nvf, cfg.nsf
         d.nproduct = len(cfg.products)
         d.products = prods
-        d.tier, d.nslice, d.device, d.flags = tier, nslice, device, 0
+        d.tier, d.nslice, d.device, d.flags = tier, nslice, device, (1 if autotune else 0)
         self._desc = d
         h = ctypes.c_void_p()
         _check(lib.kmhd_sph_create(ctypes.byref(d), ctypes.byref(h)), "kmhd_sph_create")
@@ -177,6 +178,12 @@ class SphTransform:
         t = (ctypes.c_double * 4)()
         _check(load_library().kmhd_sph_last_timing(self._h, t), "last_timing")
         return dict(leg_bwd=t[0], fft_nl=t[1], leg_fwd=t[2], total=t[3])
+
+    def uses_split(self) -> bool:
+        """True when the handle runs the split-precision Legendre path."""
+        v = ctypes.c_int32()
+        _check(load_library().kmhd_sph_get_path(self._h, ctypes.byref(v)), "get_path")
+        return v.value == 1
 
     def kernel_timing(self):
         """Per-launch ms of the last cycle (CUDA events on the handle's stream)."""
