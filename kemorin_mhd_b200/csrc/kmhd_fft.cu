@@ -16,6 +16,7 @@
 // Products: cal_cross_prod_w_coef_smp, cal_vec_scalar_prod_w_coef_smp,
 // cal_dot_prod_w_coef_smp (CORE_src/BASE/cal_products_smp.f90) as called by
 // nonlinear_terms_in_rtp (MHD_src/sph_MHD/cal_nonlinear_sph_MHD.f90:64-128).
+#include <algorithm>
 #include <utility>
 
 #include "kmhd_internal.cuh"
@@ -409,6 +410,147 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_cycle(Plan P, int nlines) {
     store_line(z, npf, P, P.rtm_f, P.ncf, P.nvf, th, r);
     __syncthreads();
     line = next;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Wide lines (one line of every component does not fit in shared memory, e.g.
+// Nphi = 3072 with 10 components): the pairs go through shared memory one at a
+// time.  The cycle keeps the line's grid in a per-CTA global scratch
+// (pairs x N x 16 bytes, L2-resident), forms the products there and runs the
+// forward transforms pair by pair from it.
+
+// First inverse pass of pair pp only: spectra from the staged records, output z[0 .. N).
+template <int R>
+__device__ void dif_first_one(const double* st, int nc, int nv, int pp, double2* z, int N, int L,
+                              const double2* __restrict__ tw) {
+  const int s = N / R;
+  for (int j = threadIdx.x; j < s; j += blockDim.x) {
+    double2 x[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) x[r] = spec_at(st, nc, nv, pp, j + r * s, N, L);
+    DFT<R, +1>::run(x);
+    z[j] = x[0];
+#pragma unroll
+    for (int q = 1; q < R; ++q) z[j + q * s] = cmul(x[q], twd<+1>(tw, j * q));
+  }
+}
+__device__ void dif_first_one_dispatch(int R, const double* st, int nc, int nv, int pp, double2* z, int N, int L,
+                                       const double2* tw) {
+  switch (R) {
+    case 8: dif_first_one<8>(st, nc, nv, pp, z, N, L, tw); break;
+    case 4: dif_first_one<4>(st, nc, nv, pp, z, N, L, tw); break;
+    case 2: dif_first_one<2>(st, nc, nv, pp, z, N, L, tw); break;
+    case 3: dif_first_one<3>(st, nc, nv, pp, z, N, L, tw); break;
+    default: dif_first_one<5>(st, nc, nv, pp, z, N, L, tw); break;
+  }
+}
+// Natural-order forward spectrum of pair q in z -> (a_m, b_m), m <= L, into rtm.
+__device__ void store_one(const double2* z, int q, const Plan& P, double* rtm, int nc, int nv, int th, int r) {
+  const int N = P.nph, L = P.L;
+  const double aN = 1.0 / (double)N;
+  const long long strideM = (long long)P.nth * P.nr * nc * 2;
+  double* base = rtm + ((long long)th * P.nr + r) * nc * 2;
+  for (int m = threadIdx.x; m <= L; m += blockDim.x) {
+    const double2 zm = z[m];
+    double a0, b0, a1, b1;
+    if (m == 0) {
+      a0 = zm.x * aN; a1 = zm.y * aN; b0 = 0.0; b1 = 0.0;
+    } else {
+      const double2 wm = z[N - m];
+      a0 = (zm.x + wm.x) * aN;
+      b0 = (wm.y - zm.y) * aN;
+      a1 = (zm.y + wm.y) * aN;
+      b1 = (zm.x - wm.x) * aN;
+    }
+    double* rec = base + m * strideM;
+    *reinterpret_cast<double2*>(rec + rec_off(2 * q, nv)) = make_double2(a0, b0);
+    if (2 * q + 1 < nc) *reinterpret_cast<double2*>(rec + rec_off(2 * q + 1, nv)) = make_double2(a1, b1);
+  }
+}
+
+template <int MVB, int MSB, int MVF, int MSF>
+__global__ void __launch_bounds__(kFftThreads) k_fft_cycle_wide(Plan P, int nlines) {
+  extern __shared__ double4 smraw[];
+  const int N = P.nph;
+  const int npb = (P.ncb + 1) / 2, npf = (P.ncf + 1) / 2;
+  const int npm = npb > npf ? npb : npf;
+  double2* z = reinterpret_cast<double2*>(smraw);
+  double* st = reinterpret_cast<double*>(z + N);
+  double2* sc = P.fft_scratch + (long long)blockIdx.x * npm * N;
+  for (int line = blockIdx.x; line < nlines; line += gridDim.x) {
+    const int r = line % P.nr, th = line / P.nr;
+    prefetch_line(st, P.rtm_b, P.ncb, P, th, r);
+    cp_async_wait<0>();
+    __syncthreads();
+    for (int pp = 0; pp < npb; ++pp) {
+      dif_first_one_dispatch(P.fac[0], st, P.ncb, P.nvb, pp, z, N, P.L, P.twid);
+      __syncthreads();
+      dif_rest(z, 1, N, P, P.twid);
+      for (int i = threadIdx.x; i < N; i += blockDim.x) sc[(long long)pp * N + i] = z[i];
+      __syncthreads();
+    }
+    products<MVB, MSB, MVF, MSF>(sc, N, P);
+    __syncthreads();
+    for (int q = 0; q < npf; ++q) {
+      for (int i = threadIdx.x; i < N; i += blockDim.x) z[i] = sc[(long long)q * N + i];
+      __syncthreads();
+      dit_all(z, 1, N, P, P.twid);
+      store_one(z, q, P, P.rtm_f, P.ncf, P.nvf, th, r);
+      __syncthreads();
+    }
+  }
+}
+
+// Separable backward for wide lines: one pair at a time straight to the grid.
+__global__ void __launch_bounds__(kFftThreads) k_fft_bwd_grid_wide(Plan P, double* __restrict__ fld) {
+  extern __shared__ double4 smraw[];
+  const int N = P.nph;
+  const int npb = (P.ncb + 1) / 2;
+  double2* z = reinterpret_cast<double2*>(smraw);
+  double* st = reinterpret_cast<double*>(z + N);
+  const int line = blockIdx.x;
+  const int r = line % P.nr, th = line / P.nr;
+  const long long nnod = (long long)P.nr * P.nth * N;
+  prefetch_line(st, P.rtm_b, P.ncb, P, th, r);
+  cp_async_wait<0>();
+  __syncthreads();
+  for (int pp = 0; pp < npb; ++pp) {
+    dif_first_one_dispatch(P.fac[0], st, P.ncb, P.nvb, pp, z, N, P.L, P.twid);
+    __syncthreads();
+    dif_rest(z, 1, N, P, P.twid);
+    const int nc2 = 2 * pp + 1 < P.ncb ? 2 : 1;
+    for (int it = threadIdx.x; it < N * nc2; it += blockDim.x) {
+      const int c = it / N, pos = it % N;
+      const int phi = P.digrev[pos];
+      const double2 v = z[pos];
+      fld[(long long)r + (long long)P.nr * (th + (long long)P.nth * phi) + nnod * (2 * pp + c)] = c ? v.y : v.x;
+    }
+    __syncthreads();
+  }
+}
+
+// Separable forward for wide lines: one pair at a time from the grid.
+__global__ void __launch_bounds__(kFftThreads) k_fft_fwd_grid_wide(Plan P, const double* __restrict__ frc) {
+  extern __shared__ double4 smraw[];
+  const int N = P.nph;
+  const int npf = (P.ncf + 1) / 2;
+  double2* z = reinterpret_cast<double2*>(smraw);
+  const int line = blockIdx.x;
+  const int r = line % P.nr, th = line / P.nr;
+  const long long nnod = (long long)P.nr * P.nth * N;
+  for (int q = 0; q < npf; ++q) {
+    for (int pos = threadIdx.x; pos < N; pos += blockDim.x) {
+      const int phi = P.digrev[pos];
+      const long long node = (long long)r + (long long)P.nr * (th + (long long)P.nth * phi);
+      const double lo = frc[node + nnod * (2 * q)];
+      const double hi = (2 * q + 1 < P.ncf) ? frc[node + nnod * (2 * q + 1)] : 0.0;
+      z[pos] = make_double2(lo, hi);
+    }
+    __syncthreads();
+    dit_all(z, 1, N, P, P.twid);
+    store_one(z, q, P, P.rtm_f, P.ncf, P.nvf, th, r);
+    __syncthreads();
   }
 }
 
@@ -1021,12 +1163,37 @@ cudaError_t run_cycle(const Plan& p, cudaStream_t s) {
 
 }  // namespace
 
+bool fft_line_fits(const Plan& p) {
+  return smem_cycle(p) <= 227 * 1024 || smem_cycle_f(p) <= 227 * 1024;
+}
+
 size_t fft_smem_bytes(const Plan& p, int npair) {
   (void)npair;
   return smem_cycle(p);
 }
 
+size_t smem_wide(const Plan& p) {
+  return sizeof(double2) * (size_t)p.nph + sizeof(double) * 2 * (size_t)(p.L + 1) * p.ncb;
+}
+
+template <int MVB, int MSB, int MVF, int MSF>
+cudaError_t run_cycle_wide(const Plan& p, cudaStream_t s) {
+  auto kern = k_fft_cycle_wide<MVB, MSB, MVF, MSF>;
+  const size_t smem = smem_wide(p);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  if (!p.fft_scratch) return cudaErrorInvalidValue;
+  const int nlines = p.nr * p.nth;
+  const int grid = std::min(p.fft_scratch_ctas, nlines);
+  kern<<<grid, kFftThreads, smem, s>>>(p, nlines);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_fft_cycle(const Plan& p, cudaStream_t s) {
+  if (smem_cycle(p) > 227 * 1024 && smem_cycle_f(p) > 227 * 1024) {
+    if (p.nvb == 3 && p.nsb == 1 && p.nvf == 3 && p.nsf == 1) return run_cycle_wide<3, 1, 3, 1>(p, s);
+    return run_cycle_wide<kMaxVec, kMaxScl, kMaxVec, kMaxScl>(p, s);
+  }
   if (p.nvb == 3 && p.nsb == 1 && p.nvf == 3 && p.nsf == 1) {
     bool handled = false;
     const cudaError_t e = run_cycle_n<3, 1, 3, 1>(p, s, &handled);
@@ -1051,6 +1218,13 @@ cudaError_t launch_fft_cycle(const Plan& p, cudaStream_t s) {
 cudaError_t launch_fft_bwd_grid(const Plan& p, double* fld, cudaStream_t s) {
   const int npb = (p.ncb + 1) / 2;
   const size_t smem = sizeof(double2) * (size_t)npb * p.nph + sizeof(double) * 2 * (size_t)(p.L + 1) * p.ncb;
+  if (smem > 227 * 1024) {
+    const size_t sw = smem_wide(p);
+    cudaError_t e = cudaFuncSetAttribute(k_fft_bwd_grid_wide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw);
+    if (e != cudaSuccess) return e;
+    k_fft_bwd_grid_wide<<<p.nr * p.nth, kFftThreads, sw, s>>>(p, fld);
+    return cudaGetLastError();
+  }
   cudaError_t e = cudaFuncSetAttribute(k_fft_bwd_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   k_fft_bwd_grid<<<p.nr * p.nth, kFftThreads, smem, s>>>(p, fld);
@@ -1060,6 +1234,13 @@ cudaError_t launch_fft_bwd_grid(const Plan& p, double* fld, cudaStream_t s) {
 cudaError_t launch_fft_fwd_grid(const Plan& p, const double* frc, cudaStream_t s) {
   const int npf = (p.ncf + 1) / 2;
   const size_t smem = sizeof(double2) * (size_t)npf * p.nph;
+  if (smem > 227 * 1024) {
+    const size_t sw = sizeof(double2) * (size_t)p.nph;
+    cudaError_t e = cudaFuncSetAttribute(k_fft_fwd_grid_wide, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw);
+    if (e != cudaSuccess) return e;
+    k_fft_fwd_grid_wide<<<p.nr * p.nth, kFftThreads, sw, s>>>(p, frc);
+    return cudaGetLastError();
+  }
   cudaError_t e = cudaFuncSetAttribute(k_fft_fwd_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   k_fft_fwd_grid<<<p.nr * p.nth, kFftThreads, smem, s>>>(p, frc);

@@ -45,6 +45,8 @@ struct Plan {
   int fac[kMaxFftFactors];
   const double2* twid;    // [nph] e^{+2 pi i k/nph}
   const int* digrev;      // [nph] frequency index of DIF output slot
+  double2* fft_scratch;   // wide lines only: [fft_scratch_ctas][pairs][nph] grid of the line
+  int fft_scratch_ctas;
   // products
   int nprod;
   int pkind[kMaxProd], pa[kMaxProd], pb[kMaxProd];
@@ -115,6 +117,8 @@ cudaError_t launch_leg_fwd_f64(const Plan& p, double* d_rj, long long ld, const 
                                cudaStream_t s, int m_count = 0);
 cudaError_t launch_fft_cycle(const Plan& p, cudaStream_t s);
 cudaError_t launch_fft_bwd_grid(const Plan& p, double* fld, cudaStream_t s);
+// true when one (r, theta) line of every component fits in shared memory
+bool fft_line_fits(const Plan& p);
 cudaError_t launch_fft_fwd_grid(const Plan& p, const double* frc, cudaStream_t s);
 
 }  // namespace kmhd

@@ -148,11 +148,10 @@ int validate(const kmhd_sph_desc* d) {
   if (d->nproduct > 0 && (nv != d->nvector_f || ns != d->nscalar_f)) return KMHD_ERR_ARG;
   std::vector<int> f;
   if (!factor_fft(d->nph, f)) return KMHD_ERR_SIZE;
-  // one (r, theta) line of every component plus the staged spectra must fit in
-  // shared memory (fused FFT / products kernel)
-  const int ncb = 3 * d->nvector_b + d->nscalar_b, ncf = 3 * d->nvector_f + d->nscalar_f;
-  const int npair = (std::max(ncb, ncf) + 1) / 2;
-  if (sizeof(double2) * (size_t)npair * d->nph + sizeof(double) * 2 * (size_t)(d->ltr + 1) * ncb > 227 * 1024)
+  // one (r, theta) line of one component pair plus the staged spectra of the
+  // line must fit in shared memory (wide lines go through the FFT pair by pair)
+  const int ncb = 3 * d->nvector_b + d->nscalar_b;
+  if (sizeof(double2) * (size_t)d->nph + sizeof(double) * 2 * (size_t)(d->ltr + 1) * ncb > 227 * 1024)
     return KMHD_ERR_SIZE;
   return KMHD_OK;
 }
@@ -386,6 +385,16 @@ int kmhd_sph_create(const kmhd_sph_desc* d, kmhd_sph** out) {
   p.rtm_f = h->rtm_f;
   p.twid = h->twid;
   p.digrev = h->digrev;
+  if (!fft_line_fits(p)) {
+    // wide lines: per-CTA grid scratch of the pair-by-pair FFT cycle (L2-resident)
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, d->device);
+    const int npm = (std::max(p.ncb, p.ncf) + 1) / 2;
+    double2* sc = nullptr;
+    if ((st = dalloc(h, &sc, (size_t)nsm * npm * p.nph))) return fail(st);
+    p.fft_scratch = sc;
+    p.fft_scratch_ctas = nsm;
+  }
   if (launch_tables(p, h->colat, h->weight, h->asin_t, h->P, h->dP, s) != cudaSuccess)
     return fail(KMHD_ERR_CUDA);
   h->autotune = (d->flags & KMHD_FLAG_AUTOTUNE) != 0 && d->tier != KMHD_TIER_FP64;

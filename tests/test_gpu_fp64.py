@@ -18,6 +18,7 @@ CFGS = [
     SphConfig(47, 73, 144, 6, name="L47_odd_nth"),          # odd N_theta: equator row
     SphConfig(16, 26, 40, 5, nvb=1, nsb=2, nvf=1, nsf=1,     # nph = 40 = 8*5
               products=((1, 0, 1, 0.5), (3, 0, 1, 2.0)), name="L16_mixed"),
+    SphConfig(63, 96, 3072, 3, name="L63_wide_nph3072"),    # line too wide for shared memory: pair by pair
 ]
 
 
@@ -41,9 +42,11 @@ def test_tables_match_oracle(pair):
         Pref = t["P"][idx][:, :cfg.nh]
         dPref = t["dP"][idx][:, :cfg.nh]
         # FMA contraction and sqrt rounding differ between the device and host
-        # recurrences; dP mixes two recurrences and cancels, hence 1e-13.
-        assert np.abs(P - Pref).max() <= 1e-14 * max(1.0, np.abs(Pref).max())
-        assert np.abs(dP - dPref).max() <= 1e-13 * max(1.0, np.abs(dPref).max())
+        # recurrences, and the difference grows with the number of recurrence
+        # steps (~ (L+1) ulps); dP mixes two recurrences and cancels.
+        tolP, toldP = 4e-16 * (cfg.ltr + 1), 3e-15 * (cfg.ltr + 1)
+        assert np.abs(P - Pref).max() <= tolP * max(1.0, np.abs(Pref).max())
+        assert np.abs(dP - dPref).max() <= toldP * max(1.0, np.abs(dPref).max())
 
 
 @pytest.mark.gpu

@@ -37,6 +37,7 @@ CFGS = [
     SphConfig(16, 26, 40, 5, nvb=1, nsb=2, nvf=1, nsf=1,
               products=((1, 0, 1, 0.5), (3, 0, 1, 2.0)), name="L16_mixed"),
     SphConfig(127, 192, 384, 17, name="L127"),
+    SphConfig(63, 96, 3072, 3, name="L63_wide"),
 ]
 
 
@@ -109,3 +110,25 @@ def test_split_dipole_modes_fp64(tier):
     den = np.abs(ref).max(axis=0)
     err = (np.abs(got[rows] - ref[rows]).max(axis=0) / den).max()
     assert err <= 1e-13, err
+
+
+@pytest.mark.gpu
+def test_split_vs_fp64_L1023():
+    """cfg5 angular grid (L=1023, Ntheta=1536, Nphi=3072; wide lines go through
+    the FFT pair by pair): split tier against the FP64 GPU tier on the same
+    input (the CPU oracle at this L takes minutes; the FP64 tier is pinned to
+    the oracle at L <= 511 and on the wide-line path at L=63)."""
+    import torch
+    from kemorin_mhd_b200.config import TIER_FP64
+    from kemorin_mhd_b200.sph_trans import SphTransform
+    cfg = SphConfig(1023, 1536, 3072, 3, name="L1023_Nr3")
+    d = to_dev_fortran(make_d_rj(cfg, seed=19))
+    outs = []
+    for tier in (TIER_FP64, TIER_SPLIT_I8):
+        tr = SphTransform(cfg, tier=tier)
+        out = torch.zeros((cfg.ncf, cfg.J * cfg.nr), dtype=torch.float64, device="cuda")
+        tr.nonlinear_cycle(d, out)
+        outs.append(from_dev_fortran(out))
+        tr.close()
+    err = col_relerr(outs[1], outs[0])
+    assert err.max() <= TOL[TIER_SPLIT_I8], err
