@@ -245,7 +245,7 @@ __device__ void dit_all(double2* z, int npair, int N, const Plan& P, const doubl
 // Stage the records of line (th, r) for all m into st via cp.async (16 B each).
 __device__ void prefetch_line(double* st, const double* rtm, int nc, const Plan& P, int th, int r) {
   const long long strideM = (long long)P.nth * P.nr * nc * 2;
-  const double* base = rtm + ((long long)th * P.nr + r) * nc * 2;
+  const double* base = rtm + rtm_off(P, 0, th, r, nc);
   const int n = (P.L + 1) * nc;
   for (int it = threadIdx.x; it < n; it += blockDim.x) {
     const int m = it / nc, c = it % nc;
@@ -259,7 +259,7 @@ __device__ void store_line(const double2* z, int npair, const Plan& P, double* r
   const int N = P.nph, L = P.L;
   const double aN = 1.0 / (double)N;
   const long long strideM = (long long)P.nth * P.nr * nc * 2;
-  double* base = rtm + ((long long)th * P.nr + r) * nc * 2;
+  double* base = rtm + rtm_off(P, 0, th, r, nc);
   for (int it = threadIdx.x; it < (L + 1) * npair; it += blockDim.x) {
     const int m = it / npair, pp = it % npair;
     const double2* zp = z + pp * N;
@@ -394,15 +394,15 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_cycle(Plan P, int nlines) {
   double* st = reinterpret_cast<double*>(z + npair * N);
   int line = blockIdx.x;
   if (line >= nlines) return;
-  prefetch_line(st, P.rtm_b, P.ncb, P, line / P.nr, line % P.nr);
+  prefetch_line(st, P.rtm_b, P.ncb, P, line % P.nth, line / P.nth);
   while (line < nlines) {
-    const int r = line % P.nr, th = line / P.nr;
+    const int th = line % P.nth, r = line / P.nth;
     cp_async_wait<0>();
     __syncthreads();
     dif_first_dispatch(P.fac[0], st, P.ncb, P.nvb, z, npb, N, P.L, P.twid);
     __syncthreads();
     const int next = line + gridDim.x;
-    if (next < nlines) prefetch_line(st, P.rtm_b, P.ncb, P, next / P.nr, next % P.nr);
+    if (next < nlines) prefetch_line(st, P.rtm_b, P.ncb, P, next % P.nth, next / P.nth);
     dif_rest(z, npb, N, P, P.twid);
     products<MVB, MSB, MVF, MSF>(z, N, P);
     __syncthreads();
@@ -450,7 +450,7 @@ __device__ void store_one(const double2* z, int q, const Plan& P, double* rtm, i
   const int N = P.nph, L = P.L;
   const double aN = 1.0 / (double)N;
   const long long strideM = (long long)P.nth * P.nr * nc * 2;
-  double* base = rtm + ((long long)th * P.nr + r) * nc * 2;
+  double* base = rtm + rtm_off(P, 0, th, r, nc);
   for (int m = threadIdx.x; m <= L; m += blockDim.x) {
     const double2 zm = z[m];
     double a0, b0, a1, b1;
@@ -479,7 +479,7 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_cycle_wide(Plan P, int nlin
   double* st = reinterpret_cast<double*>(z + N);
   double2* sc = P.fft_scratch + (long long)blockIdx.x * npm * N;
   for (int line = blockIdx.x; line < nlines; line += gridDim.x) {
-    const int r = line % P.nr, th = line / P.nr;
+    const int th = line % P.nth, r = line / P.nth;
     prefetch_line(st, P.rtm_b, P.ncb, P, th, r);
     cp_async_wait<0>();
     __syncthreads();
@@ -606,7 +606,7 @@ __device__ __forceinline__ int ncs_of(int nc) { return nc | 1; }
 
 __device__ void prefetch_line_t(double* st, const double* rtm, int nc, const Plan& P, int th, int r) {
   const long long strideM = (long long)P.nth * P.nr * nc * 2;
-  const double* base = rtm + ((long long)th * P.nr + r) * nc * 2;
+  const double* base = rtm + rtm_off(P, 0, th, r, nc);
   const int ncs = ncs_of(nc);
   const int n = (P.L + 1) * nc;
   for (int it = threadIdx.x; it < n; it += blockDim.x) {
@@ -1029,7 +1029,7 @@ __device__ void ff_store_line(const double2* z, int npair, const Plan& P, double
   const int L = P.L;
   const double aN = 1.0 / (double)N;
   const long long strideM = (long long)P.nth * P.nr * nc * 2;
-  double* base = rtm + ((long long)th * P.nr + r) * nc * 2;
+  double* base = rtm + rtm_off(P, 0, th, r, nc);
   for (int it = threadIdx.x; it < (L + 1) * npair; it += blockDim.x) {
     const int pp = it / (L + 1), m = it - pp * (L + 1);
     const double2* zp = z + pp * NP;
@@ -1060,15 +1060,16 @@ __global__ void __launch_bounds__(kFftThreadsF, 1) k_fft_cycle_f(Plan P, int nli
   double* st = reinterpret_cast<double*>(z + npair * NP + 1);  // keep 16-byte alignment
   int line = blockIdx.x;
   if (line >= nlines) return;
-  prefetch_line_t(st, P.rtm_b, P.ncb, P, line / P.nr, line % P.nr);
+  // lines theta fastest: concurrent CTAs touch neighbouring records of one (m, r)
+  prefetch_line_t(st, P.rtm_b, P.ncb, P, line % P.nth, line / P.nth);
   while (line < nlines) {
-    const int r = line % P.nr, th = line / P.nr;
+    const int th = line % P.nth, r = line / P.nth;
     cp_async_wait<0>();
     __syncthreads();
     ff_dif_first<N, PR>(st, P.ncb, P.nvb, z, npb, P.L, P.twid);
     __syncthreads();
     const int next = line + gridDim.x;
-    if (next < nlines) prefetch_line_t(st, P.rtm_b, P.ncb, P, next / P.nr, next % P.nr);
+    if (next < nlines) prefetch_line_t(st, P.rtm_b, P.ncb, P, next % P.nth, next / P.nth);
     ff_mid_pass<N, +1>(z, npb, P.twid);
     __syncthreads();
     ff_fused<N, MVB, MSB, MVF, MSF, PK>(z, P);

@@ -38,8 +38,8 @@ struct Plan {
   // work buffers
   double* SB;             // packed backward spectra [m][p][kpad][nrb*ncolb_blk]
   const long long* sboff; // [(L+1)*2]
-  double* rtm_b;          // [m][th][r][record of ncb (cos, sin) pairs, see rec_off]
-  double* rtm_f;          // [m][th][r][record of ncf pairs]
+  double* rtm_b;          // [m][r][th][record of ncb (cos, sin) pairs, see rec_off, rtm_off]
+  double* rtm_f;          // [m][r][th][record of ncf pairs]
   // FFT
   int nfac;
   int fac[kMaxFftFactors];
@@ -83,6 +83,13 @@ __host__ __device__ __forceinline__ int rec_off(int c, int nv) {
     return q == 0 ? 4 * nv + 2 * v : 4 * v + 2 * (q - 1);
   }
   return 6 * nv + 2 * (c - 3 * nv);
+}
+
+// Offset (in doubles) of the rtm record of (m, theta, r) holding nc (cos, sin)
+// pairs: layout [m][r][theta][record], so the records of one (m, r) are
+// contiguous over theta.
+__host__ __device__ __forceinline__ long long rtm_off(const Plan& P, int m, int th, int r, int nc) {
+  return (((long long)m * P.nr + r) * P.nth + th) * (2LL * nc);
 }
 
 __host__ __device__ __forceinline__ int kcount(int L, int m, int p) {

@@ -212,9 +212,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_leg_bwd_f64(Plan p) {
   const bool pair = i < p.nth / 2;
   const double ms = (double)m * p.asin_t[i];
   const int nc = p.ncb;
-  const long long strideTh = (long long)p.nr * nc * 2;
-  double* outN = p.rtm_b + ((long long)m * p.nth + i) * strideTh + (long long)r * nc * 2;
-  double* outS = p.rtm_b + ((long long)m * p.nth + (p.nth - 1 - i)) * strideTh + (long long)r * nc * 2;
+  double* outN = p.rtm_b + rtm_off(p, m, i, r, nc);
+  double* outS = p.rtm_b + rtm_off(p, m, p.nth - 1 - i, r, nc);
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
     double sym[6], asym[6];  // r cos, r sin, th cos, th sin, ph cos, ph sin
@@ -304,7 +303,6 @@ k_leg_fwd_f64(Plan p, double* __restrict__ d_rj, long long ld, const int* __rest
 #pragma unroll
   for (int s = 0; s < (NS > 0 ? NS : 1); ++s) accS[s][0] = accS[s][1] = 0.0;
 
-  const long long strideTh = (long long)p.nr * nc * 2;
   constexpr int kItems = (kKC * kRB * (3 * NV + NS) + kThreads - 1) / kThreads;
   double2 pfN[kItems], pfS[kItems];
   // global loads of one chunk's rtm_f values into registers (overlaps the MMAs)
@@ -320,11 +318,9 @@ k_leg_fwd_f64(Plan p, double* __restrict__ d_rj, long long ld, const int* __rest
         const int i = th0 + row, r = kRB * rb + u;
         if (i < p.nh && r < p.nr) {
           const int ro = rec_off(c, NV);
-          pfN[q] = *reinterpret_cast<const double2*>(p.rtm_f + ((long long)m * p.nth + i) * strideTh +
-                                                     (long long)r * nc * 2 + ro);
+          pfN[q] = *reinterpret_cast<const double2*>(p.rtm_f + rtm_off(p, m, i, r, nc) + ro);
           if (i < p.nth / 2)
-            pfS[q] = *reinterpret_cast<const double2*>(p.rtm_f + ((long long)m * p.nth + (p.nth - 1 - i)) * strideTh +
-                                                       (long long)r * nc * 2 + ro);
+            pfS[q] = *reinterpret_cast<const double2*>(p.rtm_f + rtm_off(p, m, p.nth - 1 - i, r, nc) + ro);
         }
       }
     }

@@ -359,8 +359,8 @@ __global__ void __launch_bounds__(256) k_slice_mr(Plan P, SliceTabs S, const dou
   // ---- pass 1: derived columns
   if (FWD) {
     const int rec = 2 * P.ncf;
-    const long long strideTh = (long long)P.nr * rec;
-    const double* base = P.rtm_f + (long long)m * P.nth * strideTh + (long long)r * rec + (vgrp ? 4 * v : 4 * nv);
+    const long long strideTh = rec;  // records of one (m, r) are contiguous over theta
+    const double* base = P.rtm_f + rtm_off(P, m, 0, r, P.ncf) + (vgrp ? 4 * v : 4 * nv);
     for (int th = threadIdx.x; th < P.nh; th += blockDim.x) {
       const bool hasS = th < P.nth / 2;
       const double w = __ldg(P.weight + th);
@@ -877,9 +877,9 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
           if (th < P.nh && ok) {
             const bool pairrow = th < P.nth / 2;
             const double* sr = stash + row * kXS + cbase;
-            const long long rec = (long long)P.ncb * 2;
-            double* baseN = P.rtm_b + ((long long)w.m * P.nth + th) * P.nr * rec;
-            double* baseS = P.rtm_b + ((long long)w.m * P.nth + (P.nth - 1 - th)) * P.nr * rec;
+            const long long rec = (long long)P.nth * P.ncb * 2;  // radius stride of the rtm records
+            double* baseN = P.rtm_b + rtm_off(P, w.m, th, 0, P.ncb);
+            double* baseS = P.rtm_b + rtm_off(P, w.m, P.nth - 1 - th, 0, P.ncb);
             if (w.t <= 1) {
               // column c = 4 (r + nrT v) + q: one vector's (theta c, theta s, phi c, phi s)
 #pragma unroll
