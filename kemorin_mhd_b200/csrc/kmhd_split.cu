@@ -284,8 +284,11 @@ __device__ __forceinline__ ColRef colref_fwd(const Plan& P, const SliceTabs& S, 
 // values, packed as bytes (value i in byte i) into one word per slice; w[NS-1]
 // holds the least significant digits.  A balanced digit's two's-complement
 // byte is the low byte of the running value x, and the next value is
-// (x + 128) >> 8.  Each value is split exactly into hi 2^24 + lo with both
-// halves in int32; the top digit (|d| <= 64) is what remains of hi.
+// (x + 128) >> 8.  Each value is rounded to the nearest integer x (ties to
+// even) by adding 1.5 2^52, whose double then holds 2^52 + 2^51 + x in its
+// mantissa, and split exactly into hi 2^24 + lo with both halves in int32
+// (lo = the sign-extended low 24 bits); the top digit (|d| <= 64) is what
+// remains of hi.
 __device__ __forceinline__ uint32_t pack4(int b0, int b1, int b2, int b3) {
   return __byte_perm(__byte_perm(b0, b1, 0x0040), __byte_perm(b2, b3, 0x0040), 0x5410);
 }
@@ -294,10 +297,9 @@ __device__ __forceinline__ void digits4(const double (&v)[4], uint32_t (&w)[NS])
   int lo[4], hi[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const double x = rint(v[i]);
-    const double h = rint(x * 0x1p-24);
-    lo[i] = (int)fma(-h, 0x1p24, x);
-    hi[i] = (int)h;
+    const long long x = __double_as_longlong(v[i] + 6755399441055744.0) - 0x4338000000000000LL;
+    lo[i] = (int)((unsigned)x << 8) >> 8;
+    hi[i] = (int)((x - lo[i]) >> 24);
   }
 #pragma unroll
   for (int s = NS - 1; s >= 1; --s) {
