@@ -121,7 +121,12 @@ int kmhd_sph_f_trans(kmhd_sph *handle, const double *frc_rtp, double *d_rj,
 /* Full cycle: backward transform, grid products, forward transform.  Replaces
  * the copy_mhd_spectr_to_send -> sph_b_trans -> nonlinear_terms_in_rtp ->
  * sph_f_trans -> copy_mhd_spectr_from_recv segment of nonlinear_by_pseudo_sph
- * (MHD_src/sph_MHD/cal_nonlinear.f90:118-171). */
+ * (MHD_src/sph_MHD/cal_nonlinear.f90:118-171).  With host pointers and more
+ * than 64 MiB of copies the call runs over radial chunks whose copies in and
+ * out overlap the kernels (page-locked host memory overlaps; pageable memory
+ * gives the same result more slowly); the result equals the device-pointer
+ * call's, input and output columns may share one array, and only the whole
+ * call is timed (kmhd_sph_last_timing stages 0..2 read 0). */
 int kmhd_sph_cycle(kmhd_sph *handle, const double *d_rj_in, int64_t ld_in,
                    const int32_t *cols_b, double *d_rj_out, int64_t ld_out,
                    const int32_t *cols_f, int32_t ptr_kind);

@@ -385,14 +385,14 @@ __device__ void products(double2* z, int N, const Plan& P) {
 }
 
 template <int MVB, int MSB, int MVF, int MSF>
-__global__ void __launch_bounds__(kFftThreads) k_fft_cycle(Plan P, int nlines) {
+__global__ void __launch_bounds__(kFftThreads) k_fft_cycle(Plan P, int line0, int nlines) {
   extern __shared__ double4 smraw[];
   const int N = P.nph;
   const int npb = (P.ncb + 1) / 2, npf = (P.ncf + 1) / 2;
   const int npair = npb > npf ? npb : npf;
   double2* z = reinterpret_cast<double2*>(smraw);
   double* st = reinterpret_cast<double*>(z + npair * N);
-  int line = blockIdx.x;
+  int line = line0 + blockIdx.x;
   if (line >= nlines) return;
   prefetch_line(st, P.rtm_b, P.ncb, P, line % P.nth, line / P.nth);
   while (line < nlines) {
@@ -470,7 +470,7 @@ __device__ void store_one(const double2* z, int q, const Plan& P, double* rtm, i
 }
 
 template <int MVB, int MSB, int MVF, int MSF>
-__global__ void __launch_bounds__(kFftThreads) k_fft_cycle_wide(Plan P, int nlines) {
+__global__ void __launch_bounds__(kFftThreads) k_fft_cycle_wide(Plan P, int line0, int nlines) {
   extern __shared__ double4 smraw[];
   const int N = P.nph;
   const int npb = (P.ncb + 1) / 2, npf = (P.ncf + 1) / 2;
@@ -478,7 +478,7 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_cycle_wide(Plan P, int nlin
   double2* z = reinterpret_cast<double2*>(smraw);
   double* st = reinterpret_cast<double*>(z + N);
   double2* sc = P.fft_scratch + (long long)blockIdx.x * npm * N;
-  for (int line = blockIdx.x; line < nlines; line += gridDim.x) {
+  for (int line = line0 + blockIdx.x; line < nlines; line += gridDim.x) {
     const int th = line % P.nth, r = line / P.nth;
     prefetch_line(st, P.rtm_b, P.ncb, P, th, r);
     cp_async_wait<0>();
@@ -1051,14 +1051,14 @@ __device__ void ff_store_line(const double2* z, int npair, const Plan& P, double
 }
 
 template <int N, int MVB, int MSB, int MVF, int MSF, bool PR, int PK>
-__global__ void __launch_bounds__(kFftThreadsF, 1) k_fft_cycle_f(Plan P, int nlines) {
+__global__ void __launch_bounds__(kFftThreadsF, 1) k_fft_cycle_f(Plan P, int line0, int nlines) {
   extern __shared__ double4 smraw[];
   constexpr int NP = N + 1;
   const int npb = (P.ncb + 1) / 2, npf = (P.ncf + 1) / 2;
   const int npair = npb > npf ? npb : npf;
   double2* z = reinterpret_cast<double2*>(smraw);
   double* st = reinterpret_cast<double*>(z + npair * NP + 1);  // keep 16-byte alignment
-  int line = blockIdx.x;
+  int line = line0 + blockIdx.x;
   if (line >= nlines) return;
   // lines theta fastest: concurrent CTAs touch neighbouring records of one (m, r)
   prefetch_line_t(st, P.rtm_b, P.ncb, P, line % P.nth, line / P.nth);
@@ -1095,10 +1095,12 @@ cudaError_t run_cycle_fk(const Plan& p, cudaStream_t s) {
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kFftThreadsF, smem);
   if (occ < 1) occ = 1;
-  const int nlines = p.nr * p.nth;
+  // lines (r, theta) of the radial window, theta fastest
+  const int line0 = p.r_lo * p.nth, nlines = p.r_hi * p.nth;
   int grid = nsm * occ;
-  if (grid > nlines) grid = nlines;
-  kern<<<grid, kFftThreadsF, smem, s>>>(p, nlines);
+  if (grid > nlines - line0) grid = nlines - line0;
+  if (grid <= 0) return cudaSuccess;
+  kern<<<grid, kFftThreadsF, smem, s>>>(p, line0, nlines);
   return cudaGetLastError();
 }
 
@@ -1155,10 +1157,11 @@ cudaError_t run_cycle(const Plan& p, cudaStream_t s) {
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kFftThreads, smem);
   if (occ < 1) occ = 1;
-  const int nlines = p.nr * p.nth;
+  const int line0 = p.r_lo * p.nth, nlines = p.r_hi * p.nth;
   int grid = nsm * occ;
-  if (grid > nlines) grid = nlines;
-  kern<<<grid, kFftThreads, smem, s>>>(p, nlines);
+  if (grid > nlines - line0) grid = nlines - line0;
+  if (grid <= 0) return cudaSuccess;
+  kern<<<grid, kFftThreads, smem, s>>>(p, line0, nlines);
   return cudaGetLastError();
 }
 
@@ -1184,9 +1187,10 @@ cudaError_t run_cycle_wide(const Plan& p, cudaStream_t s) {
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   if (!p.fft_scratch) return cudaErrorInvalidValue;
-  const int nlines = p.nr * p.nth;
-  const int grid = std::min(p.fft_scratch_ctas, nlines);
-  kern<<<grid, kFftThreads, smem, s>>>(p, nlines);
+  const int line0 = p.r_lo * p.nth, nlines = p.r_hi * p.nth;
+  const int grid = std::min(p.fft_scratch_ctas, nlines - line0);
+  if (grid <= 0) return cudaSuccess;
+  kern<<<grid, kFftThreads, smem, s>>>(p, line0, nlines);
   return cudaGetLastError();
 }
 

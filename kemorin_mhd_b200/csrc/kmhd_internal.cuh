@@ -23,6 +23,10 @@ constexpr int kMaxFftFactors = 16;
 // Plan of one transform instance (device pointers + sizes).
 struct Plan {
   int L, nth, nph, nr, nh, nh_pad, nr4, nrb;
+  // radial window [r_lo, r_hi) of the cycle launches (0, nr: every radius);
+  // r_lo is a multiple of 16, so the window covers whole radial blocks and
+  // whole split-GEMM column tiles
+  int r_lo, r_hi;
   long long J;
   int nvb, nsb, nvf, nsf, ncb, ncf;
   // tables
@@ -91,6 +95,10 @@ __host__ __device__ __forceinline__ int rec_off(int c, int nv) {
 __host__ __device__ __forceinline__ long long rtm_off(const Plan& P, int m, int th, int r, int nc) {
   return (((long long)m * P.nr + r) * P.nth + th) * (2LL * nc);
 }
+
+// Radial blocks (kRB radii each) of the window: first block and count.
+__host__ __device__ __forceinline__ int win_rb0(const Plan& P) { return P.r_lo / kRB; }
+__host__ __device__ __forceinline__ int win_nrb(const Plan& P) { return (P.r_hi + kRB - 1) / kRB - P.r_lo / kRB; }
 
 __host__ __device__ __forceinline__ int kcount(int L, int m, int p) {
   // number of l in [m, L] with (l - m) % 2 == p

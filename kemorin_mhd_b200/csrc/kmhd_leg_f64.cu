@@ -47,8 +47,9 @@ __global__ void k_pack_b(Plan p, const double* __restrict__ d_rj, long long ld,
   extern __shared__ double sm[];
   const int m = blockIdx.y;
   const int nlc = p.kpad[2 * m] / kKC;  // chunks of 32 l (16 k per parity)
-  const int lc = blockIdx.x / p.nrb;
-  const int rb = blockIdx.x % p.nrb;
+  const int nrbw = win_nrb(p);
+  const int lc = blockIdx.x / nrbw;
+  const int rb = win_rb0(p) + blockIdx.x % nrbw;
   if (lc >= nlc) return;
   const int nc = 3 * nv + ns;
   const int L = p.L;
@@ -113,8 +114,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_leg_bwd_f64(Plan p) {
   double* sB = sm + 2 * G::A_STAGE;    // [2 stages][kKC][CBp]
   const int nthb = p.nh_pad / kThBlk;
   int b = blockIdx.x;
-  const int rb = b % p.nrb;
-  b /= p.nrb;
+  const int nrbw = win_nrb(p);
+  const int rb = win_rb0(p) + b % nrbw;
+  b /= nrbw;
   const int thb = b % nthb;
   const int m = b / nthb;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -284,8 +286,9 @@ k_leg_fwd_f64(Plan p, double* __restrict__ d_rj, long long ld, const int* __rest
   double* sA = sm;                      // [P_e, P_o, dP_e, dP_o][kLBlk][AS]
   double* sB = sm + 4 * G::A_TILE;      // [par][kKC][CFp]
   const int m = blockIdx.y;
-  const int kb = blockIdx.x / p.nrb;
-  const int rb = blockIdx.x % p.nrb;
+  const int nrbw = win_nrb(p);
+  const int kb = blockIdx.x / nrbw;
+  const int rb = win_rb0(p) + blockIdx.x % nrbw;
   const int K0 = kcount(p.L, m, 0);
   if (kb * kLBlk >= K0) return;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -457,7 +460,8 @@ cudaError_t run_bwd(const Plan& p, cudaStream_t s) {
   using G = BwdGeo<NV, NS>;
   auto kern = k_leg_bwd_f64<NV, NS>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
-  const long long nblk = (long long)(p.L + 1) * (p.nh_pad / kThBlk) * p.nrb;
+  const long long nblk = (long long)(p.L + 1) * (p.nh_pad / kThBlk) * win_nrb(p);
+  if (nblk <= 0) return cudaSuccess;
   kern<<<(unsigned)nblk, kThreads, G::SMEM, s>>>(p);
   return cudaGetLastError();
 }
@@ -468,7 +472,8 @@ cudaError_t run_fwd(const Plan& p, double* d_rj, long long ld, const int* cols, 
   auto kern = k_leg_fwd_f64<NV, NS>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
   const int nkb = (kcount(p.L, 0, 0) + kLBlk - 1) / kLBlk;
-  dim3 grid(nkb * p.nrb, m_count);
+  if (win_nrb(p) <= 0) return cudaSuccess;
+  dim3 grid(nkb * win_nrb(p), m_count);
   kern<<<grid, kThreads, G::SMEM, s>>>(p, d_rj, ld, cols);
   return cudaGetLastError();
 }
@@ -500,7 +505,8 @@ cudaError_t launch_pack_b(const Plan& p, int nlc_max, const double* d_rj, long l
   const int CB = 24 * nv + 8 * ns;
   const size_t smem = sizeof(double) * 2 * kRB * nc * 32;
   cudaFuncSetAttribute(k_pack_b, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  dim3 grid(nlc_max * p.nrb, p.L + 1);
+  if (win_nrb(p) <= 0) return cudaSuccess;
+  dim3 grid(nlc_max * win_nrb(p), p.L + 1);
   k_pack_b<<<grid, kThreads, smem, s>>>(p, d_rj, ld, cols, nv, ns, CB);
   return cudaGetLastError();
 }

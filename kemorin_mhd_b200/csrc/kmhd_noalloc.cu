@@ -132,6 +132,8 @@ int na_plan(const kmhd_sph_desc* d, Plan& p, NaHost& H) {
   p.nh_pad = (p.nh + kThBlk - 1) / kThBlk * kThBlk;
   p.nr4 = (d->nr + kRB - 1) / kRB * kRB;
   p.nrb = p.nr4 / kRB;
+  p.r_lo = 0;
+  p.r_hi = p.nr;
   p.J = (long long)(p.L + 1) * (p.L + 1);
   p.nvb = d->nvector_b;
   p.nsb = d->nscalar_b;

@@ -56,6 +56,11 @@ struct kmhd_sph {
   bool tuned = false;
   // batched cycles whose first handle this is: captured graph and its signature
   struct BatchGraph* batch = nullptr;
+  // host-pointer cycles: radial chunks (bounds, empty = no chunking) whose
+  // copies in and out run on their own streams beside the chunk kernels
+  std::vector<int> chunks;
+  cudaStream_t s_in = nullptr, s_out = nullptr;
+  std::vector<cudaEvent_t> ev_in, ev_out;
   // timing
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t ev_mid[2] = {nullptr, nullptr};  // after the bwd pack/slicer, after the fwd slicer
@@ -206,6 +211,10 @@ int kmhd_sph_destroy(kmhd_sph* h) {
     if (e) cudaEventDestroy(e);
   for (auto& e : h->ev_mid)
     if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : h->ev_in) cudaEventDestroy(e);
+  for (cudaEvent_t e : h->ev_out) cudaEventDestroy(e);
+  if (h->s_in) cudaStreamDestroy(h->s_in);
+  if (h->s_out) cudaStreamDestroy(h->s_out);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
   return KMHD_OK;
@@ -250,6 +259,8 @@ int kmhd_sph_create(const kmhd_sph_desc* d, kmhd_sph** out) {
   p.nh_pad = (p.nh + kThBlk - 1) / kThBlk * kThBlk;
   p.nr4 = (d->nr + kRB - 1) / kRB * kRB;
   p.nrb = p.nr4 / kRB;
+  p.r_lo = 0;
+  p.r_hi = p.nr;
   p.J = (long long)(p.L + 1) * (p.L + 1);
   p.nvb = d->nvector_b;
   p.nsb = d->nscalar_b;
@@ -403,6 +414,18 @@ int kmhd_sph_create(const kmhd_sph_desc* d, kmhd_sph** out) {
     if (st != KMHD_OK) return fail(st);
     h->bytes += split_bytes(h->split);
   }
+  // Radial chunks of host-pointer cycles: about eight chunks of a multiple of
+  // 16 radii when the copies are large enough to be worth overlapping.
+  {
+    const double copy_bytes = 8.0 * (double)nrj * (p.ncb + p.ncf);
+    const int step = 16 * std::max(1, (int)std::lround(p.nr / 128.0));
+    if (copy_bytes >= 64.0 * (1 << 20) && p.nr >= 2 * step) {
+      for (int r = 0; r + step < p.nr || r == 0; r += step) h->chunks.push_back(r);
+      if (p.nr - h->chunks.back() < step / 2 && h->chunks.size() > 1) h->chunks.pop_back();
+      h->chunks.push_back(p.nr);
+      if (h->split && (st = split_set_chunks(h->split, p, h->chunks, s)) != KMHD_OK) return fail(st);
+    }
+  }
   if (cudaStreamSynchronize(s) != cudaSuccess) return fail(KMHD_ERR_CUDA);
   *out = h;
   return KMHD_OK;
@@ -454,8 +477,9 @@ int timed_begin(kmhd_sph* h) {
   return KMHD_OK;
 }
 
-int run_bwd_spectral(kmhd_sph* h, const double* d_rj, int64_t ld, bool timed = true) {
-  const Plan& p = h->plan;
+// `win` (optional): a copy of the plan restricted to one radial chunk.
+int run_bwd_spectral(kmhd_sph* h, const double* d_rj, int64_t ld, bool timed = true, const Plan* win = nullptr) {
+  const Plan& p = win ? *win : h->plan;
   if (h->split && h->use_split) {
     int st = split_bwd(h->split, p, h->nlc_max, d_rj, ld, h->cols_b_d, h->stream, timed ? h->ev_mid[0] : nullptr);
     return st;
@@ -466,8 +490,8 @@ int run_bwd_spectral(kmhd_sph* h, const double* d_rj, int64_t ld, bool timed = t
   return KMHD_OK;
 }
 
-int run_fwd_spectral(kmhd_sph* h, double* d_rj, int64_t ld, bool timed = true) {
-  const Plan& p = h->plan;
+int run_fwd_spectral(kmhd_sph* h, double* d_rj, int64_t ld, bool timed = true, const Plan* win = nullptr) {
+  const Plan& p = win ? *win : h->plan;
   if (h->split && h->use_split) {
     // split tiers: slicer + INT8 GEMM for every mode, then the dipole (l <= 2)
     // modes are accumulated again in FP64 by the DMMA kernel over orders m <= 2
@@ -488,6 +512,78 @@ int enqueue_cycle(kmhd_sph* h, const double* in, int64_t ld_in, double* out, int
   if ((st = run_bwd_spectral(h, in, ld_in, false))) return st;
   KCHECK(launch_fft_cycle(h->plan, h->stream));
   return run_fwd_spectral(h, out, ld_out, false);
+}
+
+// Host-pointer cycle over the radial chunks.  Every stage is independent per
+// radius, so chunk c's kernels run on the handle's stream while chunk c + 1's
+// spectra come in on s_in and chunk c - 1's results go out on s_out.  The
+// staging buffers hold every radius, so no chunk waits for a buffer to free.
+int cycle_host_chunked(kmhd_sph* h, const double* d_rj_in, int64_t ld_in, const int32_t* cols_b,
+                       double* d_rj_out, int64_t ld_out, const int32_t* cols_f) {
+  const Plan& p = h->plan;
+  const size_t nrj = (size_t)p.J * p.nr;
+  const int nc = (int)h->chunks.size() - 1;
+  if (!h->s_in) KCHECK(cudaStreamCreateWithFlags(&h->s_in, cudaStreamNonBlocking));
+  if (!h->s_out) KCHECK(cudaStreamCreateWithFlags(&h->s_out, cudaStreamNonBlocking));
+  while ((int)h->ev_in.size() < nc) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    KCHECK(cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
+    h->ev_in.push_back(a);
+    KCHECK(cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
+    h->ev_out.push_back(b);
+  }
+  int st;
+  if (!h->stage_in && (st = dalloc(h, &h->stage_in, nrj * std::max(p.ncb, p.ncf)))) return st;
+  if (!h->stage_out && (st = dalloc(h, &h->stage_out, nrj * std::max(p.ncf, 1)))) return st;
+  std::vector<int> cb(p.nvb + p.nsb), cf(p.nvf + p.nsf);
+  for (int f = 0; f < p.nvb + p.nsb; ++f) cb[f] = f < p.nvb ? 3 * f : 3 * p.nvb + (f - p.nvb);
+  for (int f = 0; f < p.nvf + p.nsf; ++f) cf[f] = f < p.nvf ? 3 * f : 3 * p.nvf + (f - p.nvf);
+  if ((st = sync_cols(h, cb.data(), p.nvb + p.nsb, h->cols_b_cache, h->cols_b_d))) return st;
+  if ((st = sync_cols(h, cf.data(), p.nvf + p.nsf, h->cols_f_cache, h->cols_f_d))) return st;
+  // copies start after the work already queued on the handle's stream
+  KCHECK(cudaEventRecord(h->ev[0], h->stream));
+  KCHECK(cudaStreamWaitEvent(h->s_in, h->ev[0], 0));
+  for (int c = 0; c < nc; ++c) {
+    const long long o = p.J * (long long)h->chunks[c];
+    const size_t bytes = sizeof(double) * (size_t)(p.J * (long long)(h->chunks[c + 1] - h->chunks[c]));
+    for (int f = 0; f < p.nvb + p.nsb; ++f)
+      for (int q = 0; q < (f < p.nvb ? 3 : 1); ++q)
+        KCHECK(cudaMemcpyAsync(h->stage_in + nrj * (cb[f] + q) + o, d_rj_in + ld_in * (cols_b[f] + q) + o, bytes,
+                               cudaMemcpyHostToDevice, h->s_in));
+    KCHECK(cudaEventRecord(h->ev_in[c], h->s_in));
+  }
+  for (int c = 0; c < nc; ++c) {
+    Plan w = p;
+    w.r_lo = h->chunks[c];
+    w.r_hi = h->chunks[c + 1];
+    KCHECK(cudaStreamWaitEvent(h->stream, h->ev_in[c], 0));
+    if ((st = run_bwd_spectral(h, h->stage_in, (int64_t)nrj, false, &w))) return st;
+    KCHECK(launch_fft_cycle(w, h->stream));
+    if ((st = run_fwd_spectral(h, h->stage_out, (int64_t)nrj, false, &w))) return st;
+    KCHECK(cudaEventRecord(h->ev_out[c], h->stream));
+    KCHECK(cudaStreamWaitEvent(h->s_out, h->ev_out[c], 0));
+    const long long o = p.J * (long long)w.r_lo;
+    const size_t bytes = sizeof(double) * (size_t)(p.J * (long long)(w.r_hi - w.r_lo));
+    for (int f = 0; f < p.nvf + p.nsf; ++f)
+      for (int q = 0; q < (f < p.nvf ? 3 : 1); ++q)
+        KCHECK(cudaMemcpyAsync(d_rj_out + ld_out * (cols_f[f] + q) + o, h->stage_out + nrj * (cf[f] + q) + o, bytes,
+                               cudaMemcpyDeviceToHost, h->s_out));
+  }
+  KCHECK(cudaEventRecord(h->ev[1], h->s_out));
+  KCHECK(cudaStreamWaitEvent(h->stream, h->ev[1], 0));
+  KCHECK(cudaEventRecord(h->ev[3], h->stream));
+  KCHECK(cudaEventSynchronize(h->ev[3]));
+  if (h->split) {
+    const int e = split_check_error(h->split, h->stream);
+    if (e != KMHD_OK) return e;
+  }
+  // the stages overlap: only the whole call is timed
+  float t = 0;
+  KCHECK(cudaEventElapsedTime(&t, h->ev[0], h->ev[3]));
+  h->last_ms[0] = h->last_ms[1] = h->last_ms[2] = 0.0;
+  h->last_ms[3] = t;
+  h->kernel_timed = false;
+  return KMHD_OK;
 }
 
 int finish_timing(kmhd_sph* h) {
@@ -619,6 +715,8 @@ int kmhd_sph_cycle(kmhd_sph* h, const double* d_rj_in, int64_t ld_in, const int3
   int64_t old = ld_out;
   std::vector<int> cb, cf(p.nvf + p.nsf);
   int st;
+  if (ptr_kind == KMHD_PTR_HOST && h->chunks.size() > 2)
+    return cycle_host_chunked(h, d_rj_in, ld_in, cols_b, d_rj_out, ld_out, cols_f);
   if (ptr_kind == KMHD_PTR_HOST) {
     if ((st = stage_host_in(h, d_rj_in, ld_in, cols_b, p.nvb, p.nsb, &src, &sld, cb))) return st;
     if ((st = sync_cols(h, cb.data(), p.nvb + p.nsb, h->cols_b_cache, h->cols_b_d))) return st;

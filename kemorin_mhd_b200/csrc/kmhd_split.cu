@@ -335,7 +335,7 @@ template <bool FWD, int NS>
 __global__ void __launch_bounds__(256) k_slice_mr(Plan P, SliceTabs S, const double* __restrict__ d_rj, long long ld,
                                                    const int* __restrict__ cols) {
   extern __shared__ double X[];
-  const int z = blockIdx.x, r = blockIdx.y, m = blockIdx.z;
+  const int z = blockIdx.x, r = P.r_lo + blockIdx.y, m = blockIdx.z;
   const int L = P.L;
   const int Kall = L - m + 1;
   const int nv = FWD ? P.nvf : P.nvb;
@@ -971,6 +971,12 @@ struct SplitState {
   Work* work_b = nullptr;  // backward work (parity tile pairs)
   Work* work_f = nullptr;  // forward work
   int nwork_b = 0, nwork_f = 0;
+  std::vector<Work> wb_h, wf_h;  // host copies of the work lists
+  // radial chunks: bounds [chunk_lo[c], chunk_lo[c + 1]) and each chunk's
+  // slice of the chunk-ordered work lists work_bc / work_fc
+  std::vector<int> chunk_lo, cb_off, cf_off;
+  Work* work_bc = nullptr;
+  Work* work_fc = nullptr;
   int* err = nullptr;
   int nlc_max = 0;
 };
@@ -1116,6 +1122,8 @@ int split_create(SplitState** out, const Plan& p, int tier, int nslice, cudaStre
   S.beoff = beoff_d;
   s->nwork_b = (int)wb.size();
   s->nwork_f = (int)wf.size();
+  s->wb_h = wb;
+  s->wf_h = wf;
   auto up = [&](void* d, const void* h, size_t b) { return cudaMemcpyAsync(d, h, b, cudaMemcpyHostToDevice, st); };
   if (up(aoff_d, s->aoff.data(), sizeof(long long) * s->aoff.size()) ||
       up(aeoff_d, s->aeoff.data(), sizeof(long long) * s->aeoff.size()) ||
@@ -1148,6 +1156,67 @@ int split_create(SplitState** out, const Plan& p, int tier, int nslice, cudaStre
   return KMHD_OK;
 }
 
+// First radius of a work tile's columns: vector types (0, 1, 6, 7) hold
+// columns (v nrT + r) 4 + q, 16 radii per 64-column tile; radial/scalar types
+// (2..5) hold (4 r + f) 2 + slot, 8 radii per tile.
+static int tile_r0(const SliceTabs& S, const Work& w) {
+  if (w.t <= 1 || w.t >= 6) return (16 * w.nt) % S.nrT;
+  return 8 * w.nt;
+}
+
+int split_set_chunks(SplitState* s, const Plan& p, const std::vector<int>& bounds, cudaStream_t st) {
+  const int nc = (int)bounds.size() - 1;
+  if (nc < 1 || bounds.front() != 0 || bounds.back() != p.nr) return KMHD_ERR_ARG;
+  for (int c = 0; c < nc; ++c)
+    if (bounds[c + 1] <= bounds[c] || bounds[c] % 16 != 0) return KMHD_ERR_ARG;
+  auto chunk_of = [&](int r0) {
+    int c = 0;
+    while (c + 1 < nc && r0 >= bounds[c + 1]) ++c;
+    return c;
+  };
+  // stable per-chunk filtering keeps each parity pair together and the
+  // m-tile-fastest order inside a chunk
+  auto split_list = [&](const std::vector<Work>& w, std::vector<Work>& out, std::vector<int>& off) {
+    out.clear();
+    off.assign(nc + 1, 0);
+    for (int c = 0; c < nc; ++c) {
+      off[c] = (int)out.size();
+      for (size_t i = 0; i < w.size(); ++i)
+        if (chunk_of(tile_r0(s->S, w[i])) == c) out.push_back(w[i]);
+    }
+    off[nc] = (int)out.size();
+  };
+  std::vector<Work> bc, fc;
+  split_list(s->wb_h, bc, s->cb_off);
+  split_list(s->wf_h, fc, s->cf_off);
+  if (bc.size() != s->wb_h.size() || fc.size() != s->wf_h.size()) return KMHD_ERR_ARG;
+  int e;
+  if (!s->work_bc && (e = salloc(s, &s->work_bc, bc.size()))) return e;
+  if (!s->work_fc && (e = salloc(s, &s->work_fc, fc.size()))) return e;
+  if ((bc.size() && cudaMemcpyAsync(s->work_bc, bc.data(), sizeof(Work) * bc.size(), cudaMemcpyHostToDevice, st)) ||
+      (fc.size() && cudaMemcpyAsync(s->work_fc, fc.data(), sizeof(Work) * fc.size(), cudaMemcpyHostToDevice, st)))
+    return KMHD_ERR_CUDA;
+  s->chunk_lo = bounds;
+  return cudaStreamSynchronize(st) == cudaSuccess ? KMHD_OK : KMHD_ERR_CUDA;
+}
+
+// Work list of the plan's radial window: the whole list, or one chunk's slice.
+static int select_work(const SplitState* s, const Plan& p, bool fwd, const Work** w, int* n) {
+  if (p.r_lo == 0 && p.r_hi == p.nr) {
+    *w = fwd ? s->work_f : s->work_b;
+    *n = fwd ? s->nwork_f : s->nwork_b;
+    return KMHD_OK;
+  }
+  for (size_t c = 0; c + 1 < s->chunk_lo.size(); ++c)
+    if (s->chunk_lo[c] == p.r_lo && s->chunk_lo[c + 1] == p.r_hi) {
+      const std::vector<int>& off = fwd ? s->cf_off : s->cb_off;
+      *w = (fwd ? s->work_fc : s->work_bc) + off[c];
+      *n = off[c + 1] - off[c];
+      return KMHD_OK;
+    }
+  return KMHD_ERR_ARG;
+}
+
 // dynamic shared memory of one slicer CTA (largest field group): the derived
 // columns X[col][k] (k up to the padded K of the group's types), the column
 // maxima and exponents, and eight per-warp slice staging blocks
@@ -1169,21 +1238,21 @@ int split_bwd(SplitState* s, const Plan& p, int, const double* d_rj, long long l
     const size_t smem = slice_smem(p, false, s->ns);
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
       return KMHD_ERR_CUDA;
-    kern<<<dim3(p.nvb + 1, p.nr, p.L + 1), 256, smem, st>>>(p, S, d_rj, ld, cols);
+    if (p.r_hi > p.r_lo) kern<<<dim3(p.nvb + 1, p.r_hi - p.r_lo, p.L + 1), 256, smem, st>>>(p, S, d_rj, ld, cols);
   }
   if (cudaGetLastError() != cudaSuccess) return KMHD_ERR_CUDA;
   if (mid && cudaEventRecord(mid, st) != cudaSuccess) return KMHD_ERR_CUDA;
   GemmArgs a;
   a.P = p;
   a.S = S;
-  a.work = s->work_b;
-  a.nwork = s->nwork_b;
+  int e = select_work(s, p, false, &a.work, &a.nwork);
+  if (e != KMHD_OK) return e;
   a.pair = 1;
   a.d_rj = nullptr;
   a.ld = 0;
   a.cols = nullptr;
   a.err = s->err;
-  if (s->nwork_b > 0 && run_gemm(s, a, st) != cudaSuccess) return KMHD_ERR_CUDA;
+  if (a.nwork > 0 && run_gemm(s, a, st) != cudaSuccess) return KMHD_ERR_CUDA;
   return KMHD_OK;
 }
 
@@ -1195,21 +1264,21 @@ int split_fwd(SplitState* s, const Plan& p, double* d_rj, long long ld, const in
     auto kern = s->ns == 6 ? k_slice_mr<true, 6> : k_slice_mr<true, 4>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
       return KMHD_ERR_CUDA;
-    kern<<<dim3(p.nvf + 1, p.nr, p.L + 1), 256, smem, st>>>(p, S, nullptr, 0, nullptr);
+    if (p.r_hi > p.r_lo) kern<<<dim3(p.nvf + 1, p.r_hi - p.r_lo, p.L + 1), 256, smem, st>>>(p, S, nullptr, 0, nullptr);
   }
   if (cudaGetLastError() != cudaSuccess) return KMHD_ERR_CUDA;
   if (mid && cudaEventRecord(mid, st) != cudaSuccess) return KMHD_ERR_CUDA;
   GemmArgs a;
   a.P = p;
   a.S = S;
-  a.work = s->work_f;
-  a.nwork = s->nwork_f;
+  int e = select_work(s, p, true, &a.work, &a.nwork);
+  if (e != KMHD_OK) return e;
   a.pair = 0;
   a.d_rj = d_rj;
   a.ld = ld;
   a.cols = cols;
   a.err = s->err;
-  if (s->nwork_f > 0 && run_gemm(s, a, st) != cudaSuccess) return KMHD_ERR_CUDA;
+  if (a.nwork > 0 && run_gemm(s, a, st) != cudaSuccess) return KMHD_ERR_CUDA;
   return KMHD_OK;
 }
 

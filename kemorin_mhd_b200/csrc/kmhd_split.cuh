@@ -1,5 +1,7 @@
 // kmhd_split.cuh -- split-precision (Ozaki-style INT8 slice) Legendre tiers on tcgen05.
 #pragma once
+#include <vector>
+
 #include "kmhd_internal.cuh"
 
 namespace kmhd {
@@ -14,6 +16,10 @@ int split_bwd(SplitState* s, const Plan& p, int nlc_max, const double* d_rj, lon
               const int* cols, cudaStream_t st, cudaEvent_t mid = nullptr);
 int split_fwd(SplitState* s, const Plan& p, double* d_rj, long long ld, const int* cols,
               cudaStream_t st, cudaEvent_t mid = nullptr);
+// Radial chunks for windowed launches: bounds[0] = 0 < bounds[1] < ... =
+// p.nr, every bound but the last a multiple of 16.  split_bwd / split_fwd on a
+// plan whose window [r_lo, r_hi) is one chunk run only that chunk's tiles.
+int split_set_chunks(SplitState* s, const Plan& p, const std::vector<int>& bounds, cudaStream_t st);
 // Reads and returns the device error word (KMHD_OK or KMHD_ERR_TIMEOUT); synchronises st.
 int split_check_error(SplitState* s, cudaStream_t st);
 
