@@ -174,6 +174,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-tier comparison run")
     ap.add_argument("--nr", type=int, default=0, help="override the radius count (small profiling cases)")
+    ap.add_argument("--p-on-the-fly", action="store_true",
+                    help="FP64 tier: P_l^m generated inside the Legendre kernels (no stored tables); "
+                         "also times the stored-table FP64 tier on the same input")
     args = ap.parse_args()
 
     if args.config == "cfg4":
@@ -216,11 +219,14 @@ def main():
         tier = "split"
     lib = sph_trans.load_library()
 
-    def make(tier_name):
-        return sph_trans.SphTransform(cfg, tier=TIERS[tier_name], device=local)
+    if args.p_on_the_fly and args.tier != "fp64":
+        raise SystemExit("--p-on-the-fly needs --tier fp64")
+
+    def make(tier_name, otf=False):
+        return sph_trans.SphTransform(cfg, tier=TIERS[tier_name], device=local, p_on_the_fly=otf)
 
     try:
-        tr = make(tier)
+        tr = make(tier, otf=args.p_on_the_fly)
     except sph_trans.KmhdError:
         if args.tier != "auto":
             raise
@@ -288,6 +294,37 @@ def main():
                  "speedup_vs_fp64_gpu": ms64 / ms_step,
                  "rel_err_vs_fp64_per_field": err, "rel_err_max": max(err)}
         del ref64, out64
+    if args.p_on_the_fly:
+        # the stored-table FP64 tier on the same input (one handle at a time:
+        # at L=1023 each holds ~80 GB)
+        tr_bytes = tr.device_bytes()
+        tr.close()
+        torch.cuda.synchronize()
+        st = make("fp64")
+        st.set_stream(stream.cuda_stream)
+        out_st = torch.zeros_like(d_out)
+        for _ in range(2):
+            st.nonlinear_cycle(d_in, out_st)
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        nst = max(2, args.steps // 2)
+        f0.record(stream)
+        for _ in range(nst):
+            st.nonlinear_cycle(d_in, out_st)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        ms_st = max_over_ranks(f0.elapsed_time(f1) / nst)
+        den = out_st.abs().amax(dim=1)
+        err = ((d_out - out_st).abs().amax(dim=1) / den).tolist()
+        extra = {"p_tables": "generated in the Legendre kernels (KMHD_FLAG_P_ON_THE_FLY)",
+                 "device_bytes": tr_bytes,
+                 "fp64_stored_tables": {"value": ws * 1e3 / ms_st, "unit": UNIT, "ms_per_step": ms_st,
+                                        "device_bytes": st.device_bytes(), "kernels_ms": st.kernel_timing()},
+                 "speed_vs_stored_tables": ms_st / ms_step,
+                 "rel_err_vs_stored_per_field": err, "rel_err_vs_stored_max": max(err)}
+        tr = st
+        del out_st
 
     # roofline of the dominant kernel: the Legendre GEMM (split tiers: the one
     # tcgen05 kernel, launched once per direction; FP64: the slower of the two
@@ -320,7 +357,7 @@ def main():
 
     # end to end through the public API with pinned host buffers
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and not args.p_on_the_fly:  # (the on-the-fly handle is closed by now)
         h_in = torch.empty((cfg.ncb, cfg.J * cfg.nr), dtype=torch.float64, pin_memory=True)
         h_in.copy_(d_in)
         h_out = torch.empty((cfg.ncf, cfg.J * cfg.nr), dtype=torch.float64, pin_memory=True)

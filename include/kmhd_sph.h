@@ -85,6 +85,13 @@ typedef struct kmhd_sph kmhd_sph;
  * the split path on the first kmhd_sph_batch_cycle call and keep the faster
  * (both meet the tier's error bound).  The reference has no counterpart. */
 #define KMHD_FLAG_AUTOTUNE 1
+/* kmhd_sph_desc.flags, FP64 tier only: no stored P / dP tables; the Legendre
+ * kernels generate P_l^m and dP_l^m/dtheta by the fixed-order recurrence as
+ * they go, from O(L^2) coefficients, O(L Ntheta) start values and seeds every
+ * 64 degrees (about 20x less memory than the O(L^2 Ntheta) tables).  Values
+ * differ from the stored tables in the last bits only.  The reference stores
+ * the tables (schmidt_poly_on_rtm_grid.f90:145-197). */
+#define KMHD_FLAG_P_ON_THE_FLY 2
 
 /* Pointer-location flag for data arguments. */
 #define KMHD_PTR_DEVICE 0
@@ -159,7 +166,8 @@ int kmhd_sph_last_kernel_timing(kmhd_sph *handle, double *ms5);
 
 /* Copies the device Gauss colatitudes/weights [nth] and the hemisphere
  * P / dP tables of order m ([nth_hemi x (L-m+1)], rows theta, cols l) to host
- * arrays, for parity checks of the set-up stage. */
+ * arrays, for parity checks of the set-up stage (with KMHD_FLAG_P_ON_THE_FLY:
+ * the values the kernels generate). */
 int kmhd_sph_get_tables(kmhd_sph *handle, int32_t m, double *colat, double *weight,
                         double *P, double *dP);
 

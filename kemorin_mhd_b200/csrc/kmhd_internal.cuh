@@ -19,6 +19,7 @@ constexpr int kMaxVec = 4;    // vectors per field group
 constexpr int kMaxScl = 2;    // scalars per field group
 constexpr int kMaxProd = 16;
 constexpr int kMaxFftFactors = 16;
+constexpr int kSeedL = 32;    // degrees between on-the-fly recurrence seeds
 
 // Plan of one transform instance (device pointers + sizes).
 struct Plan {
@@ -39,6 +40,16 @@ struct Plan {
   const long long* poff;  // [(L+1)*2] element offset of (m,p) block in P/dP
   const int* kpad;        // [(L+1)*2]
   const int* jmap;        // [(L+1)][2][L+1] -> rj j, -1 if absent
+  // P / dP generated inside the FP64 Legendre kernels (otf = 1) instead of
+  // read from P / dP: per-order recurrence and dP coefficients, start values
+  // and the forward kernel's block seeds (see pchain)
+  int otf;
+  const double* cos_t;      // [nh] cos(colat)
+  const double2* pco;       // [(L+2)][L+1] (a_l, b_l) of order mo, l >= mo + 2
+  const double2* dco;       // [(L+1)][L+1] (e, f): dP_l^m = (e P_l^{m-1} - f P_l^{m+1}) / 2
+  const double2* pst;       // [(L+2)][nh_pad] (P_mo^mo, P_{mo+1}^mo)
+  const double* pseed;      // [m][s][6][nh_pad] chain states before l = m + kSeedL s
+  const long long* pseed_off;  // [L+1] first seed of order m
   // work buffers
   double* SB;             // packed backward spectra [m][p][kpad][nrb*ncolb_blk]
   const long long* sboff; // [(L+1)*2]
@@ -96,6 +107,72 @@ __host__ __device__ __forceinline__ long long rtm_off(const Plan& P, int m, int 
   return (((long long)m * P.nr + r) * P.nth + th) * (2LL * nc);
 }
 
+// One step of the Schmidt recurrence of order mo at hemisphere latitude th:
+// returns P_l^mo from the chain state (p1, p2) = (P_{l-1}^mo, P_{l-2}^mo) and
+// advances it.  P_l^mo = 0 for l < mo (and mo < 0); l = mo, mo + 1 take the
+// start values (the fixed-order closed forms times sin^mo, formed as the
+// stored tables form them); above, P_l = a_l cos(theta) P_{l-1} - b_l P_{l-2},
+// a_l = (2l - 1) / sqrt(l^2 - mo^2), b_l = sqrt((l-1)^2 - mo^2) / sqrt(l^2 - mo^2)
+// (schmidt_legendre_m, CORE_src/spherical_harmonics/schmidt_fix_m.f90:86-140,
+// with sin^mo carried in the recurrence instead of multiplied in afterwards).
+__device__ __forceinline__ double pchain(double& p1, double& p2, const Plan& P, int mo, int l, double ct, int th,
+                                        double2 ab) {
+  double v;
+  if (mo < 0 || l < mo) {
+    v = 0.0;
+  } else if (l <= mo + 1) {
+    const double2 s = P.pst[(long long)mo * P.nh_pad + th];
+    v = l == mo ? s.x : s.y;
+  } else {
+    v = fma(ab.x * ct, p1, -(ab.y * p2));
+  }
+  p2 = p1;
+  p1 = v;
+  return v;
+}
+
+// Coefficients of degree l for pgen_step: (a_l, b_l) of orders m - 1, m, m + 1
+// and the dP factors (e, f); zero where a chain takes no recurrence step.
+__device__ __forceinline__ double2 pgen_coef(const Plan& P, int m, int l, int q) {
+  if (l > P.L) return make_double2(0.0, 0.0);
+  if (q == 3) return __ldg(P.dco + (long long)m * (P.L + 1) + l);
+  const int mo = m - 1 + q;
+  if (mo < 0 || l < mo + 2) return make_double2(0.0, 0.0);
+  return __ldg(P.pco + (long long)mo * (P.L + 1) + l);
+}
+
+// P_l^m and dP_l^m/dtheta at (l, th) from the three chains of orders m - 1,
+// m, m + 1 (state st), as diff_schmidt_legendre_m
+// (schmidt_fix_m.f90:143-175): dP = (e P^{m-1} - f P^{m+1}) / 2.  cf holds
+// the four coefficient pairs of degree l (pgen_coef q = 0..3).
+__device__ __forceinline__ void pgen_step(double (&st)[6], const Plan& P, int m, int l, double ct, int th,
+                                          const double2* cf, double& p, double& dp) {
+  const double pm = pchain(st[0], st[1], P, m - 1, l, ct, th, cf[0]);
+  p = pchain(st[2], st[3], P, m, l, ct, th, cf[1]);
+  const double pp = pchain(st[4], st[5], P, m + 1, l, ct, th, cf[2]);
+  const double2 ef = cf[3];
+  dp = 0.5 * (ef.x * pm - ef.y * pp);
+}
+// pgen_step for l >= m + 3, where every chain takes a plain recurrence step
+// (order m - 1 < 0 has zero coefficients and state).
+__device__ __forceinline__ void pgen_step_fast(double (&st)[6], double ct, const double2* cf, double& p, double& dp) {
+  const double pm = fma(cf[0].x * ct, st[0], -(cf[0].y * st[1]));
+  st[1] = st[0];
+  st[0] = pm;
+  p = fma(cf[1].x * ct, st[2], -(cf[1].y * st[3]));
+  st[3] = st[2];
+  st[2] = p;
+  const double pp = fma(cf[2].x * ct, st[4], -(cf[2].y * st[5]));
+  st[5] = st[4];
+  st[4] = pp;
+  dp = 0.5 * (cf[3].x * pm - cf[3].y * pp);
+}
+__device__ __forceinline__ void pgen_step(double (&st)[6], const Plan& P, int m, int l, double ct, int th,
+                                          double& p, double& dp) {
+  const double2 cf[4] = {pgen_coef(P, m, l, 0), pgen_coef(P, m, l, 1), pgen_coef(P, m, l, 2), pgen_coef(P, m, l, 3)};
+  pgen_step(st, P, m, l, ct, th, cf, p, dp);
+}
+
 // Radial blocks (kRB radii each) of the window: first block and count.
 __host__ __device__ __forceinline__ int win_rb0(const Plan& P) { return P.r_lo / kRB; }
 __host__ __device__ __forceinline__ int win_nrb(const Plan& P) { return (P.r_hi + kRB - 1) / kRB - P.r_lo / kRB; }
@@ -124,6 +201,11 @@ __host__ __device__ __forceinline__ double g3_of(int l) {
 // Launchers (defined in the .cu files).
 cudaError_t launch_tables(const Plan& p, double* colat, double* weight, double* asin_t,
                           double* P, double* dP, cudaStream_t s);
+// Set-up of the on-the-fly tables (cos_t, pco, dco, pst, pseed of the plan).
+cudaError_t launch_otf_tables(const Plan& p, double* cos_t, double2* pco, double2* dco, double2* pst,
+                              double* pseed, const long long* pseed_off, cudaStream_t s);
+// P / dP of order m as the on-the-fly kernels generate them, [l - m][nh] (device).
+cudaError_t launch_otf_order(const Plan& p, int m, double* P, double* dP, cudaStream_t s);
 cudaError_t launch_pack_b(const Plan& p, int nlc_max, const double* d_rj, long long ld,
                           const int* cols, int nv, int ns, cudaStream_t s);
 cudaError_t launch_leg_bwd_f64(const Plan& p, cudaStream_t s);

@@ -38,6 +38,8 @@ struct BwdGeo {
   static constexpr int A_STAGE = 2 * kKC * AS;                       // P and dP
   static constexpr int B_STAGE = kKC * CBp;
   static constexpr size_t SMEM = sizeof(double) * 2 * (A_STAGE + B_STAGE);
+  // both parities per stage, and two chunk pairs' recurrence coefficients
+  static constexpr size_t SMEM_OTF = sizeof(double) * 4 * (A_STAGE + B_STAGE) + sizeof(double2) * 16 * kKC;
 };
 
 // ---------------------------------------------------------------------------
@@ -106,12 +108,19 @@ __global__ void k_pack_b(Plan p, const double* __restrict__ d_rj, long long ld,
 }
 
 // ---------------------------------------------------------------------------
-template <int NV, int NS>
-__global__ void __launch_bounds__(kThreads, 1) k_leg_bwd_f64(Plan p) {
+constexpr int kGenThreadsB = 64;  // generator warps of the on-the-fly backward kernel (one per latitude)
+
+// OTF: P / dP of the CTA's 64 latitudes come from two generator warps that run
+// the recurrence one chunk pair ahead of the tensor warps (chunk pair c = the
+// parity-0 and parity-1 chunks c, i.e. l = m + 32c .. m + 32c + 31); each
+// parity still accumulates its chunks in order, so only P's last bits differ
+// from the stored-table kernel.
+template <int NV, int NS, bool OTF>
+__global__ void __launch_bounds__(kThreads + (OTF ? kGenThreadsB : 0), 1) k_leg_bwd_f64(Plan p) {
   using G = BwdGeo<NV, NS>;
   extern __shared__ double sm[];
-  double* sA = sm;                     // [2 stages][2][kKC][AS]
-  double* sB = sm + 2 * G::A_STAGE;    // [2 stages][kKC][CBp]
+  double* sA = sm;                                   // [2 stages][(OTF: 2 parities)][2][kKC][AS]
+  double* sB = sm + (OTF ? 4 : 2) * G::A_STAGE;      // [2 stages][(OTF: 2 parities)][kKC][CBp]
   const int nthb = p.nh_pad / kThBlk;
   int b = blockIdx.x;
   const int nrbw = win_nrb(p);
@@ -126,6 +135,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_leg_bwd_f64(Plan p) {
   const int total = n0 + n1;
   const long long rowB = (long long)p.nrb * G::CB;
 
+  auto loadB = [&](double* bs, int par, int ch) {
+    const double* Bg = p.SB + p.sboff[2 * m + par] + (long long)(ch * kKC) * rowB + rb * G::CB;
+    for (int it = tid; it < kKC * (G::CB / 2); it += kThreads) {
+      const int row = it / (G::CB / 2), c2 = it % (G::CB / 2);
+      cp_async16(bs + row * G::CBp + 2 * c2, Bg + (long long)row * rowB + 2 * c2);
+    }
+  };
   auto load = [&](int stage, int step) {
     const int par = step < n0 ? 0 : 1;
     const int ch = step < n0 ? step : step - n0;
@@ -140,12 +156,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_leg_bwd_f64(Plan p) {
       const double* src = (tb ? dPg : Pg) + (long long)row * p.nh_pad + 2 * c2;
       cp_async16(a + tb * kKC * G::AS + row * G::AS + 2 * c2, src);
     }
-    const double* Bg = p.SB + p.sboff[2 * m + par] + (long long)(ch * kKC) * rowB + rb * G::CB;
-    double* bs = sB + stage * G::B_STAGE;
-    for (int it = tid; it < kKC * (G::CB / 2); it += kThreads) {
-      const int row = it / (G::CB / 2), c2 = it % (G::CB / 2);
-      cp_async16(bs + row * G::CBp + 2 * c2, Bg + (long long)row * rowB + 2 * c2);
-    }
+    loadB(sB + stage * G::B_STAGE, par, ch);
   };
 
   // accumulators: [field][tile][parity][2]; tiles XP, XdP, YP, YdP, ZP
@@ -162,10 +173,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_leg_bwd_f64(Plan p) {
 #pragma unroll
     for (int s = 0; s < 2; ++s) accS[v][s][0] = accS[v][s][1] = 0.0;
 
-  auto compute = [&](int stage, auto parc) {
+  auto compute = [&](const double* a, const double* bs, auto parc) {
     constexpr int par = decltype(parc)::value;
-    const double* a = sA + stage * G::A_STAGE;
-    const double* bs = sB + stage * G::B_STAGE;
 #pragma unroll
     for (int kk = 0; kk < kKC / 4; ++kk) {
       const int kr = 4 * kk + t;
@@ -189,22 +198,105 @@ __global__ void __launch_bounds__(kThreads, 1) k_leg_bwd_f64(Plan p) {
     }
   };
 
-  if (total > 0) {
-    load(0, 0);
-    cp_async_commit();
-  }
-  for (int step = 0; step < total; ++step) {
-    if (step + 1 < total) {
-      load((step + 1) & 1, step + 1);
+  if constexpr (!OTF) {
+    if (total > 0) {
+      load(0, 0);
       cp_async_commit();
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
     }
-    __syncthreads();
-    if (step < n0) compute(step & 1, std::integral_constant<int, 0>());
-    else compute(step & 1, std::integral_constant<int, 1>());
-    __syncthreads();
+    for (int step = 0; step < total; ++step) {
+      if (step + 1 < total) {
+        load((step + 1) & 1, step + 1);
+        cp_async_commit();
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncthreads();
+      const double* a = sA + (step & 1) * G::A_STAGE;
+      const double* bs = sB + (step & 1) * G::B_STAGE;
+      if (step < n0) compute(a, bs, std::integral_constant<int, 0>());
+      else compute(a, bs, std::integral_constant<int, 1>());
+      __syncthreads();
+    }
+  } else {
+    const bool gen = warp >= kWarps;
+    const int gi = tid - kThreads, ig = th0 + gi;  // generator thread: latitude ig
+    double st6[6];
+    double ct = 0.0;
+    if (gen) {
+      const double* sd = p.pseed + p.pseed_off[m] * 6 * p.nh_pad + ig;  // block 0: before l = m
+#pragma unroll
+      for (int q = 0; q < 6; ++q) st6[q] = sd[(long long)q * p.nh_pad];
+      if (ig < p.nh) ct = p.cos_t[ig];
+    }
+    // recurrence coefficients of a chunk pair's 32 degrees, [2 buffers][j][4];
+    // each call prefetches the next pair's into registers while it steps
+    double2* cb = reinterpret_cast<double2*>(sm + 4 * (G::A_STAGE + G::B_STAGE));
+    constexpr int kCE = 8 * kKC;  // coefficient pairs of one chunk pair
+    if (gen)
+      for (int e = gi; e < kCE; e += kGenThreadsB) cb[e] = pgen_coef(p, m, m + (e >> 2), e & 3);
+    auto genA = [&](int stage, int c) {
+      double* a = sA + stage * 2 * G::A_STAGE;
+      asm volatile("bar.sync 1, %0;\n" ::"n"(kGenThreadsB));  // cb[c & 1] complete
+      double2 nx[kCE / kGenThreadsB];
+#pragma unroll
+      for (int q = 0; q < kCE / kGenThreadsB; ++q) {
+        const int e = gi + q * kGenThreadsB;
+        nx[q] = c + 1 < n0 ? pgen_coef(p, m, m + 2 * kKC * (c + 1) + (e >> 2), e & 3) : make_double2(0.0, 0.0);
+      }
+      const double2* cc = cb + (c & 1) * kCE;
+      const int l0 = m + 2 * kKC * c;
+      const int nj = min(2 * kKC, p.L - l0 + 1);
+      if (l0 >= m + 3 && ig < p.nh) {
+#pragma unroll 4
+        for (int j = 0; j < 2 * kKC; ++j) {
+          double pv = 0.0, dpv = 0.0;
+          if (j < nj) pgen_step_fast(st6, ct, cc + 4 * j, pv, dpv);
+          double* ap = a + (j & 1) * G::A_STAGE + (j >> 1) * G::AS + gi;
+          ap[0] = pv;
+          ap[kKC * G::AS] = dpv;
+        }
+      } else {
+        for (int j = 0; j < 2 * kKC; ++j) {
+          double pv = 0.0, dpv = 0.0;
+          if (j < nj && ig < p.nh) pgen_step(st6, p, m, l0 + j, ct, ig, cc + 4 * j, pv, dpv);
+          double* ap = a + (j & 1) * G::A_STAGE + (j >> 1) * G::AS + gi;
+          ap[0] = pv;
+          ap[kKC * G::AS] = dpv;
+        }
+      }
+      double2* cn = cb + ((c + 1) & 1) * kCE;
+#pragma unroll
+      for (int q = 0; q < kCE / kGenThreadsB; ++q) cn[gi + q * kGenThreadsB] = nx[q];
+    };
+    auto loadB2 = [&](int stage, int c) {
+      loadB(sB + (2 * stage) * G::B_STAGE, 0, c);
+      if (c < n1) loadB(sB + (2 * stage + 1) * G::B_STAGE, 1, c);
+    };
+    // separate loops (same __syncthreads count), so the generator state is
+    // not live in the tensor warps
+    if (gen) {
+      genA(0, 0);
+      for (int c = 0; c < n0; ++c) {
+        __syncthreads();
+        if (c + 1 < n0) genA((c + 1) & 1, c + 1);
+      }
+      return;  // the generator warps take no part in the epilogue
+    }
+    loadB2(0, 0);
+    cp_async_commit();
+    for (int c = 0; c < n0; ++c) {
+      cp_async_wait<0>();
+      __syncthreads();
+      if (c + 1 < n0) {
+        loadB2((c + 1) & 1, c + 1);
+        cp_async_commit();
+      }
+      const double* a = sA + (c & 1) * 2 * G::A_STAGE;
+      const double* bs = sB + (c & 1) * 2 * G::B_STAGE;
+      compute(a, bs, std::integral_constant<int, 0>());
+      if (c < n1) compute(a + G::A_STAGE, bs + G::B_STAGE, std::integral_constant<int, 1>());
+    }
   }
 
   // ---- epilogue: N/S recombination and +-m cross terms
@@ -276,15 +368,21 @@ struct FwdGeo {
   static constexpr int A_TILE = kLBlk * AS;
   static constexpr int B_TILE = kKC * CFp;
   static constexpr size_t SMEM = sizeof(double) * (4 * A_TILE + 2 * B_TILE);
+  // A double-buffered, the block's recurrence coefficients and two chunks' seeds
+  static constexpr size_t SMEM_OTF =
+      sizeof(double) * (8 * A_TILE + 2 * B_TILE) + sizeof(double2) * 8 * kLBlk + sizeof(double) * 2 * 2 * 6 * kKC;
 };
 
-template <int NV, int NS>
+// OTF: the A tiles (P / dP of the block's 64 degrees at 16 latitudes) are
+// generated by warp 0 one latitude chunk ahead, each latitude's recurrence
+// starting from the seeds at the block's two 32-degree halves.
+template <int NV, int NS, bool OTF>
 __global__ void __launch_bounds__(kThreads, 2)
 k_leg_fwd_f64(Plan p, double* __restrict__ d_rj, long long ld, const int* __restrict__ cols) {
   using G = FwdGeo<NV, NS>;
   extern __shared__ double sm[];
-  double* sA = sm;                      // [P_e, P_o, dP_e, dP_o][kLBlk][AS]
-  double* sB = sm + 4 * G::A_TILE;      // [par][kKC][CFp]
+  double* sA = sm;                              // [(OTF: 2 stages)][P_e, P_o, dP_e, dP_o][kLBlk][AS]
+  double* sB = sm + (OTF ? 8 : 4) * G::A_TILE;  // [par][kKC][CFp]
   const int m = blockIdx.y;
   const int nrbw = win_nrb(p);
   const int kb = blockIdx.x / nrbw;
@@ -328,11 +426,71 @@ k_leg_fwd_f64(Plan p, double* __restrict__ d_rj, long long ld, const int* __rest
       }
     }
   };
+  // OTF: warp 0 generates the next chunk's A tile (before its share of the
+  // current chunk's MMAs).  Recurrence coefficients of the block's 64 degrees
+  // [j][4] are loaded once; the seeds of the next chunk's 16 latitudes and two
+  // 32-degree halves, [stage][half][6][kKC], arrive by cp.async a chunk ahead.
+  double2* cb = reinterpret_cast<double2*>(sB + 2 * G::B_TILE);
+  double* sS = reinterpret_cast<double*>(cb + 8 * kLBlk);
+  const int nsd = (p.L - m + kSeedL) / kSeedL;  // seeds of order m
+  auto seeds_async = [&](int stage, int ch) {
+    for (int e = lane; e < 2 * 6 * (kKC / 2); e += 32) {
+      const int h = e / (6 * (kKC / 2)), rem = e % (6 * (kKC / 2)), q = rem / (kKC / 2), c2 = rem % (kKC / 2);
+      const int sdi = 2 * kb + h;
+      if (sdi < nsd)
+        cp_async16(sS + ((stage * 2 + h) * 6 + q) * kKC + 2 * c2,
+                   p.pseed + ((p.pseed_off[m] + sdi) * 6 + q) * p.nh_pad + ch * kKC + 2 * c2);
+    }
+    cp_async_commit();
+  };
+  // lane: latitude ch * kKC + (lane & 15), degrees lh .. lh + 31 with
+  // lh = l0 + 32 h (h = lane >> 4); block row j (l = l0 + j) is parity j & 1,
+  // A row j >> 1
+  auto genA = [&](int stage, int ch) {
+    const int h = lane >> 4, tl = lane & 15;
+    const int ig = ch * kKC + tl;
+    double* a = sA + stage * 4 * G::A_TILE + tl;
+    const int l0 = m + 2 * kLBlk * kb, lh = l0 + kSeedL * h;
+    const int nj = min(kSeedL, p.L - lh + 1);
+    const bool ok = ig < p.nh && nj > 0;
+    double st6[6];
+    const double* sd = sS + ((stage * 2 + h) * 6) * kKC + tl;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) st6[q] = ok ? sd[q * kKC] : 0.0;
+    const double ct = ok ? p.cos_t[ig] : 0.0;
+    const double2* cc = cb + 4 * kSeedL * h;
+    if (lh >= m + 3) {
+#pragma unroll 4
+      for (int jj = 0; jj < kSeedL; ++jj) {
+        const int j = kSeedL * h + jj;
+        double pv = 0.0, dpv = 0.0;
+        if (ok && jj < nj) pgen_step_fast(st6, ct, cc + 4 * jj, pv, dpv);
+        a[(j & 1) * G::A_TILE + (j >> 1) * G::AS] = pv;
+        a[(2 + (j & 1)) * G::A_TILE + (j >> 1) * G::AS] = dpv;
+      }
+    } else {
+      for (int jj = 0; jj < kSeedL; ++jj) {
+        const int j = kSeedL * h + jj;
+        double pv = 0.0, dpv = 0.0;
+        if (ok && jj < nj) pgen_step(st6, p, m, lh + jj, ct, ig, cc + 4 * jj, pv, dpv);
+        a[(j & 1) * G::A_TILE + (j >> 1) * G::AS] = pv;
+        a[(2 + (j & 1)) * G::A_TILE + (j >> 1) * G::AS] = dpv;
+      }
+    }
+  };
+  if (OTF && warp == 0) {
+    for (int e = lane; e < 8 * kLBlk; e += 32) cb[e] = pgen_coef(p, m, m + 2 * kLBlk * kb + (e >> 2), e & 3);
+    seeds_async(0, 0);
+    cp_async_wait<0>();
+    __syncwarp();
+    genA(0, 0);
+    if (nchunk > 1) seeds_async(1, 1);
+  }
   prefetch(0);
   for (int ch = 0; ch < nchunk; ++ch) {
     const int th0 = ch * kKC;
     // A: 4 tables x 32 k-rows x 16 theta
-    for (int it = tid; it < 4 * kLBlk * (kKC / 2); it += kThreads) {
+    for (int it = tid; !OTF && it < 4 * kLBlk * (kKC / 2); it += kThreads) {
       const int tb = it / (kLBlk * (kKC / 2));   // 0 P_e, 1 P_o, 2 dP_e, 3 dP_o
       const int rem = it % (kLBlk * (kKC / 2));
       const int row = rem / (kKC / 2), c2 = rem % (kKC / 2);
@@ -401,10 +559,17 @@ k_leg_fwd_f64(Plan p, double* __restrict__ d_rj, long long ld, const int* __rest
       }
     }
     if (ch + 1 < nchunk) prefetch(ch + 1);
-    cp_async_wait<0>();
+    if (!OTF) cp_async_wait<0>();
     __syncthreads();
-    const double* aP = sA + par * G::A_TILE + (rgi * 8 + g) * G::AS;
-    const double* adP = sA + (2 + par) * G::A_TILE + (rgi * 8 + g) * G::AS;
+    if (OTF && warp == 0 && ch + 1 < nchunk) {
+      cp_async_wait<0>();  // seeds of chunk ch + 1
+      __syncwarp();
+      if (ch + 2 < nchunk) seeds_async(ch & 1, ch + 2);
+      genA((ch + 1) & 1, ch + 1);
+    }
+    const double* sAc = sA + (OTF ? (ch & 1) * 4 * G::A_TILE : 0);
+    const double* aP = sAc + par * G::A_TILE + (rgi * 8 + g) * G::AS;
+    const double* adP = sAc + (2 + par) * G::A_TILE + (rgi * 8 + g) * G::AS;
     const double* bb = sB + par * G::B_TILE;
 #pragma unroll
     for (int kk = 0; kk < kKC / 4; ++kk) {
@@ -455,27 +620,38 @@ k_leg_fwd_f64(Plan p, double* __restrict__ d_rj, long long ld, const int* __rest
   }
 }
 
-template <int NV, int NS>
-cudaError_t run_bwd(const Plan& p, cudaStream_t s) {
+template <int NV, int NS, bool OTF>
+cudaError_t run_bwd_t(const Plan& p, cudaStream_t s) {
   using G = BwdGeo<NV, NS>;
-  auto kern = k_leg_bwd_f64<NV, NS>;
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
+  auto kern = k_leg_bwd_f64<NV, NS, OTF>;
+  const size_t smem = OTF ? G::SMEM_OTF : G::SMEM;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const long long nblk = (long long)(p.L + 1) * (p.nh_pad / kThBlk) * win_nrb(p);
   if (nblk <= 0) return cudaSuccess;
-  kern<<<(unsigned)nblk, kThreads, G::SMEM, s>>>(p);
+  kern<<<(unsigned)nblk, kThreads + (OTF ? kGenThreadsB : 0), smem, s>>>(p);
   return cudaGetLastError();
 }
-
 template <int NV, int NS>
-cudaError_t run_fwd(const Plan& p, double* d_rj, long long ld, const int* cols, cudaStream_t s, int m_count) {
+cudaError_t run_bwd(const Plan& p, cudaStream_t s) {
+  return p.otf ? run_bwd_t<NV, NS, true>(p, s) : run_bwd_t<NV, NS, false>(p, s);
+}
+
+template <int NV, int NS, bool OTF>
+cudaError_t run_fwd_t(const Plan& p, double* d_rj, long long ld, const int* cols, cudaStream_t s, int m_count) {
   using G = FwdGeo<NV, NS>;
-  auto kern = k_leg_fwd_f64<NV, NS>;
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
+  auto kern = k_leg_fwd_f64<NV, NS, OTF>;
+  const size_t smem = OTF ? G::SMEM_OTF : G::SMEM;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int nkb = (kcount(p.L, 0, 0) + kLBlk - 1) / kLBlk;
   if (win_nrb(p) <= 0) return cudaSuccess;
   dim3 grid(nkb * win_nrb(p), m_count);
-  kern<<<grid, kThreads, G::SMEM, s>>>(p, d_rj, ld, cols);
+  kern<<<grid, kThreads, smem, s>>>(p, d_rj, ld, cols);
   return cudaGetLastError();
+}
+template <int NV, int NS>
+cudaError_t run_fwd(const Plan& p, double* d_rj, long long ld, const int* cols, cudaStream_t s, int m_count) {
+  return p.otf ? run_fwd_t<NV, NS, true>(p, d_rj, ld, cols, s, m_count)
+               : run_fwd_t<NV, NS, false>(p, d_rj, ld, cols, s, m_count);
 }
 
 #define KMHD_DISPATCH(NVv, NSv, FN, ...)                                   \

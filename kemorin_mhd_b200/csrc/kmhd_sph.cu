@@ -42,6 +42,10 @@ struct kmhd_sph {
   int64_t bytes = 0;
   double *radius = nullptr, *colat = nullptr, *weight = nullptr, *asin_t = nullptr;
   double *P = nullptr, *dP = nullptr, *SB = nullptr, *rtm_b = nullptr, *rtm_f = nullptr;
+  // on-the-fly P (KMHD_FLAG_P_ON_THE_FLY)
+  double *cos_t = nullptr, *pseed = nullptr;
+  double2 *pco = nullptr, *dco = nullptr, *pst = nullptr;
+  long long* pseed_off = nullptr;
   long long *poff = nullptr, *sboff = nullptr;
   int *kpad = nullptr, *jmap = nullptr, *digrev = nullptr;
   double2* twid = nullptr;
@@ -129,6 +133,8 @@ int validate(const kmhd_sph_desc* d) {
     return KMHD_ERR_SIZE;
   if (d->nvector_b + d->nscalar_b == 0) return KMHD_ERR_ARG;
   if (d->tier < KMHD_TIER_FP64 || d->tier > KMHD_TIER_FP32ACC) return KMHD_ERR_ARG;
+  if ((d->flags & KMHD_FLAG_P_ON_THE_FLY) && d->tier != KMHD_TIER_FP64) return KMHD_ERR_ARG;
+  if (d->flags & ~(KMHD_FLAG_AUTOTUNE | KMHD_FLAG_P_ON_THE_FLY)) return KMHD_ERR_ARG;
   if (d->nproduct < 0 || d->nproduct > kMaxProd) return KMHD_ERR_SIZE;
   if (d->nproduct > 0 && !d->products) return KMHD_ERR_ARG;
   int nv = 0, ns = 0;
@@ -354,13 +360,14 @@ int kmhd_sph_create(const kmhd_sph_desc* d, kmhd_sph** out) {
 
   // ---- device allocations
   const size_t nP = (size_t)po, nSB = (size_t)so;
+  const bool otf = (d->flags & KMHD_FLAG_P_ON_THE_FLY) != 0;
   const size_t nrtm_b = (size_t)(L + 1) * p.nth * p.nr * p.ncb * 2;
   const size_t nrtm_f = (size_t)(L + 1) * p.nth * p.nr * std::max(p.ncf, 1) * 2;
   const size_t nrj = (size_t)p.J * p.nr;
   const size_t nnod = (size_t)p.nr * p.nth * p.nph;
   if ((st = dalloc(h, &h->radius, p.nr)) || (st = dalloc(h, &h->colat, p.nth)) ||
       (st = dalloc(h, &h->weight, p.nth)) || (st = dalloc(h, &h->asin_t, p.nth)) ||
-      (st = dalloc(h, &h->P, nP)) || (st = dalloc(h, &h->dP, nP)) ||
+      (!otf && ((st = dalloc(h, &h->P, nP)) || (st = dalloc(h, &h->dP, nP)))) ||
       (st = dalloc(h, &h->poff, 2 * (L + 1))) || (st = dalloc(h, &h->sboff, 2 * (L + 1))) ||
       (st = dalloc(h, &h->kpad, 2 * (L + 1))) || (st = dalloc(h, &h->jmap, h->jmap_h.size())) ||
       (st = dalloc(h, &h->twid, p.nph)) || (st = dalloc(h, &h->digrev, p.nph)) ||
@@ -379,7 +386,7 @@ int kmhd_sph_create(const kmhd_sph_desc* d, kmhd_sph** out) {
       up(h->kpad, h->kpad_h.data(), sizeof(int) * 2 * (L + 1)) ||
       up(h->jmap, h->jmap_h.data(), sizeof(int) * h->jmap_h.size()) ||
       up(h->twid, tw.data(), sizeof(double2) * p.nph) || up(h->digrev, rev.data(), sizeof(int) * p.nph) ||
-      cudaMemsetAsync(h->P, 0, sizeof(double) * nP, s) || cudaMemsetAsync(h->dP, 0, sizeof(double) * nP, s))
+      (!otf && (cudaMemsetAsync(h->P, 0, sizeof(double) * nP, s) || cudaMemsetAsync(h->dP, 0, sizeof(double) * nP, s))))
     return fail(KMHD_ERR_CUDA);
   p.radius = h->radius;
   p.colat = h->colat;
@@ -408,17 +415,44 @@ int kmhd_sph_create(const kmhd_sph_desc* d, kmhd_sph** out) {
   }
   if (launch_tables(p, h->colat, h->weight, h->asin_t, h->P, h->dP, s) != cudaSuccess)
     return fail(KMHD_ERR_CUDA);
+  if (otf) {
+    // recurrence coefficients, start values and the forward block seeds
+    std::vector<long long> soff(L + 1);
+    long long nseed = 0;
+    for (int m = 0; m <= L; ++m) {
+      soff[m] = nseed;
+      nseed += (L - m + kSeedL) / kSeedL;
+    }
+    if ((st = dalloc(h, &h->cos_t, p.nh_pad)) || (st = dalloc(h, &h->pco, (size_t)(L + 2) * (L + 1))) ||
+        (st = dalloc(h, &h->dco, (size_t)(L + 1) * (L + 1))) || (st = dalloc(h, &h->pst, (size_t)(L + 2) * p.nh_pad)) ||
+        (st = dalloc(h, &h->pseed, (size_t)nseed * 6 * p.nh_pad)) || (st = dalloc(h, &h->pseed_off, (size_t)(L + 1))))
+      return fail(st);
+    if (up(h->pseed_off, soff.data(), sizeof(long long) * (L + 1)) ||
+        cudaMemsetAsync(h->cos_t, 0, sizeof(double) * p.nh_pad, s))
+      return fail(KMHD_ERR_CUDA);
+    p.otf = 1;
+    p.cos_t = h->cos_t;
+    p.pco = h->pco;
+    p.dco = h->dco;
+    p.pst = h->pst;
+    p.pseed = h->pseed;
+    p.pseed_off = h->pseed_off;
+    if (launch_otf_tables(p, h->cos_t, h->pco, h->dco, h->pst, h->pseed, h->pseed_off, s) != cudaSuccess)
+      return fail(KMHD_ERR_CUDA);
+  }
   h->autotune = (d->flags & KMHD_FLAG_AUTOTUNE) != 0 && d->tier != KMHD_TIER_FP64;
   if (d->tier != KMHD_TIER_FP64) {
     st = split_create(&h->split, p, d->tier, d->nslice, s);
     if (st != KMHD_OK) return fail(st);
     h->bytes += split_bytes(h->split);
   }
-  // Radial chunks of host-pointer cycles: about eight chunks of a multiple of
-  // 16 radii when the copies are large enough to be worth overlapping.
+  // Radial chunks of host-pointer cycles: about sixteen chunks of a multiple
+  // of 16 radii when the copies are large enough to be worth overlapping (the
+  // first chunk's copy in and the last chunk's kernels and copy out are not
+  // overlapped, so more chunks shorten the pipeline's fill and drain).
   {
     const double copy_bytes = 8.0 * (double)nrj * (p.ncb + p.ncf);
-    const int step = 16 * std::max(1, (int)std::lround(p.nr / 128.0));
+    const int step = 16 * std::max(1, (int)std::lround(p.nr / 256.0));
     if (copy_bytes >= 64.0 * (1 << 20) && p.nr >= 2 * step) {
       for (int r = 0; r + step < p.nr || r == 0; r += step) h->chunks.push_back(r);
       if (p.nr - h->chunks.back() < step / 2 && h->chunks.size() > 1) h->chunks.pop_back();
@@ -765,6 +799,19 @@ int kmhd_sph_get_tables(kmhd_sph* h, int32_t m, double* colat, double* weight, d
   if (colat) KCHECK(cudaMemcpy(colat, h->colat, sizeof(double) * p.nth, cudaMemcpyDeviceToHost));
   if (weight) KCHECK(cudaMemcpy(weight, h->weight, sizeof(double) * p.nth, cudaMemcpyDeviceToHost));
   const int nl = p.L - m + 1;
+  if (p.otf) {
+    if (!P && !dP) return KMHD_OK;
+    double *gP = nullptr, *gdP = nullptr;
+    KCHECK(cudaMalloc(&gP, sizeof(double) * 2 * (size_t)nl * p.nh));
+    gdP = gP + (size_t)nl * p.nh;
+    cudaError_t e = launch_otf_order(p, m, gP, gdP, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess && P) e = cudaMemcpy(P, gP, sizeof(double) * (size_t)nl * p.nh, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && dP) e = cudaMemcpy(dP, gdP, sizeof(double) * (size_t)nl * p.nh, cudaMemcpyDeviceToHost);
+    cudaFree(gP);
+    KCHECK(e);
+    return KMHD_OK;
+  }
   for (int which = 0; which < 2; ++which) {
     double* dst = which ? dP : P;
     if (!dst) continue;

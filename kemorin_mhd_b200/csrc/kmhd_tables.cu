@@ -178,7 +178,126 @@ __global__ void k_legendre(int L, int nh, int nh_pad, const double* __restrict__
   }
 }
 
+// ---------------------------------------------------------------------------
+// On-the-fly P tables (FP64 tier, KMHD_FLAG_P_ON_THE_FLY): O(L^2) coefficients,
+// O(L Ntheta) start values and the forward kernel's block seeds replace the
+// O(L^2 Ntheta) P / dP tables.
+
+// Recurrence coefficients of order mo (block y, 0..L+1) and dP coefficients of
+// order m = mo (mo <= L), one thread per degree l.
+__global__ void k_otf_coef(int L, double2* pco, double2* dco) {
+  const int mo = blockIdx.y;
+  for (int l = blockIdx.x * blockDim.x + threadIdx.x; l <= L; l += gridDim.x * blockDim.x) {
+    double2 ab = make_double2(0.0, 0.0);
+    if (l >= mo + 2) {
+      const double s2 = sqrt((double)(l * l - mo * mo));
+      ab.x = (double)(2 * l - 1) / s2;
+      ab.y = sqrt((double)((l - 1) * (l - 1) - mo * mo)) / s2;
+    }
+    pco[(long long)mo * (L + 1) + l] = ab;
+    if (mo > L) continue;
+    // dP = (e P^{m-1} - f P^{m+1}) / 2 with the factors of k_legendre (the
+    // m = 0 form -sqrt(l(l+1)/2) P^1 and the m = 1, l = 1 form P^0 included)
+    const int m = mo;
+    double2 ef = make_double2(0.0, 0.0);
+    if (m == 0) {
+      if (l >= 1) ef.y = 2.0 * sqrt((double)(l * (l + 1) / 2));
+    } else if (m == 1) {
+      if (l == 1) ef.x = 2.0;
+      else if (l > 1) ef = make_double2(sqrt((double)(2 * l * (l + 1))), sqrt((double)((l - 1) * (l + 2))));
+    } else {
+      if (l == m) ef.x = sqrt((double)(2 * m));
+      else if (l > m) ef = make_double2(sqrt((double)((l + m) * (l - m + 1))), sqrt((double)((l - m) * (l + m + 1))));
+    }
+    dco[(long long)m * (L + 1) + l] = ef;
+  }
+}
+
+// Start values (P_mo^mo, P_{mo+1}^mo) per (order mo = block y, latitude), the
+// same operations as k_legendre's first two values of the order; cos(colat).
+__global__ void k_otf_start(int nh, int nh_pad, const double* __restrict__ colat, double* cos_t, double2* pst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int mo = blockIdx.y;
+  if (i >= nh_pad) return;
+  double2 v = make_double2(0.0, 0.0);
+  if (i < nh) {
+    const double th = colat[i];
+    const double ct = cos(th), st = sin(th);
+    if (mo == 0) {
+      v = make_double2(1.0, ct);
+      cos_t[i] = ct;
+    } else {
+      SchmidtRec r;
+      r.init(mo, ct);
+      v = make_double2(times_sin_m(r.c0, st, mo), times_sin_m(r.c1, st, mo));
+    }
+  }
+  pst[(long long)mo * nh_pad + i] = v;
+}
+
+// Chain states (orders m - 1, m, m + 1) before every l0 = m + kSeedL s, one
+// thread per (latitude, order m = block y).
+__global__ void k_otf_seed(Plan p, double* pseed, const long long* __restrict__ pseed_off) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int m = blockIdx.y;
+  if (i >= p.nh_pad) return;
+  const int L = p.L;
+  const int nsd = (L - m + kSeedL) / kSeedL;
+  double* out = pseed + pseed_off[m] * 6 * p.nh_pad + i;
+  const bool ok = i < p.nh;
+  const double ct = ok ? p.cos_t[i] : 0.0;
+  double st[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  int sd = 0;
+  for (int l = m > 0 ? m - 1 : 0; l <= L && sd < nsd; ++l) {
+    if (l == m + kSeedL * sd) {
+      for (int q = 0; q < 6; ++q) out[((long long)sd * 6 + q) * p.nh_pad] = st[q];
+      ++sd;
+    }
+    if (ok) {
+      double a, b;
+      pgen_step(st, p, m, l, ct, i, a, b);
+    }
+  }
+}
+
+// Generated P / dP of one order m, [l - m][latitude] (nh per row): the values
+// the on-the-fly kernels use, for kmhd_sph_get_tables.
+__global__ void k_otf_order(Plan p, int m, double* __restrict__ P, double* __restrict__ dP) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.nh) return;
+  double st[6];
+  const double* sd = p.pseed + p.pseed_off[m] * 6 * p.nh_pad + i;
+  for (int q = 0; q < 6; ++q) st[q] = sd[(long long)q * p.nh_pad];
+  const double ct = p.cos_t[i];
+  for (int l = m; l <= p.L; ++l) {
+    double a, b;
+    pgen_step(st, p, m, l, ct, i, a, b);
+    P[(long long)(l - m) * p.nh + i] = a;
+    dP[(long long)(l - m) * p.nh + i] = b;
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_otf_order(const Plan& p, int m, double* P, double* dP, cudaStream_t s) {
+  k_otf_order<<<(p.nh + 127) / 128, 128, 0, s>>>(p, m, P, dP);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_otf_tables(const Plan& p, double* cos_t, double2* pco, double2* dco, double2* pst,
+                              double* pseed, const long long* pseed_off, cudaStream_t s) {
+  k_otf_coef<<<dim3((p.L + 1 + 127) / 128, p.L + 2), 128, 0, s>>>(p.L, pco, dco);
+  k_otf_start<<<dim3((p.nh_pad + 127) / 128, p.L + 2), 128, 0, s>>>(p.nh, p.nh_pad, p.colat, cos_t, pst);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  Plan q = p;
+  q.cos_t = cos_t;
+  q.pco = pco;
+  q.dco = dco;
+  q.pst = pst;
+  k_otf_seed<<<dim3((p.nh_pad + 63) / 64, p.L + 1), 64, 0, s>>>(q, pseed, pseed_off);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_tables(const Plan& p, double* colat, double* weight, double* asin_t,
                           double* P, double* dP, cudaStream_t s) {
@@ -186,6 +305,7 @@ cudaError_t launch_tables(const Plan& p, double* colat, double* weight, double* 
   k_gauss<<<(mh + 127) / 128, 128, 0, s>>>(p.nth, colat, weight, asin_t);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  if (!P) return cudaSuccess;  // on-the-fly P: no tables
   dim3 grid((p.nh + 63) / 64, p.L + 1);
   k_legendre<<<grid, 64, 0, s>>>(p.L, p.nh, p.nh_pad, colat, p.poff, P, dP);
   return cudaGetLastError();

@@ -27,6 +27,9 @@ _LIBPATH = os.path.join(_HERE, "libkmhd_sph.so")
 
 KMHD_PTR_DEVICE = 0
 KMHD_PTR_HOST = 1
+# kmhd_sph_desc.flags bits (include/kmhd_sph.h)
+FLAG_AUTOTUNE = 1
+FLAG_P_ON_THE_FLY = 2
 
 
 class KmhdError(RuntimeError):
@@ -127,7 +130,7 @@ class SphTransform:
     """One transform instance on one GPU (handle of the C-ABI)."""
 
     def __init__(self, cfg: SphConfig, tier: int = 0, nslice: int = 0, device: int = 0,
-                 radius=None, idx_rj_lm=None, autotune: bool = False):
+                 radius=None, idx_rj_lm=None, autotune: bool = False, p_on_the_fly: bool = False):
         lib = load_library()
         self.cfg = cfg
         self.tier = tier
@@ -145,7 +148,8 @@ class SphTransform:
         d.nvector_b, d.nscalar_b, d.nvector_f, d.nscalar_f = cfg.nvb, cfg.nsb, cfg.nvf, cfg.nsf
         d.nproduct = len(cfg.products)
         d.products = prods
-        d.tier, d.nslice, d.device, d.flags = tier, nslice, device, (1 if autotune else 0)
+        flags = (FLAG_AUTOTUNE if autotune else 0) | (FLAG_P_ON_THE_FLY if p_on_the_fly else 0)
+        d.tier, d.nslice, d.device, d.flags = tier, nslice, device, flags
         self._desc = d
         h = ctypes.c_void_p()
         _check(lib.kmhd_sph_create(ctypes.byref(d), ctypes.byref(h)), "kmhd_sph_create")

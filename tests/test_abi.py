@@ -57,3 +57,17 @@ def test_create_rejects_bad_descriptors():
     prods = (sph_trans.Product * 1)(sph_trans.Product(0, 0, 3, 1.0))  # cross with bad index
     d.nproduct, d.products = 1, prods
     assert lib.kmhd_sph_create(ctypes.byref(d), ctypes.byref(h)) == 1
+
+
+def test_create_rejects_bad_flags():
+    # on-the-fly P is an FP64-tier option; unknown flag bits are refused
+    lib = sph_trans.load_library()
+    d = sph_trans.Desc()
+    h = ctypes.c_void_p()
+    r = (ctypes.c_double * 4)(1.0, 1.1, 1.2, 1.3)
+    d.ltr, d.nth, d.nph, d.nr, d.radius = 31, 48, 96, 4, r
+    d.nvector_b, d.nscalar_b = 1, 1
+    d.tier, d.flags = 1, sph_trans.FLAG_P_ON_THE_FLY
+    assert lib.kmhd_sph_create(ctypes.byref(d), ctypes.byref(h)) == 1
+    d.tier, d.flags = 0, 8
+    assert lib.kmhd_sph_create(ctypes.byref(d), ctypes.byref(h)) == 1
