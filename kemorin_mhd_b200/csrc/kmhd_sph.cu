@@ -24,6 +24,11 @@ struct BatchGraph {
   cudaGraphExec_t exec = nullptr;
   cudaEvent_t fork = nullptr;
   std::vector<cudaEvent_t> join;
+  // split-path instances of one tier (6 or 4 slices) share one grouped GEMM
+  // launch per direction, on the group's stream
+  SplitGroup* group[2] = {nullptr, nullptr};
+  cudaStream_t gs[2] = {nullptr, nullptr};
+  std::vector<cudaEvent_t> ev;  // phase events of the grouped instances
 };
 
 struct kmhd_sph {
@@ -209,6 +214,11 @@ int kmhd_sph_destroy(kmhd_sph* h) {
     if (h->batch->exec) cudaGraphExecDestroy(h->batch->exec);
     if (h->batch->fork) cudaEventDestroy(h->batch->fork);
     for (cudaEvent_t e : h->batch->join) cudaEventDestroy(e);
+    for (cudaEvent_t e : h->batch->ev) cudaEventDestroy(e);
+    for (int k = 0; k < 2; ++k) {
+      split_group_destroy(h->batch->group[k]);
+      if (h->batch->gs[k]) cudaStreamDestroy(h->batch->gs[k]);
+    }
     if (h->batch->s0) cudaStreamDestroy(h->batch->s0);
     delete h->batch;
   }
@@ -935,17 +945,91 @@ int batch_cycle_impl(kmhd_sph** hs, int32_t n, const double* const* d_rj_in, con
         KCHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         bg->join.push_back(e);
       }
+      // split-path instances by tier: grouped GEMMs (built before the capture)
+      std::vector<int> grp[2];
+      for (int i = 0; i < n; ++i)
+        if (hs[i]->split && hs[i]->use_split) grp[split_ns(hs[i]->split) == 6 ? 0 : 1].push_back(i);
+      for (int k = 0; k < 2; ++k) {
+        split_group_destroy(bg->group[k]);
+        bg->group[k] = nullptr;
+        if (grp[k].size() < 2) {
+          grp[k].clear();  // a lone instance runs its own cycle
+          continue;
+        }
+        std::vector<SplitState*> ss;
+        std::vector<Plan> pl;
+        std::vector<double*> outs;
+        std::vector<long long> lds;
+        std::vector<const int*> cfs;
+        for (int i : grp[k]) {
+          ss.push_back(hs[i]->split);
+          pl.push_back(hs[i]->plan);
+          outs.push_back(d_rj_out[i]);
+          lds.push_back(ld_out[i]);
+          cfs.push_back(hs[i]->cols_f_d);
+        }
+        if ((st = split_group_create(&bg->group[k], ss.data(), pl.data(), (int)ss.size(), outs.data(), lds.data(),
+                                     cfs.data(), bg->s0)))
+          return st;
+        if (!bg->gs[k]) KCHECK(cudaStreamCreateWithFlags(&bg->gs[k], cudaStreamNonBlocking));
+      }
+      std::vector<char> grouped(n, 0);
+      for (int k = 0; k < 2; ++k)
+        for (int i : grp[k]) grouped[i] = 1;
+      while (bg->ev.size() < (size_t)(2 * n + 4)) {
+        cudaEvent_t e;
+        KCHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        bg->ev.push_back(e);
+      }
       cudaGraph_t graph = nullptr;
       KCHECK(cudaStreamBeginCapture(bg->s0, cudaStreamCaptureModeRelaxed));
       int cst = KMHD_OK;
-      if (cudaEventRecord(bg->fork, bg->s0) != cudaSuccess) cst = KMHD_ERR_CUDA;
+      auto ck = [&](cudaError_t e) {
+        if (e != cudaSuccess && cst == KMHD_OK) cst = KMHD_ERR_CUDA;
+      };
+      ck(cudaEventRecord(bg->fork, bg->s0));
+      // ungrouped instances: the whole cycle on the instance's stream
       for (int i = 0; i < n && cst == KMHD_OK; ++i) {
-        if (cudaStreamWaitEvent(hs[i]->stream, bg->fork, 0) != cudaSuccess) { cst = KMHD_ERR_CUDA; break; }
-        cst = enqueue_cycle(hs[i], d_rj_in[i], ld_in[i], d_rj_out[i], ld_out[i]);
-        if (cst) break;
-        if (cudaEventRecord(bg->join[i], hs[i]->stream) != cudaSuccess ||
-            cudaStreamWaitEvent(bg->s0, bg->join[i], 0) != cudaSuccess)
-          cst = KMHD_ERR_CUDA;
+        if (grouped[i]) continue;
+        ck(cudaStreamWaitEvent(hs[i]->stream, bg->fork, 0));
+        if (cst == KMHD_OK) cst = enqueue_cycle(hs[i], d_rj_in[i], ld_in[i], d_rj_out[i], ld_out[i]);
+        ck(cudaEventRecord(bg->join[i], hs[i]->stream));
+        ck(cudaStreamWaitEvent(bg->s0, bg->join[i], 0));
+      }
+      // grouped instances: slicers, FFT and the FP64 dipole modes on the
+      // instance streams, one grouped GEMM per direction on the group stream
+      for (int k = 0; k < 2 && cst == KMHD_OK; ++k) {
+        if (grp[k].empty()) continue;
+        cudaStream_t g = bg->gs[k];
+        cudaEvent_t eg0 = bg->ev[2 * n + 2 * k], eg1 = bg->ev[2 * n + 2 * k + 1];
+        ck(cudaStreamWaitEvent(g, bg->fork, 0));
+        for (int i : grp[k]) {
+          kmhd_sph* h = hs[i];
+          ck(cudaStreamWaitEvent(h->stream, bg->fork, 0));
+          if (cst == KMHD_OK) cst = split_slicer(h->split, h->plan, false, d_rj_in[i], ld_in[i], h->cols_b_d, h->stream);
+          ck(cudaEventRecord(bg->ev[2 * i], h->stream));
+          ck(cudaStreamWaitEvent(g, bg->ev[2 * i], 0));
+        }
+        if (cst == KMHD_OK) cst = split_group_gemm(bg->group[k], false, g);
+        ck(cudaEventRecord(eg0, g));
+        for (int i : grp[k]) {
+          kmhd_sph* h = hs[i];
+          ck(cudaStreamWaitEvent(h->stream, eg0, 0));
+          ck(launch_fft_cycle(h->plan, h->stream));
+          if (cst == KMHD_OK) cst = split_slicer(h->split, h->plan, true, nullptr, 0, nullptr, h->stream);
+          ck(cudaEventRecord(bg->ev[2 * i + 1], h->stream));
+          ck(cudaStreamWaitEvent(g, bg->ev[2 * i + 1], 0));
+        }
+        if (cst == KMHD_OK) cst = split_group_gemm(bg->group[k], true, g);
+        ck(cudaEventRecord(eg1, g));
+        for (int i : grp[k]) {
+          kmhd_sph* h = hs[i];
+          ck(cudaStreamWaitEvent(h->stream, eg1, 0));
+          // the dipole (l <= 2) modes again in FP64, as in the single cycle
+          ck(launch_leg_fwd_f64(h->plan, d_rj_out[i], ld_out[i], h->cols_f_d, h->stream, std::min(3, h->plan.L + 1)));
+          ck(cudaEventRecord(bg->join[i], h->stream));
+          ck(cudaStreamWaitEvent(bg->s0, bg->join[i], 0));
+        }
       }
       const cudaError_t ec = cudaStreamEndCapture(bg->s0, &graph);
       if (cst == KMHD_OK && ec == cudaSuccess && graph) {

@@ -22,6 +22,7 @@
 // combined (N = sym + asym, S = sym - asym) through distributed shared memory.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -638,8 +639,18 @@ __device__ __forceinline__ void st_global_v4(double* p, double a, double b, doub
   asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};\n" ::"l"(p), "d"(a), "d"(b), "d"(c), "d"(d) : "memory");
 }
 
-template <int NS, int TG>
-__global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args) {
+// Launch parameters: one instance (a), or a group of instances of one tier
+// whose pair units run in one persistent launch (GROUPED: unit u is pair
+// gunit[u].y of instance gunit[u].x, with that instance's arguments inst[.]).
+struct GemmLaunch {
+  GemmArgs a;  // grouped: only pair and err are used
+  const GemmArgs* inst;
+  const int2* gunit;
+  int gunits;
+};
+
+template <int NS, int TG, bool GROUPED>
+__global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_constant__ GemmLaunch L) {
   extern __shared__ __align__(1024) unsigned char sm[];
   constexpr int A_BYTES = NS * kTM * kTK, B_BYTES = NS * kTN * kTK;
   constexpr int STAGE = A_BYTES + B_BYTES;
@@ -651,13 +662,22 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
   unsigned long long* tfree = done + 1;         // TMEM drained by the epilogue
   unsigned* tmem_slot = reinterpret_cast<unsigned*>(tfree + 1);
 
-  const Plan& P = args.P;
-  const SliceTabs& S = args.S;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // units are (even, odd) parity tile pairs run back to back by one CTA
-  const bool bwd = args.pair != 0;
+  const bool bwd = L.a.pair != 0;
   const int per = 2;
-  const int nunits = args.nwork / per;
+  const int nunits = GROUPED ? L.gunits : L.a.nwork / per;
+  // arguments of unit u and the index of its first work item
+  auto unit = [&](int u, int& base) -> const GemmArgs& {
+    if constexpr (GROUPED) {
+      const int2 g = L.gunit[u];
+      base = per * g.y;
+      return L.inst[g.x];
+    } else {
+      base = per * u;
+      return L.a;
+    }
+  };
 
   if (threadIdx.x == 0) {
     for (int q = 0; q < kRing; ++q) {
@@ -677,7 +697,7 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
   tc_fence_after();
   const unsigned tmem = *tmem_slot;
 
-  auto nk_of = [&](const Work& w) -> int {
+  auto nk_of = [&](const Plan& P, const Work& w) -> int {
     const TypeGeo g = type_geo(w.t, P.L, w.m, P.nh);
     return (g.rows > 0 && w.mt * kTM < g.rpad) ? g.kpad / kTK : 0;
   };
@@ -688,9 +708,12 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
       long long gc = 0;
       bool ok = true;
       for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+        int base;
+        const GemmArgs& A = unit(u, base);
+        const SliceTabs& S = A.S;
         for (int h = 0; h < per && ok; ++h) {
-          const Work w = args.work[u * per + h];
-          const int nk = nk_of(w);
+          const Work w = A.work[base + h];
+          const int nk = nk_of(A.P, w);
           const signed char* Ag = S.A + S.aoff[w.m * kNT + w.t] + (long long)w.mt * nk * A_BYTES;
           const signed char* Bg = S.B + S.boff[w.m * kNT + w.t] + (long long)w.nt * nk * B_BYTES;
           for (int kc = 0; kc < nk; ++kc, ++gc) {
@@ -702,7 +725,7 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
           }
         }
       }
-      if (!ok) atomicExch(args.err, KMHD_ERR_TIMEOUT);
+      if (!ok) atomicExch(L.a.err, KMHD_ERR_TIMEOUT);
     }
   } else if (warp == 0) {
     if (lane == 0) {
@@ -712,9 +735,11 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
       int it = 0;
       bool ok = true;
       for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        int base;
+        const GemmArgs& A = unit(u, base);
         for (int h = 0; h < per; ++h, ++it) {
-          const Work w = args.work[u * per + h];
-          const int nk = nk_of(w);
+          const Work w = A.work[base + h];
+          const int nk = nk_of(A.P, w);
           if (it > 0 && ok && !mbar_wait(tfree, (unsigned)((it - 1) & 1))) ok = false;
           tc_fence_after();
           for (int kc = 0; kc < nk && ok; ++kc, ++gc) {
@@ -735,7 +760,7 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
           mma_commit(done);
         }
       }
-      if (!ok) atomicExch(args.err, KMHD_ERR_TIMEOUT);
+      if (!ok) atomicExch(L.a.err, KMHD_ERR_TIMEOUT);
     }
   } else {
     // ---- epilogue warps 2..9: TMEM lane quadrant = warp % 4, two warps per
@@ -745,14 +770,18 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
     const int cbase = kHalf * half;
     const int row = quad * 32 + lane;
     const double wscale = pow2(8 * (2 * NS - 2 - TG));
-    // 32-byte stores into the rtm records need 32-byte aligned records
-    const bool v4ok = ((reinterpret_cast<uintptr_t>(P.rtm_b) | (uintptr_t)(P.ncb * 16)) & 31) == 0;
     int it = 0;
     bool ok = true;
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+      int base;
+      const GemmArgs& A = unit(u, base);
+      const Plan& P = A.P;
+      const SliceTabs& S = A.S;
+      // 32-byte stores into the rtm records need 32-byte aligned records
+      const bool v4ok = ((reinterpret_cast<uintptr_t>(P.rtm_b) | (uintptr_t)(P.ncb * 16)) & 31) == 0;
       for (int h = 0; h < per; ++h, ++it) {
-        const Work w = args.work[u * per + h];
-        const int nk = nk_of(w);
+        const Work w = A.work[base + h];
+        const int nk = nk_of(P, w);
         const TypeGeo g = type_geo(w.t, P.L, w.m, P.nh);
         const int grow = w.mt * kTM + row;
         const int eA = (grow < g.rows) ? S.aexp[S.aeoff[w.m * kNT + w.t] + grow] : 0;
@@ -830,7 +859,7 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
                 if (f >= P.nvf + P.nsf) break;
                 const bool vec = f < P.nvf;
                 const double fac0 = vec ? r1 * r1 * g70 : g60, fac1 = vec ? r1 * r1 * g71 : g61;
-                double* dst = args.d_rj + jr + args.ld * args.cols[f];
+                double* dst = A.d_rj + jr + A.ld * A.cols[f];
                 const int c = 8 * rr + 2 * f;
                 if (ok0) {
                   dst[j00] = sr[c] * fac0;
@@ -852,22 +881,22 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
               if (r >= P.nr) continue;
               const double rr1 = P.radius[r];
               const double fac0 = rr1 * g70, fac1 = rr1 * g71;
-              double* dst = args.d_rj + P.J * (long long)r + args.ld * (args.cols[v] + 1);
+              double* dst = A.d_rj + P.J * (long long)r + A.ld * (A.cols[v] + 1);
               const int c = 4 * c4;
               if (ok0) {
                 dst[j00] = sr[c] * fac0;
-                dst[j00 + args.ld] = sr[c + 2] * fac0;
+                dst[j00 + A.ld] = sr[c + 2] * fac0;
                 if (s1) {
                   dst[j01] = sr[c + 1] * fac0;
-                  dst[j01 + args.ld] = sr[c + 3] * fac0;
+                  dst[j01 + A.ld] = sr[c + 3] * fac0;
                 }
               }
               if (ok1) {
                 dst[j10] = val[c] * fac1;
-                dst[j10 + args.ld] = val[c + 2] * fac1;
+                dst[j10 + A.ld] = val[c + 2] * fac1;
                 if (s1) {
                   dst[j11] = val[c + 1] * fac1;
-                  dst[j11 + args.ld] = val[c + 3] * fac1;
+                  dst[j11 + A.ld] = val[c + 3] * fac1;
                 }
               }
             }
@@ -952,7 +981,7 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(GemmArgs args
         }
       }
     }
-    if (!ok) atomicExch(args.err, KMHD_ERR_TIMEOUT);
+    if (!ok) atomicExch(L.a.err, KMHD_ERR_TIMEOUT);
   }
   tc_fence_before();
   __syncthreads();
@@ -998,20 +1027,29 @@ size_t gemm_smem(int ns) {
   return kRing * stage + sizeof(double) * kTM * kXS + (2 * kRing + 6) * 8 + 64;
 }
 
-template <int NS, int TG>
-cudaError_t launch_gemm(const GemmArgs& a, cudaStream_t st) {
-  auto kern = k_split_gemm<NS, TG>;
+template <int NS, int TG, bool GROUPED>
+cudaError_t launch_gemm(const GemmLaunch& l, int units, cudaStream_t st) {
+  auto kern = k_split_gemm<NS, TG, GROUPED>;
   const size_t smem = gemm_smem(NS);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int dev = 0, nsm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const int units = a.nwork / 2;
   const int grid = std::min(units, nsm);
   if (grid <= 0) return cudaSuccess;
-  kern<<<grid, kGemmWarps * 32, smem, st>>>(a);
+  kern<<<grid, kGemmWarps * 32, smem, st>>>(l);
   return cudaGetLastError();
+}
+
+template <int NS, int TG>
+cudaError_t launch_gemm(const GemmArgs& a, cudaStream_t st) {
+  GemmLaunch l;
+  l.a = a;
+  l.inst = nullptr;
+  l.gunit = nullptr;
+  l.gunits = 0;
+  return launch_gemm<NS, TG, false>(l, a.nwork / 2, st);
 }
 
 cudaError_t run_gemm(const SplitState* s, const GemmArgs& a, cudaStream_t st) {
@@ -1230,56 +1268,133 @@ size_t slice_smem(const Plan& p, bool fwd, int ns) {
   return sizeof(double) * (nx + 1 + kGrpCols) + kGrpCols * sizeof(int) + 8 * (size_t)ns * kSlab + 16;
 }
 
+int split_slicer(SplitState* s, const Plan& p, bool fwd, const double* d_rj, long long ld, const int* cols,
+                 cudaStream_t st) {
+  const SliceTabs& S = s->S;
+  const size_t smem = slice_smem(p, fwd, s->ns);
+  auto kern = fwd ? (s->ns == 6 ? k_slice_mr<true, 6> : k_slice_mr<true, 4>)
+                  : (s->ns == 6 ? k_slice_mr<false, 6> : k_slice_mr<false, 4>);
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return KMHD_ERR_CUDA;
+  if (p.r_hi > p.r_lo)
+    kern<<<dim3((fwd ? p.nvf : p.nvb) + 1, p.r_hi - p.r_lo, p.L + 1), 256, smem, st>>>(p, S, d_rj, ld, cols);
+  return cudaGetLastError() == cudaSuccess ? KMHD_OK : KMHD_ERR_CUDA;
+}
+
+// Arguments of one instance's GEMM in direction fwd over the plan's window.
+static int gemm_args(const SplitState* s, const Plan& p, bool fwd, double* d_rj, long long ld, const int* cols,
+                     GemmArgs* a) {
+  a->P = p;
+  a->S = s->S;
+  const int e = select_work(s, p, fwd, &a->work, &a->nwork);
+  if (e != KMHD_OK) return e;
+  a->pair = fwd ? 0 : 1;
+  a->d_rj = fwd ? d_rj : nullptr;
+  a->ld = fwd ? ld : 0;
+  a->cols = fwd ? cols : nullptr;
+  a->err = s->err;
+  return KMHD_OK;
+}
+
 int split_bwd(SplitState* s, const Plan& p, int, const double* d_rj, long long ld, const int* cols, cudaStream_t st,
               cudaEvent_t mid) {
-  const SliceTabs& S = s->S;
-  {
-    auto kern = s->ns == 6 ? k_slice_mr<false, 6> : k_slice_mr<false, 4>;
-    const size_t smem = slice_smem(p, false, s->ns);
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-      return KMHD_ERR_CUDA;
-    if (p.r_hi > p.r_lo) kern<<<dim3(p.nvb + 1, p.r_hi - p.r_lo, p.L + 1), 256, smem, st>>>(p, S, d_rj, ld, cols);
-  }
-  if (cudaGetLastError() != cudaSuccess) return KMHD_ERR_CUDA;
+  int e = split_slicer(s, p, false, d_rj, ld, cols, st);
+  if (e != KMHD_OK) return e;
   if (mid && cudaEventRecord(mid, st) != cudaSuccess) return KMHD_ERR_CUDA;
   GemmArgs a;
-  a.P = p;
-  a.S = S;
-  int e = select_work(s, p, false, &a.work, &a.nwork);
-  if (e != KMHD_OK) return e;
-  a.pair = 1;
-  a.d_rj = nullptr;
-  a.ld = 0;
-  a.cols = nullptr;
-  a.err = s->err;
+  if ((e = gemm_args(s, p, false, nullptr, 0, nullptr, &a)) != KMHD_OK) return e;
   if (a.nwork > 0 && run_gemm(s, a, st) != cudaSuccess) return KMHD_ERR_CUDA;
   return KMHD_OK;
 }
 
 int split_fwd(SplitState* s, const Plan& p, double* d_rj, long long ld, const int* cols, cudaStream_t st,
               cudaEvent_t mid) {
-  const SliceTabs& S = s->S;
-  {
-    const size_t smem = slice_smem(p, true, s->ns);
-    auto kern = s->ns == 6 ? k_slice_mr<true, 6> : k_slice_mr<true, 4>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-      return KMHD_ERR_CUDA;
-    if (p.r_hi > p.r_lo) kern<<<dim3(p.nvf + 1, p.r_hi - p.r_lo, p.L + 1), 256, smem, st>>>(p, S, nullptr, 0, nullptr);
-  }
-  if (cudaGetLastError() != cudaSuccess) return KMHD_ERR_CUDA;
+  int e = split_slicer(s, p, true, nullptr, 0, nullptr, st);
+  if (e != KMHD_OK) return e;
   if (mid && cudaEventRecord(mid, st) != cudaSuccess) return KMHD_ERR_CUDA;
   GemmArgs a;
-  a.P = p;
-  a.S = S;
-  int e = select_work(s, p, true, &a.work, &a.nwork);
-  if (e != KMHD_OK) return e;
-  a.pair = 0;
-  a.d_rj = d_rj;
-  a.ld = ld;
-  a.cols = cols;
-  a.err = s->err;
+  if ((e = gemm_args(s, p, true, d_rj, ld, cols, &a)) != KMHD_OK) return e;
   if (a.nwork > 0 && run_gemm(s, a, st) != cudaSuccess) return KMHD_ERR_CUDA;
   return KMHD_OK;
+}
+
+int split_ns(const SplitState* s) { return s ? s->ns : 0; }
+
+// ---------------------------------------------------------------------------
+// Grouped GEMM of several instances of one tier: per direction one device
+// array of the instances' arguments and one list of (instance, pair unit),
+// largest instance first; one persistent launch runs them all.
+struct SplitGroup {
+  int ns = 0, n = 0;
+  GemmArgs* inst[2] = {nullptr, nullptr};  // [bwd, fwd]
+  int2* unit[2] = {nullptr, nullptr};
+  int nunit[2] = {0, 0};
+  int* err = nullptr;
+};
+
+void split_group_destroy(SplitGroup* g) {
+  if (!g) return;
+  for (int d = 0; d < 2; ++d) {
+    cudaFree(g->inst[d]);
+    cudaFree(g->unit[d]);
+  }
+  delete g;
+}
+
+int split_group_create(SplitGroup** out, SplitState* const* ss, const Plan* plans, int n, double* const* d_rj_out,
+                       const long long* ld_out, const int* const* cols_f, cudaStream_t st) {
+  *out = nullptr;
+  if (n < 1) return KMHD_ERR_ARG;
+  SplitGroup* g = new SplitGroup();
+  g->ns = ss[0]->ns;
+  g->n = n;
+  g->err = ss[0]->err;
+  for (int d = 0; d < 2; ++d) {
+    const bool fwd = d == 1;
+    std::vector<GemmArgs> args(n);
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) {
+      if (ss[i]->ns != g->ns) { split_group_destroy(g); return KMHD_ERR_ARG; }
+      Plan p = plans[i];
+      p.r_lo = 0;
+      p.r_hi = p.nr;
+      const int e = gemm_args(ss[i], p, fwd, d_rj_out[i], ld_out[i], cols_f[i], &args[i]);
+      if (e != KMHD_OK) { split_group_destroy(g); return e; }
+      order[i] = i;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return args[a].nwork > args[b].nwork; });
+    std::vector<int2> units;
+    for (int i : order)
+      for (int u = 0; u < args[i].nwork / 2; ++u) units.push_back(make_int2(i, u));
+    g->nunit[d] = (int)units.size();
+    if (cudaMalloc(&g->inst[d], sizeof(GemmArgs) * n) != cudaSuccess ||
+        cudaMalloc(&g->unit[d], sizeof(int2) * std::max<size_t>(units.size(), 1)) != cudaSuccess) {
+      split_group_destroy(g);
+      return KMHD_ERR_NOMEM;
+    }
+    if (cudaMemcpyAsync(g->inst[d], args.data(), sizeof(GemmArgs) * n, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        (units.size() && cudaMemcpyAsync(g->unit[d], units.data(), sizeof(int2) * units.size(),
+                                         cudaMemcpyHostToDevice, st) != cudaSuccess) ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+      split_group_destroy(g);
+      return KMHD_ERR_CUDA;
+    }
+  }
+  *out = g;
+  return KMHD_OK;
+}
+
+int split_group_gemm(SplitGroup* g, bool fwd, cudaStream_t st) {
+  const int d = fwd ? 1 : 0;
+  GemmLaunch l;
+  std::memset(&l.a, 0, sizeof(l.a));
+  l.a.pair = fwd ? 0 : 1;
+  l.a.err = g->err;
+  l.inst = g->inst[d];
+  l.gunit = g->unit[d];
+  l.gunits = g->nunit[d];
+  const cudaError_t e = g->ns == 6 ? launch_gemm<6, 6, true>(l, l.gunits, st) : launch_gemm<4, 3, true>(l, l.gunits, st);
+  return e == cudaSuccess ? KMHD_OK : KMHD_ERR_CUDA;
 }
 
 int split_check_error(SplitState* s, cudaStream_t st) {

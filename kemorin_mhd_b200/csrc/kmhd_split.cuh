@@ -16,6 +16,19 @@ int split_bwd(SplitState* s, const Plan& p, int nlc_max, const double* d_rj, lon
               const int* cols, cudaStream_t st, cudaEvent_t mid = nullptr);
 int split_fwd(SplitState* s, const Plan& p, double* d_rj, long long ld, const int* cols,
               cudaStream_t st, cudaEvent_t mid = nullptr);
+// The two halves of split_bwd / split_fwd: the slicer alone.
+int split_slicer(SplitState* s, const Plan& p, bool fwd, const double* d_rj, long long ld, const int* cols,
+                 cudaStream_t st);
+int split_ns(const SplitState* s);
+// Grouped GEMM over n instances of one split tier (one persistent launch per
+// direction over every instance's pair units; d_rj_out / ld_out / cols_f are
+// the forward outputs, device pointers).  The arguments are copied to the
+// device at creation, so the group is tied to those pointers.
+struct SplitGroup;
+int split_group_create(SplitGroup** g, SplitState* const* ss, const Plan* plans, int n, double* const* d_rj_out,
+                       const long long* ld_out, const int* const* cols_f, cudaStream_t st);
+int split_group_gemm(SplitGroup* g, bool fwd, cudaStream_t st);
+void split_group_destroy(SplitGroup* g);
 // Radial chunks for windowed launches: bounds[0] = 0 < bounds[1] < ... =
 // p.nr, every bound but the last a multiple of 16.  split_bwd / split_fwd on a
 // plan whose window [r_lo, r_hi) is one chunk run only that chunk's tiles.

@@ -43,3 +43,31 @@ def test_batch_matches_oracle(tier):
     batch_cycle(trs, d_in, outs2)
     for c, o, ref in zip(CFGS, outs2, refs):
         assert col_relerr(from_dev_fortran(o), ref).max() <= tol, c.name
+
+
+@pytest.mark.gpu
+def test_grouped_gemm_batch_equals_single_cycles():
+    """Split-path instances of one tier share one grouped GEMM launch per
+    direction (work units of every instance in one persistent grid); the
+    results are bit-identical to each instance's own cycle, with instances of
+    both split tiers and an FP64 instance in the same batch."""
+    import torch
+    from kemorin_mhd_b200.config import TIER_FP32ACC
+    from kemorin_mhd_b200.sph_trans import SphTransform, batch_cycle
+    tiers = [TIER_SPLIT_I8, TIER_SPLIT_I8, TIER_SPLIT_I8, TIER_FP32ACC, TIER_FP32ACC, TIER_FP64]
+    cfgs = CFGS + [SphConfig(31, 48, 96, 7, name="b4"), SphConfig(63, 96, 192, 4, name="b5")]
+    cfgs = [cfgs[i] for i in (0, 2, 3, 4, 1, 5)]
+    trs = [SphTransform(c, tier=t) for c, t in zip(cfgs, tiers)]
+    d_in = [to_dev_fortran(make_d_rj(c, seed=60 + i)) for i, c in enumerate(cfgs)]
+    singles = []
+    for tr, c, d in zip(trs, cfgs, d_in):
+        o = torch.zeros((c.ncf, c.J * c.nr), dtype=torch.float64, device="cuda")
+        tr.nonlinear_cycle(d, o)
+        singles.append(o.cpu())
+    outs = [torch.zeros((c.ncf, c.J * c.nr), dtype=torch.float64, device="cuda") for c in cfgs]
+    for call in range(2):
+        for o in outs:
+            o.zero_()
+        batch_cycle(trs, d_in, outs)
+        for c, o, ref in zip(cfgs, outs, singles):
+            assert torch.equal(o.cpu(), ref), (call, c.name)
