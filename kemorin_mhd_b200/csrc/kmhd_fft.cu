@@ -616,6 +616,26 @@ __device__ void prefetch_line_t(double* st, const double* rtm, int nc, const Pla
   cp_async_commit();
 }
 
+// prefetch_line_t for a compile-time component count NC: thread t copies the
+// 16-byte pieces of component t % NC of orders t / NC, t / NC + T / NC, ...
+// (T = the largest multiple of NC not above the thread count), with pointer
+// increments instead of divisions.
+template <int NC>
+__device__ void prefetch_line_c(double* st, const double* rtm, const Plan& P, int th, int r) {
+  constexpr int NCS = NC | 1;
+  const int per = blockDim.x / NC;  // orders per sweep
+  if ((int)threadIdx.x < per * NC) {
+    const int c = threadIdx.x % NC;
+    int m = threadIdx.x / NC;
+    const long long strideM = (long long)P.nth * P.nr * NC * 2;
+    const double* src = rtm + rtm_off(P, m, th, r, NC) + 2 * c;
+    double* dst = st + (m * NCS + c) * 2;
+    const long long sstep = strideM * per;
+    for (; m <= P.L; m += per, src += sstep, dst += 2 * NCS * per) cp_async16(dst, src);
+  }
+  cp_async_commit();
+}
+
 __device__ __forceinline__ double2 spec_at_t(const double* st, int nc, int nv, int pp, int k, int N, int L) {
   int m;
   bool mirror;
@@ -655,6 +675,10 @@ constexpr int kFftThreadsF = 384;
 __host__ __device__ constexpr int ff_mid(int n) { return (n % 64 == 0 && (n / 64 == 3 || n / 64 == 6 || n / 64 == 12 || n / 64 == 24)) ? 16 : 4; }
 __host__ __device__ constexpr int ff_first(int n) { return n / (4 * ff_mid(n)); }
 __device__ __forceinline__ int swf(int i) { return i ^ (((i >> 3) ^ (i >> 6)) & 7); }
+// 32-byte global store; p 32-byte aligned
+__device__ __forceinline__ void st_v4(double* p, double a, double b, double c, double d) {
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};\n" ::"l"(p), "d"(a), "d"(b), "d"(c), "d"(d) : "memory");
+}
 
 // e^{2 pi i k / 48}: cos and sin of the first quadrant, k = 0..11
 __host__ __device__ constexpr double c48q(int k) {
@@ -777,14 +801,28 @@ __device__ __forceinline__ void ff_dif_first(const double* st, int nc, int nv, d
     const int pp = it / S1, j = it - pp * S1;
     double2 x[R];
     if constexpr (PR) {
+      // N = 3 (L + 1), S1 = (L + 1) / T3: input r < T3 is order m = j + r S1
+      // (m = 0 only at j = r = 0); input r >= 2 T3 is the mirror of order
+      // m = N - j - r S1 (m = L + 1, a zero, only at j = 0, r = 2 T3); the
+      // pair's two components sit at record offsets o0, o1 (o1 < 0: none)
+      const int o0 = rec_off(2 * pp, nv), o1 = 2 * pp + 1 < nc ? rec_off(2 * pp + 1, nv) : -1;
+      const int rs = 2 * ncs_of(nc);
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        if (r < T3) {
-          x[r] = spec_at_t(st, nc, nv, pp, j + r * S1, N, L);  // k <= L
-        } else if (r >= 2 * T3) {
-          x[r] = spec_at_t(st, nc, nv, pp, j + r * S1, N, L);  // k >= 2N/3
-        } else {
+        if (r >= T3 && r < 2 * T3) {
           x[r] = make_double2(0.0, 0.0);
+          continue;
+        }
+        const bool mir = r >= 2 * T3;
+        const int m = mir ? N - j - r * S1 : j + r * S1;
+        const double* rec = st + (m <= L ? m : 0) * rs;
+        const double2 c0 = *reinterpret_cast<const double2*>(rec + o0);
+        const double2 c1 = o1 >= 0 ? *reinterpret_cast<const double2*>(rec + o1) : make_double2(0.0, 0.0);
+        if (mir) {
+          x[r] = m <= L ? make_double2(0.5 * c0.x - 0.5 * c1.y, 0.5 * c0.y + 0.5 * c1.x) : make_double2(0.0, 0.0);
+        } else {
+          x[r] = (r == 0 && m == 0) ? make_double2(c0.x, c1.x)
+                                    : make_double2(0.5 * c0.x + 0.5 * c1.y, 0.5 * c1.x - 0.5 * c0.y);
         }
       }
       DFT2F_ZM<3, T3, +1>::run(x);
@@ -1050,6 +1088,47 @@ __device__ void ff_store_line(const double2* z, int npair, const Plan& P, double
   }
 }
 
+// Store of the line's forward spectra, one thread per order m writing the
+// whole rtm record (every component's (cos, sin) pair, assembled in registers)
+// as 32-byte stores: each record sector is written once, by one store.  The
+// record holds NC = 3 MVF + MSF pairs (NC even: 16 NC bytes, a multiple of 32).
+template <int N, int MVF, int MSF>
+__device__ void ff_store_records(const double2* z, const Plan& P, double* rtm, int th, int r) {
+  constexpr int NP = N + 1;
+  constexpr int NC = 3 * MVF + MSF, NPF = (NC + 1) / 2;
+  static_assert(NC % 2 == 0, "32-byte record stores need an even component count");
+  const int L = P.L;
+  const double aN = 1.0 / (double)N;
+  const long long strideM = (long long)P.nth * P.nr * NC * 2;
+  double* base = rtm + rtm_off(P, 0, th, r, NC);
+  for (int m = threadIdx.x; m <= L; m += blockDim.x) {
+    double rec[2 * NC];
+    const int im = swf(m), iw = swf(N - m);
+#pragma unroll
+    for (int pp = 0; pp < NPF; ++pp) {
+      const double2* zp = z + pp * NP;
+      const double2 zm = zp[im];
+      double a0, b0, a1, b1;
+      if (m == 0) {
+        a0 = zm.x * aN; a1 = zm.y * aN; b0 = 0.0; b1 = 0.0;
+      } else {
+        const double2 wm = zp[iw];
+        a0 = (zm.x + wm.x) * aN;
+        b0 = (wm.y - zm.y) * aN;
+        a1 = (zm.y + wm.y) * aN;
+        b1 = (zm.x - wm.x) * aN;
+      }
+      rec[rec_off(2 * pp, MVF)] = a0;
+      rec[rec_off(2 * pp, MVF) + 1] = b0;
+      rec[rec_off(2 * pp + 1, MVF)] = a1;
+      rec[rec_off(2 * pp + 1, MVF) + 1] = b1;
+    }
+    double* dst = base + m * strideM;
+#pragma unroll
+    for (int q = 0; q < 2 * NC; q += 4) st_v4(dst + q, rec[q], rec[q + 1], rec[q + 2], rec[q + 3]);
+  }
+}
+
 template <int N, int MVB, int MSB, int MVF, int MSF, bool PR, int PK>
 __global__ void __launch_bounds__(kFftThreadsF, 1) k_fft_cycle_f(Plan P, int line0, int nlines) {
   extern __shared__ double4 smraw[];
@@ -1061,7 +1140,7 @@ __global__ void __launch_bounds__(kFftThreadsF, 1) k_fft_cycle_f(Plan P, int lin
   int line = line0 + blockIdx.x;
   if (line >= nlines) return;
   // lines theta fastest: concurrent CTAs touch neighbouring records of one (m, r)
-  prefetch_line_t(st, P.rtm_b, P.ncb, P, line % P.nth, line / P.nth);
+  prefetch_line_c<3 * MVB + MSB>(st, P.rtm_b, P, line % P.nth, line / P.nth);
   while (line < nlines) {
     const int th = line % P.nth, r = line / P.nth;
     cp_async_wait<0>();
@@ -1069,7 +1148,7 @@ __global__ void __launch_bounds__(kFftThreadsF, 1) k_fft_cycle_f(Plan P, int lin
     ff_dif_first<N, PR>(st, P.ncb, P.nvb, z, npb, P.L, P.twid);
     __syncthreads();
     const int next = line + gridDim.x;
-    if (next < nlines) prefetch_line_t(st, P.rtm_b, P.ncb, P, next % P.nth, next / P.nth);
+    if (next < nlines) prefetch_line_c<3 * MVB + MSB>(st, P.rtm_b, P, next % P.nth, next / P.nth);
     ff_mid_pass<N, +1>(z, npb, P.twid);
     __syncthreads();
     ff_fused<N, MVB, MSB, MVF, MSF, PK>(z, P);
@@ -1078,7 +1157,8 @@ __global__ void __launch_bounds__(kFftThreadsF, 1) k_fft_cycle_f(Plan P, int lin
     __syncthreads();
     ff_dit_last<N, PR>(z, npf, P.twid);
     __syncthreads();
-    ff_store_line<N>(z, npf, P, P.rtm_f, P.ncf, P.nvf, th, r);
+    if constexpr ((3 * MVF + MSF) % 2 == 0) ff_store_records<N, MVF, MSF>(z, P, P.rtm_f, th, r);
+    else ff_store_line<N>(z, npf, P, P.rtm_f, P.ncf, P.nvf, th, r);
     __syncthreads();
     line = next;
   }

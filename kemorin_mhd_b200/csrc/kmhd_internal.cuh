@@ -50,6 +50,7 @@ struct Plan {
   const double2* pst;       // [(L+2)][nh_pad] (P_mo^mo, P_{mo+1}^mo)
   const double* pseed;      // [m][s][6][nh_pad] chain states before l = m + kSeedL s
   const long long* pseed_off;  // [L+1] first seed of order m
+  int* err;               // device error word of the instance (KMHD_ERR_TIMEOUT from a bounded wait), or null
   // work buffers
   double* SB;             // packed backward spectra [m][p][kpad][nrb*ncolb_blk]
   const long long* sboff; // [(L+1)*2]

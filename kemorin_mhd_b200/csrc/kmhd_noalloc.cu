@@ -229,7 +229,7 @@ int na_tables(const kmhd_sph_desc* d, const Plan& p, NaHost& H) {
 struct NaBufs {
   double *radius, *colat, *weight, *asin_t, *P, *dP, *SB, *rtm_b, *rtm_f;
   long long *poff, *sboff;
-  int *kpad, *jmap, *digrev, *cols_b, *cols_f;
+  int *kpad, *jmap, *digrev, *cols_b, *cols_f, *err;
   double2* twid;
 };
 
@@ -248,6 +248,7 @@ size_t na_layout(const Plan& p, const NaHost& H, unsigned char* base, NaBufs& b)
   b.digrev = c.take<int>(p.nph);
   b.cols_b = c.take<int>(kMaxVec + kMaxScl);
   b.cols_f = c.take<int>(kMaxVec + kMaxScl);
+  b.err = c.take<int>(1);
   b.P = c.take<double>(H.nP);
   b.dP = c.take<double>(H.nP);
   b.SB = c.take<double>(H.nSB);
@@ -304,8 +305,10 @@ extern "C" int kmhd_sph_cycle_noalloc(const kmhd_sph_desc* desc, const double* d
       up(b.cols_b, cols_b, sizeof(int) * (p.nvb + p.nsb)) ||
       up(b.cols_f, cols_f, sizeof(int) * (p.nvf + p.nsf)) ||
       cudaMemsetAsync(b.P, 0, sizeof(double) * H.nP, s) != cudaSuccess ||
-      cudaMemsetAsync(b.dP, 0, sizeof(double) * H.nP, s) != cudaSuccess)
+      cudaMemsetAsync(b.dP, 0, sizeof(double) * H.nP, s) != cudaSuccess ||
+      cudaMemsetAsync(b.err, 0, sizeof(int), s) != cudaSuccess)
     return KMHD_ERR_CUDA;
+  p.err = b.err;
   p.radius = b.radius;
   p.colat = b.colat;
   p.weight = b.weight;
@@ -328,5 +331,7 @@ extern "C" int kmhd_sph_cycle_noalloc(const kmhd_sph_desc* desc, const double* d
       launch_leg_fwd_f64(p, d_rj_out, ld_out, b.cols_f, s) != cudaSuccess)
     return KMHD_ERR_CUDA;
   if (cudaStreamSynchronize(s) != cudaSuccess) return KMHD_ERR_CUDA;
-  return KMHD_OK;
+  int herr = 0;  // a bounded device wait that expired
+  if (cudaMemcpy(&herr, b.err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return KMHD_ERR_CUDA;
+  return herr ? herr : KMHD_OK;
 }

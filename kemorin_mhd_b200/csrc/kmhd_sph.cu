@@ -55,6 +55,7 @@ struct kmhd_sph {
   int *kpad = nullptr, *jmap = nullptr, *digrev = nullptr;
   double2* twid = nullptr;
   int *cols_b_d = nullptr, *cols_f_d = nullptr;
+  int* err = nullptr;  // device error word (bounded waits of the FFT and tcgen05 kernels)
   std::vector<int> cols_b_cache, cols_f_cache;
   // host-pointer staging
   double *stage_in = nullptr, *stage_out = nullptr, *stage_grid = nullptr;
@@ -381,7 +382,7 @@ int kmhd_sph_create(const kmhd_sph_desc* d, kmhd_sph** out) {
       (st = dalloc(h, &h->poff, 2 * (L + 1))) || (st = dalloc(h, &h->sboff, 2 * (L + 1))) ||
       (st = dalloc(h, &h->kpad, 2 * (L + 1))) || (st = dalloc(h, &h->jmap, h->jmap_h.size())) ||
       (st = dalloc(h, &h->twid, p.nph)) || (st = dalloc(h, &h->digrev, p.nph)) ||
-      (st = dalloc(h, &h->cols_b_d, 16)) || (st = dalloc(h, &h->cols_f_d, 16)) ||
+      (st = dalloc(h, &h->cols_b_d, 16)) || (st = dalloc(h, &h->cols_f_d, 16)) || (st = dalloc(h, &h->err, 1)) ||
       (st = dalloc(h, &h->SB, nSB)) || (st = dalloc(h, &h->rtm_b, nrtm_b)) ||
       (st = dalloc(h, &h->rtm_f, nrtm_f)))
     return fail(st);
@@ -396,8 +397,10 @@ int kmhd_sph_create(const kmhd_sph_desc* d, kmhd_sph** out) {
       up(h->kpad, h->kpad_h.data(), sizeof(int) * 2 * (L + 1)) ||
       up(h->jmap, h->jmap_h.data(), sizeof(int) * h->jmap_h.size()) ||
       up(h->twid, tw.data(), sizeof(double2) * p.nph) || up(h->digrev, rev.data(), sizeof(int) * p.nph) ||
-      (!otf && (cudaMemsetAsync(h->P, 0, sizeof(double) * nP, s) || cudaMemsetAsync(h->dP, 0, sizeof(double) * nP, s))))
+      (!otf && (cudaMemsetAsync(h->P, 0, sizeof(double) * nP, s) || cudaMemsetAsync(h->dP, 0, sizeof(double) * nP, s))) ||
+      cudaMemsetAsync(h->err, 0, sizeof(int), s))
     return fail(KMHD_ERR_CUDA);
+  p.err = h->err;
   p.radius = h->radius;
   p.colat = h->colat;
   p.weight = h->weight;
@@ -558,6 +561,15 @@ int enqueue_cycle(kmhd_sph* h, const double* in, int64_t ld_in, double* out, int
   return run_fwd_spectral(h, out, ld_out, false);
 }
 
+// The instance's device error word (KMHD_ERR_TIMEOUT from a bounded wait of
+// the FFT or tcgen05 kernels); synchronises the handle's stream.
+int check_dev_err(kmhd_sph* h) {
+  int v = 0;
+  KCHECK(cudaMemcpyAsync(&v, h->err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  KCHECK(cudaStreamSynchronize(h->stream));
+  return v;
+}
+
 // Host-pointer cycle over the radial chunks.  Every stage is independent per
 // radius, so chunk c's kernels run on the handle's stream while chunk c + 1's
 // spectra come in on s_in and chunk c - 1's results go out on s_out.  The
@@ -617,8 +629,8 @@ int cycle_host_chunked(kmhd_sph* h, const double* d_rj_in, int64_t ld_in, const 
   KCHECK(cudaStreamWaitEvent(h->stream, h->ev[1], 0));
   KCHECK(cudaEventRecord(h->ev[3], h->stream));
   KCHECK(cudaEventSynchronize(h->ev[3]));
-  if (h->split) {
-    const int e = split_check_error(h->split, h->stream);
+  {
+    const int e = check_dev_err(h);
     if (e != KMHD_OK) return e;
   }
   // the stages overlap: only the whole call is timed
@@ -632,8 +644,8 @@ int cycle_host_chunked(kmhd_sph* h, const double* d_rj_in, int64_t ld_in, const 
 
 int finish_timing(kmhd_sph* h) {
   KCHECK(cudaEventSynchronize(h->ev[3]));
-  if (h->split) {
-    const int e = split_check_error(h->split, h->stream);
+  {
+    const int e = check_dev_err(h);
     if (e != KMHD_OK) return e;
   }
   float a = 0, b = 0, c = 0, t = 0;
@@ -1048,10 +1060,9 @@ int batch_cycle_impl(kmhd_sph** hs, int32_t n, const double* const* d_rj_in, con
       return st;
     }
   }
-  for (int i = 0; i < n; ++i)
-    if (hs[i]->split) {
-      const int e = split_check_error(hs[i]->split, hs[i]->stream);
-      if (e != KMHD_OK) return e;
-    }
+  for (int i = 0; i < n; ++i) {
+    const int e = check_dev_err(hs[i]);
+    if (e != KMHD_OK) return e;
+  }
   return KMHD_OK;
 }

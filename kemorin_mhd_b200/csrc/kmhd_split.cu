@@ -1143,13 +1143,14 @@ int split_create(SplitState** out, const Plan& p, int tier, int nslice, cudaStre
   }
   int st_ = KMHD_OK;
   long long *aoff_d, *aeoff_d, *deoff_d, *boff_d, *beoff_d;
+  if (p.err) s->err = p.err;  // the instance's error word
   if ((st_ = salloc(s, &S.A, (size_t)ao)) || (st_ = salloc(s, &S.aexp, (size_t)aeo)) ||
       (st_ = salloc(s, &S.dexp, (size_t)deo)) || (st_ = salloc(s, &S.B, (size_t)bo)) ||
       (st_ = salloc(s, &S.bexp, (size_t)beo)) || (st_ = salloc(s, &aoff_d, s->aoff.size())) ||
       (st_ = salloc(s, &aeoff_d, s->aeoff.size())) || (st_ = salloc(s, &deoff_d, s->deoff.size())) ||
       (st_ = salloc(s, &boff_d, s->boff.size())) || (st_ = salloc(s, &beoff_d, s->beoff.size())) ||
       (st_ = salloc(s, &s->work_b, wb.size())) || (st_ = salloc(s, &s->work_f, wf.size())) ||
-      (st_ = salloc(s, &s->err, 1))) {
+      (!p.err && (st_ = salloc(s, &s->err, 1)))) {
     split_destroy(s);
     return st_;
   }
