@@ -276,49 +276,32 @@ __device__ __forceinline__ ColRef colref_fwd(const Plan& P, const SliceTabs& S, 
   return c;
 }
 
-// Balanced base-256 digits of round(v), |round(v)| < 2^(8 NS - 2): d[NS-1] is
-// the least significant, every digit in [-128, 127] except d[0], which holds
-// the remaining high part (|d[0]| <= 64).  The value is split exactly into
-// hi 2^24 + lo with both halves in int32, so the digit loop runs on 32-bit
-// integers.
 // Balanced base-256 digits of round(v[i]), |round(v[i])| < 2^(8 NS - 2), for four
 // values, packed as bytes (value i in byte i) into one word per slice; w[NS-1]
-// holds the least significant digits.  A balanced digit's two's-complement
-// byte is the low byte of the running value x, and the next value is
-// (x + 128) >> 8.  Each value is rounded to the nearest integer x (ties to
-// even) by adding 1.5 2^52, whose double then holds 2^52 + 2^51 + x in its
-// mantissa, and split exactly into hi 2^24 + lo with both halves in int32
-// (lo = the sign-extended low 24 bits); the top digit (|d| <= 64) is what
-// remains of hi.
-__device__ __forceinline__ uint32_t pack4(int b0, int b1, int b2, int b3) {
-  return __byte_perm(__byte_perm(b0, b1, 0x0040), __byte_perm(b2, b3, 0x0040), 0x5410);
-}
+// holds the least significant digits.  Every digit d_s lies in [-128, 127],
+// so x + K with K = 0x80 in each of the NS bytes has the bytes d_s + 128
+// (0 < x + K < 2^(8 NS)); a balanced digit's two's-complement byte is that
+// byte XOR 0x80.  The rounding to the nearest integer x (ties to even) adds
+// 1.5 2^52, whose double then holds 2^52 + 2^51 + x in its mantissa; K is
+// folded into the constant subtracted from those bits.
 template <int NS>
 __device__ __forceinline__ void digits4(const double (&v)[4], uint32_t (&w)[NS]) {
-  int lo[4], hi[4];
+  static_assert(NS == 4 || NS == 6, "slice count");
+  constexpr unsigned long long K = NS == 6 ? 0x808080808080ull : 0x80808080ull;
+  constexpr long long C = 0x4338000000000000LL - (long long)K;
+  uint32_t lo[4], hi[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const long long x = __double_as_longlong(v[i] + 6755399441055744.0) - 0x4338000000000000LL;
-    lo[i] = (int)((unsigned)x << 8) >> 8;
-    hi[i] = (int)((x - lo[i]) >> 24);
+    const long long y = __double_as_longlong(v[i] + 6755399441055744.0) - C;
+    lo[i] = (uint32_t)y ^ 0x80808080u;
+    hi[i] = (uint32_t)((unsigned long long)y >> 32) ^ 0x80808080u;
   }
 #pragma unroll
-  for (int s = NS - 1; s >= 1; --s) {
-    if (s >= NS - 3) {
-      w[s] = pack4(lo[0], lo[1], lo[2], lo[3]);
-#pragma unroll
-      for (int i = 0; i < 4; ++i) lo[i] = (lo[i] + 128) >> 8;
-      if (s == NS - 3) {
-#pragma unroll
-        for (int i = 0; i < 4; ++i) hi[i] += lo[i];
-      }
-    } else {
-      w[s] = pack4(hi[0], hi[1], hi[2], hi[3]);
-#pragma unroll
-      for (int i = 0; i < 4; ++i) hi[i] = (hi[i] + 128) >> 8;
-    }
+  for (int b = 0; b < NS; ++b) {
+    const uint32_t* q = b < 4 ? lo : hi;
+    const uint32_t sel = (uint32_t)(b & 3) | ((uint32_t)((b & 3) + 4) << 4);
+    w[NS - 1 - b] = __byte_perm(__byte_perm(q[0], q[1], sel), __byte_perm(q[2], q[3], sel), 0x5410);
   }
-  w[0] = pack4(hi[0], hi[1], hi[2], hi[3]);
 }
 
 // Slicer: one CTA per (field group z, radius r, order m).  Backward groups:
