@@ -19,12 +19,31 @@
 #include <algorithm>
 #include <utility>
 
+#include <cuda.h>
+
+#include <cstring>
+
 #include "kmhd_internal.cuh"
 
 namespace kmhd {
 namespace {
 
 constexpr int kFftThreads = 256;
+
+// mbarrier + TMA tensor load (staging of a line's spectra)
+constexpr long long kFftSpinCap = 1ll << 24;  // bounded waits (about a second), then KMHD_ERR_TIMEOUT
+__device__ __forceinline__ unsigned ssa(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ bool fbar_wait(unsigned long long* b, unsigned parity) {
+  for (long long it = 0; it < kFftSpinCap; ++it) {
+    unsigned ok;
+    asm volatile(
+        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(ssa(b)), "r"(parity));
+    if (ok) return true;
+  }
+  return false;
+}
 
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
@@ -658,7 +677,25 @@ __device__ __forceinline__ double2 spec_at_t(const double* st, int nc, int nv, i
 
 size_t smem_cycle_f(const Plan& p) {
   const int npair = ((p.ncb > p.ncf ? p.ncb : p.ncf) + 1) / 2;
-  return sizeof(double2) * ((size_t)npair * (p.nph + 1) + 1) + sizeof(double) * 2 * (size_t)(p.L + 1) * (p.ncb | 1);
+  // grid pairs, alignment of the staging to 128 bytes, staged spectra, mbarrier
+  return sizeof(double2) * ((size_t)npair * (p.nph + 1)) + 128 + sizeof(double) * 2 * (size_t)(p.L + 1) * (p.ncb | 1) + 16;
+}
+
+// Tensor map of rtm_b for the TMA staging of k_fft_cycle_f: [m][r][theta][record]
+// doubles, box (2 (ncb | 1), 1, 1, mbox).  False when the orders do not split
+// into whole boxes or the driver refuses the map (the kernel then uses cp.async).
+bool make_rtm_map(const Plan& p, CUtensorMap* map, int* mbox) {
+  const int nc = p.ncb, ncs2 = 2 * (nc | 1);
+  const int mb = p.L + 1 < 256 ? p.L + 1 : 256;
+  *mbox = mb;
+  if ((p.L + 1) % mb != 0 || !p.rtm_b || (reinterpret_cast<uintptr_t>(p.rtm_b) & 15)) return false;
+  const cuuint64_t dims[4] = {(cuuint64_t)(2 * nc), (cuuint64_t)p.nth, (cuuint64_t)p.nr, (cuuint64_t)(p.L + 1)};
+  const cuuint64_t strides[3] = {16ull * nc, 16ull * nc * p.nth, 16ull * nc * p.nth * p.nr};
+  const cuuint32_t box[4] = {(cuuint32_t)ncs2, 1, 1, (cuuint32_t)mb};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  return cuTensorMapEncodeTiled(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double*>(p.rtm_b), dims, strides, box,
+                                es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // ---------------------------------------------------------------------------
@@ -1129,26 +1166,71 @@ __device__ void ff_store_records(const double2* z, const Plan& P, double* rtm, i
   }
 }
 
+// Staging of the next line's spectra: with a tensor map (tma != 0) thread 0
+// issues one TMA tensor load per mbox orders: the map views rtm_b as
+// [m][r][theta][record] doubles with a box of (2 ncs, 1, 1, mbox), the two
+// doubles past each record zero-filled, which lands the records at the
+// conflict-free stride 2 ncs that the first pass reads; completion on an
+// mbarrier with a bounded wait.  Otherwise 16-byte cp.async pieces.
 template <int N, int MVB, int MSB, int MVF, int MSF, bool PR, int PK>
-__global__ void __launch_bounds__(kFftThreadsF, 1) k_fft_cycle_f(Plan P, int line0, int nlines) {
+__global__ void __launch_bounds__(kFftThreadsF, 1)
+    k_fft_cycle_f(Plan P, int line0, int nlines, const __grid_constant__ CUtensorMap tmap, int tma, int mbox) {
   extern __shared__ double4 smraw[];
   constexpr int NP = N + 1;
+  constexpr int NCB = 3 * MVB + MSB, NCS2 = 2 * (NCB | 1);
   const int npb = (P.ncb + 1) / 2, npf = (P.ncf + 1) / 2;
   const int npair = npb > npf ? npb : npf;
   double2* z = reinterpret_cast<double2*>(smraw);
-  double* st = reinterpret_cast<double*>(z + npair * NP + 1);  // keep 16-byte alignment
+  // staged spectra, 128-byte aligned (TMA destination), then the mbarrier
+  double* st = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(z + npair * NP) + 127) & ~static_cast<uintptr_t>(127));
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(st + (P.L + 1) * NCS2);
   int line = line0 + blockIdx.x;
   if (line >= nlines) return;
+  if (tma && threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(ssa(bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  auto stage = [&](int ln) {
+    const int sth = ln % P.nth, sr = ln / P.nth;
+    if (!tma) {
+      prefetch_line_c<NCB>(st, P.rtm_b, P, sth, sr);
+    } else if (threadIdx.x == 0) {
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(ssa(bar)),
+                   "r"((unsigned)((P.L + 1) * NCS2 * 8)));
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // the first pass's reads of st
+      for (int m0 = 0; m0 <= P.L; m0 += mbox)
+        asm volatile(
+            "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+            "[%6];\n" ::"r"(ssa(st + m0 * NCS2)),
+            "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(0), "r"(sth), "r"(sr), "r"(m0), "r"(ssa(bar))
+            : "memory");
+    }
+  };
+  __syncthreads();
   // lines theta fastest: concurrent CTAs touch neighbouring records of one (m, r)
-  prefetch_line_c<3 * MVB + MSB>(st, P.rtm_b, P, line % P.nth, line / P.nth);
+  stage(line);
+  unsigned phase = 0;
   while (line < nlines) {
     const int th = line % P.nth, r = line / P.nth;
-    cp_async_wait<0>();
-    __syncthreads();
+    if (tma) {
+      const bool late = !fbar_wait(bar, phase);
+      phase ^= 1u;
+      if (__syncthreads_or(late)) {
+        // the staging did not complete in time: report it, let the copy land, stop
+        if (threadIdx.x == 0) {
+          if (P.err) atomicExch(P.err, KMHD_ERR_TIMEOUT);
+          (void)fbar_wait(bar, phase ^ 1u);
+        }
+        return;
+      }
+    } else {
+      cp_async_wait<0>();
+      __syncthreads();
+    }
     ff_dif_first<N, PR>(st, P.ncb, P.nvb, z, npb, P.L, P.twid);
     __syncthreads();
     const int next = line + gridDim.x;
-    if (next < nlines) prefetch_line_c<3 * MVB + MSB>(st, P.rtm_b, P, next % P.nth, next / P.nth);
+    if (next < nlines) stage(next);
     ff_mid_pass<N, +1>(z, npb, P.twid);
     __syncthreads();
     ff_fused<N, MVB, MSB, MVF, MSF, PK>(z, P);
@@ -1180,7 +1262,11 @@ cudaError_t run_cycle_fk(const Plan& p, cudaStream_t s) {
   int grid = nsm * occ;
   if (grid > nlines - line0) grid = nlines - line0;
   if (grid <= 0) return cudaSuccess;
-  kern<<<grid, kFftThreadsF, smem, s>>>(p, line0, nlines);
+  CUtensorMap map;
+  std::memset(&map, 0, sizeof(map));
+  int mbox = 1;
+  const int tma = make_rtm_map(p, &map, &mbox) ? 1 : 0;
+  kern<<<grid, kFftThreadsF, smem, s>>>(p, line0, nlines, map, tma, mbox);
   return cudaGetLastError();
 }
 
