@@ -245,6 +245,9 @@ __global__ void k_a_slices(Plan P, SliceTabs S, int t) {
 // quantity q (8 columns), for each field f < 4: types 2/3 slots (4 columns);
 // forward: types 4/5 (field f, slot) and types 6/7 (vector v, quantity q).
 constexpr int kGrpCols = 16;  // derived columns of one slicer field group (at most 4 fields x 2 slots x 2 types)
+// slicer CTA size (measured at L = 511: 256 threads 14.2 ms, 384 18.6 ms,
+// 512 15.0 ms for the forward slicer)
+constexpr int kSliceThreads = 256;
 constexpr int kSlab = 320;    // per-slice staging bytes of one 256-byte tile block (k halves 192 apart)
 
 struct ColRef {
@@ -316,7 +319,7 @@ __device__ __forceinline__ void digits4(const double (&v)[4], uint32_t (&w)[NS])
 // column written out explicitly (the same algebra as the FP64 tier's operand
 // loaders).  Pass 2 takes the column maxima, pass 3 cuts the digits.
 template <bool FWD, int NS>
-__global__ void __launch_bounds__(256) k_slice_mr(Plan P, SliceTabs S, const double* __restrict__ d_rj, long long ld,
+__global__ void __launch_bounds__(kSliceThreads) k_slice_mr(Plan P, SliceTabs S, const double* __restrict__ d_rj, long long ld,
                                                    const int* __restrict__ cols) {
   extern __shared__ double X[];
   const int z = blockIdx.x, r = P.r_lo + blockIdx.y, m = blockIdx.z;
@@ -1249,7 +1252,7 @@ size_t slice_smem(const Plan& p, bool fwd, int ns) {
   const size_t kv = std::max(type_geo(tv, p.L, 0, p.nh).kpad, type_geo(tv + 1, p.L, 0, p.nh).kpad);
   const size_t kr = std::max(type_geo(tr, p.L, 0, p.nh).kpad, type_geo(tr + 1, p.L, 0, p.nh).kpad);
   const size_t nx = std::max(8 * kv, 4 * (size_t)nF * kr);
-  return sizeof(double) * (nx + 1 + kGrpCols) + kGrpCols * sizeof(int) + 8 * (size_t)ns * kSlab + 16;
+  return sizeof(double) * (nx + 1 + kGrpCols) + kGrpCols * sizeof(int) + (kSliceThreads / 32) * (size_t)ns * kSlab + 16;
 }
 
 int split_slicer(SplitState* s, const Plan& p, bool fwd, const double* d_rj, long long ld, const int* cols,
@@ -1261,7 +1264,7 @@ int split_slicer(SplitState* s, const Plan& p, bool fwd, const double* d_rj, lon
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return KMHD_ERR_CUDA;
   if (p.r_hi > p.r_lo)
-    kern<<<dim3((fwd ? p.nvf : p.nvb) + 1, p.r_hi - p.r_lo, p.L + 1), 256, smem, st>>>(p, S, d_rj, ld, cols);
+    kern<<<dim3((fwd ? p.nvf : p.nvb) + 1, p.r_hi - p.r_lo, p.L + 1), kSliceThreads, smem, st>>>(p, S, d_rj, ld, cols);
   return cudaGetLastError() == cudaSuccess ? KMHD_OK : KMHD_ERR_CUDA;
 }
 
