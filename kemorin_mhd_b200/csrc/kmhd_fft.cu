@@ -681,6 +681,24 @@ size_t smem_cycle_f(const Plan& p) {
   return sizeof(double2) * ((size_t)npair * (p.nph + 1)) + 128 + sizeof(double) * 2 * (size_t)(p.L + 1) * (p.ncb | 1) + 16;
 }
 
+// cuTensorMapEncodeTiled, resolved through the runtime (no link-time
+// dependency on the driver library, so the library also loads on hosts
+// without a GPU driver); null when unavailable.
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+  static const EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return static_cast<EncodeTiledFn>(nullptr);
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
 // Tensor map of rtm_b for the TMA staging of k_fft_cycle_f: [m][r][theta][record]
 // doubles, box (2 (ncb | 1), 1, 1, mbox).  False when the orders do not split
 // into whole boxes or the driver refuses the map (the kernel then uses cp.async).
@@ -693,9 +711,11 @@ bool make_rtm_map(const Plan& p, CUtensorMap* map, int* mbox) {
   const cuuint64_t strides[3] = {16ull * nc, 16ull * nc * p.nth, 16ull * nc * p.nth * p.nr};
   const cuuint32_t box[4] = {(cuuint32_t)ncs2, 1, 1, (cuuint32_t)mb};
   const cuuint32_t es[4] = {1, 1, 1, 1};
-  return cuTensorMapEncodeTiled(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double*>(p.rtm_b), dims, strides, box,
-                                es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                                CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  const EncodeTiledFn enc = encode_tiled();
+  if (!enc) return false;
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double*>(p.rtm_b), dims, strides, box, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // ---------------------------------------------------------------------------
@@ -1331,7 +1351,24 @@ cudaError_t run_cycle(const Plan& p, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// Failure-path self-test: the staging wait on an mbarrier that nothing
+// completes runs out and records KMHD_ERR_TIMEOUT; the kernel returns.
+__global__ void k_selftest_fft_wait(int* err) {
+  __shared__ unsigned long long bar;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(ssa(&bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !fbar_wait(&bar, 0)) atomicExch(err, KMHD_ERR_TIMEOUT);
+}
+
 }  // namespace
+
+cudaError_t launch_selftest_fft_wait(int* err, cudaStream_t s) {
+  k_selftest_fft_wait<<<1, 32, 0, s>>>(err);
+  return cudaGetLastError();
+}
 
 bool fft_line_fits(const Plan& p) {
   return smem_cycle(p) <= 227 * 1024 || smem_cycle_f(p) <= 227 * 1024;

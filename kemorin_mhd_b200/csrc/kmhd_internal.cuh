@@ -217,6 +217,8 @@ cudaError_t launch_fft_cycle(const Plan& p, cudaStream_t s);
 cudaError_t launch_fft_bwd_grid(const Plan& p, double* fld, cudaStream_t s);
 // true when one (r, theta) line of every component fits in shared memory
 bool fft_line_fits(const Plan& p);
+// failure-path self-test of the FFT's bounded staging wait (kmhd_selftest_wait_timeout)
+cudaError_t launch_selftest_fft_wait(int* err, cudaStream_t s);
 cudaError_t launch_fft_fwd_grid(const Plan& p, const double* frc, cudaStream_t s);
 
 }  // namespace kmhd

@@ -1440,6 +1440,42 @@ __global__ void __launch_bounds__(128, 1) k_selftest_mma(const signed char* A, c
 }  // namespace
 }  // namespace kmhd
 
+namespace kmhd {
+namespace {
+// Failure-path self-test: the tcgen05 pipeline's bounded mbarrier wait on a
+// barrier that nothing arrives on runs out and records KMHD_ERR_TIMEOUT.
+__global__ void k_selftest_pipe_wait(int* err) {
+  __shared__ unsigned long long bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait(&bar, 0)) atomicExch(err, KMHD_ERR_TIMEOUT);
+}
+}  // namespace
+}  // namespace kmhd
+
+extern "C" int kmhd_selftest_wait_timeout(int device, int which) {
+  using namespace kmhd;
+  if (which != 0 && which != 1) return KMHD_ERR_ARG;
+  if (cudaSetDevice(device) != cudaSuccess) return KMHD_ERR_DEVICE;
+  int* err = nullptr;
+  if (cudaMalloc(&err, sizeof(int)) != cudaSuccess) return KMHD_ERR_NOMEM;
+  int st = KMHD_OK;
+  if (cudaMemset(err, 0, sizeof(int)) != cudaSuccess) st = KMHD_ERR_CUDA;
+  if (!st) {
+    if (which == 0) k_selftest_pipe_wait<<<1, 32>>>(err);
+    else if (launch_selftest_fft_wait(err, nullptr) != cudaSuccess) st = KMHD_ERR_CUDA;
+  }
+  // the kernel ends by itself (bounded wait) and leaves the context usable
+  if (!st && cudaDeviceSynchronize() != cudaSuccess) st = KMHD_ERR_CUDA;
+  int h = 0;
+  if (!st && cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) st = KMHD_ERR_CUDA;
+  cudaFree(err);
+  return st ? st : h;
+}
+
 extern "C" int kmhd_selftest_i8_mma(int lbo, int sbo, const signed char* A, const signed char* B, int* D) {
   using namespace kmhd;
   signed char *dA = nullptr, *dB = nullptr;

@@ -57,7 +57,7 @@ class Desc(ctypes.Structure):
 EXPORTS = ["kmhd_sph_create", "kmhd_sph_destroy", "kmhd_sph_set_stream", "kmhd_sph_b_trans",
            "kmhd_sph_f_trans", "kmhd_sph_cycle", "kmhd_sph_batch_cycle", "kmhd_sph_last_timing",
            "kmhd_sph_get_tables", "kmhd_sph_device_bytes", "kmhd_strerror", "kmhd_sph_cycle_noalloc",
-           "kmhd_sph_last_kernel_timing", "kmhd_sph_get_path"]
+           "kmhd_sph_last_kernel_timing", "kmhd_sph_get_path", "kmhd_selftest_wait_timeout"]
 
 _lib = None
 
