@@ -204,7 +204,7 @@ const char *kmhd_strerror(int status);
 /* Failure-path self-test (no counterpart in the reference): runs one of the
  * library's bounded device waits -- which = 0 the tcgen05 pipeline's mbarrier
  * wait, 1 the FFT's staging wait -- on an mbarrier that nothing completes.
- * The wait runs out after about a second, the kernel records
+ * The wait runs out (2^16 wait rounds, well under a second), the kernel records
  * KMHD_ERR_TIMEOUT in a device error word and returns, and the call returns
  * that status; the CUDA context stays usable.  No GPU fault is involved. */
 int kmhd_selftest_wait_timeout(int device, int which);

@@ -31,10 +31,10 @@ namespace {
 constexpr int kFftThreads = 256;
 
 // mbarrier + TMA tensor load (staging of a line's spectra)
-constexpr long long kFftSpinCap = 1ll << 24;  // bounded waits (about a second), then KMHD_ERR_TIMEOUT
+constexpr long long kFftSpinCap = 1ll << 22;  // try_wait rounds (each may suspend for microseconds)
 __device__ __forceinline__ unsigned ssa(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ bool fbar_wait(unsigned long long* b, unsigned parity) {
-  for (long long it = 0; it < kFftSpinCap; ++it) {
+__device__ __forceinline__ bool fbar_wait(unsigned long long* b, unsigned parity, long long cap = kFftSpinCap) {
+  for (long long it = 0; it < cap; ++it) {
     unsigned ok;
     asm volatile(
         "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
@@ -1360,7 +1360,7 @@ __global__ void k_selftest_fft_wait(int* err) {
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
-  if (threadIdx.x == 0 && !fbar_wait(&bar, 0)) atomicExch(err, KMHD_ERR_TIMEOUT);
+  if (threadIdx.x == 0 && !fbar_wait(&bar, 0, kSelfTestSpinCap)) atomicExch(err, KMHD_ERR_TIMEOUT);
 }
 
 }  // namespace

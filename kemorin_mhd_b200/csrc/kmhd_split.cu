@@ -36,7 +36,7 @@ constexpr int kTM = 128;     // rows per tile (MMA M)
 constexpr int kTN = 64;      // columns per tile (MMA N)
 constexpr int kTK = 32;      // K per chunk (one kind::i8 MMA)
 constexpr int kNT = 8;       // operand types
-constexpr long long kSpinCap = 1ll << 24;
+constexpr long long kSpinCap = 1ll << 22;  // try_wait rounds (each may suspend for microseconds)
 
 // types: 0 theta/phi sym, 1 theta/phi asym, 2 r/scalar sym, 3 r/scalar asym (backward)
 //        4 F1 even, 5 F1 odd, 6 F2 even, 7 F2 odd (forward)
@@ -59,8 +59,8 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, unsigned b
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(sptr(b)), "r"(bytes));
 }
 // bounded wait on phase parity; returns false on timeout
-__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity) {
-  for (long long it = 0; it < kSpinCap; ++it) {
+__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity, long long cap = kSpinCap) {
+  for (long long it = 0; it < cap; ++it) {
     unsigned ok;
     asm volatile(
         "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
@@ -1451,7 +1451,7 @@ __global__ void k_selftest_pipe_wait(int* err) {
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
-  if (threadIdx.x == 0 && !mbar_wait(&bar, 0)) atomicExch(err, KMHD_ERR_TIMEOUT);
+  if (threadIdx.x == 0 && !mbar_wait(&bar, 0, kSelfTestSpinCap)) atomicExch(err, KMHD_ERR_TIMEOUT);
 }
 }  // namespace
 }  // namespace kmhd
