@@ -191,13 +191,16 @@ __device__ void dit_dispatch(int R, double2* z, int npair, int N, int span, cons
 // Complex spectrum of pair pp at frequency k from staged records
 // st[(m*nc + c)*2 + {0: a, 1: b}], m <= L.  z = X_{2pp} + i X_{2pp+1},
 // X_c[m] = (a - i b)/2 for m > 0, X_c[0] = a, X_c[N-m] = conj(X_c[m]).
-__device__ __forceinline__ double2 spec_at(const double* st, int nc, int nv, int pp, int k, int N, int L) {
+// rs: doubles between the records of consecutive orders (staged: 2 nc; in
+// place in rtm: the order stride of the rtm layout)
+__device__ __forceinline__ double2 spec_at(const double* st, int nc, int nv, int pp, int k, int N, int L,
+                                           long long rs) {
   int m;
   bool mirror;
   if (k <= L) { m = k; mirror = false; }
   else if (k >= N - L) { m = N - k; mirror = true; }
   else return make_double2(0.0, 0.0);
-  const double* rec = st + m * nc * 2;
+  const double* rec = st + m * rs;
   const double* r0 = rec + rec_off(2 * pp, nv);
   const double a0 = r0[0], b0 = r0[1];
   double a1 = 0.0, b1 = 0.0;
@@ -220,7 +223,7 @@ __device__ void dif_first(const double* st, int nc, int nv, double2* z, int npai
     const int pp = it / nbf, j = it % nbf;
     double2 x[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) x[r] = spec_at(st, nc, nv, pp, j + r * s, N, L);
+    for (int r = 0; r < R; ++r) x[r] = spec_at(st, nc, nv, pp, j + r * s, N, L, 2LL * nc);
     DFT<R, +1>::run(x);
     double2* base = z + pp * N + j;
     base[0] = x[0];
@@ -442,12 +445,12 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_cycle(Plan P, int line0, in
 // First inverse pass of pair pp only: spectra from the staged records, output z[0 .. N).
 template <int R>
 __device__ void dif_first_one(const double* st, int nc, int nv, int pp, double2* z, int N, int L,
-                              const double2* __restrict__ tw) {
+                              const double2* __restrict__ tw, long long rs) {
   const int s = N / R;
   for (int j = threadIdx.x; j < s; j += blockDim.x) {
     double2 x[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) x[r] = spec_at(st, nc, nv, pp, j + r * s, N, L);
+    for (int r = 0; r < R; ++r) x[r] = spec_at(st, nc, nv, pp, j + r * s, N, L, rs);
     DFT<R, +1>::run(x);
     z[j] = x[0];
 #pragma unroll
@@ -455,13 +458,13 @@ __device__ void dif_first_one(const double* st, int nc, int nv, int pp, double2*
   }
 }
 __device__ void dif_first_one_dispatch(int R, const double* st, int nc, int nv, int pp, double2* z, int N, int L,
-                                       const double2* tw) {
+                                       const double2* tw, long long rs) {
   switch (R) {
-    case 8: dif_first_one<8>(st, nc, nv, pp, z, N, L, tw); break;
-    case 4: dif_first_one<4>(st, nc, nv, pp, z, N, L, tw); break;
-    case 2: dif_first_one<2>(st, nc, nv, pp, z, N, L, tw); break;
-    case 3: dif_first_one<3>(st, nc, nv, pp, z, N, L, tw); break;
-    default: dif_first_one<5>(st, nc, nv, pp, z, N, L, tw); break;
+    case 8: dif_first_one<8>(st, nc, nv, pp, z, N, L, tw, rs); break;
+    case 4: dif_first_one<4>(st, nc, nv, pp, z, N, L, tw, rs); break;
+    case 2: dif_first_one<2>(st, nc, nv, pp, z, N, L, tw, rs); break;
+    case 3: dif_first_one<3>(st, nc, nv, pp, z, N, L, tw, rs); break;
+    default: dif_first_one<5>(st, nc, nv, pp, z, N, L, tw, rs); break;
   }
 }
 // Natural-order forward spectrum of pair q in z -> (a_m, b_m), m <= L, into rtm.
@@ -495,15 +498,16 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_cycle_wide(Plan P, int line
   const int npb = (P.ncb + 1) / 2, npf = (P.ncf + 1) / 2;
   const int npm = npb > npf ? npb : npf;
   double2* z = reinterpret_cast<double2*>(smraw);
-  double* st = reinterpret_cast<double*>(z + N);
   double2* sc = P.fft_scratch + (long long)blockIdx.x * npm * N;
+  // the first pass reads the line's spectra in place (rtm records, order
+  // stride rs): one line of a wide grid is too large to stage, and a small
+  // CTA keeps several resident per SM
+  const long long rs = (long long)P.nth * P.nr * P.ncb * 2;
   for (int line = line0 + blockIdx.x; line < nlines; line += gridDim.x) {
     const int th = line % P.nth, r = line / P.nth;
-    prefetch_line(st, P.rtm_b, P.ncb, P, th, r);
-    cp_async_wait<0>();
-    __syncthreads();
+    const double* st = P.rtm_b + rtm_off(P, 0, th, r, P.ncb);
     for (int pp = 0; pp < npb; ++pp) {
-      dif_first_one_dispatch(P.fac[0], st, P.ncb, P.nvb, pp, z, N, P.L, P.twid);
+      dif_first_one_dispatch(P.fac[0], st, P.ncb, P.nvb, pp, z, N, P.L, P.twid, rs);
       __syncthreads();
       dif_rest(z, 1, N, P, P.twid);
       for (int i = threadIdx.x; i < N; i += blockDim.x) sc[(long long)pp * N + i] = z[i];
@@ -527,15 +531,13 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_bwd_grid_wide(Plan P, doubl
   const int N = P.nph;
   const int npb = (P.ncb + 1) / 2;
   double2* z = reinterpret_cast<double2*>(smraw);
-  double* st = reinterpret_cast<double*>(z + N);
   const int line = blockIdx.x;
   const int r = line % P.nr, th = line / P.nr;
   const long long nnod = (long long)P.nr * P.nth * N;
-  prefetch_line(st, P.rtm_b, P.ncb, P, th, r);
-  cp_async_wait<0>();
-  __syncthreads();
+  const double* st = P.rtm_b + rtm_off(P, 0, th, r, P.ncb);  // spectra read in place
+  const long long rs = (long long)P.nth * P.nr * P.ncb * 2;
   for (int pp = 0; pp < npb; ++pp) {
-    dif_first_one_dispatch(P.fac[0], st, P.ncb, P.nvb, pp, z, N, P.L, P.twid);
+    dif_first_one_dispatch(P.fac[0], st, P.ncb, P.nvb, pp, z, N, P.L, P.twid, rs);
     __syncthreads();
     dif_rest(z, 1, N, P, P.twid);
     const int nc2 = 2 * pp + 1 < P.ncb ? 2 : 1;
@@ -1379,9 +1381,7 @@ size_t fft_smem_bytes(const Plan& p, int npair) {
   return smem_cycle(p);
 }
 
-size_t smem_wide(const Plan& p) {
-  return sizeof(double2) * (size_t)p.nph + sizeof(double) * 2 * (size_t)(p.L + 1) * p.ncb;
-}
+size_t smem_wide(const Plan& p) { return sizeof(double2) * (size_t)p.nph; }
 
 template <int MVB, int MSB, int MVF, int MSF>
 cudaError_t run_cycle_wide(const Plan& p, cudaStream_t s) {

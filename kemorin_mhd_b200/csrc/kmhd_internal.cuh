@@ -20,6 +20,7 @@ constexpr int kMaxScl = 2;    // scalars per field group
 constexpr int kMaxProd = 16;
 constexpr int kMaxFftFactors = 16;
 constexpr int kSeedL = 32;    // degrees between on-the-fly recurrence seeds
+constexpr int kWideCtasPerSm = 2;  // resident CTAs per SM of the wide-line FFT cycle (one grid scratch each)
 constexpr long long kSelfTestSpinCap = 1ll << 16;  // bounded-wait rounds of the failure self-test
 
 // Plan of one transform instance (device pointers + sizes).

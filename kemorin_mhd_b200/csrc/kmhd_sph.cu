@@ -417,14 +417,16 @@ int kmhd_sph_create(const kmhd_sph_desc* d, kmhd_sph** out) {
   p.twid = h->twid;
   p.digrev = h->digrev;
   if (!fft_line_fits(p)) {
-    // wide lines: per-CTA grid scratch of the pair-by-pair FFT cycle (L2-resident)
+    // wide lines: per-CTA grid scratch of the pair-by-pair FFT cycle
+    // (kWideCtasPerSm CTAs per SM; 72 MB at Nphi = 3072, L2-resident)
     int nsm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, d->device);
     const int npm = (std::max(p.ncb, p.ncf) + 1) / 2;
+    const int nctas = kWideCtasPerSm * nsm;
     double2* sc = nullptr;
-    if ((st = dalloc(h, &sc, (size_t)nsm * npm * p.nph))) return fail(st);
+    if ((st = dalloc(h, &sc, (size_t)nctas * npm * p.nph))) return fail(st);
     p.fft_scratch = sc;
-    p.fft_scratch_ctas = nsm;
+    p.fft_scratch_ctas = nctas;
   }
   if (launch_tables(p, h->colat, h->weight, h->asin_t, h->P, h->dP, s) != cudaSuccess)
     return fail(KMHD_ERR_CUDA);
