@@ -22,12 +22,14 @@ CFG = SphConfig(127, 192, 384, 65, name="L127_Nr65")
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("tier", [TIER_FP64, TIER_SPLIT_I8, TIER_FP32ACC])
-def test_host_chunked_cycle_equals_device_cycle(tier):
+@pytest.mark.parametrize("tier,otf", [(TIER_FP64, False), (TIER_FP64, True), (TIER_SPLIT_I8, False),
+                                      (TIER_FP32ACC, False)],
+                         ids=["fp64", "fp64_p_on_the_fly", "split", "fp32acc"])
+def test_host_chunked_cycle_equals_device_cycle(tier, otf):
     import torch
     from kemorin_mhd_b200.sph_trans import SphTransform
     cfg = CFG
-    tr = SphTransform(cfg, tier=tier)
+    tr = SphTransform(cfg, tier=tier, p_on_the_fly=otf)
     d = make_d_rj(cfg, seed=31)
     n = cfg.J * cfg.nr
     out_dev = torch.zeros((cfg.ncf, n), dtype=torch.float64, device="cuda")
