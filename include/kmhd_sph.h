@@ -192,6 +192,20 @@ int kmhd_sph_cycle_noalloc(const kmhd_sph_desc *desc, const double *d_rj_in, int
                            const int32_t *cols_b, double *d_rj_out, int64_t ld_out,
                            const int32_t *cols_f, void *stream);
 
+/* Divergence of a flux vector's spectra, the step after the forward transform
+ * that closes the u.grad(T) term (heat advection = -div(u T)): column
+ * col_div = (dS/dr by the reference's radial FDM - dS/dr column) * max(g3, 1/2)
+ * / r^2 for the vector in columns col_flux (S) and col_flux + 1 (dS/dr), with
+ * fixed-field rows at the first and last radius, whose node values S are
+ * replaced by fix_in[J] / fix_out[J] (NULL = zero).  Replaces
+ * const_sph_scalar_advect with fixed-field boundaries
+ * (MHD_src/sph_MHD/const_sph_divergence.f90:49-74: cal_sph_nod_vect_div2,
+ * cal_sph_exp_rotation.f90:254-290; cal_sph_div_flux_4_fix_in / _fix_out,
+ * cal_sph_exp_fixed_scalar.f90:381-456).  Needs Nr >= 3; host or device
+ * pointers (ptr_kind). */
+int kmhd_sph_div_flux(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t col_flux, int32_t col_div,
+                      const double *fix_in, const double *fix_out, int32_t ptr_kind);
+
 /* Legendre path the handle runs: 1 = the tier's split path, 0 = FP64 DMMA
  * (FP64 tier, or a split-tier handle the autotuner moved to FP64). */
 int kmhd_sph_get_path(const kmhd_sph *handle, int32_t *path);

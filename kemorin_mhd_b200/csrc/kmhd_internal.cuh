@@ -204,6 +204,11 @@ __host__ __device__ __forceinline__ double g3_of(int l) {
 // Launchers (defined in the .cu files).
 cudaError_t launch_tables(const Plan& p, double* colat, double* weight, double* asin_t,
                           double* P, double* dP, cudaStream_t s);
+// Divergence of a flux vector's spectra (kmhd_post.cu): S, dS, out are one
+// J*nr column each; coef = d1[3 nr], bnd[6], ar2[nr], g3[J]; fin / fout the
+// fixed boundary values (null: zero).
+cudaError_t launch_div_flux(long long J, int nr, const double* S, const double* dS, double* out, const double* coef,
+                            const double* fin, const double* fout, cudaStream_t s);
 // Set-up of the on-the-fly tables (cos_t, pco, dco, pst, pseed of the plan).
 cudaError_t launch_otf_tables(const Plan& p, double* cos_t, double2* pco, double2* dco, double2* pst,
                               double* pseed, const long long* pseed_off, cudaStream_t s);

@@ -1,0 +1,55 @@
+// kmhd_post.cu -- spectral post-processing after the forward transform: the
+// divergence of a flux vector's spectra (the reference's u.grad(T) term is
+// -div(u T), formed this way after sph_f_trans).
+//
+// Interior rows as cal_sph_nod_vect_div2 (MHD_src/sph_MHD/cal_sph_exp_rotation.f90:254-290),
+// fixed-field boundary rows as cal_sph_div_flux_4_fix_in / _fix_out
+// (MHD_src/sph_MHD/cal_sph_exp_fixed_scalar.f90:381-456); the FDM coefficients
+// are built on the host (kmhd_sph.cu) as the reference builds them.
+#include "kmhd_internal.cuh"
+
+namespace kmhd {
+namespace {
+
+// One thread per (j, k), j fastest.  coef: d1[3 nr] (offsets -1, 0, +1 of
+// row k), bnd[6] (inner: nodes 0, 1, 2; outer: nodes nr-1, nr-2, nr-3),
+// ar2[nr] = (1/r)^2, g3[J] = max(l(l+1), 1/2).
+__global__ void k_div_flux(long long J, int nr, const double* __restrict__ S, const double* __restrict__ dS,
+                           double* __restrict__ out, const double* __restrict__ coef, const double* __restrict__ fin,
+                           const double* __restrict__ fout) {
+  const double* d1 = coef;
+  const double* bnd = coef + 3 * nr;
+  const double* ar2 = bnd + 6;
+  const double* g3 = ar2 + nr;
+  const long long n = J * nr;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(i / J);
+    const long long j = i - (long long)k * J;
+    double d1s;
+    if (k == 0) {
+      d1s = bnd[0] * (fin ? fin[j] : 0.0) + bnd[1] * S[i + J] + bnd[2] * S[i + 2 * J];
+    } else if (k == nr - 1) {
+      d1s = bnd[5] * S[i - 2 * J] + bnd[4] * S[i - J] + bnd[3] * (fout ? fout[j] : 0.0);
+    } else {
+      d1s = d1[3 * k] * S[i - J] + d1[3 * k + 1] * S[i] + d1[3 * k + 2] * S[i + J];
+    }
+    out[i] = (d1s - dS[i]) * g3[j] * ar2[k];
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_div_flux(long long J, int nr, const double* S, const double* dS, double* out, const double* coef,
+                            const double* fin, const double* fout, cudaStream_t s) {
+  const long long n = J * nr;
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const long long want = (n + 255) / 256;
+  const int grid = (int)(want < 8LL * nsm ? want : 8LL * nsm);
+  if (grid <= 0) return cudaSuccess;
+  k_div_flux<<<grid, 256, 0, s>>>(J, nr, S, dS, out, coef, fin, fout);
+  return cudaGetLastError();
+}
+
+}  // namespace kmhd

@@ -1,6 +1,7 @@
 // kmhd_sph.cu -- C-ABI of the B200 spherical-transform cycle (include/kmhd_sph.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -56,6 +57,9 @@ struct kmhd_sph {
   double2* twid = nullptr;
   int *cols_b_d = nullptr, *cols_f_d = nullptr;
   int* err = nullptr;  // device error word (bounded waits of the FFT and tcgen05 kernels)
+  // divergence post-processing: FDM / normalisation coefficients, host-pointer staging
+  double *div_coef = nullptr, *div_stage = nullptr;
+  std::vector<double> radius_h;
   std::vector<int> cols_b_cache, cols_f_cache;
   // host-pointer staging
   double *stage_in = nullptr, *stage_out = nullptr, *stage_grid = nullptr;
@@ -392,6 +396,7 @@ int kmhd_sph_create(const kmhd_sph_desc* d, kmhd_sph** out) {
   auto up = [&](void* dst, const void* src, size_t bytes) {
     return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
   };
+  h->radius_h.assign(d->radius, d->radius + p.nr);
   if (up(h->radius, d->radius, sizeof(double) * p.nr) || up(h->poff, h->poff_h.data(), sizeof(long long) * 2 * (L + 1)) ||
       up(h->sboff, h->sboff_h.data(), sizeof(long long) * 2 * (L + 1)) ||
       up(h->kpad, h->kpad_h.data(), sizeof(int) * 2 * (L + 1)) ||
@@ -805,6 +810,125 @@ int kmhd_sph_cycle(kmhd_sph* h, const double* d_rj_in, int64_t ld_in, const int3
   KCHECK(cudaStreamSynchronize(h->stream));
   if ((st = finish_timing(h))) return st;
   return finish_kernel_timing(h);
+}
+
+}  // extern "C"
+
+namespace {
+
+// 3x3 inverse by cofactors, as cal_inverse_33_matrix / cal_det_33_matrix
+// (CORE_src/BASE/cal_inverse_small_matrix.f90:57-80, 176-215).
+double det22(double a00, double a01, double a10, double a11) { return a00 * a11 - a10 * a01; }
+void inverse33(const double a[3][3], double inv[3][3]) {
+  double det = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    int c[2], n = 0;
+    for (int q = 0; q < 3; ++q)
+      if (q != k) c[n++] = q;
+    det = det + ((k % 2) ? -1.0 : 1.0) * det22(a[1][c[0]], a[1][c[1]], a[2][c[0]], a[2][c[1]]) * a[0][k];
+  }
+  const double adet = 1.0 / det;
+  for (int kj = 0; kj < 3; ++kj)
+    for (int ki = 0; ki < 3; ++ki) {
+      int rr[2], cc[2], nr = 0, nc = 0;
+      for (int q = 0; q < 3; ++q) {
+        if (q != ki) rr[nr++] = q;
+        if (q != kj) cc[nc++] = q;
+      }
+      inv[kj][ki] = (((ki + kj) % 2) ? -1.0 : 1.0) * det22(a[rr[0]][cc[0]], a[rr[0]][cc[1]], a[rr[1]][cc[0]], a[rr[1]][cc[1]]) * adet;
+    }
+}
+
+// Divergence coefficients on the device: d1[3 nr] (interior 3-point first
+// derivative, nod_r_2nd_fdm_coef_noequi + copy_fdm2_nod_coefs_from_mat,
+// CORE_src/SPH_SPECTR_src/set_radius_func_noequi.f90:193-260, t_fdm_coefs.f90:146-163),
+// bnd[6] (fixed-field one-sided rows, cal_fdm2_coef_fix_fld_ICB / _CMB,
+// MHD_src/sph_MHD/cal_fdm_coefs_4_boundaries.f90:155-190, 256-290), ar2[nr] =
+// (1/r)^2 (set_radius_4_sph_dynamo.f90:105), g3[J] = max(l(l+1), 1/2).
+int build_div_coef(kmhd_sph* h) {
+  const Plan& p = h->plan;
+  const int nr = p.nr, L = p.L;
+  const std::vector<double>& r = h->radius_h;
+  std::vector<double> c(3 * (size_t)nr + 6 + nr + (size_t)p.J, 0.0);
+  for (int k = 1; k < nr - 1; ++k) {
+    const double dp = r[k + 1] - r[k], dn = r[k] - r[k - 1];
+    const double t[3][3] = {{1.0, 0.0, 0.0}, {1.0, dp, 0.5 * dp * dp}, {1.0, -dn, 0.5 * dn * dn}};
+    double inv[3][3];
+    inverse33(t, inv);
+    c[3 * k + 0] = inv[1][2];
+    c[3 * k + 1] = inv[1][0];
+    c[3 * k + 2] = inv[1][1];
+  }
+  {
+    const double d1 = r[1] - r[0], d2 = r[2] - r[0];
+    const double t[3][3] = {{1.0, 0.0, 0.0}, {1.0, d1, d1 * d1 / 2.0}, {1.0, d2, d2 * d2 / 2.0}};
+    double inv[3][3];
+    inverse33(t, inv);
+    for (int q = 0; q < 3; ++q) c[3 * nr + q] = inv[1][q];
+  }
+  {
+    const double d1 = r[nr - 1] - r[nr - 2], d2 = r[nr - 1] - r[nr - 3];
+    const double t[3][3] = {{1.0, 0.0, 0.0}, {1.0, -d1, d1 * d1 / 2.0}, {1.0, -d2, d2 * d2 / 2.0}};
+    double inv[3][3];
+    inverse33(t, inv);
+    for (int q = 0; q < 3; ++q) c[3 * nr + 3 + q] = inv[1][q];
+  }
+  for (int k = 0; k < nr; ++k) {
+    const double a1 = 1.0 / r[k];
+    c[3 * nr + 6 + k] = a1 * a1;
+  }
+  double* g3 = c.data() + 4 * nr + 6;
+  for (int m = 0; m <= L; ++m)
+    for (int slot = 0; slot < 2; ++slot)
+      for (int l = m; l <= L; ++l) {
+        const int j = h->jmap_h[((size_t)m * 2 + slot) * (L + 1) + l];
+        if (j >= 0) g3[j] = std::max(g3_of(l), 0.5);
+      }
+  int st;
+  if ((st = dalloc(h, &h->div_coef, c.size()))) return st;
+  KCHECK(cudaMemcpyAsync(h->div_coef, c.data(), sizeof(double) * c.size(), cudaMemcpyHostToDevice, h->stream));
+  KCHECK(cudaStreamSynchronize(h->stream));
+  return KMHD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int kmhd_sph_div_flux(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_flux, int32_t col_div,
+                      const double* fix_in, const double* fix_out, int32_t ptr_kind) {
+  if (!h || !d_rj) return KMHD_ERR_ARG;
+  if (check_ld(h, ld)) return KMHD_ERR_ARG;
+  if (col_flux < 0 || col_div < 0 || col_div == col_flux || col_div == col_flux + 1) return KMHD_ERR_ARG;
+  const Plan& p = h->plan;
+  if (p.nr < 3) return KMHD_ERR_SIZE;
+  KCHECK(cudaSetDevice(h->device));
+  int st;
+  if (!h->div_coef && (st = build_div_coef(h))) return st;
+  const size_t nrj = (size_t)p.J * p.nr;
+  const double *S = d_rj + ld * col_flux, *dS = d_rj + ld * (col_flux + 1), *fin = fix_in, *fout = fix_out;
+  double* out = d_rj + ld * col_div;
+  if (ptr_kind == KMHD_PTR_HOST) {
+    // columns S, dS, div and the two boundary rows
+    if (!h->div_stage && (st = dalloc(h, &h->div_stage, 3 * nrj + 2 * (size_t)p.J))) return st;
+    double* s0 = h->div_stage;
+    KCHECK(cudaMemcpyAsync(s0, S, sizeof(double) * nrj, cudaMemcpyHostToDevice, h->stream));
+    KCHECK(cudaMemcpyAsync(s0 + nrj, dS, sizeof(double) * nrj, cudaMemcpyHostToDevice, h->stream));
+    if (fix_in) {
+      KCHECK(cudaMemcpyAsync(s0 + 3 * nrj, fix_in, sizeof(double) * p.J, cudaMemcpyHostToDevice, h->stream));
+      fin = s0 + 3 * nrj;
+    }
+    if (fix_out) {
+      KCHECK(cudaMemcpyAsync(s0 + 3 * nrj + p.J, fix_out, sizeof(double) * p.J, cudaMemcpyHostToDevice, h->stream));
+      fout = s0 + 3 * nrj + p.J;
+    }
+    KCHECK(launch_div_flux(p.J, p.nr, s0, s0 + nrj, s0 + 2 * nrj, h->div_coef, fin, fout, h->stream));
+    KCHECK(cudaMemcpyAsync(out, s0 + 2 * nrj, sizeof(double) * nrj, cudaMemcpyDeviceToHost, h->stream));
+  } else {
+    KCHECK(launch_div_flux(p.J, p.nr, S, dS, out, h->div_coef, fin, fout, h->stream));
+  }
+  KCHECK(cudaStreamSynchronize(h->stream));
+  return KMHD_OK;
 }
 
 int kmhd_sph_last_kernel_timing(kmhd_sph* h, double* ms5) {

@@ -57,7 +57,8 @@ class Desc(ctypes.Structure):
 EXPORTS = ["kmhd_sph_create", "kmhd_sph_destroy", "kmhd_sph_set_stream", "kmhd_sph_b_trans",
            "kmhd_sph_f_trans", "kmhd_sph_cycle", "kmhd_sph_batch_cycle", "kmhd_sph_last_timing",
            "kmhd_sph_get_tables", "kmhd_sph_device_bytes", "kmhd_strerror", "kmhd_sph_cycle_noalloc",
-           "kmhd_sph_last_kernel_timing", "kmhd_sph_get_path", "kmhd_selftest_wait_timeout"]
+           "kmhd_sph_last_kernel_timing", "kmhd_sph_get_path", "kmhd_selftest_wait_timeout",
+           "kmhd_sph_div_flux"]
 
 _lib = None
 
@@ -85,6 +86,8 @@ def load_library(path: str | None = None):
     lib.kmhd_sph_last_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     lib.kmhd_sph_last_kernel_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     lib.kmhd_sph_get_path.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
+    lib.kmhd_sph_div_flux.argtypes = [vp, vp, i64, i32, i32, vp, vp, i32]
+    lib.kmhd_selftest_wait_timeout.argtypes = [ctypes.c_int, ctypes.c_int]
     lib.kmhd_sph_get_tables.argtypes = [vp, i32] + [ctypes.POINTER(ctypes.c_double)] * 4
     lib.kmhd_sph_device_bytes.restype = i64
     lib.kmhd_sph_device_bytes.argtypes = [vp]
@@ -236,6 +239,19 @@ class SphTransform:
         _check(load_library().kmhd_sph_cycle(self._h, src, ld_in or n, cb, dst, ld_out or n, cf, kind),
                "kmhd_sph_cycle")
         return d_rj_out
+
+
+    def div_flux(self, d_rj, col_flux: int, col_div: int, fix_in=None, fix_out=None, ld: int | None = None):
+        """Divergence of the flux vector in columns col_flux (S), col_flux + 1
+        (dS/dr) into column col_div, fixed-field boundary values fix_in /
+        fix_out (J each, same host/device kind as d_rj, None = zero)."""
+        p, kind = _ptr(d_rj)
+        fi = _ptr(fix_in)[0] if fix_in is not None else None
+        fo = _ptr(fix_out)[0] if fix_out is not None else None
+        n = self.cfg.J * self.cfg.nr
+        _check(load_library().kmhd_sph_div_flux(self._h, p, ld or n, col_flux, col_div, fi, fo, kind),
+               "kmhd_sph_div_flux")
+        return d_rj
 
 
 def batch_cycle(transforms: Sequence[SphTransform], d_in, d_out):

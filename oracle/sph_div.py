@@ -1,0 +1,98 @@
+"""CPU oracle (test infrastructure only) of the spectral divergence of a flux
+vector, the post-processing step that closes the reference's u.grad(T) term
+(heat advection = -div(u T), taken in spectral space after the forward
+transform).
+
+Restates, in plain numpy:
+- const_sph_scalar_advect (MHD_src/sph_MHD/const_sph_divergence.f90:49-74);
+- the interior rows, cal_sph_nod_vect_div2
+  (MHD_src/sph_MHD/cal_sph_exp_rotation.f90:254-290):
+      div(j,k) = (sum_s d1(k,s) S(j,k+s) - dS/dr(j,k)) * max(g3(j), 1/2) / r_k^2;
+- the fixed-field boundary rows, cal_sph_div_flux_4_fix_in / _fix_out
+  (MHD_src/sph_MHD/cal_sph_exp_fixed_scalar.f90:381-456), where the boundary
+  node's S is replaced by the caller's fixed value;
+- the radial FDM coefficients: 3x3 Taylor matrices inverted by cofactors,
+  nod_r_2nd_fdm_coef_noequi (CORE_src/SPH_SPECTR_src/set_radius_func_noequi.f90:193-260),
+  copy_fdm2_nod_coefs_from_mat (CORE_src/SPH_SPECTR_src/t_fdm_coefs.f90:146-163),
+  cal_fdm2_coef_fix_fld_ICB / _CMB (MHD_src/sph_MHD/cal_fdm_coefs_4_boundaries.f90:155-190, 256-290),
+  cal_inverse_33_matrix and cal_det_33_matrix (CORE_src/BASE/cal_inverse_small_matrix.f90:57-80, 176-215);
+- 1/r^2 as (1/r)^2 (CORE_src/SPH_SPECTR_src/set_radius_4_sph_dynamo.f90:105).
+
+Parity unpinned against the reference's own outputs (no Fortran compiler in
+this image); the tests pin this restatement by the FDM being exact for
+quadratic radial profiles.
+"""
+import numpy as np
+
+
+def _det22(a):
+    return a[0, 0] * a[1, 1] - a[1, 0] * a[0, 1]
+
+
+def _det33(a):
+    det = 0.0
+    for k in range(3):
+        cols = [c for c in range(3) if c != k]
+        t = a[1:3][:, cols]
+        det = det + (-1) ** k * _det22(t) * a[0, k]
+    return det
+
+
+def inverse33(a):
+    """cal_inverse_33_matrix: a_inv(kj, ki) = (-1)^(ki+kj) det(minor(ki, kj)) / det(a)."""
+    a = np.asarray(a, dtype=np.float64)
+    a_det = 1.0 / _det33(a)
+    inv = np.zeros((3, 3))
+    for kj in range(3):
+        for ki in range(3):
+            rows = [r for r in range(3) if r != ki]
+            cols = [c for c in range(3) if c != kj]
+            t = a[rows][:, cols]
+            inv[kj, ki] = (-1) ** (ki + kj) * _det22(t) * a_det
+    return inv
+
+
+def fdm_coefs(radius):
+    """(d1[k, 0..2] for the offsets -1, 0, +1 at interior k; icb[0..2] for
+    nodes kr_in, kr_in+1, kr_in+2; cmb[0..2] for kr_out, kr_out-1, kr_out-2)."""
+    r = np.asarray(radius, dtype=np.float64)
+    nr = len(r)
+    d1 = np.zeros((nr, 3))
+    for k in range(1, nr - 1):
+        dp, dn = r[k + 1] - r[k], r[k] - r[k - 1]
+        t = np.array([[1.0, 0.0, 0.0], [1.0, dp, 0.5 * dp * dp], [1.0, -dn, 0.5 * dn * dn]])
+        inv = inverse33(t)
+        d1[k] = [inv[1, 2], inv[1, 0], inv[1, 1]]  # S(k-1), S(k), S(k+1)
+    dp1, dp2 = r[1] - r[0], r[2] - r[0]
+    t = np.array([[1.0, 0.0, 0.0], [1.0, dp1, dp1 * dp1 / 2.0], [1.0, dp2, dp2 * dp2 / 2.0]])
+    icb = inverse33(t)[1, :]
+    dn1, dn2 = r[-1] - r[-2], r[-1] - r[-3]
+    t = np.array([[1.0, 0.0, 0.0], [1.0, -dn1, dn1 * dn1 / 2.0], [1.0, -dn2, dn2 * dn2 / 2.0]])
+    cmb = inverse33(t)[1, :]
+    return d1, icb, cmb
+
+
+def div_flux(radius, l_of_j, S, dS, fix_in=None, fix_out=None):
+    """Divergence spectra (J*Nr, j fastest) of the flux vector with poloidal
+    column S and radial-derivative column dS, fixed-field values fix_in /
+    fix_out (J each, default zero) at the first and last radius."""
+    r = np.asarray(radius, dtype=np.float64)
+    nr, J = len(r), len(l_of_j)
+    S = np.asarray(S).reshape(nr, J)
+    dS = np.asarray(dS).reshape(nr, J)
+    l = np.asarray(l_of_j)
+    g3 = np.where(l == 0, 0.5, (l * (l + 1)).astype(np.float64))
+    g3 = np.maximum(g3, 0.5)
+    ar2 = (1.0 / r) ** 2
+    d1, icb, cmb = fdm_coefs(r)
+    fin = np.zeros(J) if fix_in is None else np.asarray(fix_in)
+    fout = np.zeros(J) if fix_out is None else np.asarray(fix_out)
+    out = np.zeros((nr, J))
+    for k in range(1, nr - 1):
+        d1s = d1[k, 0] * S[k - 1] + d1[k, 1] * S[k] + d1[k, 2] * S[k + 1]
+        out[k] = (d1s - dS[k]) * g3 * ar2[k]
+    d1s = icb[0] * fin + icb[1] * S[1] + icb[2] * S[2]
+    out[0] = (d1s - dS[0]) * g3 * ar2[0]
+    d1s = cmb[2] * S[nr - 3] + cmb[1] * S[nr - 2] + cmb[0] * fout
+    out[nr - 1] = (d1s - dS[nr - 1]) * g3 * ar2[nr - 1]
+    return out.reshape(-1)

@@ -1,0 +1,45 @@
+"""CPU checks of the divergence oracle (oracle/sph_div.py): the 3x3 cofactor
+inverse, and the radial FDM of the reference being exact for quadratic
+radial profiles (interior three-point rows and the fixed-field one-sided
+boundary rows), so the divergence of an exactly differentiated quadratic
+vanishes and that of S = r^2 with dS/dr = 0 is 2 g3 / r."""
+import numpy as np
+
+from kemorin_mhd_b200.config import SphConfig, rj_order
+from oracle.sph_div import div_flux, fdm_coefs, inverse33
+
+
+def test_inverse33_matches_numpy():
+    rng = np.random.default_rng(3)
+    for _ in range(20):
+        a = rng.standard_normal((3, 3)) + 3 * np.eye(3)
+        assert np.abs(inverse33(a) - np.linalg.inv(a)).max() < 1e-13
+
+
+def test_fdm_exact_for_quadratics():
+    r = SphConfig(15, 24, 48, 17).radius()
+    d1, icb, cmb = fdm_coefs(r)
+    for f, df in ((lambda x: 1.0 + 0 * x, lambda x: 0 * x), (lambda x: x, lambda x: 1 + 0 * x),
+                  (lambda x: x * x, lambda x: 2 * x)):
+        v = f(r)
+        for k in range(1, len(r) - 1):
+            assert abs(d1[k] @ v[k - 1:k + 2] - df(r[k])) < 1e-11
+        assert abs(icb @ v[0:3] - df(r[0])) < 1e-11
+        assert abs(cmb @ v[::-1][0:3] - df(r[-1])) < 1e-11
+
+
+def test_divergence_of_quadratic_profiles():
+    cfg = SphConfig(15, 24, 48, 9)
+    r = cfg.radius()
+    l, _ = rj_order(cfg.ltr)
+    rng = np.random.default_rng(4)
+    a, b, c = (rng.standard_normal(cfg.J) for _ in range(3))
+    S = np.outer(np.ones_like(r), a) + np.outer(r, b) + np.outer(r * r, c)
+    dS = np.outer(np.ones_like(r), b) + np.outer(2 * r, c)
+    out = div_flux(r, l, S.reshape(-1), dS.reshape(-1), fix_in=S[0], fix_out=S[-1])
+    assert np.abs(out).max() < 1e-9 * np.abs(S).max() * (cfg.ltr + 1) ** 2
+    # S = r^2, dS/dr column zero: div = 2 r max(l(l+1), 1/2) / r^2
+    S2 = np.outer(r * r, np.ones(cfg.J))
+    out2 = div_flux(r, l, S2.reshape(-1), np.zeros(S2.size), fix_in=S2[0], fix_out=S2[-1]).reshape(len(r), -1)
+    g3 = np.maximum(np.where(l == 0, 0.5, l * (l + 1.0)), 0.5)
+    assert np.abs(out2 - 2.0 * np.outer(1.0 / r, g3)).max() < 1e-10 * g3.max()

@@ -1,0 +1,72 @@
+"""Spectral divergence of a flux vector (kmhd_sph_div_flux) against the CPU
+oracle of the reference's const_sph_scalar_advect with fixed-field
+boundaries (oracle/sph_div.py): max-norm relative error <= 1e-13, device and
+host pointers; and on the heat flux uT produced by the split-tier cycle."""
+import numpy as np
+import pytest
+
+from kemorin_mhd_b200.config import SphConfig, TIER_FP64, TIER_SPLIT_I8, rj_order
+from kemorin_mhd_b200.synthetic import make_d_rj
+from oracle.sph_div import div_flux
+from tests.gpu_util import to_dev_fortran, from_dev_fortran
+
+CFG = SphConfig(31, 48, 96, 9, name="L31")
+
+
+def _relerr(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("host", [False, True], ids=["device", "host"])
+def test_div_flux_matches_oracle(host):
+    import torch
+    from kemorin_mhd_b200.sph_trans import SphTransform
+    cfg = CFG
+    tr = SphTransform(cfg, tier=TIER_FP64)
+    n = cfg.J * cfg.nr
+    rng = np.random.default_rng(7)
+    d = np.asfortranarray(rng.standard_normal((n, 4)))
+    fin, fout = rng.standard_normal(cfg.J), rng.standard_normal(cfg.J)
+    l, _ = rj_order(cfg.ltr)
+    ref = div_flux(cfg.radius(), l, d[:, 1], d[:, 2], fin, fout)
+    if host:
+        arr = d.copy(order="F")
+        tr.div_flux(arr, 1, 3, fin, fout)
+        got = arr[:, 3]
+        assert np.array_equal(arr[:, :3], d[:, :3])
+    else:
+        t = to_dev_fortran(d)
+        tr.div_flux(t, 1, 3, torch.from_numpy(fin).cuda(), torch.from_numpy(fout).cuda())
+        got = from_dev_fortran(t)[:, 3]
+    assert _relerr(got, ref) <= 1e-13
+
+
+@pytest.mark.gpu
+def test_div_flux_rejects_overlapping_columns():
+    import torch
+    from kemorin_mhd_b200.sph_trans import KmhdError, SphTransform
+    tr = SphTransform(CFG, tier=TIER_FP64)
+    t = torch.zeros((4, CFG.J * CFG.nr), dtype=torch.float64, device="cuda")
+    for col_div in (1, 2):
+        with pytest.raises(KmhdError):
+            tr.div_flux(t, 1, col_div)
+
+
+@pytest.mark.gpu
+def test_heat_advection_after_split_cycle():
+    """-div(u T) from the cycle's heat-flux output, GPU end to end, against the
+    oracle applied to the same uT spectra."""
+    import torch
+    from kemorin_mhd_b200.sph_trans import SphTransform
+    cfg = CFG
+    tr = SphTransform(cfg, tier=TIER_SPLIT_I8)
+    d = to_dev_fortran(make_d_rj(cfg, seed=8))
+    out = torch.zeros((cfg.ncf + 1, cfg.J * cfg.nr), dtype=torch.float64, device="cuda")
+    tr.nonlinear_cycle(d, out)                      # columns: omega x u (0-2), u x B (3-5), uT (6-8), u.omega (9)
+    uT = from_dev_fortran(out)[:, 6:9].copy()
+    tr.div_flux(out, 6, cfg.ncf)                    # div(uT) into the spare column
+    got = from_dev_fortran(out)[:, cfg.ncf]
+    l, _ = rj_order(cfg.ltr)
+    ref = div_flux(cfg.radius(), l, uT[:, 0], uT[:, 1])
+    assert _relerr(got, ref) <= 1e-13
