@@ -206,6 +206,19 @@ int kmhd_sph_cycle_noalloc(const kmhd_sph_desc *desc, const double *d_rj_in, int
 int kmhd_sph_div_flux(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t col_flux, int32_t col_div,
                       const double *fix_in, const double *fix_out, int32_t ptr_kind);
 
+/* Curl of u x B, the induction term of the magnetic field equation: columns
+ * col_rot .. col_rot + 2 = (pol, dpol/dr, tor) of the curl of the vector in
+ * columns col_fld .. col_fld + 2 = (S, dS/dr, T): pol = T, dpol/dr = dT/dr and
+ * tor = -d(dS/dr)/dr + l(l+1) S / r^2 by the reference's radial FDM, with
+ * insulating boundaries (dpol/dr = (l+1) T / r at the first radius, -l T / r
+ * at the last, tor = 0 there).  Replaces const_sph_rotation_uxb with
+ * insulating boundaries (MHD_src/sph_MHD/const_sph_rotation.f90:167-187;
+ * cal_sph_nod_vect_w_div_rot2, cal_sph_exp_rotation.f90:207-248;
+ * cal_sph_nod_icb_ins_vp_rot2 / cal_sph_nod_cmb_ins_vp_rot2).  The column
+ * ranges must not overlap; Nr >= 3; host or device pointers. */
+int kmhd_sph_rot_induction(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t col_fld, int32_t col_rot,
+                           int32_t ptr_kind);
+
 /* Legendre path the handle runs: 1 = the tier's split path, 0 = FP64 DMMA
  * (FP64 tier, or a split-tier handle the autotuner moved to FP64). */
 int kmhd_sph_get_path(const kmhd_sph *handle, int32_t *path);

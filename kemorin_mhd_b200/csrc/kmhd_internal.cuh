@@ -209,6 +209,11 @@ cudaError_t launch_tables(const Plan& p, double* colat, double* weight, double* 
 // fixed boundary values (null: zero).
 cudaError_t launch_div_flux(long long J, int nr, const double* S, const double* dS, double* out, const double* coef,
                             const double* fin, const double* fout, cudaStream_t s);
+// Curl of u x B with insulating boundaries (kmhd_post.cu): input S, dS, T,
+// output pol, dpol, tor (one J*nr column each); coef as launch_div_flux, then
+// ar1[nr] = 1/r and gl[J] = l.
+cudaError_t launch_rot_uxb(long long J, int nr, const double* S, const double* dS, const double* T, double* pol,
+                           double* dpol, double* tor, const double* coef, cudaStream_t s);
 // Set-up of the on-the-fly tables (cos_t, pco, dco, pst, pseed of the plan).
 cudaError_t launch_otf_tables(const Plan& p, double* cos_t, double2* pco, double2* dco, double2* pst,
                               double* pseed, const long long* pseed_off, cudaStream_t s);

@@ -1,6 +1,7 @@
 // kmhd_post.cu -- spectral post-processing after the forward transform: the
 // divergence of a flux vector's spectra (the reference's u.grad(T) term is
-// -div(u T), formed this way after sph_f_trans).
+// -div(u T), formed this way after sph_f_trans) and the curl of u x B (the
+// induction term).
 //
 // Interior rows as cal_sph_nod_vect_div2 (MHD_src/sph_MHD/cal_sph_exp_rotation.f90:254-290),
 // fixed-field boundary rows as cal_sph_div_flux_4_fix_in / _fix_out
@@ -37,7 +38,57 @@ __global__ void k_div_flux(long long J, int nr, const double* __restrict__ S, co
   }
 }
 
+// Curl of u x B (insulating boundaries), one thread per (j, k): input (S,
+// dS/dr, T) columns, output (pol, dpol/dr, tor) columns.  Interior rows as
+// cal_sph_nod_vect_w_div_rot2 (MHD_src/sph_MHD/cal_sph_exp_rotation.f90:207-248),
+// boundary rows as cal_sph_nod_icb_ins_vp_rot2 / cal_sph_nod_cmb_ins_vp_rot2
+// (cal_sph_exp_nod_icb_ins.f90:135-160, cal_sph_exp_nod_cmb_ins.f90:131-157).
+// coef as k_div_flux, then ar1[nr] = 1/r and gl[J] = l.
+__global__ void k_rot_uxb(long long J, int nr, const double* __restrict__ S, const double* __restrict__ dS,
+                          const double* __restrict__ T, double* __restrict__ pol, double* __restrict__ dpol,
+                          double* __restrict__ tor, const double* __restrict__ coef) {
+  const double* d1 = coef;
+  const double* ar2 = coef + 3 * nr + 6;
+  const double* g3 = ar2 + nr;
+  const double* ar1 = g3 + J;
+  const double* gl = ar1 + nr;
+  const long long n = J * nr;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(i / J);
+    const long long j = i - (long long)k * J;
+    const double t = T[i];
+    double dp, tr;
+    if (k == 0) {
+      dp = (gl[j] + 1.0) * ar1[0] * t;
+      tr = 0.0;
+    } else if (k == nr - 1) {
+      dp = -gl[j] * ar1[k] * t;
+      tr = 0.0;
+    } else {
+      const double d1d = d1[3 * k] * dS[i - J] + d1[3 * k + 1] * dS[i] + d1[3 * k + 2] * dS[i + J];
+      dp = d1[3 * k] * T[i - J] + d1[3 * k + 1] * t + d1[3 * k + 2] * T[i + J];
+      tr = -d1d + g3[j] * ar2[k] * S[i];
+    }
+    pol[i] = t;
+    dpol[i] = dp;
+    tor[i] = tr;
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_rot_uxb(long long J, int nr, const double* S, const double* dS, const double* T, double* pol,
+                           double* dpol, double* tor, const double* coef, cudaStream_t s) {
+  const long long n = J * nr;
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const long long want = (n + 255) / 256;
+  const int grid = (int)(want < 8LL * nsm ? want : 8LL * nsm);
+  if (grid <= 0) return cudaSuccess;
+  k_rot_uxb<<<grid, 256, 0, s>>>(J, nr, S, dS, T, pol, dpol, tor, coef);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_div_flux(long long J, int nr, const double* S, const double* dS, double* out, const double* coef,
                             const double* fin, const double* fout, cudaStream_t s) {

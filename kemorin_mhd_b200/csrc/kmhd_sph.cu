@@ -58,7 +58,7 @@ struct kmhd_sph {
   int *cols_b_d = nullptr, *cols_f_d = nullptr;
   int* err = nullptr;  // device error word (bounded waits of the FFT and tcgen05 kernels)
   // divergence post-processing: FDM / normalisation coefficients, host-pointer staging
-  double *div_coef = nullptr, *div_stage = nullptr;
+  double *div_coef = nullptr, *div_stage = nullptr, *rot_stage = nullptr;
   std::vector<double> radius_h;
   std::vector<int> cols_b_cache, cols_f_cache;
   // host-pointer staging
@@ -849,7 +849,7 @@ int build_div_coef(kmhd_sph* h) {
   const Plan& p = h->plan;
   const int nr = p.nr, L = p.L;
   const std::vector<double>& r = h->radius_h;
-  std::vector<double> c(3 * (size_t)nr + 6 + nr + (size_t)p.J, 0.0);
+  std::vector<double> c(3 * (size_t)nr + 6 + nr + (size_t)p.J + nr + (size_t)p.J, 0.0);
   for (int k = 1; k < nr - 1; ++k) {
     const double dp = r[k + 1] - r[k], dn = r[k] - r[k - 1];
     const double t[3][3] = {{1.0, 0.0, 0.0}, {1.0, dp, 0.5 * dp * dp}, {1.0, -dn, 0.5 * dn * dn}};
@@ -878,11 +878,17 @@ int build_div_coef(kmhd_sph* h) {
     c[3 * nr + 6 + k] = a1 * a1;
   }
   double* g3 = c.data() + 4 * nr + 6;
+  double* ar1 = g3 + p.J;  // 1/r (ar_1d_rj(k,1)) and l (g_sph_rj(j,1)) for the curl's boundary rows
+  double* gl = ar1 + nr;
+  for (int k = 0; k < nr; ++k) ar1[k] = 1.0 / r[k];
   for (int m = 0; m <= L; ++m)
     for (int slot = 0; slot < 2; ++slot)
       for (int l = m; l <= L; ++l) {
         const int j = h->jmap_h[((size_t)m * 2 + slot) * (L + 1) + l];
-        if (j >= 0) g3[j] = std::max(g3_of(l), 0.5);
+        if (j >= 0) {
+          g3[j] = std::max(g3_of(l), 0.5);
+          gl[j] = (double)l;
+        }
       }
   int st;
   if ((st = dalloc(h, &h->div_coef, c.size()))) return st;
@@ -926,6 +932,37 @@ int kmhd_sph_div_flux(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_flux, i
     KCHECK(cudaMemcpyAsync(out, s0 + 2 * nrj, sizeof(double) * nrj, cudaMemcpyDeviceToHost, h->stream));
   } else {
     KCHECK(launch_div_flux(p.J, p.nr, S, dS, out, h->div_coef, fin, fout, h->stream));
+  }
+  KCHECK(cudaStreamSynchronize(h->stream));
+  return KMHD_OK;
+}
+
+int kmhd_sph_rot_induction(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_fld, int32_t col_rot,
+                           int32_t ptr_kind) {
+  if (!h || !d_rj) return KMHD_ERR_ARG;
+  if (check_ld(h, ld)) return KMHD_ERR_ARG;
+  if (col_fld < 0 || col_rot < 0 || (col_rot < col_fld + 3 && col_fld < col_rot + 3)) return KMHD_ERR_ARG;
+  const Plan& p = h->plan;
+  if (p.nr < 3) return KMHD_ERR_SIZE;
+  KCHECK(cudaSetDevice(h->device));
+  int st;
+  if (!h->div_coef && (st = build_div_coef(h))) return st;
+  const size_t nrj = (size_t)p.J * p.nr;
+  if (ptr_kind == KMHD_PTR_HOST) {
+    if (!h->rot_stage && (st = dalloc(h, &h->rot_stage, 6 * nrj))) return st;
+    double* s0 = h->rot_stage;
+    for (int q = 0; q < 3; ++q)
+      KCHECK(cudaMemcpyAsync(s0 + q * nrj, d_rj + ld * (col_fld + q), sizeof(double) * nrj, cudaMemcpyHostToDevice,
+                             h->stream));
+    KCHECK(launch_rot_uxb(p.J, p.nr, s0, s0 + nrj, s0 + 2 * nrj, s0 + 3 * nrj, s0 + 4 * nrj, s0 + 5 * nrj,
+                          h->div_coef, h->stream));
+    for (int q = 0; q < 3; ++q)
+      KCHECK(cudaMemcpyAsync(d_rj + ld * (col_rot + q), s0 + (3 + q) * nrj, sizeof(double) * nrj,
+                             cudaMemcpyDeviceToHost, h->stream));
+  } else {
+    const double* in = d_rj + ld * col_fld;
+    double* out = d_rj + ld * col_rot;
+    KCHECK(launch_rot_uxb(p.J, p.nr, in, in + ld, in + 2 * ld, out, out + ld, out + 2 * ld, h->div_coef, h->stream));
   }
   KCHECK(cudaStreamSynchronize(h->stream));
   return KMHD_OK;

@@ -58,7 +58,7 @@ EXPORTS = ["kmhd_sph_create", "kmhd_sph_destroy", "kmhd_sph_set_stream", "kmhd_s
            "kmhd_sph_f_trans", "kmhd_sph_cycle", "kmhd_sph_batch_cycle", "kmhd_sph_last_timing",
            "kmhd_sph_get_tables", "kmhd_sph_device_bytes", "kmhd_strerror", "kmhd_sph_cycle_noalloc",
            "kmhd_sph_last_kernel_timing", "kmhd_sph_get_path", "kmhd_selftest_wait_timeout",
-           "kmhd_sph_div_flux"]
+           "kmhd_sph_div_flux", "kmhd_sph_rot_induction"]
 
 _lib = None
 
@@ -87,6 +87,7 @@ def load_library(path: str | None = None):
     lib.kmhd_sph_last_kernel_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     lib.kmhd_sph_get_path.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
     lib.kmhd_sph_div_flux.argtypes = [vp, vp, i64, i32, i32, vp, vp, i32]
+    lib.kmhd_sph_rot_induction.argtypes = [vp, vp, i64, i32, i32, i32]
     lib.kmhd_selftest_wait_timeout.argtypes = [ctypes.c_int, ctypes.c_int]
     lib.kmhd_sph_get_tables.argtypes = [vp, i32] + [ctypes.POINTER(ctypes.c_double)] * 4
     lib.kmhd_sph_device_bytes.restype = i64
@@ -251,6 +252,16 @@ class SphTransform:
         n = self.cfg.J * self.cfg.nr
         _check(load_library().kmhd_sph_div_flux(self._h, p, ld or n, col_flux, col_div, fi, fo, kind),
                "kmhd_sph_div_flux")
+        return d_rj
+
+
+    def rot_induction(self, d_rj, col_fld: int, col_rot: int, ld: int | None = None):
+        """Curl of the vector (S, dS/dr, T) in columns col_fld.. into
+        col_rot.. (pol, dpol/dr, tor), insulating boundaries."""
+        p, kind = _ptr(d_rj)
+        n = self.cfg.J * self.cfg.nr
+        _check(load_library().kmhd_sph_rot_induction(self._h, p, ld or n, col_fld, col_rot, kind),
+               "kmhd_sph_rot_induction")
         return d_rj
 
 

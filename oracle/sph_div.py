@@ -1,7 +1,6 @@
-"""CPU oracle (test infrastructure only) of the spectral divergence of a flux
-vector, the post-processing step that closes the reference's u.grad(T) term
-(heat advection = -div(u T), taken in spectral space after the forward
-transform).
+"""CPU oracle (test infrastructure only) of the spectral post-processing after
+the forward transform: the divergence of a flux vector (the reference's
+u.grad(T) term is -div(u T)) and the curl of u x B (the induction term).
 
 Restates, in plain numpy:
 - const_sph_scalar_advect (MHD_src/sph_MHD/const_sph_divergence.f90:49-74);
@@ -96,3 +95,33 @@ def div_flux(radius, l_of_j, S, dS, fix_in=None, fix_out=None):
     d1s = cmb[2] * S[nr - 3] + cmb[1] * S[nr - 2] + cmb[0] * fout
     out[nr - 1] = (d1s - dS[nr - 1]) * g3 * ar2[nr - 1]
     return out.reshape(-1)
+
+
+def rot_uxb(radius, l_of_j, S, dS, T):
+    """Curl (pol, dpol/dr, tor) of the vector (S, dS/dr, T) with insulating
+    boundaries, as const_sph_rotation_uxb
+    (MHD_src/sph_MHD/const_sph_rotation.f90:167-187): interior rows
+    cal_sph_nod_vect_w_div_rot2 (cal_sph_exp_rotation.f90:207-248)
+        pol = T, dpol/dr = dT/dr (FDM), tor = -d(dS/dr)/dr (FDM) + g3 S / r^2;
+    boundary rows cal_sph_nod_icb_ins_vp_rot2 (cal_sph_exp_nod_icb_ins.f90:135-160)
+    and cal_sph_nod_cmb_ins_vp_rot2 (cal_sph_exp_nod_cmb_ins.f90:131-157):
+        pol = T, dpol/dr = (l + 1) T / r (inner) or -l T / r (outer), tor = 0."""
+    r = np.asarray(radius, dtype=np.float64)
+    nr, J = len(r), len(l_of_j)
+    S = np.asarray(S).reshape(nr, J)
+    dS = np.asarray(dS).reshape(nr, J)
+    T = np.asarray(T).reshape(nr, J)
+    l = np.asarray(l_of_j).astype(np.float64)
+    g3 = np.where(l == 0, 0.5, l * (l + 1.0))
+    ar1 = 1.0 / r
+    ar2 = ar1 ** 2
+    d1, _, _ = fdm_coefs(r)
+    pol, dpol, tor = T.copy(), np.zeros((nr, J)), np.zeros((nr, J))
+    for k in range(1, nr - 1):
+        d1d = d1[k, 0] * dS[k - 1] + d1[k, 1] * dS[k] + d1[k, 2] * dS[k + 1]
+        d1t = d1[k, 0] * T[k - 1] + d1[k, 1] * T[k] + d1[k, 2] * T[k + 1]
+        dpol[k] = d1t
+        tor[k] = -d1d + g3 * ar2[k] * S[k]
+    dpol[0] = (l + 1.0) * ar1[0] * T[0]
+    dpol[nr - 1] = -l * ar1[nr - 1] * T[nr - 1]
+    return pol.reshape(-1), dpol.reshape(-1), tor.reshape(-1)

@@ -43,3 +43,27 @@ def test_divergence_of_quadratic_profiles():
     out2 = div_flux(r, l, S2.reshape(-1), np.zeros(S2.size), fix_in=S2[0], fix_out=S2[-1]).reshape(len(r), -1)
     g3 = np.maximum(np.where(l == 0, 0.5, l * (l + 1.0)), 0.5)
     assert np.abs(out2 - 2.0 * np.outer(1.0 / r, g3)).max() < 1e-10 * g3.max()
+
+
+def test_rot_uxb_oracle_on_quadratic_profiles():
+    """pol = T, dpol/dr = dT/dr, tor = -d(dS/dr)/dr + g3 S / r^2 exactly for
+    quadratic radial profiles in the interior; insulating boundary rows."""
+    from oracle.sph_div import rot_uxb
+    cfg = SphConfig(15, 24, 48, 9)
+    r = cfg.radius()
+    l, _ = rj_order(cfg.ltr)
+    rng = np.random.default_rng(5)
+    a, b, c, e = (rng.standard_normal(cfg.J) for _ in range(4))
+    one = np.ones_like(r)
+    S = np.outer(one, a) + np.outer(r, b)
+    dS = np.outer(one, b) + np.outer(r * r, c)         # d(dS)/dr = 2 c r
+    T = np.outer(r * r, e)                              # dT/dr = 2 e r
+    pol, dpol, tor = (x.reshape(len(r), -1) for x in rot_uxb(r, l, S.reshape(-1), dS.reshape(-1), T.reshape(-1)))
+    g3 = np.where(l == 0, 0.5, l * (l + 1.0))
+    assert np.array_equal(pol, T)
+    inner = slice(1, len(r) - 1)
+    assert np.abs(dpol[inner] - np.outer(2 * r, e)[inner]).max() < 1e-10
+    tor_ref = -np.outer(2 * r, c) + np.outer(1 / r ** 2, g3) * S
+    assert np.abs(tor[inner] - tor_ref[inner]).max() < 1e-9 * np.abs(tor_ref).max()
+    assert np.allclose(dpol[0], (l + 1.0) / r[0] * T[0]) and np.allclose(dpol[-1], -l / r[-1] * T[-1])
+    assert not tor[0].any() and not tor[-1].any()

@@ -70,3 +70,49 @@ def test_heat_advection_after_split_cycle():
     l, _ = rj_order(cfg.ltr)
     ref = div_flux(cfg.radius(), l, uT[:, 0], uT[:, 1])
     assert _relerr(got, ref) <= 1e-13
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("host", [False, True], ids=["device", "host"])
+def test_rot_induction_matches_oracle(host):
+    import torch
+    from kemorin_mhd_b200.sph_trans import SphTransform
+    from oracle.sph_div import rot_uxb
+    cfg = CFG
+    tr = SphTransform(cfg, tier=TIER_FP64)
+    n = cfg.J * cfg.nr
+    rng = np.random.default_rng(11)
+    d = np.asfortranarray(rng.standard_normal((n, 7)))
+    l, _ = rj_order(cfg.ltr)
+    ref = np.stack(rot_uxb(cfg.radius(), l, d[:, 0], d[:, 1], d[:, 2]), axis=1)
+    if host:
+        arr = d.copy(order="F")
+        tr.rot_induction(arr, 0, 4)
+        got = arr[:, 4:7]
+        assert np.array_equal(arr[:, :4], d[:, :4])
+    else:
+        t = to_dev_fortran(d)
+        tr.rot_induction(t, 0, 4)
+        got = from_dev_fortran(t)[:, 4:7]
+    for q in range(3):
+        assert _relerr(got[:, q], ref[:, q]) <= 1e-13, q
+
+
+@pytest.mark.gpu
+def test_induction_after_split_cycle():
+    """curl(u x B) from the cycle's u x B output (columns 3-5), on the GPU."""
+    import torch
+    from kemorin_mhd_b200.sph_trans import SphTransform
+    from oracle.sph_div import rot_uxb
+    cfg = CFG
+    tr = SphTransform(cfg, tier=TIER_SPLIT_I8)
+    d = to_dev_fortran(make_d_rj(cfg, seed=12))
+    out = torch.zeros((cfg.ncf + 3, cfg.J * cfg.nr), dtype=torch.float64, device="cuda")
+    tr.nonlinear_cycle(d, out)
+    uxb = from_dev_fortran(out)[:, 3:6].copy()
+    tr.rot_induction(out, 3, cfg.ncf)
+    got = from_dev_fortran(out)[:, cfg.ncf:cfg.ncf + 3]
+    l, _ = rj_order(cfg.ltr)
+    ref = rot_uxb(cfg.radius(), l, uxb[:, 0], uxb[:, 1], uxb[:, 2])
+    for q in range(3):
+        assert _relerr(got[:, q], ref[q]) <= 1e-13, q
