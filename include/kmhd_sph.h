@@ -219,6 +219,36 @@ int kmhd_sph_div_flux(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t col
 int kmhd_sph_rot_induction(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t col_fld, int32_t col_rot,
                            int32_t ptr_kind);
 
+/* Velocity boundary conditions of the momentum equation (the reference's
+ * iflag_icb / iflag_cmb for the velocity): non-slip and free slip. */
+#define KMHD_BC_NON_SLIP 0
+#define KMHD_BC_FREE_SLIP 1
+
+/* Curl of a momentum force (advection, Lorentz force), the source of the
+ * vorticity equation: as kmhd_sph_rot_induction in the interior; on each
+ * boundary pol = T, dpol/dr = one-sided dT/dr and tor = -(d2S/dr2 - l(l+1)
+ * S / r^2), with the two-point second derivative of the velocity condition
+ * bc_icb / bc_cmb (KMHD_BC_*).  Replaces const_sph_force_rot2
+ * (MHD_src/sph_MHD/const_sph_rotation.f90:225-250), called by
+ * cal_rot_of_forces_sph_2 (cal_sph_field_by_rotation.f90:83-121), with the
+ * rows of sel_bc_sph_vorticity (select_exp_velocity_bc.f90:215-262):
+ * cal_sph_nod_icb_rigid_rot2 / cal_sph_nod_cmb_rigid_rot2
+ * (set_sph_exp_rigid_ICB.f90:159-197, set_sph_exp_rigid_CMB.f90:129-166) and
+ * cal_sph_nod_icb_free_rot2 / cal_sph_nod_cmb_free_rot2
+ * (set_sph_exp_free_ICB.f90:131-166, set_sph_exp_free_CMB.f90).  The full-sphere
+ * centre row and the rotating inner core's torque are not provided.  Column
+ * ranges must not overlap; Nr >= 3; host or device pointers. */
+int kmhd_sph_rot_force(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t col_fld, int32_t col_rot,
+                       int32_t bc_icb, int32_t bc_cmb, int32_t ptr_kind);
+
+/* Divergence of a momentum force (the pressure equation's source): as
+ * kmhd_sph_div_flux with each boundary node's own S in the one-sided rows.
+ * Replaces const_sph_div_force (MHD_src/sph_MHD/const_sph_divergence.f90:79-108:
+ * cal_sph_nod_vect_div2, cal_sph_nod_nobc_in_div2 / _out_div2,
+ * cal_sph_exp_nod_none_bc.f90:153-185, 309-341). */
+int kmhd_sph_div_force(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t col_fld, int32_t col_div,
+                       int32_t ptr_kind);
+
 /* Legendre path the handle runs: 1 = the tier's split path, 0 = FP64 DMMA
  * (FP64 tier, or a split-tier handle the autotuner moved to FP64). */
 int kmhd_sph_get_path(const kmhd_sph *handle, int32_t *path);

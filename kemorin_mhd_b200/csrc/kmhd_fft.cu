@@ -625,20 +625,8 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_fwd_grid(Plan P, const doub
 // staged records of one line: [m][ncs pairs], ncs = nc rounded up to odd
 __device__ __forceinline__ int ncs_of(int nc) { return nc | 1; }
 
-__device__ void prefetch_line_t(double* st, const double* rtm, int nc, const Plan& P, int th, int r) {
-  const long long strideM = (long long)P.nth * P.nr * nc * 2;
-  const double* base = rtm + rtm_off(P, 0, th, r, nc);
-  const int ncs = ncs_of(nc);
-  const int n = (P.L + 1) * nc;
-  for (int it = threadIdx.x; it < n; it += blockDim.x) {
-    const int m = it / nc, c = it - m * nc;
-    cp_async16(st + (m * ncs + c) * 2, base + m * strideM + c * 2);
-  }
-  cp_async_commit();
-}
-
-// prefetch_line_t for a compile-time component count NC: thread t copies the
-// 16-byte pieces of component t % NC of orders t / NC, t / NC + T / NC, ...
+// Stages the spectra of one line (NC components, all orders) into shared
+// memory with cp.async: thread t copies the 16-byte pieces of component t % NC of orders t / NC, t / NC + T / NC, ...
 // (T = the largest multiple of NC not above the thread count), with pointer
 // increments instead of divisions.
 template <int NC>

@@ -209,11 +209,17 @@ cudaError_t launch_tables(const Plan& p, double* colat, double* weight, double* 
 // fixed boundary values (null: zero).
 cudaError_t launch_div_flux(long long J, int nr, const double* S, const double* dS, double* out, const double* coef,
                             const double* fin, const double* fout, cudaStream_t s);
-// Curl of u x B with insulating boundaries (kmhd_post.cu): input S, dS, T,
-// output pol, dpol, tor (one J*nr column each); coef as launch_div_flux, then
-// ar1[nr] = 1/r and gl[J] = l.
-cudaError_t launch_rot_uxb(long long J, int nr, const double* S, const double* dS, const double* T, double* pol,
-                           double* dpol, double* tor, const double* coef, cudaStream_t s);
+// Boundary rows of the spectral curl, per side: insulating (the magnetic
+// field's condition), else d2S/dr2 = s[0] S(boundary) + s[1] S(neighbour) and
+// dT/dr = t[0] T(boundary) + t[1] T(neighbour) + t[2] T(second neighbour).
+struct RotBnd {
+  int insulating_in, insulating_out;
+  double s_in[2], t_in[3], s_out[2], t_out[3];
+};
+// Curl of a vector (kmhd_post.cu): input S, dS, T, output pol, dpol, tor (one
+// J*nr column each); coef as launch_div_flux, then ar1[nr] = 1/r and gl[J] = l.
+cudaError_t launch_rot_vec(long long J, int nr, const double* S, const double* dS, const double* T, double* pol,
+                           double* dpol, double* tor, const double* coef, const RotBnd& b, cudaStream_t s);
 // Set-up of the on-the-fly tables (cos_t, pco, dco, pst, pseed of the plan).
 cudaError_t launch_otf_tables(const Plan& p, double* cos_t, double2* pco, double2* dco, double2* pst,
                               double* pseed, const long long* pseed_off, cudaStream_t s);

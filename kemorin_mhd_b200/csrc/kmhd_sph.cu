@@ -897,12 +897,11 @@ int build_div_coef(kmhd_sph* h) {
   return KMHD_OK;
 }
 
-}  // namespace
-
-extern "C" {
-
-int kmhd_sph_div_flux(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_flux, int32_t col_div,
-                      const double* fix_in, const double* fix_out, int32_t ptr_kind) {
+// Divergence of the vector in columns col_flux, col_flux + 1 into col_div;
+// own_bnd = 1 puts each boundary node's own S into the one-sided rows (the
+// force divergence), else fix_in / fix_out (NULL = zero).
+int div_vec(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_flux, int32_t col_div, const double* fix_in,
+            const double* fix_out, int own_bnd, int32_t ptr_kind) {
   if (!h || !d_rj) return KMHD_ERR_ARG;
   if (check_ld(h, ld)) return KMHD_ERR_ARG;
   if (col_flux < 0 || col_div < 0 || col_div == col_flux || col_div == col_flux + 1) return KMHD_ERR_ARG;
@@ -911,7 +910,7 @@ int kmhd_sph_div_flux(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_flux, i
   KCHECK(cudaSetDevice(h->device));
   int st;
   if (!h->div_coef && (st = build_div_coef(h))) return st;
-  const size_t nrj = (size_t)p.J * p.nr;
+  const size_t nrj = (size_t)p.J * p.nr, last = (size_t)p.J * (p.nr - 1);
   const double *S = d_rj + ld * col_flux, *dS = d_rj + ld * (col_flux + 1), *fin = fix_in, *fout = fix_out;
   double* out = d_rj + ld * col_div;
   if (ptr_kind == KMHD_PTR_HOST) {
@@ -920,25 +919,35 @@ int kmhd_sph_div_flux(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_flux, i
     double* s0 = h->div_stage;
     KCHECK(cudaMemcpyAsync(s0, S, sizeof(double) * nrj, cudaMemcpyHostToDevice, h->stream));
     KCHECK(cudaMemcpyAsync(s0 + nrj, dS, sizeof(double) * nrj, cudaMemcpyHostToDevice, h->stream));
-    if (fix_in) {
-      KCHECK(cudaMemcpyAsync(s0 + 3 * nrj, fix_in, sizeof(double) * p.J, cudaMemcpyHostToDevice, h->stream));
-      fin = s0 + 3 * nrj;
-    }
-    if (fix_out) {
-      KCHECK(cudaMemcpyAsync(s0 + 3 * nrj + p.J, fix_out, sizeof(double) * p.J, cudaMemcpyHostToDevice, h->stream));
-      fout = s0 + 3 * nrj + p.J;
+    if (own_bnd) {
+      fin = s0;
+      fout = s0 + last;
+    } else {
+      if (fix_in) {
+        KCHECK(cudaMemcpyAsync(s0 + 3 * nrj, fix_in, sizeof(double) * p.J, cudaMemcpyHostToDevice, h->stream));
+        fin = s0 + 3 * nrj;
+      }
+      if (fix_out) {
+        KCHECK(cudaMemcpyAsync(s0 + 3 * nrj + p.J, fix_out, sizeof(double) * p.J, cudaMemcpyHostToDevice, h->stream));
+        fout = s0 + 3 * nrj + p.J;
+      }
     }
     KCHECK(launch_div_flux(p.J, p.nr, s0, s0 + nrj, s0 + 2 * nrj, h->div_coef, fin, fout, h->stream));
     KCHECK(cudaMemcpyAsync(out, s0 + 2 * nrj, sizeof(double) * nrj, cudaMemcpyDeviceToHost, h->stream));
   } else {
+    if (own_bnd) {
+      fin = S;
+      fout = S + last;
+    }
     KCHECK(launch_div_flux(p.J, p.nr, S, dS, out, h->div_coef, fin, fout, h->stream));
   }
   KCHECK(cudaStreamSynchronize(h->stream));
   return KMHD_OK;
 }
 
-int kmhd_sph_rot_induction(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_fld, int32_t col_rot,
-                           int32_t ptr_kind) {
+// Curl of the vector in columns col_fld .. col_fld + 2 into col_rot .. col_rot + 2.
+int rot_vec(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_fld, int32_t col_rot, const RotBnd& b,
+            int32_t ptr_kind) {
   if (!h || !d_rj) return KMHD_ERR_ARG;
   if (check_ld(h, ld)) return KMHD_ERR_ARG;
   if (col_fld < 0 || col_rot < 0 || (col_rot < col_fld + 3 && col_fld < col_rot + 3)) return KMHD_ERR_ARG;
@@ -954,18 +963,104 @@ int kmhd_sph_rot_induction(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_fl
     for (int q = 0; q < 3; ++q)
       KCHECK(cudaMemcpyAsync(s0 + q * nrj, d_rj + ld * (col_fld + q), sizeof(double) * nrj, cudaMemcpyHostToDevice,
                              h->stream));
-    KCHECK(launch_rot_uxb(p.J, p.nr, s0, s0 + nrj, s0 + 2 * nrj, s0 + 3 * nrj, s0 + 4 * nrj, s0 + 5 * nrj,
-                          h->div_coef, h->stream));
+    KCHECK(launch_rot_vec(p.J, p.nr, s0, s0 + nrj, s0 + 2 * nrj, s0 + 3 * nrj, s0 + 4 * nrj, s0 + 5 * nrj,
+                          h->div_coef, b, h->stream));
     for (int q = 0; q < 3; ++q)
       KCHECK(cudaMemcpyAsync(d_rj + ld * (col_rot + q), s0 + (3 + q) * nrj, sizeof(double) * nrj,
                              cudaMemcpyDeviceToHost, h->stream));
   } else {
     const double* in = d_rj + ld * col_fld;
     double* out = d_rj + ld * col_rot;
-    KCHECK(launch_rot_uxb(p.J, p.nr, in, in + ld, in + 2 * ld, out, out + ld, out + 2 * ld, h->div_coef, h->stream));
+    KCHECK(launch_rot_vec(p.J, p.nr, in, in + ld, in + 2 * ld, out, out + ld, out + 2 * ld, h->div_coef, b,
+                          h->stream));
   }
   KCHECK(cudaStreamSynchronize(h->stream));
   return KMHD_OK;
+}
+
+// Boundary rows of the curl of a force for the velocity conditions, built as
+// the reference builds them (cofactor inverses of 3x3 Taylor matrices):
+// non-slip d2S/dr2 from cal_fdm2_coef_fix_df_ICB / _CMB
+// (MHD_src/sph_MHD/cal_fdm_coefs_4_boundaries.f90:195-231, 297-334), whose
+// unknowns are ordered (dS/dr, S, d2S/dr2) at the inner and (S, dS/dr,
+// d2S/dr2) at the outer boundary; dT/dr from the fixed-field one-sided rows;
+// free slip from cal_fdm2_ICB_free_vp / _vt and cal_fdm2_CMB_free_vp / _vt
+// (coef_fdm2_free_ICB.f90, coef_fdm2_free_CMB.f90).
+RotBnd velocity_bnd(const std::vector<double>& r, int bc_icb, int bc_cmb) {
+  const int nr = (int)r.size();
+  RotBnd b{};
+  double inv[3][3];
+  if (bc_icb == KMHD_BC_NON_SLIP) {
+    const double dr = r[1] - r[0];
+    const double t[3][3] = {{1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {dr, 1.0, dr * dr / 2.0}};
+    inverse33(t, inv);
+    b.s_in[0] = inv[2][1];
+    b.s_in[1] = inv[2][2];
+    const double d1 = r[1] - r[0], d2 = r[2] - r[0];
+    const double f[3][3] = {{1.0, 0.0, 0.0}, {1.0, d1, d1 * d1 / 2.0}, {1.0, d2, d2 * d2 / 2.0}};
+    inverse33(f, inv);
+    for (int q = 0; q < 3; ++q) b.t_in[q] = inv[1][q];
+  } else {
+    const double dr = r[1] - r[0], r0 = r[0];
+    const double vp[3][3] = {{1.0, 0.0, 0.0}, {1.0, -r0, 0.5 * r0 * r0}, {1.0, dr, 0.5 * dr * dr}};
+    inverse33(vp, inv);
+    b.s_in[0] = inv[2][0];
+    b.s_in[1] = inv[2][2];
+    const double vt[3][3] = {{1.0, 0.0, 0.0}, {2.0, -r0, 0.0}, {1.0, dr, 0.5 * dr * dr}};
+    inverse33(vt, inv);
+    b.t_in[0] = inv[1][0];
+  }
+  if (bc_cmb == KMHD_BC_NON_SLIP) {
+    const double dn = r[nr - 1] - r[nr - 2];
+    const double t[3][3] = {{1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {1.0, -dn, dn * dn / 2.0}};
+    inverse33(t, inv);
+    b.s_out[0] = inv[2][0];
+    b.s_out[1] = inv[2][2];
+    const double d1 = r[nr - 1] - r[nr - 2], d2 = r[nr - 1] - r[nr - 3];
+    const double f[3][3] = {{1.0, 0.0, 0.0}, {1.0, -d1, d1 * d1 / 2.0}, {1.0, -d2, d2 * d2 / 2.0}};
+    inverse33(f, inv);
+    for (int q = 0; q < 3; ++q) b.t_out[q] = inv[1][q];
+  } else {
+    const double dn = r[nr - 1] - r[nr - 2], r0 = r[nr - 1];
+    const double vp[3][3] = {{1.0, 0.0, 0.0}, {1.0, -r0, 0.5 * r0 * r0}, {1.0, -dn, 0.5 * dn * dn}};
+    inverse33(vp, inv);
+    b.s_out[0] = inv[2][0];
+    b.s_out[1] = inv[2][2];
+    const double vt[3][3] = {{1.0, 0.0, 0.0}, {2.0, -r0, 0.0}, {1.0, -dn, 0.5 * dn * dn}};
+    inverse33(vt, inv);
+    b.t_out[0] = inv[1][0];
+  }
+  return b;
+}
+
+}  // namespace
+
+extern "C" {
+
+int kmhd_sph_div_flux(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_flux, int32_t col_div,
+                      const double* fix_in, const double* fix_out, int32_t ptr_kind) {
+  return div_vec(h, d_rj, ld, col_flux, col_div, fix_in, fix_out, 0, ptr_kind);
+}
+
+int kmhd_sph_rot_induction(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_fld, int32_t col_rot,
+                           int32_t ptr_kind) {
+  RotBnd b{};
+  b.insulating_in = b.insulating_out = 1;
+  return rot_vec(h, d_rj, ld, col_fld, col_rot, b, ptr_kind);
+}
+
+int kmhd_sph_rot_force(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_fld, int32_t col_rot, int32_t bc_icb,
+                       int32_t bc_cmb, int32_t ptr_kind) {
+  if (!h) return KMHD_ERR_ARG;
+  const int ok_in = bc_icb == KMHD_BC_NON_SLIP || bc_icb == KMHD_BC_FREE_SLIP;
+  const int ok_out = bc_cmb == KMHD_BC_NON_SLIP || bc_cmb == KMHD_BC_FREE_SLIP;
+  if (!ok_in || !ok_out) return KMHD_ERR_ARG;
+  if (h->plan.nr < 3) return KMHD_ERR_SIZE;
+  return rot_vec(h, d_rj, ld, col_fld, col_rot, velocity_bnd(h->radius_h, bc_icb, bc_cmb), ptr_kind);
+}
+
+int kmhd_sph_div_force(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_fld, int32_t col_div, int32_t ptr_kind) {
+  return div_vec(h, d_rj, ld, col_fld, col_div, nullptr, nullptr, 1, ptr_kind);
 }
 
 int kmhd_sph_last_kernel_timing(kmhd_sph* h, double* ms5) {

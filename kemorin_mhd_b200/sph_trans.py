@@ -30,6 +30,8 @@ KMHD_PTR_HOST = 1
 # kmhd_sph_desc.flags bits (include/kmhd_sph.h)
 FLAG_AUTOTUNE = 1
 FLAG_P_ON_THE_FLY = 2
+BC_NON_SLIP = 0       # KMHD_BC_NON_SLIP
+BC_FREE_SLIP = 1      # KMHD_BC_FREE_SLIP
 
 
 class KmhdError(RuntimeError):
@@ -58,7 +60,7 @@ EXPORTS = ["kmhd_sph_create", "kmhd_sph_destroy", "kmhd_sph_set_stream", "kmhd_s
            "kmhd_sph_f_trans", "kmhd_sph_cycle", "kmhd_sph_batch_cycle", "kmhd_sph_last_timing",
            "kmhd_sph_get_tables", "kmhd_sph_device_bytes", "kmhd_strerror", "kmhd_sph_cycle_noalloc",
            "kmhd_sph_last_kernel_timing", "kmhd_sph_get_path", "kmhd_selftest_wait_timeout",
-           "kmhd_sph_div_flux", "kmhd_sph_rot_induction"]
+           "kmhd_sph_div_flux", "kmhd_sph_rot_induction", "kmhd_sph_rot_force", "kmhd_sph_div_force"]
 
 _lib = None
 
@@ -88,6 +90,8 @@ def load_library(path: str | None = None):
     lib.kmhd_sph_get_path.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
     lib.kmhd_sph_div_flux.argtypes = [vp, vp, i64, i32, i32, vp, vp, i32]
     lib.kmhd_sph_rot_induction.argtypes = [vp, vp, i64, i32, i32, i32]
+    lib.kmhd_sph_rot_force.argtypes = [vp, vp, i64, i32, i32, i32, i32, i32]
+    lib.kmhd_sph_div_force.argtypes = [vp, vp, i64, i32, i32, i32]
     lib.kmhd_selftest_wait_timeout.argtypes = [ctypes.c_int, ctypes.c_int]
     lib.kmhd_sph_get_tables.argtypes = [vp, i32] + [ctypes.POINTER(ctypes.c_double)] * 4
     lib.kmhd_sph_device_bytes.restype = i64
@@ -262,6 +266,24 @@ class SphTransform:
         n = self.cfg.J * self.cfg.nr
         _check(load_library().kmhd_sph_rot_induction(self._h, p, ld or n, col_fld, col_rot, kind),
                "kmhd_sph_rot_induction")
+        return d_rj
+
+    def rot_force(self, d_rj, col_fld: int, col_rot: int, bc_icb: int = 0, bc_cmb: int = 0,
+                  ld: int | None = None):
+        """Curl of the force (S, dS/dr, T) in columns col_fld.. into col_rot..
+        with the velocity conditions bc_icb / bc_cmb (BC_NON_SLIP, BC_FREE_SLIP)."""
+        p, kind = _ptr(d_rj)
+        n = self.cfg.J * self.cfg.nr
+        _check(load_library().kmhd_sph_rot_force(self._h, p, ld or n, col_fld, col_rot, bc_icb, bc_cmb, kind),
+               "kmhd_sph_rot_force")
+        return d_rj
+
+    def div_force(self, d_rj, col_fld: int, col_div: int, ld: int | None = None):
+        """Divergence of the force (S, dS/dr) in columns col_fld.. into col_div."""
+        p, kind = _ptr(d_rj)
+        n = self.cfg.J * self.cfg.nr
+        _check(load_library().kmhd_sph_div_force(self._h, p, ld or n, col_fld, col_div, kind),
+               "kmhd_sph_div_force")
         return d_rj
 
 

@@ -1,6 +1,8 @@
 """CPU oracle (test infrastructure only) of the spectral post-processing after
 the forward transform: the divergence of a flux vector (the reference's
-u.grad(T) term is -div(u T)) and the curl of u x B (the induction term).
+u.grad(T) term is -div(u T)), the curl of u x B (the induction term), and the
+curl and divergence of the momentum forces (the vorticity equation's inertia
+and Lorentz terms, the pressure source).
 
 Restates, in plain numpy:
 - const_sph_scalar_advect (MHD_src/sph_MHD/const_sph_divergence.f90:49-74);
@@ -16,6 +18,20 @@ Restates, in plain numpy:
   cal_fdm2_coef_fix_fld_ICB / _CMB (MHD_src/sph_MHD/cal_fdm_coefs_4_boundaries.f90:155-190, 256-290),
   cal_inverse_33_matrix and cal_det_33_matrix (CORE_src/BASE/cal_inverse_small_matrix.f90:57-80, 176-215);
 - 1/r^2 as (1/r)^2 (CORE_src/SPH_SPECTR_src/set_radius_4_sph_dynamo.f90:105).
+
+- const_sph_force_rot2 (MHD_src/sph_MHD/const_sph_rotation.f90:225-250), the
+  curl of a force with the velocity boundary rows of sel_bc_sph_vorticity
+  (MHD_src/sph_MHD/select_exp_velocity_bc.f90:215-262): non-slip rows
+  cal_sph_nod_icb_rigid_rot2 / cal_sph_nod_cmb_rigid_rot2
+  (set_sph_exp_rigid_ICB.f90:159-197, set_sph_exp_rigid_CMB.f90:129-166) with
+  cal_fdm2_coef_fix_df_ICB / _CMB (cal_fdm_coefs_4_boundaries.f90:195-231,
+  297-334); free-slip rows cal_sph_nod_icb_free_rot2 / cal_sph_nod_cmb_free_rot2
+  (set_sph_exp_free_ICB.f90:131-166, set_sph_exp_free_CMB.f90) with
+  cal_fdm2_ICB_free_vp / _vt and cal_fdm2_CMB_free_vp / _vt
+  (coef_fdm2_free_ICB.f90, coef_fdm2_free_CMB.f90);
+- const_sph_div_force (const_sph_divergence.f90:79-108): the divergence rows
+  with the boundary node's own value, cal_sph_nod_nobc_in_div2 / _out_div2
+  (cal_sph_exp_nod_none_bc.f90:153-185, 309-341).
 
 Parity unpinned against the reference's own outputs (no Fortran compiler in
 this image); the tests pin this restatement by the FDM being exact for
@@ -125,3 +141,69 @@ def rot_uxb(radius, l_of_j, S, dS, T):
     dpol[0] = (l + 1.0) * ar1[0] * T[0]
     dpol[nr - 1] = -l * ar1[nr - 1] * T[nr - 1]
     return pol.reshape(-1), dpol.reshape(-1), tor.reshape(-1)
+
+
+NON_SLIP, FREE_SLIP = "non_slip", "free_slip"
+
+
+def velocity_bnd_coefs(radius, bc_icb=NON_SLIP, bc_cmb=NON_SLIP):
+    """Boundary-row coefficients of the curl of a force: for each side,
+    (s0, s1) of d2S/dr2 = s0 S(boundary) + s1 S(neighbour) and (t0, t1, t2) of
+    dT/dr on the boundary node and its first and second neighbours."""
+    r = np.asarray(radius, dtype=np.float64)
+    _, icb, cmb = fdm_coefs(r)
+    if bc_icb == NON_SLIP:
+        dr = r[1] - r[0]
+        # unknowns (S', S, S''), rows: S' fixed, S, S(kr + 1)
+        m = inverse33([[1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [dr, 1.0, dr * dr / 2.0]])
+        s_in, t_in = (m[2, 1], m[2, 2]), tuple(icb)
+    elif bc_icb == FREE_SLIP:
+        dr, r0 = r[1] - r[0], r[0]
+        mvp = inverse33([[1.0, 0.0, 0.0], [1.0, -r0, 0.5 * r0 * r0], [1.0, dr, 0.5 * dr * dr]])
+        mvt = inverse33([[1.0, 0.0, 0.0], [2.0, -r0, 0.0], [1.0, dr, 0.5 * dr * dr]])
+        s_in, t_in = (mvp[2, 0], mvp[2, 2]), (mvt[1, 0], 0.0, 0.0)
+    else:
+        raise ValueError(bc_icb)
+    if bc_cmb == NON_SLIP:
+        dn = r[-1] - r[-2]
+        m = inverse33([[1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [1.0, -dn, dn * dn / 2.0]])
+        s_out, t_out = (m[2, 0], m[2, 2]), tuple(cmb)
+    elif bc_cmb == FREE_SLIP:
+        dn, r0 = r[-1] - r[-2], r[-1]
+        mvp = inverse33([[1.0, 0.0, 0.0], [1.0, -r0, 0.5 * r0 * r0], [1.0, -dn, 0.5 * dn * dn]])
+        mvt = inverse33([[1.0, 0.0, 0.0], [2.0, -r0, 0.0], [1.0, -dn, 0.5 * dn * dn]])
+        s_out, t_out = (mvp[2, 0], mvp[2, 2]), (mvt[1, 0], 0.0, 0.0)
+    else:
+        raise ValueError(bc_cmb)
+    return s_in, t_in, s_out, t_out
+
+
+def rot_force(radius, l_of_j, S, dS, T, bc_icb=NON_SLIP, bc_cmb=NON_SLIP):
+    """Curl (pol, dpol/dr, tor) of the force (S, dS/dr, T), as
+    const_sph_force_rot2: interior rows as rot_uxb; boundary rows
+        pol = T, dpol/dr = one-sided dT/dr, tor = -(d2S/dr2 - g3 S / r^2)
+    with the velocity condition's coefficients (velocity_bnd_coefs)."""
+    r = np.asarray(radius, dtype=np.float64)
+    nr, J = len(r), len(l_of_j)
+    pol, dpol, tor = (x.reshape(nr, J) for x in rot_uxb(r, l_of_j, S, dS, T))
+    S = np.asarray(S).reshape(nr, J)
+    T = np.asarray(T).reshape(nr, J)
+    l = np.asarray(l_of_j).astype(np.float64)
+    g3 = np.where(l == 0, 0.5, l * (l + 1.0))
+    ar2 = (1.0 / r) ** 2
+    s_in, t_in, s_out, t_out = velocity_bnd_coefs(r, bc_icb, bc_cmb)
+    d2s = s_in[0] * S[0] + s_in[1] * S[1]
+    dpol[0] = t_in[0] * T[0] + t_in[1] * T[1] + t_in[2] * T[2]
+    tor[0] = -(d2s - g3 * ar2[0] * S[0])
+    d2s = s_out[1] * S[nr - 2] + s_out[0] * S[nr - 1]
+    dpol[nr - 1] = t_out[2] * T[nr - 3] + t_out[1] * T[nr - 2] + t_out[0] * T[nr - 1]
+    tor[nr - 1] = -(d2s - g3 * ar2[nr - 1] * S[nr - 1])
+    return pol.reshape(-1), dpol.reshape(-1), tor.reshape(-1)
+
+
+def div_force(radius, l_of_j, S, dS):
+    """Divergence of a force (S, dS/dr), as const_sph_div_force: the fixed-field
+    rows of div_flux with the boundary nodes' own S values."""
+    nr = len(radius)
+    S2 = np.asarray(S).reshape(nr, -1)
+    return div_flux(radius, l_of_j, S, dS, fix_in=S2[0], fix_out=S2[-1])

@@ -67,3 +67,70 @@ def test_rot_uxb_oracle_on_quadratic_profiles():
     assert np.abs(tor[inner] - tor_ref[inner]).max() < 1e-9 * np.abs(tor_ref).max()
     assert np.allclose(dpol[0], (l + 1.0) / r[0] * T[0]) and np.allclose(dpol[-1], -l / r[-1] * T[-1])
     assert not tor[0].any() and not tor[-1].any()
+
+
+def _rot_force_case(bc, S, T):
+    from oracle.sph_div import rot_force
+    cfg = SphConfig(15, 24, 48, 9)
+    r = cfg.radius()
+    l, _ = rj_order(cfg.ltr)
+    dS = np.zeros_like(S)
+    out = rot_force(r, l, S.reshape(-1), dS.reshape(-1), T.reshape(-1), bc, bc)
+    g3 = np.where(l == 0, 0.5, l * (l + 1.0))
+    return r, g3, [x.reshape(len(r), -1) for x in out]
+
+
+def test_rot_force_non_slip_rows_exact_for_quadratics():
+    """Non-slip rows assume dS/dr = 0 on the boundary: d2S/dr2 = 2 for
+    S = (r - r_b)^2; the one-sided dT/dr is exact for T = r^2."""
+    cfg = SphConfig(15, 24, 48, 9)
+    r = cfg.radius()
+    ones = np.ones(cfg.J)
+    T = np.outer(r * r, ones)
+    for b in (0, -1):
+        S = np.outer((r - r[b]) ** 2, ones)
+        _, g3, (pol, dpol, tor) = _rot_force_case("non_slip", S, T)
+        assert np.array_equal(pol, T)
+        assert np.abs(dpol[b] - 2 * r[b]).max() < 1e-10
+        assert np.abs(tor[b] + 2.0).max() < 1e-9
+
+
+def test_rot_force_free_slip_rows_exact():
+    """Free-slip rows: d2S/dr2 exact for S = a r + c r^2 (S extrapolates to 0
+    at r = 0), dT/dr = 2 T / r on the boundary (T = r^2 exact)."""
+    cfg = SphConfig(15, 24, 48, 9)
+    r = cfg.radius()
+    ones = np.ones(cfg.J)
+    S = np.outer(0.3 * r + 1.7 * r * r, ones)
+    T = np.outer(r * r, ones)
+    _, g3, (pol, dpol, tor) = _rot_force_case("free_slip", S, T)
+    for b in (0, -1):
+        assert np.abs(dpol[b] - 2 * r[b]).max() < 1e-10
+        ref = -(2 * 1.7 - g3 / r[b] ** 2 * S[b])
+        assert np.abs(tor[b] - ref).max() < 1e-9 * np.abs(ref).max()
+
+
+def test_rot_force_interior_equals_rot_uxb():
+    from oracle.sph_div import rot_force, rot_uxb
+    cfg = SphConfig(15, 24, 48, 9)
+    r = cfg.radius()
+    l, _ = rj_order(cfg.ltr)
+    rng = np.random.default_rng(9)
+    S, dS, T = (rng.standard_normal(cfg.J * cfg.nr) for _ in range(3))
+    a = [x.reshape(cfg.nr, -1)[1:-1] for x in rot_force(r, l, S, dS, T)]
+    b = [x.reshape(cfg.nr, -1)[1:-1] for x in rot_uxb(r, l, S, dS, T)]
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+
+
+def test_div_force_uses_boundary_values():
+    from oracle.sph_div import div_force
+    cfg = SphConfig(15, 24, 48, 9)
+    r = cfg.radius()
+    l, _ = rj_order(cfg.ltr)
+    rng = np.random.default_rng(10)
+    a, b, c = (rng.standard_normal(cfg.J) for _ in range(3))
+    S = np.outer(np.ones_like(r), a) + np.outer(r, b) + np.outer(r * r, c)
+    dS = np.outer(np.ones_like(r), b) + np.outer(2 * r, c)
+    out = div_force(r, l, S.reshape(-1), dS.reshape(-1))
+    assert np.abs(out).max() < 1e-9 * np.abs(S).max() * (cfg.ltr + 1) ** 2

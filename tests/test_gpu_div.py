@@ -116,3 +116,88 @@ def test_induction_after_split_cycle():
     ref = rot_uxb(cfg.radius(), l, uxb[:, 0], uxb[:, 1], uxb[:, 2])
     for q in range(3):
         assert _relerr(got[:, q], ref[q]) <= 1e-13, q
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("bc_icb,bc_cmb,host", [(0, 0, False), (1, 1, False), (0, 1, True), (1, 0, False)],
+                         ids=["non_slip", "free_slip", "mixed_host", "free_in_non_slip_out"])
+def test_rot_force_matches_oracle(bc_icb, bc_cmb, host):
+    from kemorin_mhd_b200.sph_trans import SphTransform
+    from oracle.sph_div import FREE_SLIP, NON_SLIP, rot_force
+    cfg = CFG
+    tr = SphTransform(cfg, tier=TIER_FP64)
+    n = cfg.J * cfg.nr
+    rng = np.random.default_rng(13 + bc_icb + 2 * bc_cmb)
+    d = np.asfortranarray(rng.standard_normal((n, 6)))
+    l, _ = rj_order(cfg.ltr)
+    names = {0: NON_SLIP, 1: FREE_SLIP}
+    ref = rot_force(cfg.radius(), l, d[:, 0], d[:, 1], d[:, 2], names[bc_icb], names[bc_cmb])
+    if host:
+        arr = d.copy(order="F")
+        tr.rot_force(arr, 0, 3, bc_icb, bc_cmb)
+        got = arr[:, 3:6]
+        assert np.array_equal(arr[:, :3], d[:, :3])
+    else:
+        t = to_dev_fortran(d)
+        tr.rot_force(t, 0, 3, bc_icb, bc_cmb)
+        got = from_dev_fortran(t)[:, 3:6]
+    for q in range(3):
+        assert _relerr(got[:, q], ref[q]) <= 1e-13, q
+
+
+@pytest.mark.gpu
+def test_rot_force_rejects_unknown_condition():
+    import torch
+    from kemorin_mhd_b200.sph_trans import KmhdError, SphTransform
+    tr = SphTransform(CFG, tier=TIER_FP64)
+    t = torch.zeros((6, CFG.J * CFG.nr), dtype=torch.float64, device="cuda")
+    with pytest.raises(KmhdError):
+        tr.rot_force(t, 0, 3, 2, 0)
+    with pytest.raises(KmhdError):
+        tr.rot_force(t, 0, 2)      # overlapping columns
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("host", [False, True], ids=["device", "host"])
+def test_div_force_matches_oracle(host):
+    from kemorin_mhd_b200.sph_trans import SphTransform
+    from oracle.sph_div import div_force
+    cfg = CFG
+    tr = SphTransform(cfg, tier=TIER_FP64)
+    n = cfg.J * cfg.nr
+    rng = np.random.default_rng(17)
+    d = np.asfortranarray(rng.standard_normal((n, 3)))
+    l, _ = rj_order(cfg.ltr)
+    ref = div_force(cfg.radius(), l, d[:, 0], d[:, 1])
+    if host:
+        arr = d.copy(order="F")
+        tr.div_force(arr, 0, 2)
+        got = arr[:, 2]
+    else:
+        t = to_dev_fortran(d)
+        tr.div_force(t, 0, 2)
+        got = from_dev_fortran(t)[:, 2]
+    assert _relerr(got, ref) <= 1e-13
+
+
+@pytest.mark.gpu
+def test_vorticity_source_after_split_cycle():
+    """curl and div of the advection force omega x u (cycle columns 0-2),
+    non-slip boundaries, on the GPU against the oracle on the same spectra."""
+    import torch
+    from kemorin_mhd_b200.sph_trans import SphTransform
+    from oracle.sph_div import div_force, rot_force
+    cfg = CFG
+    tr = SphTransform(cfg, tier=TIER_SPLIT_I8)
+    d = to_dev_fortran(make_d_rj(cfg, seed=14))
+    out = torch.zeros((cfg.ncf + 4, cfg.J * cfg.nr), dtype=torch.float64, device="cuda")
+    tr.nonlinear_cycle(d, out)
+    adv = from_dev_fortran(out)[:, 0:3].copy()
+    tr.rot_force(out, 0, cfg.ncf)
+    tr.div_force(out, 0, cfg.ncf + 3)
+    res = from_dev_fortran(out)
+    l, _ = rj_order(cfg.ltr)
+    ref = rot_force(cfg.radius(), l, adv[:, 0], adv[:, 1], adv[:, 2])
+    for q in range(3):
+        assert _relerr(res[:, cfg.ncf + q], ref[q]) <= 1e-13, q
+    assert _relerr(res[:, cfg.ncf + 3], div_force(cfg.radius(), l, adv[:, 0], adv[:, 1])) <= 1e-13
