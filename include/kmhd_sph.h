@@ -249,6 +249,20 @@ int kmhd_sph_rot_force(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t co
 int kmhd_sph_div_force(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t col_fld, int32_t col_div,
                        int32_t ptr_kind);
 
+/* Curl of the Coriolis term for a rotation about z, formed in spectral space
+ * from the velocity (columns col_velo .. col_velo + 2 = S, dS/dr, T) and the
+ * vorticity (col_vort .. col_vort + 2): column col_out = poloidal and
+ * col_out + 2 = toroidal part of curl(-coef_cor z x u) by the Adams-Gaunt and
+ * Elsasser couplings of each mode to (l-1, m), (l+1, m) and (l, -m); column
+ * col_out + 1 is not written.  Replaces sum_coriolis_rlm with a fixed inner
+ * core (MHD_src/sph_MHD/t_coriolis_terms_rlm.f90:190-292:
+ * sum_rot_coriolis_rlm_10, sum_coriolis_terms_rlm.f90:94-189; the tables of
+ * init_sum_coriolis_rlm, interact_coriolis_rlm.f90) and the copy into the
+ * forward transform's output (copy_coriolis_terms_rlm).  The two written
+ * columns may not be input columns; host or device pointers. */
+int kmhd_sph_rot_coriolis(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t col_velo, int32_t col_vort,
+                          int32_t col_out, double coef_cor, int32_t ptr_kind);
+
 /* Legendre path the handle runs: 1 = the tier's split path, 0 = FP64 DMMA
  * (FP64 tier, or a split-tier handle the autotuner moved to FP64). */
 int kmhd_sph_get_path(const kmhd_sph *handle, int32_t *path);

@@ -220,6 +220,12 @@ struct RotBnd {
 // J*nr column each); coef as launch_div_flux, then ar1[nr] = 1/r and gl[J] = l.
 cudaError_t launch_rot_vec(long long J, int nr, const double* S, const double* dS, const double* T, double* pol,
                            double* dpol, double* tor, const double* coef, const RotBnd& b, cudaStream_t s);
+// Curl of the Coriolis term (kmhd_post.cu): vel and vort point at the S
+// columns of (S, dS/dr, T) triples with column stride ld; idx[4 J] coupled
+// modes, cf[12 J] coefficients, radius[nr] on the device.
+cudaError_t launch_rot_coriolis(long long J, int nr, const double* vel, const double* vort, long long ld,
+                                double* pol, double* tor, const int* idx, const double* cf, const double* radius,
+                                double coef_cor, cudaStream_t s);
 // Set-up of the on-the-fly tables (cos_t, pco, dco, pst, pseed of the plan).
 cudaError_t launch_otf_tables(const Plan& p, double* cos_t, double2* pco, double2* dco, double2* pst,
                               double* pseed, const long long* pseed_off, cudaStream_t s);

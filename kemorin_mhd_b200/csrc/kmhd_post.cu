@@ -1,7 +1,8 @@
 // kmhd_post.cu -- spectral post-processing after the forward transform: the
 // divergence of a flux vector's spectra (the reference's u.grad(T) term is
 // -div(u T), formed this way after sph_f_trans), the curl of u x B (the
-// induction term) and the curl and divergence of the momentum forces.
+// induction term), the curl and divergence of the momentum forces and the
+// curl of the Coriolis term.
 //
 // Interior rows as cal_sph_nod_vect_div2 (MHD_src/sph_MHD/cal_sph_exp_rotation.f90:254-290),
 // fixed-field boundary rows as cal_sph_div_flux_4_fix_in / _fix_out
@@ -63,6 +64,9 @@ __global__ void k_rot_vec(long long J, int nr, const double* __restrict__ S, con
     const int k = (int)(i / J);
     const long long j = i - (long long)k * J;
     const double t = T[i];
+    // g_sph_rj(j,3) = l(l+1), 0 at l = 0 (the rj copy has no l = 0 override;
+    // the coefficient array holds max(l(l+1), 1/2) for the divergence)
+    const double g3j = gl[j] > 0.0 ? g3[j] : 0.0;
     double dp, tr;
     if (k == 0) {
       if (b.insulating_in) {
@@ -71,7 +75,7 @@ __global__ void k_rot_vec(long long J, int nr, const double* __restrict__ S, con
       } else {
         const double d2s = b.s_in[0] * S[i] + b.s_in[1] * S[i + J];
         dp = b.t_in[0] * t + b.t_in[1] * T[i + J] + b.t_in[2] * T[i + 2 * J];
-        tr = -(d2s - g3[j] * ar2[0] * S[i]);
+        tr = -(d2s - g3j * ar2[0] * S[i]);
       }
     } else if (k == nr - 1) {
       if (b.insulating_out) {
@@ -80,16 +84,57 @@ __global__ void k_rot_vec(long long J, int nr, const double* __restrict__ S, con
       } else {
         const double d2s = b.s_out[1] * S[i - J] + b.s_out[0] * S[i];
         dp = b.t_out[2] * T[i - 2 * J] + b.t_out[1] * T[i - J] + b.t_out[0] * t;
-        tr = -(d2s - g3[j] * ar2[k] * S[i]);
+        tr = -(d2s - g3j * ar2[k] * S[i]);
       }
     } else {
       const double d1d = d1[3 * k] * dS[i - J] + d1[3 * k + 1] * dS[i] + d1[3 * k + 2] * dS[i + J];
       dp = d1[3 * k] * T[i - J] + d1[3 * k + 1] * t + d1[3 * k + 2] * T[i + J];
-      tr = -d1d + g3[j] * ar2[k] * S[i];
+      tr = -d1d + g3j * ar2[k] * S[i];
     }
     pol[i] = t;
     dpol[i] = dp;
     tor[i] = tr;
+  }
+}
+
+// Curl of the Coriolis term (pol, tor) from the velocity (vS, vdS, vT) and
+// vorticity (wS, wdS, wT) spectra, unit z rotation (r^2/2, r, 1) times
+// coef_cor, as sum_rot_coriolis_rlm_10
+// (MHD_src/sph_MHD/sum_coriolis_terms_rlm.f90:94-189).  One thread per mode j
+// over a range of radii, so the per-mode table -- coupled modes idx[4 j ..]
+// = (l-1, m), (l+1, m), (l, -m) and cf[12 j ..] = sw(1,1), sw(2,1), sw(1,3),
+// sw(1,2), sw(2,2), tw(1,1), tw(1,2), tw(1,3), tw(2,3), tw(1,4), tw(2,4),
+// g_sph_rlm(j,3) -- is read once; every radius's loads and stores are
+// coalesced over j (the coupled modes of consecutive j are consecutive).
+__global__ void k_rot_coriolis(long long J, int nr, int kchunk, const double* __restrict__ vS,
+                               const double* __restrict__ vdS, const double* __restrict__ wS,
+                               const double* __restrict__ wdS, const double* __restrict__ wT,
+                               double* __restrict__ pol, double* __restrict__ tor, const int* __restrict__ idx,
+                               const double* __restrict__ cf, const double* __restrict__ radius, double coef_cor) {
+  const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (j >= J) return;
+  const int4 q = reinterpret_cast<const int4*>(idx)[j];
+  const double* c = cf + 12 * j;
+  const double sw11 = c[0], sw21 = c[1], sw13 = c[2], sw12 = c[3], sw22 = c[4];
+  const double tw11 = c[5], tw12 = c[6], tw13 = c[7], tw23 = c[8], tw14 = c[9], tw24 = c[10], g3 = c[11];
+  const int k0 = blockIdx.y * kchunk, k1 = min(nr, k0 + kchunk);
+  for (int k = k0; k < k1; ++k) {
+    const long long o = (long long)k * J;
+    const double r = radius[k], ar = 1.0 / r;
+    const double w0 = 0.5 * r * r, w1 = r, w2 = 1.0;
+    const double dvp1 = vdS[o + q.x], dvp2 = vdS[o + q.y];
+    const double wp_l1 = wS[o + q.z];
+    const double vp1 = vS[o + q.x], vp2 = vS[o + q.y];
+    const double vp_l1 = vS[o + q.z];
+    const double d2vp_l1 = ar * ar * g3 * vp_l1 - wT[o + q.z];
+    const double wp1 = wS[o + q.x], wp2 = wS[o + q.y];
+    const double dwp1 = wdS[o + q.x] - 2.0 * ar * wp1;
+    const double dwp2 = wdS[o + q.y] - 2.0 * ar * wp2;
+    const double rp = sw11 * w0 * dvp1 + sw21 * w0 * dvp2 + sw13 * w0 * wp_l1 + sw12 * w1 * vp1 + sw22 * w1 * vp2;
+    const double rt = tw11 * w0 * d2vp_l1 - tw12 * w2 * vp_l1 + tw13 * w1 * wp1 + tw23 * w1 * wp2 + tw14 * w0 * dwp1 +
+                      tw24 * w0 * dwp2;
+    pol[o + j] = -coef_cor * rp * ar * ar;
+    tor[o + j] = -coef_cor * rt * ar * ar;
   }
 }
 
@@ -105,6 +150,25 @@ cudaError_t launch_rot_vec(long long J, int nr, const double* S, const double* d
   const int grid = (int)(want < 8LL * nsm ? want : 8LL * nsm);
   if (grid <= 0) return cudaSuccess;
   k_rot_vec<<<grid, 256, 0, s>>>(J, nr, S, dS, T, pol, dpol, tor, coef, b);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rot_coriolis(long long J, int nr, const double* vel, const double* vort, long long ld,
+                                double* pol, double* tor, const int* idx, const double* cf, const double* radius,
+                                double coef_cor, cudaStream_t s) {
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const long long jb = (J + 255) / 256;
+  if (jb <= 0 || nr <= 0) return cudaSuccess;
+  // enough blocks for 8 per SM; each block walks a contiguous range of radii
+  long long ks = (8LL * nsm + jb - 1) / jb;
+  if (ks > nr) ks = nr;
+  const int kchunk = (int)((nr + ks - 1) / ks);
+  const int ky = (nr + kchunk - 1) / kchunk;
+  k_rot_coriolis<<<dim3((unsigned)jb, (unsigned)ky), 256, 0, s>>>(J, nr, kchunk, vel, vel + ld, vort, vort + ld,
+                                                                   vort + 2 * ld, pol, tor, idx, cf, radius,
+                                                                   coef_cor);
   return cudaGetLastError();
 }
 

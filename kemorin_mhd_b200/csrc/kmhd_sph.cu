@@ -59,6 +59,9 @@ struct kmhd_sph {
   int* err = nullptr;  // device error word (bounded waits of the FFT and tcgen05 kernels)
   // divergence post-processing: FDM / normalisation coefficients, host-pointer staging
   double *div_coef = nullptr, *div_stage = nullptr, *rot_stage = nullptr;
+  // Coriolis curl: coupled modes (4 per j), coefficients (12 per j), staging
+  int* cor_idx = nullptr;
+  double *cor_cf = nullptr, *cor_stage = nullptr;
   std::vector<double> radius_h;
   std::vector<int> cols_b_cache, cols_f_cache;
   // host-pointer staging
@@ -897,6 +900,81 @@ int build_div_coef(kmhd_sph* h) {
   return KMHD_OK;
 }
 
+// Coriolis curl tables (per mode j of the rj order): the coupled modes and
+// the sw / tw coefficients of interact_rot_coriolis_rlm
+// (MHD_src/sph_MHD/interact_coriolis_rlm.f90), from the integrals of
+// cal_gaunt_coriolis_rlm (same file) in closed form for the rotation's degree
+// 1, order 0:
+//   K(1,0; l-1,m; l,m) = 4 sqrt(l^2 - m^2) / ((2l-1)(2l+1))        (l >= 2, |m| <= l-1),
+//   K(1,0; l+1,m; l,m) = 4 sqrt((l+1)^2 - m^2) / ((2l+1)(2l+3))    (l+1 <= L),
+//   L(1,0; l,-m; l,m)  = -4 m / (2l+1)                              (l >= 1),
+// with the mode itself (zero integral) where the partner does not exist and
+// every integral of l = 0 zero.  These equal the reference's prime-factor
+// evaluations (leadki / leadli, cal_gaunt_itgs.f90) to rounding; g3, g4, g5,
+// g17 are g_sph_rlm's l(l+1) (1/2 at l = 0), (l-1)l, (l+1)(l+2),
+// (2l+1)/(4l(l+1)) (0 at l = 0) (spherical_harmonics.f90:91-140).
+int build_coriolis(kmhd_sph* h) {
+  const Plan& p = h->plan;
+  const int L = p.L;
+  const long long J = p.J;
+  auto jof = [&](int l, int m) { return h->jmap_h[((size_t)std::abs(m) * 2 + (m < 0 ? 1 : 0)) * (L + 1) + l]; };
+  std::vector<int> idx(4 * (size_t)J, 0);
+  std::vector<double> cf(12 * (size_t)J, 0.0);
+  for (int am = 0; am <= L; ++am)
+    for (int slot = 0; slot < 2; ++slot) {
+      if (am == 0 && slot == 1) continue;
+      const int m = slot ? -am : am;
+      for (int l = am; l <= L; ++l) {
+        const int j = jof(l, m);
+        int k1 = j, k2 = j, ke = jof(0, 0);
+        double gi1 = 0.0, gi2 = 0.0, ei = 0.0;
+        const double dl = (double)l, dm = (double)m;
+        if (l >= 2 && am <= l - 1) {
+          gi1 = 4.0 * std::sqrt(dl * dl - dm * dm) / ((2.0 * dl - 1.0) * (2.0 * dl + 1.0));
+          k1 = jof(l - 1, m);
+        }
+        if (l + 1 <= L) {
+          gi2 = 4.0 * std::sqrt((dl + 1.0) * (dl + 1.0) - dm * dm) / ((2.0 * dl + 1.0) * (2.0 * dl + 3.0));
+          k2 = jof(l + 1, m);
+        }
+        if (l >= 1) {
+          ei = -4.0 * dm / (2.0 * dl + 1.0);
+          ke = jof(l, -m);
+        }
+        if (l == 0) {
+          k1 = k2 = ke = j;
+          gi2 = ei = 0.0;
+        }
+        const double g3 = l == 0 ? 0.5 : dl * (dl + 1.0);
+        const double g4 = (dl - 1.0) * dl, g5 = (dl + 1.0) * (dl + 2.0);
+        const double g17 = l == 0 ? 0.0 : (2.0 * dl + 1.0) / (4.0 * dl * (dl + 1.0));
+        int* q = idx.data() + 4 * (size_t)j;
+        q[0] = k1;
+        q[1] = k2;
+        q[2] = ke;
+        double* c = cf.data() + 12 * (size_t)j;
+        c[0] = (2.0 - g4 - g3) * gi1 * g17;                                         // sw(1,1)
+        c[1] = (2.0 - g5 - g3) * gi2 * g17;                                         // sw(2,1)
+        c[2] = 2.0 * ei * g17;                                                      // sw(1,3)
+        c[3] = g4 * (2.0 - g4 + g3) * gi1 * g17 * 0.5;                              // sw(1,2)
+        c[4] = g5 * (2.0 - g5 + g3) * gi2 * g17 * 0.5;                              // sw(2,2)
+        c[5] = -2.0 * ei * g17;                                                     // tw(1,1)
+        c[6] = -g3 * ei * g17;                                                      // tw(1,2)
+        c[7] = -(g3 * (2.0 + g4 - g3) + 2.0 * (-2.0 + g4 + g3)) * gi1 * g17 * 0.5;  // tw(1,3)
+        c[8] = -(g3 * (2.0 + g5 - g3) + 2.0 * (-2.0 + g5 + g3)) * gi2 * g17 * 0.5;  // tw(2,3)
+        c[9] = -(-2.0 + g4 + g3) * gi1 * g17;                                       // tw(1,4)
+        c[10] = -(-2.0 + g5 + g3) * gi2 * g17;                                      // tw(2,4)
+        c[11] = g3;
+      }
+    }
+  int st;
+  if ((st = dalloc(h, &h->cor_idx, idx.size())) || (st = dalloc(h, &h->cor_cf, cf.size()))) return st;
+  KCHECK(cudaMemcpyAsync(h->cor_idx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, h->stream));
+  KCHECK(cudaMemcpyAsync(h->cor_cf, cf.data(), sizeof(double) * cf.size(), cudaMemcpyHostToDevice, h->stream));
+  KCHECK(cudaStreamSynchronize(h->stream));
+  return KMHD_OK;
+}
+
 // Divergence of the vector in columns col_flux, col_flux + 1 into col_div;
 // own_bnd = 1 puts each boundary node's own S into the one-sided rows (the
 // force divergence), else fix_in / fix_out (NULL = zero).
@@ -1061,6 +1139,42 @@ int kmhd_sph_rot_force(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_fld, i
 
 int kmhd_sph_div_force(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_fld, int32_t col_div, int32_t ptr_kind) {
   return div_vec(h, d_rj, ld, col_fld, col_div, nullptr, nullptr, 1, ptr_kind);
+}
+
+int kmhd_sph_rot_coriolis(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_velo, int32_t col_vort,
+                          int32_t col_out, double coef_cor, int32_t ptr_kind) {
+  if (!h || !d_rj) return KMHD_ERR_ARG;
+  if (check_ld(h, ld)) return KMHD_ERR_ARG;
+  if (col_velo < 0 || col_vort < 0 || col_out < 0) return KMHD_ERR_ARG;
+  for (int q = 0; q < 3; q += 2) {  // the two written columns may not be inputs
+    const int c = col_out + q;
+    if ((c >= col_velo && c < col_velo + 3) || (c >= col_vort && c < col_vort + 3)) return KMHD_ERR_ARG;
+  }
+  const Plan& p = h->plan;
+  KCHECK(cudaSetDevice(h->device));
+  int st;
+  if (!h->cor_idx && (st = build_coriolis(h))) return st;
+  const size_t nrj = (size_t)p.J * p.nr;
+  if (ptr_kind == KMHD_PTR_HOST) {
+    if (!h->cor_stage && (st = dalloc(h, &h->cor_stage, 8 * nrj))) return st;
+    double* s0 = h->cor_stage;
+    for (int q = 0; q < 3; ++q) {
+      KCHECK(cudaMemcpyAsync(s0 + q * nrj, d_rj + ld * (col_velo + q), sizeof(double) * nrj, cudaMemcpyHostToDevice,
+                             h->stream));
+      KCHECK(cudaMemcpyAsync(s0 + (3 + q) * nrj, d_rj + ld * (col_vort + q), sizeof(double) * nrj,
+                             cudaMemcpyHostToDevice, h->stream));
+    }
+    KCHECK(launch_rot_coriolis(p.J, p.nr, s0, s0 + 3 * nrj, (long long)nrj, s0 + 6 * nrj, s0 + 7 * nrj, h->cor_idx,
+                               h->cor_cf, h->radius, coef_cor, h->stream));
+    KCHECK(cudaMemcpyAsync(d_rj + ld * col_out, s0 + 6 * nrj, sizeof(double) * nrj, cudaMemcpyDeviceToHost, h->stream));
+    KCHECK(cudaMemcpyAsync(d_rj + ld * (col_out + 2), s0 + 7 * nrj, sizeof(double) * nrj, cudaMemcpyDeviceToHost,
+                           h->stream));
+  } else {
+    KCHECK(launch_rot_coriolis(p.J, p.nr, d_rj + ld * col_velo, d_rj + ld * col_vort, ld, d_rj + ld * col_out,
+                               d_rj + ld * (col_out + 2), h->cor_idx, h->cor_cf, h->radius, coef_cor, h->stream));
+  }
+  KCHECK(cudaStreamSynchronize(h->stream));
+  return KMHD_OK;
 }
 
 int kmhd_sph_last_kernel_timing(kmhd_sph* h, double* ms5) {

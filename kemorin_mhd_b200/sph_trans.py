@@ -60,7 +60,8 @@ EXPORTS = ["kmhd_sph_create", "kmhd_sph_destroy", "kmhd_sph_set_stream", "kmhd_s
            "kmhd_sph_f_trans", "kmhd_sph_cycle", "kmhd_sph_batch_cycle", "kmhd_sph_last_timing",
            "kmhd_sph_get_tables", "kmhd_sph_device_bytes", "kmhd_strerror", "kmhd_sph_cycle_noalloc",
            "kmhd_sph_last_kernel_timing", "kmhd_sph_get_path", "kmhd_selftest_wait_timeout",
-           "kmhd_sph_div_flux", "kmhd_sph_rot_induction", "kmhd_sph_rot_force", "kmhd_sph_div_force"]
+           "kmhd_sph_div_flux", "kmhd_sph_rot_induction", "kmhd_sph_rot_force", "kmhd_sph_div_force",
+           "kmhd_sph_rot_coriolis"]
 
 _lib = None
 
@@ -92,6 +93,7 @@ def load_library(path: str | None = None):
     lib.kmhd_sph_rot_induction.argtypes = [vp, vp, i64, i32, i32, i32]
     lib.kmhd_sph_rot_force.argtypes = [vp, vp, i64, i32, i32, i32, i32, i32]
     lib.kmhd_sph_div_force.argtypes = [vp, vp, i64, i32, i32, i32]
+    lib.kmhd_sph_rot_coriolis.argtypes = [vp, vp, i64, i32, i32, i32, ctypes.c_double, i32]
     lib.kmhd_selftest_wait_timeout.argtypes = [ctypes.c_int, ctypes.c_int]
     lib.kmhd_sph_get_tables.argtypes = [vp, i32] + [ctypes.POINTER(ctypes.c_double)] * 4
     lib.kmhd_sph_device_bytes.restype = i64
@@ -284,6 +286,16 @@ class SphTransform:
         n = self.cfg.J * self.cfg.nr
         _check(load_library().kmhd_sph_div_force(self._h, p, ld or n, col_fld, col_div, kind),
                "kmhd_sph_div_force")
+        return d_rj
+
+    def rot_coriolis(self, d_rj, col_velo: int, col_vort: int, col_out: int, coef_cor: float,
+                     ld: int | None = None):
+        """Curl of the Coriolis term -coef_cor z x u: poloidal part into
+        col_out, toroidal part into col_out + 2 (col_out + 1 untouched)."""
+        p, kind = _ptr(d_rj)
+        n = self.cfg.J * self.cfg.nr
+        _check(load_library().kmhd_sph_rot_coriolis(self._h, p, ld or n, col_velo, col_vort, col_out,
+                                                    float(coef_cor), kind), "kmhd_sph_rot_coriolis")
         return d_rj
 
 

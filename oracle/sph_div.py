@@ -118,7 +118,10 @@ def rot_uxb(radius, l_of_j, S, dS, T):
     boundaries, as const_sph_rotation_uxb
     (MHD_src/sph_MHD/const_sph_rotation.f90:167-187): interior rows
     cal_sph_nod_vect_w_div_rot2 (cal_sph_exp_rotation.f90:207-248)
-        pol = T, dpol/dr = dT/dr (FDM), tor = -d(dS/dr)/dr (FDM) + g3 S / r^2;
+        pol = T, dpol/dr = dT/dr (FDM), tor = -d(dS/dr)/dr (FDM) + g3 S / r^2,
+    g3 = g_sph_rj(j,3) = l(l+1), 0 at l = 0: copy_sph_normalization_2_rj
+    (CORE_src/SPH_SPECTR_src/schmidt_poly_on_rtm_grid.f90:117-140) applies no
+    l = 0 override, unlike the rlm copy (:89-113);
     boundary rows cal_sph_nod_icb_ins_vp_rot2 (cal_sph_exp_nod_icb_ins.f90:135-160)
     and cal_sph_nod_cmb_ins_vp_rot2 (cal_sph_exp_nod_cmb_ins.f90:131-157):
         pol = T, dpol/dr = (l + 1) T / r (inner) or -l T / r (outer), tor = 0."""
@@ -128,7 +131,7 @@ def rot_uxb(radius, l_of_j, S, dS, T):
     dS = np.asarray(dS).reshape(nr, J)
     T = np.asarray(T).reshape(nr, J)
     l = np.asarray(l_of_j).astype(np.float64)
-    g3 = np.where(l == 0, 0.5, l * (l + 1.0))
+    g3 = l * (l + 1.0)  # g_sph_rj(j,3): 0 at l = 0 in the rj copy
     ar1 = 1.0 / r
     ar2 = ar1 ** 2
     d1, _, _ = fdm_coefs(r)
@@ -189,7 +192,7 @@ def rot_force(radius, l_of_j, S, dS, T, bc_icb=NON_SLIP, bc_cmb=NON_SLIP):
     S = np.asarray(S).reshape(nr, J)
     T = np.asarray(T).reshape(nr, J)
     l = np.asarray(l_of_j).astype(np.float64)
-    g3 = np.where(l == 0, 0.5, l * (l + 1.0))
+    g3 = l * (l + 1.0)  # g_sph_rj(j,3): 0 at l = 0 in the rj copy
     ar2 = (1.0 / r) ** 2
     s_in, t_in, s_out, t_out = velocity_bnd_coefs(r, bc_icb, bc_cmb)
     d2s = s_in[0] * S[0] + s_in[1] * S[1]

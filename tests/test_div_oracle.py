@@ -59,7 +59,7 @@ def test_rot_uxb_oracle_on_quadratic_profiles():
     dS = np.outer(one, b) + np.outer(r * r, c)         # d(dS)/dr = 2 c r
     T = np.outer(r * r, e)                              # dT/dr = 2 e r
     pol, dpol, tor = (x.reshape(len(r), -1) for x in rot_uxb(r, l, S.reshape(-1), dS.reshape(-1), T.reshape(-1)))
-    g3 = np.where(l == 0, 0.5, l * (l + 1.0))
+    g3 = l * (l + 1.0)
     assert np.array_equal(pol, T)
     inner = slice(1, len(r) - 1)
     assert np.abs(dpol[inner] - np.outer(2 * r, e)[inner]).max() < 1e-10
@@ -76,7 +76,7 @@ def _rot_force_case(bc, S, T):
     l, _ = rj_order(cfg.ltr)
     dS = np.zeros_like(S)
     out = rot_force(r, l, S.reshape(-1), dS.reshape(-1), T.reshape(-1), bc, bc)
-    g3 = np.where(l == 0, 0.5, l * (l + 1.0))
+    g3 = l * (l + 1.0)
     return r, g3, [x.reshape(len(r), -1) for x in out]
 
 
@@ -134,3 +134,22 @@ def test_div_force_uses_boundary_values():
     dS = np.outer(np.ones_like(r), b) + np.outer(2 * r, c)
     out = div_force(r, l, S.reshape(-1), dS.reshape(-1))
     assert np.abs(out).max() < 1e-9 * np.abs(S).max() * (cfg.ltr + 1) ** 2
+
+
+def test_curl_rows_use_zero_g3_at_degree_zero():
+    """The curl's g3 is g_sph_rj(j,3) = l(l+1) with no l = 0 override (0 there),
+    while the divergence takes max(g3, 1/2): the interior l = 0 toroidal row is
+    -d(dS)/dr (the force curl's boundary rows still see S through d2S/dr2)."""
+    from oracle.sph_div import rot_force, rot_uxb
+    cfg = SphConfig(7, 12, 24, 6)
+    r = cfg.radius()
+    l, _ = rj_order(cfg.ltr)
+    j0 = int(np.flatnonzero(l == 0)[0])
+    rng = np.random.default_rng(12)
+    S, dS, T = (rng.standard_normal(cfg.J * cfg.nr) for _ in range(3))
+    S2 = S.reshape(cfg.nr, -1).copy()
+    S2[:, j0] += 100.0                                   # the l = 0 S must not matter
+    for f in (rot_uxb, rot_force):
+        a = f(r, l, S, dS, T)[2].reshape(cfg.nr, -1)
+        b = f(r, l, S2.reshape(-1), dS, T)[2].reshape(cfg.nr, -1)
+        assert np.array_equal(a[1:-1, j0], b[1:-1, j0])

@@ -1,0 +1,83 @@
+"""Curl of the Coriolis term (kmhd_sph_rot_coriolis) against the CPU oracle
+of the reference's sum_rot_coriolis_rlm_10 with its Gaunt / Elsasser tables
+(oracle/sph_coriolis.py): max-norm relative error <= 1e-13, device and host
+pointers, the reference's mode order and a permuted one; the column that the
+reference leaves to the forward transform (col_out + 1) stays untouched."""
+import numpy as np
+import pytest
+
+from kemorin_mhd_b200.config import SphConfig, TIER_FP64, TIER_SPLIT_I8, rj_order
+from kemorin_mhd_b200.synthetic import make_d_rj
+from oracle.sph_coriolis import rot_coriolis
+from tests.gpu_util import to_dev_fortran, from_dev_fortran
+
+CFG = SphConfig(31, 48, 96, 9, name="L31")
+
+
+def _relerr(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("host,permuted", [(False, False), (True, False), (False, True)],
+                         ids=["device", "host", "permuted_order"])
+def test_rot_coriolis_matches_oracle(host, permuted):
+    from kemorin_mhd_b200.sph_trans import SphTransform
+    cfg = CFG
+    L, J, nr = cfg.ltr, cfg.J, cfg.nr
+    l, m = rj_order(L)
+    perm = np.random.default_rng(3).permutation(J) if permuted else np.arange(J)
+    lp, mp = l[perm], m[perm]
+    tr = SphTransform(cfg, tier=TIER_FP64, idx_rj_lm=np.stack([lp, mp], 1).reshape(-1) if permuted else None)
+    rng = np.random.default_rng(21)
+    d = np.asfortranarray(rng.standard_normal((J * nr, 9)))
+    coef = 2.5e3
+    r = cfg.radius()
+    ref_pol, ref_tor = rot_coriolis(r, L, lp, mp, [d[:, q] for q in range(3)], [d[:, 3 + q] for q in range(3)], coef)
+    if host:
+        arr = d.copy(order="F")
+        tr.rot_coriolis(arr, 0, 3, 6, coef)
+        got = arr
+    else:
+        t = to_dev_fortran(d)
+        tr.rot_coriolis(t, 0, 3, 6, coef)
+        got = from_dev_fortran(t)
+    assert np.array_equal(got[:, :6], d[:, :6])
+    assert np.array_equal(got[:, 7], d[:, 7])          # dpol/dr column not written
+    assert _relerr(got[:, 6], ref_pol) <= 1e-13
+    assert _relerr(got[:, 8], ref_tor) <= 1e-13
+
+
+@pytest.mark.gpu
+def test_rot_coriolis_rejects_output_over_inputs():
+    import torch
+    from kemorin_mhd_b200.sph_trans import KmhdError, SphTransform
+    tr = SphTransform(CFG, tier=TIER_FP64)
+    t = torch.zeros((9, CFG.J * CFG.nr), dtype=torch.float64, device="cuda")
+    for col_out in (1, 3, 5):
+        with pytest.raises(KmhdError):
+            tr.rot_coriolis(t, 0, 3, col_out, 1.0)
+
+
+@pytest.mark.gpu
+def test_rot_coriolis_on_cycle_inputs():
+    """On a split-tier handle, after a cycle: the curl of the Coriolis term
+    of the cycle's own velocity and vorticity spectra (synthetic dynamo-like
+    profiles) against the oracle."""
+    import torch
+    from kemorin_mhd_b200.sph_trans import SphTransform
+    cfg = CFG
+    tr = SphTransform(cfg, tier=TIER_SPLIT_I8)
+    d_np = make_d_rj(cfg, seed=41)                   # columns: u (0-2), omega (3-5), B (6-8), T (9)
+    d = to_dev_fortran(d_np)
+    out = torch.zeros((cfg.ncf + 3, cfg.J * cfg.nr), dtype=torch.float64, device="cuda")
+    tr.nonlinear_cycle(d, out)
+    cor = torch.zeros((3, cfg.J * cfg.nr), dtype=torch.float64, device="cuda")
+    both = torch.cat([d, cor], 0)                    # velocity, vorticity, ..., output columns 10-12
+    tr.rot_coriolis(both, 0, 3, cfg.ncb, 1.0e2)
+    got = from_dev_fortran(both)
+    l, m = rj_order(cfg.ltr)
+    ref_pol, ref_tor = rot_coriolis(cfg.radius(), cfg.ltr, l, m, [d_np[:, q] for q in range(3)],
+                                    [d_np[:, 3 + q] for q in range(3)], 1.0e2)
+    assert _relerr(got[:, cfg.ncb], ref_pol) <= 1e-13
+    assert _relerr(got[:, cfg.ncb + 2], ref_tor) <= 1e-13
