@@ -263,6 +263,21 @@ int kmhd_sph_div_force(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t co
 int kmhd_sph_rot_coriolis(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t col_velo, int32_t col_vort,
                           int32_t col_out, double coef_cor, int32_t ptr_kind);
 
+/* Makes every following kmhd_sph_cycle / kmhd_sph_batch_cycle of the handle
+ * also write the curl of the Coriolis term, as the reference's
+ * sph_b_trans_w_coriolis / sph_f_trans_w_coriolis do (sum_coriolis_rlm on the
+ * received spectra, copy_coriolis_terms_rlm into the forward output;
+ * MHD_src/sph_MHD/sph_trans_w_coriols.f90:113-246): the velocity and vorticity
+ * are backward vector fields iv_velo and iv_vort (0-based among the nvector_b
+ * vectors, read through that call's cols_b); the poloidal part goes to output
+ * column col_out and the toroidal part to col_out + 2 of d_rj_out (col_out + 1
+ * is not written).  With host pointers the inputs are read from the cycle's
+ * own staged copies (no second transfer).  The two columns may not be written
+ * by a forward field, nor be input columns when input and output are one
+ * array (KMHD_ERR_ARG at the cycle call).  iv_velo < 0 switches it off.  The
+ * tables are built here (device memory), not inside the cycle. */
+int kmhd_sph_set_coriolis(kmhd_sph *handle, double coef_cor, int32_t iv_velo, int32_t iv_vort, int32_t col_out);
+
 /* Legendre path the handle runs: 1 = the tier's split path, 0 = FP64 DMMA
  * (FP64 tier, or a split-tier handle the autotuner moved to FP64). */
 int kmhd_sph_get_path(const kmhd_sph *handle, int32_t *path);

@@ -62,6 +62,11 @@ struct kmhd_sph {
   // Coriolis curl: coupled modes (4 per j), coefficients (12 per j), staging
   int* cor_idx = nullptr;
   double *cor_cf = nullptr, *cor_stage = nullptr;
+  // Coriolis curl inside the cycle (kmhd_sph_set_coriolis): backward vector
+  // indices of velocity and vorticity, output column, coefficient
+  int cor_on = 0, cor_iv_velo = 0, cor_iv_vort = 0, cor_col = 0;
+  double cor_coef = 0.0;
+  double* cor_cyc = nullptr;  // 2 J*Nr staging columns for host-pointer cycles
   std::vector<double> radius_h;
   std::vector<int> cols_b_cache, cols_f_cache;
   // host-pointer staging
@@ -580,6 +585,42 @@ int check_dev_err(kmhd_sph* h) {
   return v;
 }
 
+// The registered Coriolis curl of radii [r0, r1): vel / vort point at the S
+// columns of the velocity and vorticity triples (column stride ld), pol / tor
+// at the two output columns; every pointer is the full-radius column base.
+int enqueue_coriolis(kmhd_sph* h, const double* vel, const double* vort, int64_t ld, double* pol, double* tor,
+                     int r0, int r1, cudaStream_t s) {
+  const long long o = h->plan.J * (long long)r0;
+  KCHECK(launch_rot_coriolis(h->plan.J, r1 - r0, vel + o, vort + o, ld, pol + o, tor + o, h->cor_idx, h->cor_cf,
+                             h->radius + r0, h->cor_coef, s));
+  return KMHD_OK;
+}
+
+// The registered Coriolis curl of a device-pointer cycle (all radii).
+int enqueue_coriolis_dev(kmhd_sph* h, const double* in, int64_t ld_in, const int32_t* cols_b, double* out,
+                         int64_t ld_out) {
+  if (!h->cor_on) return KMHD_OK;
+  return enqueue_coriolis(h, in + ld_in * cols_b[h->cor_iv_velo], in + ld_in * cols_b[h->cor_iv_vort], ld_in,
+                          out + ld_out * h->cor_col, out + ld_out * (h->cor_col + 2), 0, h->plan.nr, h->stream);
+}
+
+// Column checks of a cycle with the Coriolis curl registered: its two output
+// columns may not be written by the forward fields, nor be input columns of
+// the cycle when input and output are one array.
+int check_coriolis_cols(const kmhd_sph* h, const double* in, int64_t ld_in, const int32_t* cols_b, const double* out,
+                        int64_t ld_out, const int32_t* cols_f) {
+  const Plan& p = h->plan;
+  for (int q = 0; q < 3; q += 2) {
+    const int c = h->cor_col + q;
+    for (int f = 0; f < p.nvf + p.nsf; ++f)
+      if (c >= cols_f[f] && c < cols_f[f] + (f < p.nvf ? 3 : 1)) return KMHD_ERR_ARG;
+    if (in == out && ld_in == ld_out)
+      for (int f = 0; f < p.nvb + p.nsb; ++f)
+        if (c >= cols_b[f] && c < cols_b[f] + (f < p.nvb ? 3 : 1)) return KMHD_ERR_ARG;
+  }
+  return KMHD_OK;
+}
+
 // Host-pointer cycle over the radial chunks.  Every stage is independent per
 // radius, so chunk c's kernels run on the handle's stream while chunk c + 1's
 // spectra come in on s_in and chunk c - 1's results go out on s_out.  The
@@ -601,6 +642,7 @@ int cycle_host_chunked(kmhd_sph* h, const double* d_rj_in, int64_t ld_in, const 
   int st;
   if (!h->stage_in && (st = dalloc(h, &h->stage_in, nrj * std::max(p.ncb, p.ncf)))) return st;
   if (!h->stage_out && (st = dalloc(h, &h->stage_out, nrj * std::max(p.ncf, 1)))) return st;
+  if (h->cor_on && !h->cor_cyc && (st = dalloc(h, &h->cor_cyc, 2 * nrj))) return st;
   std::vector<int> cb(p.nvb + p.nsb), cf(p.nvf + p.nsf);
   for (int f = 0; f < p.nvb + p.nsb; ++f) cb[f] = f < p.nvb ? 3 * f : 3 * p.nvb + (f - p.nvb);
   for (int f = 0; f < p.nvf + p.nsf; ++f) cf[f] = f < p.nvf ? 3 * f : 3 * p.nvf + (f - p.nvf);
@@ -623,6 +665,10 @@ int cycle_host_chunked(kmhd_sph* h, const double* d_rj_in, int64_t ld_in, const 
     w.r_lo = h->chunks[c];
     w.r_hi = h->chunks[c + 1];
     KCHECK(cudaStreamWaitEvent(h->stream, h->ev_in[c], 0));
+    if (h->cor_on &&
+        (st = enqueue_coriolis(h, h->stage_in + nrj * cb[h->cor_iv_velo], h->stage_in + nrj * cb[h->cor_iv_vort],
+                               (int64_t)nrj, h->cor_cyc, h->cor_cyc + nrj, w.r_lo, w.r_hi, h->stream)))
+      return st;
     if ((st = run_bwd_spectral(h, h->stage_in, (int64_t)nrj, false, &w))) return st;
     KCHECK(launch_fft_cycle(w, h->stream));
     if ((st = run_fwd_spectral(h, h->stage_out, (int64_t)nrj, false, &w))) return st;
@@ -633,6 +679,10 @@ int cycle_host_chunked(kmhd_sph* h, const double* d_rj_in, int64_t ld_in, const 
     for (int f = 0; f < p.nvf + p.nsf; ++f)
       for (int q = 0; q < (f < p.nvf ? 3 : 1); ++q)
         KCHECK(cudaMemcpyAsync(d_rj_out + ld_out * (cols_f[f] + q) + o, h->stage_out + nrj * (cf[f] + q) + o, bytes,
+                               cudaMemcpyDeviceToHost, h->s_out));
+    if (h->cor_on)
+      for (int q = 0; q < 2; ++q)
+        KCHECK(cudaMemcpyAsync(d_rj_out + ld_out * (h->cor_col + 2 * q) + o, h->cor_cyc + nrj * q + o, bytes,
                                cudaMemcpyDeviceToHost, h->s_out));
   }
   KCHECK(cudaEventRecord(h->ev[1], h->s_out));
@@ -781,6 +831,7 @@ int kmhd_sph_cycle(kmhd_sph* h, const double* d_rj_in, int64_t ld_in, const int3
   int64_t old = ld_out;
   std::vector<int> cb, cf(p.nvf + p.nsf);
   int st;
+  if (h->cor_on && (st = check_coriolis_cols(h, d_rj_in, ld_in, cols_b, d_rj_out, ld_out, cols_f))) return st;
   if (ptr_kind == KMHD_PTR_HOST && h->chunks.size() > 2)
     return cycle_host_chunked(h, d_rj_in, ld_in, cols_b, d_rj_out, ld_out, cols_f);
   if (ptr_kind == KMHD_PTR_HOST) {
@@ -795,7 +846,26 @@ int kmhd_sph_cycle(kmhd_sph* h, const double* d_rj_in, int64_t ld_in, const int3
     if ((st = sync_cols(h, cols_b, p.nvb + p.nsb, h->cols_b_cache, h->cols_b_d))) return st;
     if ((st = sync_cols(h, cols_f, p.nvf + p.nsf, h->cols_f_cache, h->cols_f_d))) return st;
   }
+  double *cor_pol = nullptr, *cor_tor = nullptr;
+  if (h->cor_on) {
+    if (ptr_kind == KMHD_PTR_HOST) {
+      if (!h->cor_cyc && (st = dalloc(h, &h->cor_cyc, 2 * nrj))) return st;
+      cor_pol = h->cor_cyc;
+      cor_tor = h->cor_cyc + nrj;
+    } else {
+      cor_pol = d_rj_out + ld_out * h->cor_col;
+      cor_tor = d_rj_out + ld_out * (h->cor_col + 2);
+    }
+  }
   if ((st = timed_begin(h))) return st;
+  // the Coriolis curl reads only the inputs: it runs before the forward
+  // stage can write output columns that share the input array
+  if (h->cor_on) {
+    const int iv = ptr_kind == KMHD_PTR_HOST ? cb[h->cor_iv_velo] : cols_b[h->cor_iv_velo];
+    const int iw = ptr_kind == KMHD_PTR_HOST ? cb[h->cor_iv_vort] : cols_b[h->cor_iv_vort];
+    if ((st = enqueue_coriolis(h, src + sld * iv, src + sld * iw, sld, cor_pol, cor_tor, 0, p.nr, h->stream)))
+      return st;
+  }
   if ((st = run_bwd_spectral(h, src, sld))) return st;
   KCHECK(cudaEventRecord(h->ev[1], h->stream));
   KCHECK(launch_fft_cycle(p, h->stream));
@@ -809,6 +879,10 @@ int kmhd_sph_cycle(kmhd_sph* h, const double* d_rj_in, int64_t ld_in, const int3
         KCHECK(cudaMemcpyAsync(d_rj_out + ld_out * (cols_f[f] + q), out + nrj * (cf[f] + q),
                                sizeof(double) * nrj, cudaMemcpyDeviceToHost, h->stream));
     }
+    if (h->cor_on)
+      for (int q = 0; q < 2; ++q)
+        KCHECK(cudaMemcpyAsync(d_rj_out + ld_out * (h->cor_col + 2 * q), h->cor_cyc + nrj * q,
+                               sizeof(double) * nrj, cudaMemcpyDeviceToHost, h->stream));
   }
   KCHECK(cudaStreamSynchronize(h->stream));
   if ((st = finish_timing(h))) return st;
@@ -1177,6 +1251,25 @@ int kmhd_sph_rot_coriolis(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_vel
   return KMHD_OK;
 }
 
+int kmhd_sph_set_coriolis(kmhd_sph* h, double coef_cor, int32_t iv_velo, int32_t iv_vort, int32_t col_out) {
+  if (!h) return KMHD_ERR_ARG;
+  if (iv_velo < 0) {
+    h->cor_on = 0;
+    return KMHD_OK;
+  }
+  const Plan& p = h->plan;
+  if (iv_velo >= p.nvb || iv_vort < 0 || iv_vort >= p.nvb || iv_vort == iv_velo || col_out < 0) return KMHD_ERR_ARG;
+  KCHECK(cudaSetDevice(h->device));
+  int st;
+  if (!h->cor_idx && (st = build_coriolis(h))) return st;
+  h->cor_iv_velo = iv_velo;
+  h->cor_iv_vort = iv_vort;
+  h->cor_col = col_out;
+  h->cor_coef = coef_cor;
+  h->cor_on = 1;
+  return KMHD_OK;
+}
+
 int kmhd_sph_last_kernel_timing(kmhd_sph* h, double* ms5) {
   if (!h || !ms5) return KMHD_ERR_ARG;
   if (!h->kernel_timed) return KMHD_ERR_STATE;
@@ -1259,10 +1352,11 @@ int autotune_path(kmhd_sph* h, const double* in, int64_t ld_in, double* out, int
   return KMHD_OK;
 }
 
-int batch_direct(kmhd_sph** hs, int32_t n, const double* const* in, const int64_t* ld_in, double* const* out,
-                 const int64_t* ld_out) {
+int batch_direct(kmhd_sph** hs, int32_t n, const double* const* in, const int64_t* ld_in,
+                 const int32_t* const* cols_b, double* const* out, const int64_t* ld_out) {
   for (int i = 0; i < n; ++i) {
-    const int st = enqueue_cycle(hs[i], in[i], ld_in[i], out[i], ld_out[i]);
+    int st = enqueue_coriolis_dev(hs[i], in[i], ld_in[i], cols_b[i], out[i], ld_out[i]);
+    if (!st) st = enqueue_cycle(hs[i], in[i], ld_in[i], out[i], ld_out[i]);
     if (st) return st;
   }
   for (int i = 0; i < n; ++i) KCHECK(cudaStreamSynchronize(hs[i]->stream));
@@ -1283,6 +1377,8 @@ int batch_cycle_impl(kmhd_sph** hs, int32_t n, const double* const* d_rj_in, con
     if (h->device != hs[0]->device) return KMHD_ERR_ARG;
     if (check_ld(h, ld_in[i]) || check_ld(h, ld_out[i])) return KMHD_ERR_ARG;
     if (h->plan.ncf == 0 || h->plan.nprod == 0) return KMHD_ERR_STATE;
+    if (h->cor_on && (st = check_coriolis_cols(h, d_rj_in[i], ld_in[i], cols_b[i], d_rj_out[i], ld_out[i], cols_f[i])))
+      return st;
   }
   KCHECK(cudaSetDevice(hs[0]->device));
   // column tables to the device (may synchronise: before any capture)
@@ -1301,7 +1397,7 @@ int batch_cycle_impl(kmhd_sph** hs, int32_t n, const double* const* d_rj_in, con
   for (int i = 0; i < n; ++i)
     if (hs[i]->stream == nullptr || hs[i]->stream == cudaStreamLegacy) capturable = false;
   if (!capturable) {
-    if ((st = batch_direct(hs, n, d_rj_in, ld_in, d_rj_out, ld_out))) return st;
+    if ((st = batch_direct(hs, n, d_rj_in, ld_in, cols_b, d_rj_out, ld_out))) return st;
   } else {
     std::vector<const void*> sig;
     std::vector<int64_t> sig_ld;
@@ -1313,6 +1409,13 @@ int batch_cycle_impl(kmhd_sph** hs, int32_t n, const double* const* d_rj_in, con
       sig.push_back(hs[i]->stream);
       sig_ld.push_back(ld_in[i]);
       sig_ld.push_back(ld_out[i]);
+      // the Coriolis launch's arguments are captured too
+      int64_t cbits = 0;
+      std::memcpy(&cbits, &hs[i]->cor_coef, sizeof(cbits));
+      sig_ld.push_back(hs[i]->cor_on ? cbits : 0);
+      sig_ld.push_back(hs[i]->cor_on ? (int64_t)hs[i]->cor_col * 4096 + hs[i]->cor_iv_velo * 64 + hs[i]->cor_iv_vort + 1
+                                     : 0);
+      sig_ld.push_back(hs[i]->cor_on ? cols_b[i][hs[i]->cor_iv_velo] * 65536LL + cols_b[i][hs[i]->cor_iv_vort] : 0);
     }
     kmhd_sph* h0 = hs[0];
     if (!h0->batch) h0->batch = new BatchGraph();
@@ -1376,6 +1479,7 @@ int batch_cycle_impl(kmhd_sph** hs, int32_t n, const double* const* d_rj_in, con
       for (int i = 0; i < n && cst == KMHD_OK; ++i) {
         if (grouped[i]) continue;
         ck(cudaStreamWaitEvent(hs[i]->stream, bg->fork, 0));
+        if (cst == KMHD_OK) cst = enqueue_coriolis_dev(hs[i], d_rj_in[i], ld_in[i], cols_b[i], d_rj_out[i], ld_out[i]);
         if (cst == KMHD_OK) cst = enqueue_cycle(hs[i], d_rj_in[i], ld_in[i], d_rj_out[i], ld_out[i]);
         ck(cudaEventRecord(bg->join[i], hs[i]->stream));
         ck(cudaStreamWaitEvent(bg->s0, bg->join[i], 0));
@@ -1390,6 +1494,7 @@ int batch_cycle_impl(kmhd_sph** hs, int32_t n, const double* const* d_rj_in, con
         for (int i : grp[k]) {
           kmhd_sph* h = hs[i];
           ck(cudaStreamWaitEvent(h->stream, bg->fork, 0));
+          if (cst == KMHD_OK) cst = enqueue_coriolis_dev(h, d_rj_in[i], ld_in[i], cols_b[i], d_rj_out[i], ld_out[i]);
           if (cst == KMHD_OK) cst = split_slicer(h->split, h->plan, false, d_rj_in[i], ld_in[i], h->cols_b_d, h->stream);
           ck(cudaEventRecord(bg->ev[2 * i], h->stream));
           ck(cudaStreamWaitEvent(g, bg->ev[2 * i], 0));
@@ -1428,7 +1533,7 @@ int batch_cycle_impl(kmhd_sph** hs, int32_t n, const double* const* d_rj_in, con
     if (bg->exec) {
       KCHECK(cudaGraphLaunch(bg->exec, bg->s0));
       KCHECK(cudaStreamSynchronize(bg->s0));
-    } else if ((st = batch_direct(hs, n, d_rj_in, ld_in, d_rj_out, ld_out))) {
+    } else if ((st = batch_direct(hs, n, d_rj_in, ld_in, cols_b, d_rj_out, ld_out))) {
       return st;
     }
   }

@@ -61,7 +61,7 @@ EXPORTS = ["kmhd_sph_create", "kmhd_sph_destroy", "kmhd_sph_set_stream", "kmhd_s
            "kmhd_sph_get_tables", "kmhd_sph_device_bytes", "kmhd_strerror", "kmhd_sph_cycle_noalloc",
            "kmhd_sph_last_kernel_timing", "kmhd_sph_get_path", "kmhd_selftest_wait_timeout",
            "kmhd_sph_div_flux", "kmhd_sph_rot_induction", "kmhd_sph_rot_force", "kmhd_sph_div_force",
-           "kmhd_sph_rot_coriolis"]
+           "kmhd_sph_rot_coriolis", "kmhd_sph_set_coriolis"]
 
 _lib = None
 
@@ -94,6 +94,7 @@ def load_library(path: str | None = None):
     lib.kmhd_sph_rot_force.argtypes = [vp, vp, i64, i32, i32, i32, i32, i32]
     lib.kmhd_sph_div_force.argtypes = [vp, vp, i64, i32, i32, i32]
     lib.kmhd_sph_rot_coriolis.argtypes = [vp, vp, i64, i32, i32, i32, ctypes.c_double, i32]
+    lib.kmhd_sph_set_coriolis.argtypes = [vp, ctypes.c_double, i32, i32, i32]
     lib.kmhd_selftest_wait_timeout.argtypes = [ctypes.c_int, ctypes.c_int]
     lib.kmhd_sph_get_tables.argtypes = [vp, i32] + [ctypes.POINTER(ctypes.c_double)] * 4
     lib.kmhd_sph_device_bytes.restype = i64
@@ -297,6 +298,13 @@ class SphTransform:
         _check(load_library().kmhd_sph_rot_coriolis(self._h, p, ld or n, col_velo, col_vort, col_out,
                                                     float(coef_cor), kind), "kmhd_sph_rot_coriolis")
         return d_rj
+
+    def set_coriolis(self, coef_cor: float, iv_velo: int = 0, iv_vort: int = 1, col_out: int = -1):
+        """Every following cycle also writes the curl of the Coriolis term of
+        backward vectors iv_velo / iv_vort into output columns col_out (pol)
+        and col_out + 2 (tor); iv_velo < 0 switches it off."""
+        _check(load_library().kmhd_sph_set_coriolis(self._h, float(coef_cor), iv_velo, iv_vort, col_out),
+               "kmhd_sph_set_coriolis")
 
 
 def batch_cycle(transforms: Sequence[SphTransform], d_in, d_out):
