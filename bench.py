@@ -355,6 +355,18 @@ def main():
     roof["algorithmic_flops_per_launch"] = flops
     roof["ms_per_launch"] = dur
 
+    # the largest single launch of the cycle: the fused FFT + products kernel,
+    # bounded by HBM (it reads the backward rtm records and writes the forward
+    # ones once: Nr*Ntheta*(L+1)*2*(ncb+ncf) doubles per launch)
+    fft_bytes = 8.0 * cfg.nr * cfg.nth * (cfg.ltr + 1) * 2 * (cfg.ncb + cfg.ncf)
+    dur_fft = kern["fft_nl"]
+    roof_fft = {"bound": "hbm", "kernel": "k_fft_cycle_f", "unit": "GB/s",
+                "achieved": fft_bytes / (dur_fft * 1e-3) / 1e9 if dur_fft > 0 else None,
+                "peak": peaks["hbm_gbs"], "peak_source": f"hbm_gbs of {psrc} MEASURED_PEAKS.json",
+                "algorithmic_bytes_per_launch": fft_bytes, "ms_per_launch": dur_fft,
+                "traffic": read_traffic("k_fft_cycle_f", cfg.name)}
+    roof_fft["frac"] = roof_fft["achieved"] / roof_fft["peak"] if roof_fft["achieved"] else None
+
     # end to end through the public API with pinned host buffers
     e2e = None
     if not args.no_e2e and not args.p_on_the_fly:  # (the on-the-fly handle is closed by now)
@@ -393,7 +405,8 @@ def main():
                    "fields_bwd": "u,omega,B + T", "fields_fwd": "omega x u, u x B, u T + u.omega",
                    "parallelism": f"radial-instance x{ws} (no collective)",
                    "l2": "inputs larger than L2 (d_rj 5.4 GB, rtm 16 GB per direction)"},
-        "stages_ms": stage, "kernels_ms": kern, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+        "stages_ms": stage, "kernels_ms": kern, "roofline": roof, "roofline_fft": roof_fft,
+        "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": launches * args.steps, "clocks": clk,
     }
     line.update(extra)
