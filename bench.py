@@ -539,9 +539,10 @@ def split_executed_ops(cfg, nprod):
     for m in range(L + 1):
         ke, ko = (L - m) // 2 + 1, (L - m + 1) // 2
         kep, kop, nhp = pad(ke, 32), pad(ko, 32), pad(nh, 32)
+        gb, gf = (cfg.nvb + cfg.nsb + 3) // 4, (cfg.nvf + cfg.nsf + 3) // 4  # 8-column blocks per radius
         geo = {0: (nh, kop + kep, 4 * cfg.nvb * nrT), 1: (nh, kep + kop, 4 * cfg.nvb * nrT),
-               2: (nh, kep, 8 * nrR), 3: (nh, kop, 8 * nrR),
-               4: (ke, nhp, 8 * nrR), 5: (ko, nhp, 8 * nrR),
+               2: (nh, kep, 8 * nrR * gb), 3: (nh, kop, 8 * nrR * gb),
+               4: (ke, nhp, 8 * nrR * gf), 5: (ko, nhp, 8 * nrR * gf),
                6: (ke, 2 * nhp, 4 * cfg.nvf * nrT), 7: (ko, 2 * nhp, 4 * cfg.nvf * nrT)}
         for t, (rows, kp, ncol) in geo.items():
             if rows == 0 or ncol == 0:

@@ -244,7 +244,7 @@ __global__ void k_a_slices(Plan P, SliceTabs S, int t) {
 // Slicers.  Column list of one (m, r): backward: for each vector v: types 0/1
 // quantity q (8 columns), for each field f < 4: types 2/3 slots (4 columns);
 // forward: types 4/5 (field f, slot) and types 6/7 (vector v, quantity q).
-constexpr int kGrpCols = 16;  // derived columns of one slicer field group (at most 4 fields x 2 slots x 2 types)
+constexpr int kGrpCols = 24;  // derived columns of one slicer field group (at most 6 fields x 2 slots x 2 types)
 // slicer CTA size (measured at L = 511: 256 threads 14.2 ms, 384 18.6 ms,
 // 512 15.0 ms for the forward slicer)
 constexpr int kSliceThreads = 256;
@@ -255,6 +255,15 @@ struct ColRef {
   int f, q;       // field (vector or scalar slot) and quantity/slot selector
 };
 
+// Columns of the radial-component / scalar types (2..5): one 8-column block
+// per (group of four fields, radius), group-major like the vector types'
+// (vector, radius) blocks: field f, slot s of radius r is column
+// ((f / 4) nrR + r) 8 + 2 (f % 4) + s.
+__host__ __device__ __forceinline__ int rs_col(const SliceTabs& S, int r, int f, int slot) {
+  return (((f >> 2) * S.nrR + r) * 4 + (f & 3)) * 2 + slot;
+}
+__host__ __device__ __forceinline__ int rs_groups(int nF) { return (nF + 3) >> 2; }
+
 __device__ __forceinline__ ColRef colref_bwd(const Plan& P, const SliceTabs& S, int r, int i) {
   ColRef c;
   if (i < 8 * P.nvb) {
@@ -262,7 +271,7 @@ __device__ __forceinline__ ColRef colref_bwd(const Plan& P, const SliceTabs& S, 
     c.t = t; c.f = v; c.q = q; c.col = (v * S.nrT + r) * 4 + q;
   } else {
     const int j = i - 8 * P.nvb, f = j >> 2, t = 2 + ((j >> 1) & 1), slot = j & 1;
-    c.t = t; c.f = f; c.q = slot; c.col = (r * 4 + f) * 2 + slot;
+    c.t = t; c.f = f; c.q = slot; c.col = rs_col(S, r, f, slot);
   }
   return c;
 }
@@ -271,7 +280,7 @@ __device__ __forceinline__ ColRef colref_fwd(const Plan& P, const SliceTabs& S, 
   const int nf1 = 4 * (P.nvf + P.nsf);
   if (i < nf1) {
     const int f = i >> 2, t = 4 + ((i >> 1) & 1), slot = i & 1;
-    c.t = t; c.f = f; c.q = slot; c.col = (r * 4 + f) * 2 + slot;
+    c.t = t; c.f = f; c.q = slot; c.col = rs_col(S, r, f, slot);
   } else {
     const int j = i - nf1, v = j >> 3, t = 6 + ((j >> 2) & 1), q = j & 3;
     c.t = t; c.f = v; c.q = q; c.col = (v * S.nrT + r) * 4 + q;
@@ -331,9 +340,9 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_mr(Plan P, SliceTabs S,
   const int v = FWD ? z - 1 : z;
   const int t0 = FWD ? (vgrp ? 6 : 4) : (vgrp ? 0 : 2);  // the group's two types: t0, t0 + 1
   const int ncolg = vgrp ? 8 : 4 * nF;                    // local columns: 4 per (type) for vectors
-  int i0, g0;
-  if (!FWD) { i0 = vgrp ? 8 * v : 8 * nv; g0 = vgrp ? 2 * v : 2 * nv; }
-  else { i0 = vgrp ? 4 * nF + 8 * v : 0; g0 = vgrp ? 2 + 2 * v : 0; }
+  int i0;
+  if (!FWD) i0 = vgrp ? 8 * v : 8 * nv;
+  else i0 = vgrp ? 4 * nF + 8 * v : 0;
   const TypeGeo ga = type_geo(t0, L, m, P.nh), gb = type_geo(t0 + 1, L, m, P.nh);
   const int kst = max(ga.kpad, gb.kpad);  // X row stride
   // local column c -> type: vectors 4 (t - t0) + q; radial/scalar 4 f + 2 (t - t0) + slot
@@ -490,10 +499,11 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_mr(Plan P, SliceTabs S,
                       warp * (NS * kSlab);
   int item0 = 0;
   const int q4 = lane >> 3, kq = 4 * (lane & 7);
-  for (int gi = g0; gi < g0 + 2; ++gi) {
-    const int t = t0 + (gi - g0);
+  const int nfg = vgrp ? 1 : rs_groups(nF);  // 8-row blocks: one per group of four fields
+  for (int gi = 0; gi < 2 * nfg; ++gi) {
+    const int t = t0 + (gi & 1), fg = gi >> 1;
     const bool eight = !vgrp;  // 8-row groups: radius blocks of types 2..5
-    const int gcol = eight ? r * 8 : (v * S.nrT + r) * 4;
+    const int gcol = eight ? (fg * S.nrR + r) * 8 : (v * S.nrT + r) * 4;
     const TypeGeo& geo = (t == t0) ? ga : gb;
     const int nkc = geo.kpad / kTK;
     const int nt = gcol / kTN, blk = (gcol % kTN) >> 3, rbase = gcol & 7;
@@ -504,7 +514,7 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_mr(Plan P, SliceTabs S,
         // local column of block row rbase + q
         int c = -1;
         if (!eight) c = 4 * (t - t0) + q;
-        else if ((q >> 1) < nF) c = 4 * (q >> 1) + 2 * (t - t0) + (q & 1);
+        else if (4 * fg + (q >> 1) < nF) c = 4 * (4 * fg + (q >> 1)) + 2 * (t - t0) + (q & 1);
         uint32_t wd[NS];
         if (c >= 0 && colmax[c] > 0.0) {
           const double sc = pow2((8 * NS - 2) - colexp[c]);
@@ -832,21 +842,23 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
           const long long j10 = ok1 ? P.jmap[jm + l1] : 0, j11 = (ok1 && s1) ? P.jmap[jm + P.L + 1 + l1] : 0;
           const double g70 = g7_of(l0, w.m), g71 = g7_of(l1, w.m);
           if (w.t == 5) {
-            // column c = 8 (r - 8 nt) + 2 f + slot
+            // column c = 8 (block - 8 nt) + 2 (f % 4) + slot, block = (f / 4) nrR + r
             const double g60 = g6_of(l0, w.m), g61 = g6_of(l1, w.m);
 #pragma unroll
             for (int rr = 0; rr < kHalf / 8; ++rr) {
-              const int r = w.nt * (kTN / 8) + cbase / 8 + rr;
-              if (r >= P.nr) break;
+              const int rg = w.nt * (kTN / 8) + cbase / 8 + rr;
+              const int fg = rg / S.nrR, r = rg - fg * S.nrR;
+              if (r >= P.nr) continue;
               const double r1 = P.radius[r];
               const long long jr = P.J * (long long)r;
 #pragma unroll
-              for (int f = 0; f < 4; ++f) {
+              for (int f4 = 0; f4 < 4; ++f4) {
+                const int f = 4 * fg + f4;
                 if (f >= P.nvf + P.nsf) break;
                 const bool vec = f < P.nvf;
                 const double fac0 = vec ? r1 * r1 * g70 : g60, fac1 = vec ? r1 * r1 * g71 : g61;
                 double* dst = A.d_rj + jr + A.ld * A.cols[f];
-                const int c = 8 * rr + 2 * f;
+                const int c = 8 * rr + 2 * f4;
                 if (ok0) {
                   dst[j00] = sr[c] * fac0;
                   if (s1) dst[j01] = sr[c + 1] * fac0;
@@ -928,18 +940,21 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
                 }
               }
             } else {
-              // column c = 8 (r - 8 nt) + 2 f + slot: radial components and scalars
+              // column c = 8 (block - 8 nt) + 2 (f % 4) + slot, block = (f / 4) nrR + r:
+              // radial components and scalars, record words 4 nvb + 2 f
               const int nF = P.nvb + P.nsb;
 #pragma unroll
               for (int rr = 0; rr < kHalf / 8; ++rr) {
-                const int r = w.nt * (kTN / 8) + cbase / 8 + rr;
-                if (r >= P.nr) break;
-                double* dN = baseN + (long long)r * rec + 4 * P.nvb;
-                double* dS = baseS + (long long)r * rec + 4 * P.nvb;
+                const int rg = w.nt * (kTN / 8) + cbase / 8 + rr;
+                const int fg = rg / S.nrR, r = rg - fg * S.nrR;
+                if (r >= P.nr || 4 * fg >= nF) continue;
+                double* dN = baseN + (long long)r * rec + 4 * P.nvb + 8 * fg;
+                double* dS = baseS + (long long)r * rec + 4 * P.nvb + 8 * fg;
+                const int nFg = nF - 4 * fg;  // fields of this group (at most 4 used)
 #pragma unroll
                 for (int fp = 0; fp < 2; ++fp) {
                   const int c = 8 * rr + 4 * fp;
-                  if (2 * fp >= nF) break;
+                  if (2 * fp >= nFg) break;
                   const double2 a01 = *reinterpret_cast<const double2*>(sr + c);
                   const double2 a23 = *reinterpret_cast<const double2*>(sr + c + 2);
                   const double a[4] = {a01.x, a01.y, a23.x, a23.y};
@@ -949,13 +964,13 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
                     n[q] = pairrow ? a[q] + val[c + q] : a[q];
                     s_[q] = a[q] - val[c + q];
                   }
-                  if (v4ok && 2 * fp + 1 < nF) {
+                  if (v4ok && 2 * fp + 1 < nFg) {
                     st_global_v4(dN + 4 * fp, n[0], n[1], n[2], n[3]);
                     if (pairrow) st_global_v4(dS + 4 * fp, s_[0], s_[1], s_[2], s_[3]);
                   } else {
                     reinterpret_cast<double2*>(dN + 4 * fp)[0] = make_double2(n[0], n[1]);
                     if (pairrow) reinterpret_cast<double2*>(dS + 4 * fp)[0] = make_double2(s_[0], s_[1]);
-                    if (2 * fp + 1 < nF) {
+                    if (2 * fp + 1 < nFg) {
                       reinterpret_cast<double2*>(dN + 4 * fp)[1] = make_double2(n[2], n[3]);
                       if (pairrow) reinterpret_cast<double2*>(dS + 4 * fp)[1] = make_double2(s_[2], s_[3]);
                     }
@@ -1055,7 +1070,7 @@ void split_destroy(SplitState* s) {
 
 int split_create(SplitState** out, const Plan& p, int tier, int nslice, cudaStream_t st) {
   *out = nullptr;
-  if (p.nvb + p.nsb > 4 || p.nvf + p.nsf > 4) return KMHD_ERR_SIZE;
+  if (4 * (p.nvb + p.nsb) > kGrpCols || 4 * (p.nvf + p.nsf) > kGrpCols) return KMHD_ERR_SIZE;
   SplitState* s = new SplitState();
   s->tier = tier;
   s->ns = tier == KMHD_TIER_SPLIT_I8 ? 6 : 4;
@@ -1070,8 +1085,8 @@ int split_create(SplitState** out, const Plan& p, int tier, int nslice, cudaStre
   for (int t = 0; t < kNT; ++t) {
     int n;
     if (t <= 1) n = 4 * p.nvb * S.nrT;
-    else if (t <= 3) n = 8 * S.nrR;
-    else if (t <= 5) n = 8 * S.nrR;
+    else if (t <= 3) n = 8 * S.nrR * rs_groups(p.nvb + p.nsb);
+    else if (t <= 5) n = 8 * S.nrR * rs_groups(p.nvf + p.nsf);
     else n = 4 * p.nvf * S.nrT;
     S.ncolT[t] = n;
     S.npadT[t] = pad_to(n > 0 ? n : 1, kTN);
@@ -1183,10 +1198,11 @@ int split_create(SplitState** out, const Plan& p, int tier, int nslice, cudaStre
 
 // First radius of a work tile's columns: vector types (0, 1, 6, 7) hold
 // columns (v nrT + r) 4 + q, 16 radii per 64-column tile; radial/scalar types
-// (2..5) hold (4 r + f) 2 + slot, 8 radii per tile.
+// (2..5) hold ((f / 4) nrR + r) 8 + 2 (f % 4) + slot, 8 radii per tile (nrR is
+// a multiple of 8, so no tile spans two field groups).
 static int tile_r0(const SliceTabs& S, const Work& w) {
   if (w.t <= 1 || w.t >= 6) return (16 * w.nt) % S.nrT;
-  return 8 * w.nt;
+  return (8 * w.nt) % S.nrR;
 }
 
 int split_set_chunks(SplitState* s, const Plan& p, const std::vector<int>& bounds, cudaStream_t st) {
