@@ -15,7 +15,7 @@ constexpr int kRB = 4;        // radii per column block (one "quad" per field)
 constexpr int kThBlk = 64;    // hemisphere latitudes per backward CTA
 constexpr int kKC = 16;       // reduction chunk (l for bwd, theta for fwd)
 constexpr int kLBlk = 32;     // l rows per parity per forward CTA
-constexpr int kMaxVec = 4;    // vectors per field group
+constexpr int kMaxVec = 5;    // vectors per field group
 constexpr int kMaxScl = 2;    // scalars per field group
 constexpr int kMaxProd = 16;
 constexpr int kMaxFftFactors = 16;

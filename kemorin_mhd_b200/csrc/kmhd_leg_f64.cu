@@ -670,6 +670,9 @@ cudaError_t run_fwd(const Plan& p, double* d_rj, long long ld, const int* cols, 
     case 12: return FN<4, 0>(__VA_ARGS__);                                 \
     case 13: return FN<4, 1>(__VA_ARGS__);                                 \
     case 14: return FN<4, 2>(__VA_ARGS__);                                 \
+    case 15: return FN<5, 0>(__VA_ARGS__);                                 \
+    case 16: return FN<5, 1>(__VA_ARGS__);                                 \
+    case 17: return FN<5, 2>(__VA_ARGS__);                                 \
     default: return cudaErrorInvalidValue;                                 \
   }
 

@@ -51,7 +51,7 @@ def test_create_rejects_bad_descriptors():
     d.nvector_b, d.nscalar_b = 1, 1
     d.nph = 7 * 16                                   # factor 7 unsupported
     assert lib.kmhd_sph_create(ctypes.byref(d), ctypes.byref(h)) == 2
-    d.nph, d.nvector_b, d.nscalar_b = 96, 5, 0       # too many vectors per group
+    d.nph, d.nvector_b, d.nscalar_b = 96, 6, 0       # too many vectors per group (at most 5)
     assert lib.kmhd_sph_create(ctypes.byref(d), ctypes.byref(h)) == 2
     d.nvector_b, d.nscalar_b, d.nvector_f, d.nscalar_f = 1, 1, 1, 0
     prods = (sph_trans.Product * 1)(sph_trans.Product(0, 0, 3, 1.0))  # cross with bad index

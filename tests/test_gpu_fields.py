@@ -5,7 +5,8 @@ set_address_sph_trans_MHD.f90, f_trans_address_vector_MHD /
 b_trans_address_vector_MHD with the Lorentz force on), and six fields per
 direction (+ composition C, u C, u.omega, B.J) -- more radial-component and
 scalar fields than one 8-column block of the split path holds, so its
-slicers and GEMM epilogues use two field groups per radius.  Tolerances per
+slicers and GEMM epilogues use two field groups per radius; and the full MHD
+set with the composition flux u C as a fifth forward vector (f_trns%i_c_flux).  Tolerances per
 tier: FP64 1e-13, split 1e-12, FP32-accurate 1e-6 (max-norm per field)."""
 import numpy as np
 import pytest
@@ -22,16 +23,20 @@ DYNAMO = dict(nvb=4, nsb=1, nvf=4, nsf=0,
 SIX = dict(nvb=4, nsb=2, nvf=4, nsf=2,
            products=((PROD_CROSS, 1, 0, 1.0), (PROD_CROSS, 3, 2, 0.5), (PROD_CROSS, 0, 2, 1.0),
                      (PROD_VEC_SCALAR, 0, 1, 1.0), (PROD_DOT, 0, 1, 1.0), (PROD_DOT, 2, 3, 2.0)))
+# the full MHD set: composition C, and its flux u C as a fifth forward vector
+FULL = dict(nvb=4, nsb=2, nvf=5, nsf=1,
+            products=((PROD_CROSS, 1, 0, 1.0), (PROD_CROSS, 3, 2, 1.0), (PROD_CROSS, 0, 2, 1.0),
+                      (PROD_VEC_SCALAR, 0, 0, 1.0), (PROD_VEC_SCALAR, 0, 1, 1.0), (PROD_DOT, 0, 1, 1.0)))
 TOL = {TIER_FP64: 1e-13, TIER_SPLIT_I8: 1e-12, TIER_FP32ACC: 1e-6}
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("fields", ["dynamo", "six"])
+@pytest.mark.parametrize("fields", ["dynamo", "six", "full"])
 @pytest.mark.parametrize("tier", [TIER_FP64, TIER_SPLIT_I8, TIER_FP32ACC], ids=["fp64", "split", "fp32acc"])
 def test_field_sets_match_oracle(fields, tier):
     import torch
     from kemorin_mhd_b200.sph_trans import SphTransform
-    cfg = SphConfig(31, 48, 96, 5, name="L31_" + fields, **(DYNAMO if fields == "dynamo" else SIX))
+    cfg = SphConfig(31, 48, 96, 5, name="L31_" + fields, **{"dynamo": DYNAMO, "six": SIX, "full": FULL}[fields])
     d = make_d_rj(cfg, seed=81)
     ref = Oracle(cfg, nthreads=8).cycle(d)
     tr = SphTransform(cfg, tier=tier)
