@@ -141,6 +141,7 @@ def cpu_cycle_rate(cfg, seconds_target: float = 12.0, steps: int = 1, warmup: in
 
 
 def run_reference(args, cfg):
+    from kemorin_mhd_b200.config import FIELD_NAMES
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
@@ -152,7 +153,8 @@ def run_reference(args, cfg):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded spectra N(0,1)(l+1)^-2 sin(pi(r-ri)/(ro-ri)))",
         "config": {"workload": cfg.name, "L": cfg.ltr, "Nr": cfg.nr, "Ntheta": cfg.nth,
-                   "Nphi": cfg.nph, "fields_bwd": "u,omega,B + T", "fields_fwd": "omega x u, u x B, u T + u.omega"},
+                   "Nphi": cfg.nph, "fields_bwd": FIELD_NAMES[args.fields][0],
+                   "fields_fwd": FIELD_NAMES[args.fields][1]},
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"radial slab of {nr}/{cfg.nr} radii per step, scaled x{cfg.nr / nr:.2f} (cost is linear in Nr)",
                          "stages_ms": stages},
@@ -174,6 +176,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-tier comparison run")
     ap.add_argument("--nr", type=int, default=0, help="override the radius count (small profiling cases)")
+    ap.add_argument("--fields", default="default", choices=["default", "full"],
+                    help="field set: default u,omega,B + T; full u,omega,B,J + T,C with the Lorentz force and "
+                         "the composition flux")
     ap.add_argument("--p-on-the-fly", action="store_true",
                     help="FP64 tier: P_l^m generated inside the Legendre kernels (no stored tables); "
                          "also times the stored-table FP64 tier on the same input")
@@ -186,6 +191,9 @@ def main():
     if args.nr > 0:
         cfg = SphConfig(cfg.ltr, cfg.nth, cfg.nph, args.nr, cfg.nvb, cfg.nsb, cfg.nvf, cfg.nsf, cfg.products,
                         name=f"L{cfg.ltr}_Nr{args.nr}")
+    from kemorin_mhd_b200.config import FIELD_NAMES, with_fields
+    cfg = with_fields(cfg, args.fields)
+    fields_bwd, fields_fwd = FIELD_NAMES[args.fields]
     if args.impl == "reference":
         return run_reference(args, cfg)
 
@@ -402,7 +410,7 @@ def main():
         "vs_baseline": None, "dtype": DTYPES[tier], "tier": tier,
         "data": "synthetic (seeded spectra N(0,1)(l+1)^-2 sin(pi(r-ri)/(ro-ri)), Chebyshev radii)",
         "config": {"workload": cfg.name, "L": cfg.ltr, "Nr": cfg.nr, "Ntheta": cfg.nth, "Nphi": cfg.nph,
-                   "fields_bwd": "u,omega,B + T", "fields_fwd": "omega x u, u x B, u T + u.omega",
+                   "fields_bwd": fields_bwd, "fields_fwd": fields_fwd,
                    "parallelism": f"radial-instance x{ws} (no collective)",
                    "l2": "inputs larger than L2 (d_rj 5.4 GB, rtm 16 GB per direction)"},
         "stages_ms": stage, "kernels_ms": kern, "roofline": roof, "roofline_fft": roof_fft,

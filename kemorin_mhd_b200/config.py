@@ -120,6 +120,29 @@ CFG5 = SphConfig(1023, 1536, 3072, 129, name="L1023_Nr129")
 
 NAMED = {"cfg1": CFG1, "cfg2": CFG2, "cfg3": CFG3, "cfg5": CFG5}
 
+# Field sets of the reference's MHD transforms (set_address_sph_trans_MHD.f90):
+# "default" = u, omega, B + T -> omega x u, u x B, u T + u.omega;
+# "full" = u, omega, B, J + T, C -> omega x u, J x B, u x B, u T, u C + u.omega.
+FIELD_SETS = {
+    "default": dict(nvb=3, nsb=1, nvf=3, nsf=1,
+                    products=((PROD_CROSS, 1, 0, 1.0), (PROD_CROSS, 0, 2, 1.0), (PROD_VEC_SCALAR, 0, 0, 1.0),
+                              (PROD_DOT, 0, 1, 1.0))),
+    "full": dict(nvb=4, nsb=2, nvf=5, nsf=1,
+                 products=((PROD_CROSS, 1, 0, 1.0), (PROD_CROSS, 3, 2, 1.0), (PROD_CROSS, 0, 2, 1.0),
+                           (PROD_VEC_SCALAR, 0, 0, 1.0), (PROD_VEC_SCALAR, 0, 1, 1.0), (PROD_DOT, 0, 1, 1.0))),
+}
+FIELD_NAMES = {
+    "default": ("u,omega,B + T", "omega x u, u x B, u T + u.omega"),
+    "full": ("u,omega,B,J + T,C", "omega x u, J x B, u x B, u T, u C + u.omega"),
+}
+
+
+def with_fields(cfg: SphConfig, fields: str) -> SphConfig:
+    """The configuration's grid with one of the FIELD_SETS."""
+    if fields == "default":
+        return cfg
+    return dataclasses.replace(cfg, name=f"{cfg.name}_{fields}", **FIELD_SETS[fields])
+
 
 def batch_configs(n: int = 64, seed: int = 2024) -> List[SphConfig]:
     """Uneven instances: L from {63,127,255}, Nr from {33,65,129}, 2-4 fields.

@@ -214,16 +214,17 @@ __device__ __forceinline__ double2 spec_at(const double* st, int nc, int nv, int
                 : make_double2(0.5 * a0 + 0.5 * b1, 0.5 * a1 - 0.5 * b0);
 }
 
-// First DIF pass: input from the staged spectra, output into z.
+// First DIF pass: input from the spectra (staged records, order stride rs =
+// 2 nc; or the rtm records in place, rs = their order stride), output into z.
 template <int R>
 __device__ void dif_first(const double* st, int nc, int nv, double2* z, int npair, int N, int L,
-                          const double2* __restrict__ tw) {
+                          const double2* __restrict__ tw, long long rs) {
   const int s = N / R, nbf = N / R;
   for (int it = threadIdx.x; it < npair * nbf; it += blockDim.x) {
     const int pp = it / nbf, j = it % nbf;
     double2 x[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) x[r] = spec_at(st, nc, nv, pp, j + r * s, N, L, 2LL * nc);
+    for (int r = 0; r < R; ++r) x[r] = spec_at(st, nc, nv, pp, j + r * s, N, L, rs);
     DFT<R, +1>::run(x);
     double2* base = z + pp * N + j;
     base[0] = x[0];
@@ -232,13 +233,14 @@ __device__ void dif_first(const double* st, int nc, int nv, double2* z, int npai
   }
 }
 __device__ void dif_first_dispatch(int R, const double* st, int nc, int nv, double2* z, int npair,
-                                   int N, int L, const double2* tw) {
+                                   int N, int L, const double2* tw, long long rs = -1) {
+  if (rs < 0) rs = 2LL * nc;
   switch (R) {
-    case 8: dif_first<8>(st, nc, nv, z, npair, N, L, tw); break;
-    case 4: dif_first<4>(st, nc, nv, z, npair, N, L, tw); break;
-    case 2: dif_first<2>(st, nc, nv, z, npair, N, L, tw); break;
-    case 3: dif_first<3>(st, nc, nv, z, npair, N, L, tw); break;
-    default: dif_first<5>(st, nc, nv, z, npair, N, L, tw); break;
+    case 8: dif_first<8>(st, nc, nv, z, npair, N, L, tw, rs); break;
+    case 4: dif_first<4>(st, nc, nv, z, npair, N, L, tw, rs); break;
+    case 2: dif_first<2>(st, nc, nv, z, npair, N, L, tw, rs); break;
+    case 3: dif_first<3>(st, nc, nv, z, npair, N, L, tw, rs); break;
+    default: dif_first<5>(st, nc, nv, z, npair, N, L, tw, rs); break;
   }
 }
 
@@ -432,6 +434,30 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_cycle(Plan P, int line0, in
     store_line(z, npf, P, P.rtm_f, P.ncf, P.nvf, th, r);
     __syncthreads();
     line = next;
+  }
+}
+
+// Lines whose grid fits in shared memory but not together with the staged
+// spectra of the next line (many fields, e.g. 14 + 16 components at
+// Nphi = 1536: 197 KB of grid pairs): the first pass reads the line's spectra
+// in place from the rtm records, everything else as k_fft_cycle.
+template <int MVB, int MSB, int MVF, int MSF>
+__global__ void __launch_bounds__(kFftThreads) k_fft_cycle_direct(Plan P, int line0, int nlines) {
+  extern __shared__ double4 smraw[];
+  const int N = P.nph;
+  const int npb = (P.ncb + 1) / 2, npf = (P.ncf + 1) / 2;
+  double2* z = reinterpret_cast<double2*>(smraw);
+  const long long rs = (long long)P.nth * P.nr * P.ncb * 2;
+  for (int line = line0 + blockIdx.x; line < nlines; line += gridDim.x) {
+    const int th = line % P.nth, r = line / P.nth;
+    dif_first_dispatch(P.fac[0], P.rtm_b + rtm_off(P, 0, th, r, P.ncb), P.ncb, P.nvb, z, npb, N, P.L, P.twid, rs);
+    __syncthreads();
+    dif_rest(z, npb, N, P, P.twid);
+    products<MVB, MSB, MVF, MSF>(z, N, P);
+    __syncthreads();
+    dit_all(z, npf, N, P, P.twid);
+    store_line(z, npf, P, P.rtm_f, P.ncf, P.nvf, th, r);
+    __syncthreads();
   }
 }
 
@@ -1371,6 +1397,30 @@ size_t fft_smem_bytes(const Plan& p, int npair) {
 
 size_t smem_wide(const Plan& p) { return sizeof(double2) * (size_t)p.nph; }
 
+size_t smem_direct(const Plan& p) {
+  const int npair = ((p.ncb > p.ncf ? p.ncb : p.ncf) + 1) / 2;
+  return sizeof(double2) * (size_t)npair * p.nph;
+}
+
+template <int MVB, int MSB, int MVF, int MSF>
+cudaError_t run_cycle_direct(const Plan& p, cudaStream_t s) {
+  auto kern = k_fft_cycle_direct<MVB, MSB, MVF, MSF>;
+  const size_t smem = smem_direct(p);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, nsm = 0, occ = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kFftThreads, smem);
+  if (occ < 1) occ = 1;
+  const int line0 = p.r_lo * p.nth, nlines = p.r_hi * p.nth;
+  int grid = nsm * occ;
+  if (grid > nlines - line0) grid = nlines - line0;
+  if (grid <= 0) return cudaSuccess;
+  kern<<<grid, kFftThreads, smem, s>>>(p, line0, nlines);
+  return cudaGetLastError();
+}
+
 template <int MVB, int MSB, int MVF, int MSF>
 cudaError_t run_cycle_wide(const Plan& p, cudaStream_t s) {
   auto kern = k_fft_cycle_wide<MVB, MSB, MVF, MSF>;
@@ -1387,6 +1437,7 @@ cudaError_t run_cycle_wide(const Plan& p, cudaStream_t s) {
 
 cudaError_t launch_fft_cycle(const Plan& p, cudaStream_t s) {
   if (smem_cycle(p) > 227 * 1024 && smem_cycle_f(p) > 227 * 1024) {
+    if (smem_direct(p) <= 227 * 1024) return run_cycle_direct<kMaxVec, kMaxScl, kMaxVec, kMaxScl>(p, s);
     if (p.nvb == 3 && p.nsb == 1 && p.nvf == 3 && p.nsf == 1) return run_cycle_wide<3, 1, 3, 1>(p, s);
     return run_cycle_wide<kMaxVec, kMaxScl, kMaxVec, kMaxScl>(p, s);
   }

@@ -62,3 +62,21 @@ def test_six_fields_host_chunked_equals_device():
     h_out = np.zeros((n, cfg.ncf), order="F")
     tr.nonlinear_cycle(np.asfortranarray(d), h_out)
     assert np.array_equal(h_out, from_dev_fortran(out))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tier", [TIER_FP64, TIER_SPLIT_I8], ids=["fp64", "split"])
+def test_full_set_wide_grid_reads_spectra_in_place(tier):
+    """L=255 on a 1536-point phi grid with the full set: the line's 8 grid
+    pairs (197 KB) fit in shared memory but not with the staged spectra, so
+    the fused FFT reads the spectra in place (k_fft_cycle_direct)."""
+    import torch
+    from kemorin_mhd_b200.sph_trans import SphTransform
+    cfg = SphConfig(255, 384, 1536, 3, name="L255_full_wide", **FULL)
+    d = make_d_rj(cfg, seed=83)
+    ref = Oracle(cfg, nthreads=16).cycle(d)
+    tr = SphTransform(cfg, tier=tier)
+    out = torch.zeros((cfg.ncf, cfg.J * cfg.nr), dtype=torch.float64, device="cuda")
+    tr.nonlinear_cycle(to_dev_fortran(d), out)
+    err = col_relerr(from_dev_fortran(out), ref)
+    assert err.max() <= TOL[tier], err
