@@ -278,6 +278,18 @@ int kmhd_sph_rot_coriolis(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t
  * tables are built here (device memory), not inside the cycle. */
 int kmhd_sph_set_coriolis(kmhd_sph *handle, double coef_cor, int32_t iv_velo, int32_t iv_vort, int32_t col_out);
 
+/* Backward transform at the poles, for grids with pole points: v_pole is a
+ * (2 Nr) x ncomp_b column-major array, row k the north pole and row Nr + k the
+ * south pole of radius k; scalars as values, vectors in Cartesian components
+ * (x, y, z; z is the radial direction at the north pole and its opposite at the
+ * south pole), from the orders 0 and +-1 of the spectra in columns cols_b
+ * (as kmhd_sph_b_trans).  Replaces pole_backward_transforms without the centre
+ * point (PARALLEL_src/SPH_SHELL_src/pole_sph_transform.f90:107-162:
+ * schmidt_b_trans_pole_vect / _scalar, schmidt_b_trans_at_pole.f90:88-289).
+ * Host or device pointers (both arrays the same kind). */
+int kmhd_sph_b_trans_pole(kmhd_sph *handle, const double *d_rj, int64_t ld_rj, const int32_t *cols_b, double *v_pole,
+                          int32_t ptr_kind);
+
 /* Legendre path the handle runs: 1 = the tier's split path, 0 = FP64 DMMA
  * (FP64 tier, or a split-tier handle the autotuner moved to FP64). */
 int kmhd_sph_get_path(const kmhd_sph *handle, int32_t *path);

@@ -226,6 +226,10 @@ cudaError_t launch_rot_vec(long long J, int nr, const double* S, const double* d
 cudaError_t launch_rot_coriolis(long long J, int nr, const double* vel, const double* vort, long long ld,
                                 double* pol, double* tor, const int* idx, const double* cf, const double* radius,
                                 double coef_cor, cudaStream_t s);
+// Backward transform at the poles (kmhd_post.cu): v rows r (north) and nr + r
+// (south) for every radius, ncb columns with stride ldv (Cartesian vectors).
+cudaError_t launch_b_trans_pole(const Plan& p, const double* d_rj, long long ld, const int* cols, double* v,
+                                long long ldv, cudaStream_t s);
 // Set-up of the on-the-fly tables (cos_t, pco, dco, pst, pseed of the plan).
 cudaError_t launch_otf_tables(const Plan& p, double* cos_t, double2* pco, double2* dco, double2* pst,
                               double* pseed, const long long* pseed_off, cudaStream_t s);

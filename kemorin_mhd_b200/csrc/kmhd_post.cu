@@ -138,6 +138,80 @@ __global__ void k_rot_coriolis(long long J, int nr, int kchunk, const double* __
   }
 }
 
+// Backward transform at the two poles of every radius, for grids with pole
+// points: schmidt_b_trans_pole_vect / schmidt_b_trans_pole_scalar
+// (PARALLEL_src/SPH_SHELL_src/schmidt_b_trans_at_pole.f90:88-289).  Only the
+// orders 0 (scalars, the vectors' radial part) and +-1 (the horizontal part)
+// are nonzero at a pole; the vector comes out in Cartesian components (x, y,
+// z at the north pole; z = -radial at the south pole).  Pole values of the
+// Schmidt functions in closed form: P_l^0 = 1 / (-1)^l, dP_l^1/dtheta =
+// sqrt(l(l+1)/2) / (-1)^l sqrt(l(l+1)/2) (north / south).  One CTA per
+// radius, one warp per field, lanes over l, warp sums.  v: rows r (north) and
+// nr + r (south), column stride ldv.
+__global__ void k_b_trans_pole(Plan P, const double* __restrict__ d_rj, long long ld, const int* __restrict__ cols,
+                               double* __restrict__ v, long long ldv) {
+  const int r = blockIdx.x, L = P.L;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const double ar = 1.0 / P.radius[r];
+  const long long jr = P.J * (long long)r;
+  auto jof = [&](int l, int m) {
+    const int am = m < 0 ? -m : m;
+    return (long long)P.jmap[((long long)am * 2 + (m < 0 ? 1 : 0)) * (L + 1) + l];
+  };
+  auto wsum = [](double x) {
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+  };
+  for (int f = warp; f < P.nvb + P.nsb; f += nw) {
+    if (f < P.nvb) {
+      const double* S = d_rj + jr + ld * cols[f];
+      const double* dS = S + ld;
+      const double* T = S + 2 * ld;
+      double zn = 0.0, zs = 0.0, xn = 0.0, yn = 0.0, xs = 0.0, ys = 0.0;
+      for (int l = lane; l <= L; l += 32) {
+        const double sgn = (l & 1) ? -1.0 : 1.0;
+        const double g3 = l == 0 ? 0.5 : (double)l * (double)(l + 1);
+        const double s0 = S[jof(l, 0)];
+        zn += s0 * g3;
+        zs -= s0 * sgn * g3;
+        if (l >= 1) {
+          const double dpn = sqrt(0.5 * (double)l * (double)(l + 1)), dps = sgn * dpn;
+          const long long jm = jof(l, -1), jp = jof(l, 1);
+          xn += T[jm] * dpn + dS[jp] * dpn;
+          yn += dS[jm] * dpn - T[jp] * dpn;
+          xs += T[jm] * dps - dS[jp] * dps;
+          ys -= dS[jm] * dps + T[jp] * dps;
+        }
+      }
+      zn = wsum(zn); zs = wsum(zs); xn = wsum(xn); yn = wsum(yn); xs = wsum(xs); ys = wsum(ys);
+      if (lane == 0) {
+        const int c = 3 * f;
+        v[r + ldv * c] = xn * ar;
+        v[r + ldv * (c + 1)] = yn * ar;
+        v[r + ldv * (c + 2)] = zn * ar * ar;
+        v[P.nr + r + ldv * c] = xs * ar;
+        v[P.nr + r + ldv * (c + 1)] = ys * ar;
+        v[P.nr + r + ldv * (c + 2)] = zs * ar * ar;
+      }
+    } else {
+      const double* s = d_rj + jr + ld * cols[f];
+      double sn = 0.0, ss = 0.0;
+      for (int l = lane; l <= L; l += 32) {
+        const double x = s[jof(l, 0)];
+        sn += x;
+        ss += (l & 1) ? -x : x;
+      }
+      sn = wsum(sn);
+      ss = wsum(ss);
+      if (lane == 0) {
+        const int c = 3 * P.nvb + (f - P.nvb);
+        v[r + ldv * c] = sn;
+        v[P.nr + r + ldv * c] = ss;
+      }
+    }
+  }
+}
+
 }  // namespace
 
 cudaError_t launch_rot_vec(long long J, int nr, const double* S, const double* dS, const double* T, double* pol,
@@ -150,6 +224,14 @@ cudaError_t launch_rot_vec(long long J, int nr, const double* S, const double* d
   const int grid = (int)(want < 8LL * nsm ? want : 8LL * nsm);
   if (grid <= 0) return cudaSuccess;
   k_rot_vec<<<grid, 256, 0, s>>>(J, nr, S, dS, T, pol, dpol, tor, coef, b);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_b_trans_pole(const Plan& p, const double* d_rj, long long ld, const int* cols, double* v,
+                                long long ldv, cudaStream_t s) {
+  if (p.nr <= 0 || p.nvb + p.nsb == 0) return cudaSuccess;
+  const int warps = p.nvb + p.nsb < 8 ? p.nvb + p.nsb : 8;
+  k_b_trans_pole<<<p.nr, 32 * warps, 0, s>>>(p, d_rj, ld, cols, v, ldv);
   return cudaGetLastError();
 }
 

@@ -67,6 +67,7 @@ struct kmhd_sph {
   int cor_on = 0, cor_iv_velo = 0, cor_iv_vort = 0, cor_col = 0;
   double cor_coef = 0.0;
   double* cor_cyc = nullptr;  // 2 J*Nr staging columns for host-pointer cycles
+  double* pole_out = nullptr;  // (2 Nr) x ncb pole values for host-pointer calls
   std::vector<double> radius_h;
   std::vector<int> cols_b_cache, cols_f_cache;
   // host-pointer staging
@@ -1267,6 +1268,34 @@ int kmhd_sph_set_coriolis(kmhd_sph* h, double coef_cor, int32_t iv_velo, int32_t
   h->cor_col = col_out;
   h->cor_coef = coef_cor;
   h->cor_on = 1;
+  return KMHD_OK;
+}
+
+int kmhd_sph_b_trans_pole(kmhd_sph* h, const double* d_rj, int64_t ld, const int32_t* cols_b, double* v_pole,
+                          int32_t ptr_kind) {
+  if (!h || !d_rj || !v_pole || !cols_b) return KMHD_ERR_ARG;
+  if (check_ld(h, ld)) return KMHD_ERR_ARG;
+  const Plan& p = h->plan;
+  if (p.nvb + p.nsb == 0) return KMHD_ERR_STATE;
+  KCHECK(cudaSetDevice(h->device));
+  int st;
+  const double* src = d_rj;
+  int64_t sld = ld;
+  std::vector<int> cc;
+  double* out = v_pole;
+  const size_t nout = 2 * (size_t)p.nr * p.ncb;
+  if (ptr_kind == KMHD_PTR_HOST) {
+    if ((st = stage_host_in(h, d_rj, ld, cols_b, p.nvb, p.nsb, &src, &sld, cc))) return st;
+    if ((st = sync_cols(h, cc.data(), p.nvb + p.nsb, h->cols_b_cache, h->cols_b_d))) return st;
+    if (!h->pole_out && (st = dalloc(h, &h->pole_out, nout))) return st;
+    out = h->pole_out;
+  } else if ((st = sync_cols(h, cols_b, p.nvb + p.nsb, h->cols_b_cache, h->cols_b_d))) {
+    return st;
+  }
+  KCHECK(launch_b_trans_pole(p, src, sld, h->cols_b_d, out, 2LL * p.nr, h->stream));
+  if (ptr_kind == KMHD_PTR_HOST)
+    KCHECK(cudaMemcpyAsync(v_pole, out, sizeof(double) * nout, cudaMemcpyDeviceToHost, h->stream));
+  KCHECK(cudaStreamSynchronize(h->stream));
   return KMHD_OK;
 }
 

@@ -61,7 +61,7 @@ EXPORTS = ["kmhd_sph_create", "kmhd_sph_destroy", "kmhd_sph_set_stream", "kmhd_s
            "kmhd_sph_get_tables", "kmhd_sph_device_bytes", "kmhd_strerror", "kmhd_sph_cycle_noalloc",
            "kmhd_sph_last_kernel_timing", "kmhd_sph_get_path", "kmhd_selftest_wait_timeout",
            "kmhd_sph_div_flux", "kmhd_sph_rot_induction", "kmhd_sph_rot_force", "kmhd_sph_div_force",
-           "kmhd_sph_rot_coriolis", "kmhd_sph_set_coriolis"]
+           "kmhd_sph_rot_coriolis", "kmhd_sph_set_coriolis", "kmhd_sph_b_trans_pole"]
 
 _lib = None
 
@@ -95,6 +95,7 @@ def load_library(path: str | None = None):
     lib.kmhd_sph_div_force.argtypes = [vp, vp, i64, i32, i32, i32]
     lib.kmhd_sph_rot_coriolis.argtypes = [vp, vp, i64, i32, i32, i32, ctypes.c_double, i32]
     lib.kmhd_sph_set_coriolis.argtypes = [vp, ctypes.c_double, i32, i32, i32]
+    lib.kmhd_sph_b_trans_pole.argtypes = [vp, vp, i64, vp, vp, i32]
     lib.kmhd_selftest_wait_timeout.argtypes = [ctypes.c_int, ctypes.c_int]
     lib.kmhd_sph_get_tables.argtypes = [vp, i32] + [ctypes.POINTER(ctypes.c_double)] * 4
     lib.kmhd_sph_device_bytes.restype = i64
@@ -298,6 +299,18 @@ class SphTransform:
         _check(load_library().kmhd_sph_rot_coriolis(self._h, p, ld or n, col_velo, col_vort, col_out,
                                                     float(coef_cor), kind), "kmhd_sph_rot_coriolis")
         return d_rj
+
+    def b_trans_pole(self, d_rj, v_pole, cols_b=None, ld: int | None = None):
+        """Values at the poles: v_pole (2 Nr x ncomp_b; torch CUDA tensor of shape
+        (ncomp_b, 2 Nr) or F-order numpy array), rows k north / Nr + k south."""
+        p, kind = _ptr(d_rj)
+        q, kind2 = _ptr(v_pole)
+        if kind != kind2:
+            raise ValueError("d_rj and v_pole must both be host or both be device arrays")
+        cb = self._cols_b if cols_b is None else _i32(cols_b)
+        n = self.cfg.J * self.cfg.nr
+        _check(load_library().kmhd_sph_b_trans_pole(self._h, p, ld or n, cb, q, kind), "kmhd_sph_b_trans_pole")
+        return v_pole
 
     def set_coriolis(self, coef_cor: float, iv_velo: int = 0, iv_vort: int = 1, col_out: int = -1):
         """Every following cycle also writes the curl of the Coriolis term of
