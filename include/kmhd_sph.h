@@ -219,6 +219,34 @@ int kmhd_sph_div_flux(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t col
 int kmhd_sph_rot_induction(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t col_fld, int32_t col_rot,
                            int32_t ptr_kind);
 
+/* Boundary conditions of a scalar (temperature, composition) for the
+ * divergence of its flux: fixed field (the one-sided FDM row takes the
+ * boundary value) or fixed flux (the row takes the given flux in place of the
+ * derivative: cal_div_sph_in_fix_flux_2 / cal_div_sph_out_fix_flux_2,
+ * MHD_src/sph_MHD/cal_sph_exp_fixed_flux.f90:134-157, 253-276); chosen as
+ * sel_bc_sph_scalar_advect does (select_exp_scalar_bc.f90:219-277). */
+#define KMHD_BC_FIXED_FIELD 0
+#define KMHD_BC_FIXED_FLUX 1
+
+/* kmhd_sph_div_flux with a boundary condition per side (KMHD_BC_FIXED_*):
+ * val_in / val_out (J each, NULL = zero) are the fixed field or the fixed
+ * flux spectra of that side. */
+int kmhd_sph_div_flux_bc(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t col_flux, int32_t col_div,
+                         int32_t bc_icb, int32_t bc_cmb, const double *val_in, const double *val_out,
+                         int32_t ptr_kind);
+
+/* Magnetic boundary conditions for the curl of u x B: insulator (as
+ * kmhd_sph_rot_induction) or pseudo-vacuum, a purely radial field (pol = T,
+ * dpol/dr = tor = 0: cal_sph_nod_icb_qvc_vp_rot2 / cal_sph_nod_cmb_qvc_vp_rot2,
+ * MHD_src/sph_MHD/cal_sph_exp_nod_icb_qvac.f90:125-147,
+ * cal_sph_exp_nod_cmb_qvac.f90:125-147); chosen as sel_bc_sph_rotation_uxb
+ * does (select_exp_magne_bc.f90:222-262). */
+#define KMHD_BC_INSULATOR 0
+#define KMHD_BC_PSEUDO_VACUUM 1
+
+int kmhd_sph_rot_induction_bc(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t col_fld, int32_t col_rot,
+                              int32_t bc_icb, int32_t bc_cmb, int32_t ptr_kind);
+
 /* Velocity boundary conditions of the momentum equation (the reference's
  * iflag_icb / iflag_cmb for the velocity): non-slip and free slip. */
 #define KMHD_BC_NON_SLIP 0

@@ -208,12 +208,14 @@ cudaError_t launch_tables(const Plan& p, double* colat, double* weight, double* 
 // J*nr column each; coef = d1[3 nr], bnd[6], ar2[nr], g3[J]; fin / fout the
 // fixed boundary values (null: zero).
 cudaError_t launch_div_flux(long long J, int nr, const double* S, const double* dS, double* out, const double* coef,
-                            const double* fin, const double* fout, cudaStream_t s);
+                            const double* fin, const double* fout, cudaStream_t s, int flux_in = 0,
+                            int flux_out = 0);
 // Boundary rows of the spectral curl, per side: insulating (the magnetic
 // field's condition), else d2S/dr2 = s[0] S(boundary) + s[1] S(neighbour) and
 // dT/dr = t[0] T(boundary) + t[1] T(neighbour) + t[2] T(second neighbour).
 struct RotBnd {
   int insulating_in, insulating_out;
+  int qvac_in, qvac_out;  // pseudo-vacuum (radial field): dpol/dr = tor = 0
   double s_in[2], t_in[3], s_out[2], t_out[3];
 };
 // Curl of a vector (kmhd_post.cu): input S, dS, T, output pol, dpol, tor (one

@@ -16,9 +16,13 @@ namespace {
 // One thread per (j, k), j fastest.  coef: d1[3 nr] (offsets -1, 0, +1 of
 // row k), bnd[6] (inner: nodes 0, 1, 2; outer: nodes nr-1, nr-2, nr-3),
 // ar2[nr] = (1/r)^2, g3[J] = max(l(l+1), 1/2).
+// flux_in / flux_out: that boundary has a fixed flux (cal_div_sph_in_fix_flux_2
+// / cal_div_sph_out_fix_flux_2, cal_sph_exp_fixed_flux.f90:134-157, 253-276):
+// the row takes the given flux in place of the one-sided derivative,
+// div = (flux - dS/dr) max(g3, 1/2) / r^2; fin / fout then hold the flux.
 __global__ void k_div_flux(long long J, int nr, const double* __restrict__ S, const double* __restrict__ dS,
                            double* __restrict__ out, const double* __restrict__ coef, const double* __restrict__ fin,
-                           const double* __restrict__ fout) {
+                           const double* __restrict__ fout, int flux_in, int flux_out) {
   const double* d1 = coef;
   const double* bnd = coef + 3 * nr;
   const double* ar2 = bnd + 6;
@@ -29,9 +33,10 @@ __global__ void k_div_flux(long long J, int nr, const double* __restrict__ S, co
     const long long j = i - (long long)k * J;
     double d1s;
     if (k == 0) {
-      d1s = bnd[0] * (fin ? fin[j] : 0.0) + bnd[1] * S[i + J] + bnd[2] * S[i + 2 * J];
+      d1s = flux_in ? (fin ? fin[j] : 0.0) : bnd[0] * (fin ? fin[j] : 0.0) + bnd[1] * S[i + J] + bnd[2] * S[i + 2 * J];
     } else if (k == nr - 1) {
-      d1s = bnd[5] * S[i - 2 * J] + bnd[4] * S[i - J] + bnd[3] * (fout ? fout[j] : 0.0);
+      d1s = flux_out ? (fout ? fout[j] : 0.0)
+                     : bnd[5] * S[i - 2 * J] + bnd[4] * S[i - J] + bnd[3] * (fout ? fout[j] : 0.0);
     } else {
       d1s = d1[3 * k] * S[i - J] + d1[3 * k + 1] * S[i] + d1[3 * k + 2] * S[i + J];
     }
@@ -69,7 +74,10 @@ __global__ void k_rot_vec(long long J, int nr, const double* __restrict__ S, con
     const double g3j = gl[j] > 0.0 ? g3[j] : 0.0;
     double dp, tr;
     if (k == 0) {
-      if (b.insulating_in) {
+      if (b.qvac_in) {  // pseudo-vacuum (radial field): cal_sph_nod_icb_qvc_vp_rot2
+        dp = 0.0;
+        tr = 0.0;
+      } else if (b.insulating_in) {
         dp = (gl[j] + 1.0) * ar1[0] * t;
         tr = 0.0;
       } else {
@@ -78,7 +86,10 @@ __global__ void k_rot_vec(long long J, int nr, const double* __restrict__ S, con
         tr = -(d2s - g3j * ar2[0] * S[i]);
       }
     } else if (k == nr - 1) {
-      if (b.insulating_out) {
+      if (b.qvac_out) {  // cal_sph_nod_cmb_qvc_vp_rot2
+        dp = 0.0;
+        tr = 0.0;
+      } else if (b.insulating_out) {
         dp = -gl[j] * ar1[k] * t;
         tr = 0.0;
       } else {
@@ -255,7 +266,7 @@ cudaError_t launch_rot_coriolis(long long J, int nr, const double* vel, const do
 }
 
 cudaError_t launch_div_flux(long long J, int nr, const double* S, const double* dS, double* out, const double* coef,
-                            const double* fin, const double* fout, cudaStream_t s) {
+                            const double* fin, const double* fout, cudaStream_t s, int flux_in, int flux_out) {
   const long long n = J * nr;
   int dev = 0, nsm = 0;
   cudaGetDevice(&dev);
@@ -263,7 +274,7 @@ cudaError_t launch_div_flux(long long J, int nr, const double* S, const double* 
   const long long want = (n + 255) / 256;
   const int grid = (int)(want < 8LL * nsm ? want : 8LL * nsm);
   if (grid <= 0) return cudaSuccess;
-  k_div_flux<<<grid, 256, 0, s>>>(J, nr, S, dS, out, coef, fin, fout);
+  k_div_flux<<<grid, 256, 0, s>>>(J, nr, S, dS, out, coef, fin, fout, flux_in, flux_out);
   return cudaGetLastError();
 }
 

@@ -1054,7 +1054,7 @@ int build_coriolis(kmhd_sph* h) {
 // own_bnd = 1 puts each boundary node's own S into the one-sided rows (the
 // force divergence), else fix_in / fix_out (NULL = zero).
 int div_vec(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_flux, int32_t col_div, const double* fix_in,
-            const double* fix_out, int own_bnd, int32_t ptr_kind) {
+            const double* fix_out, int own_bnd, int32_t ptr_kind, int flux_in = 0, int flux_out = 0) {
   if (!h || !d_rj) return KMHD_ERR_ARG;
   if (check_ld(h, ld)) return KMHD_ERR_ARG;
   if (col_flux < 0 || col_div < 0 || col_div == col_flux || col_div == col_flux + 1) return KMHD_ERR_ARG;
@@ -1085,14 +1085,15 @@ int div_vec(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_flux, int32_t col
         fout = s0 + 3 * nrj + p.J;
       }
     }
-    KCHECK(launch_div_flux(p.J, p.nr, s0, s0 + nrj, s0 + 2 * nrj, h->div_coef, fin, fout, h->stream));
+    KCHECK(launch_div_flux(p.J, p.nr, s0, s0 + nrj, s0 + 2 * nrj, h->div_coef, fin, fout, h->stream, flux_in,
+                           flux_out));
     KCHECK(cudaMemcpyAsync(out, s0 + 2 * nrj, sizeof(double) * nrj, cudaMemcpyDeviceToHost, h->stream));
   } else {
     if (own_bnd) {
       fin = S;
       fout = S + last;
     }
-    KCHECK(launch_div_flux(p.J, p.nr, S, dS, out, h->div_coef, fin, fout, h->stream));
+    KCHECK(launch_div_flux(p.J, p.nr, S, dS, out, h->div_coef, fin, fout, h->stream, flux_in, flux_out));
   }
   KCHECK(cudaStreamSynchronize(h->stream));
   return KMHD_OK;
@@ -1199,6 +1200,27 @@ int kmhd_sph_rot_induction(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_fl
                            int32_t ptr_kind) {
   RotBnd b{};
   b.insulating_in = b.insulating_out = 1;
+  return rot_vec(h, d_rj, ld, col_fld, col_rot, b, ptr_kind);
+}
+
+int kmhd_sph_div_flux_bc(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_flux, int32_t col_div, int32_t bc_icb,
+                         int32_t bc_cmb, const double* val_in, const double* val_out, int32_t ptr_kind) {
+  const int ok_in = bc_icb == KMHD_BC_FIXED_FIELD || bc_icb == KMHD_BC_FIXED_FLUX;
+  const int ok_out = bc_cmb == KMHD_BC_FIXED_FIELD || bc_cmb == KMHD_BC_FIXED_FLUX;
+  if (!ok_in || !ok_out) return KMHD_ERR_ARG;
+  return div_vec(h, d_rj, ld, col_flux, col_div, val_in, val_out, 0, ptr_kind, bc_icb == KMHD_BC_FIXED_FLUX,
+                 bc_cmb == KMHD_BC_FIXED_FLUX);
+}
+
+int kmhd_sph_rot_induction_bc(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_fld, int32_t col_rot,
+                              int32_t bc_icb, int32_t bc_cmb, int32_t ptr_kind) {
+  const int ok_in = bc_icb == KMHD_BC_INSULATOR || bc_icb == KMHD_BC_PSEUDO_VACUUM;
+  const int ok_out = bc_cmb == KMHD_BC_INSULATOR || bc_cmb == KMHD_BC_PSEUDO_VACUUM;
+  if (!ok_in || !ok_out) return KMHD_ERR_ARG;
+  RotBnd b{};
+  b.insulating_in = b.insulating_out = 1;
+  b.qvac_in = bc_icb == KMHD_BC_PSEUDO_VACUUM;
+  b.qvac_out = bc_cmb == KMHD_BC_PSEUDO_VACUUM;
   return rot_vec(h, d_rj, ld, col_fld, col_rot, b, ptr_kind);
 }
 

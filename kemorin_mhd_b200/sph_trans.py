@@ -32,6 +32,10 @@ FLAG_AUTOTUNE = 1
 FLAG_P_ON_THE_FLY = 2
 BC_NON_SLIP = 0       # KMHD_BC_NON_SLIP
 BC_FREE_SLIP = 1      # KMHD_BC_FREE_SLIP
+BC_FIXED_FIELD = 0    # KMHD_BC_FIXED_FIELD
+BC_FIXED_FLUX = 1     # KMHD_BC_FIXED_FLUX
+BC_INSULATOR = 0      # KMHD_BC_INSULATOR
+BC_PSEUDO_VACUUM = 1  # KMHD_BC_PSEUDO_VACUUM
 
 
 class KmhdError(RuntimeError):
@@ -61,7 +65,8 @@ EXPORTS = ["kmhd_sph_create", "kmhd_sph_destroy", "kmhd_sph_set_stream", "kmhd_s
            "kmhd_sph_get_tables", "kmhd_sph_device_bytes", "kmhd_strerror", "kmhd_sph_cycle_noalloc",
            "kmhd_sph_last_kernel_timing", "kmhd_sph_get_path", "kmhd_selftest_wait_timeout",
            "kmhd_sph_div_flux", "kmhd_sph_rot_induction", "kmhd_sph_rot_force", "kmhd_sph_div_force",
-           "kmhd_sph_rot_coriolis", "kmhd_sph_set_coriolis", "kmhd_sph_b_trans_pole"]
+           "kmhd_sph_rot_coriolis", "kmhd_sph_set_coriolis", "kmhd_sph_b_trans_pole",
+           "kmhd_sph_div_flux_bc", "kmhd_sph_rot_induction_bc"]
 
 _lib = None
 
@@ -96,6 +101,8 @@ def load_library(path: str | None = None):
     lib.kmhd_sph_rot_coriolis.argtypes = [vp, vp, i64, i32, i32, i32, ctypes.c_double, i32]
     lib.kmhd_sph_set_coriolis.argtypes = [vp, ctypes.c_double, i32, i32, i32]
     lib.kmhd_sph_b_trans_pole.argtypes = [vp, vp, i64, vp, vp, i32]
+    lib.kmhd_sph_div_flux_bc.argtypes = [vp, vp, i64, i32, i32, i32, i32, vp, vp, i32]
+    lib.kmhd_sph_rot_induction_bc.argtypes = [vp, vp, i64, i32, i32, i32, i32, i32]
     lib.kmhd_selftest_wait_timeout.argtypes = [ctypes.c_int, ctypes.c_int]
     lib.kmhd_sph_get_tables.argtypes = [vp, i32] + [ctypes.POINTER(ctypes.c_double)] * 4
     lib.kmhd_sph_device_bytes.restype = i64
@@ -262,6 +269,27 @@ class SphTransform:
                "kmhd_sph_div_flux")
         return d_rj
 
+
+    def div_flux_bc(self, d_rj, col_flux: int, col_div: int, bc_icb: int = 0, bc_cmb: int = 0, val_in=None,
+                    val_out=None, ld: int | None = None):
+        """div_flux with a boundary condition per side (BC_FIXED_FIELD /
+        BC_FIXED_FLUX); val_in / val_out the fixed field or flux spectra."""
+        p, kind = _ptr(d_rj)
+        vi = _ptr(val_in)[0] if val_in is not None else None
+        vo = _ptr(val_out)[0] if val_out is not None else None
+        n = self.cfg.J * self.cfg.nr
+        _check(load_library().kmhd_sph_div_flux_bc(self._h, p, ld or n, col_flux, col_div, bc_icb, bc_cmb, vi, vo,
+                                                   kind), "kmhd_sph_div_flux_bc")
+        return d_rj
+
+    def rot_induction_bc(self, d_rj, col_fld: int, col_rot: int, bc_icb: int = 0, bc_cmb: int = 0,
+                         ld: int | None = None):
+        """rot_induction with BC_INSULATOR / BC_PSEUDO_VACUUM per side."""
+        p, kind = _ptr(d_rj)
+        n = self.cfg.J * self.cfg.nr
+        _check(load_library().kmhd_sph_rot_induction_bc(self._h, p, ld or n, col_fld, col_rot, bc_icb, bc_cmb, kind),
+               "kmhd_sph_rot_induction_bc")
+        return d_rj
 
     def rot_induction(self, d_rj, col_fld: int, col_rot: int, ld: int | None = None):
         """Curl of the vector (S, dS/dr, T) in columns col_fld.. into

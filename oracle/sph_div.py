@@ -87,10 +87,14 @@ def fdm_coefs(radius):
     return d1, icb, cmb
 
 
-def div_flux(radius, l_of_j, S, dS, fix_in=None, fix_out=None):
+def div_flux(radius, l_of_j, S, dS, fix_in=None, fix_out=None, bc_in="field", bc_out="field"):
     """Divergence spectra (J*Nr, j fastest) of the flux vector with poloidal
     column S and radial-derivative column dS, fixed-field values fix_in /
-    fix_out (J each, default zero) at the first and last radius."""
+    fix_out (J each, default zero) at the first and last radius; with
+    bc_in / bc_out = "flux" that side has a fixed flux instead
+    (cal_div_sph_in_fix_flux_2 / cal_div_sph_out_fix_flux_2,
+    MHD_src/sph_MHD/cal_sph_exp_fixed_flux.f90:134-157, 253-276): the row takes
+    the given flux (fix_in / fix_out) in place of the one-sided derivative."""
     r = np.asarray(radius, dtype=np.float64)
     nr, J = len(r), len(l_of_j)
     S = np.asarray(S).reshape(nr, J)
@@ -106,14 +110,14 @@ def div_flux(radius, l_of_j, S, dS, fix_in=None, fix_out=None):
     for k in range(1, nr - 1):
         d1s = d1[k, 0] * S[k - 1] + d1[k, 1] * S[k] + d1[k, 2] * S[k + 1]
         out[k] = (d1s - dS[k]) * g3 * ar2[k]
-    d1s = icb[0] * fin + icb[1] * S[1] + icb[2] * S[2]
+    d1s = fin if bc_in == "flux" else icb[0] * fin + icb[1] * S[1] + icb[2] * S[2]
     out[0] = (d1s - dS[0]) * g3 * ar2[0]
-    d1s = cmb[2] * S[nr - 3] + cmb[1] * S[nr - 2] + cmb[0] * fout
+    d1s = fout if bc_out == "flux" else cmb[2] * S[nr - 3] + cmb[1] * S[nr - 2] + cmb[0] * fout
     out[nr - 1] = (d1s - dS[nr - 1]) * g3 * ar2[nr - 1]
     return out.reshape(-1)
 
 
-def rot_uxb(radius, l_of_j, S, dS, T):
+def rot_uxb(radius, l_of_j, S, dS, T, bc_in="insulator", bc_out="insulator"):
     """Curl (pol, dpol/dr, tor) of the vector (S, dS/dr, T) with insulating
     boundaries, as const_sph_rotation_uxb
     (MHD_src/sph_MHD/const_sph_rotation.f90:167-187): interior rows
@@ -143,6 +147,13 @@ def rot_uxb(radius, l_of_j, S, dS, T):
         tor[k] = -d1d + g3 * ar2[k] * S[k]
     dpol[0] = (l + 1.0) * ar1[0] * T[0]
     dpol[nr - 1] = -l * ar1[nr - 1] * T[nr - 1]
+    # pseudo-vacuum (radial field): cal_sph_nod_icb_qvc_vp_rot2 /
+    # cal_sph_nod_cmb_qvc_vp_rot2 (cal_sph_exp_nod_icb_qvac.f90:125-147,
+    # cal_sph_exp_nod_cmb_qvac.f90:125-147): pol = T, dpol/dr = tor = 0
+    if bc_in == "pseudo_vacuum":
+        dpol[0] = 0.0
+    if bc_out == "pseudo_vacuum":
+        dpol[nr - 1] = 0.0
     return pol.reshape(-1), dpol.reshape(-1), tor.reshape(-1)
 
 

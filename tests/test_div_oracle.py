@@ -153,3 +153,34 @@ def test_curl_rows_use_zero_g3_at_degree_zero():
         a = f(r, l, S, dS, T)[2].reshape(cfg.nr, -1)
         b = f(r, l, S2.reshape(-1), dS, T)[2].reshape(cfg.nr, -1)
         assert np.array_equal(a[1:-1, j0], b[1:-1, j0])
+
+
+def test_fixed_flux_rows_take_the_flux():
+    """A fixed-flux side gives div = (flux - dS/dr) max(g3, 1/2) / r^2 there,
+    whatever S is; the other rows are those of the fixed-field divergence."""
+    cfg = SphConfig(15, 24, 48, 9)
+    r = cfg.radius()
+    l, _ = rj_order(cfg.ltr)
+    rng = np.random.default_rng(14)
+    S, dS = rng.standard_normal(cfg.J * cfg.nr), rng.standard_normal(cfg.J * cfg.nr)
+    fi, fo = rng.standard_normal(cfg.J), rng.standard_normal(cfg.J)
+    a = div_flux(r, l, S, dS, fi, fo, "flux", "flux").reshape(cfg.nr, -1)
+    b = div_flux(r, l, S, dS, fi, fo).reshape(cfg.nr, -1)
+    g3 = np.maximum(np.where(l == 0, 0.5, l * (l + 1.0)), 0.5)
+    d = dS.reshape(cfg.nr, -1)
+    assert np.array_equal(a[1:-1], b[1:-1])
+    assert np.array_equal(a[0], (fi - d[0]) * g3 * (1.0 / r[0]) ** 2)
+    assert np.array_equal(a[-1], (fo - d[-1]) * g3 * (1.0 / r[-1]) ** 2)
+
+
+def test_pseudo_vacuum_rows():
+    from oracle.sph_div import rot_uxb
+    cfg = SphConfig(15, 24, 48, 9)
+    r = cfg.radius()
+    l, _ = rj_order(cfg.ltr)
+    rng = np.random.default_rng(15)
+    S, dS, T = (rng.standard_normal(cfg.J * cfg.nr) for _ in range(3))
+    pol, dpol, tor = (x.reshape(cfg.nr, -1) for x in rot_uxb(r, l, S, dS, T, "pseudo_vacuum", "pseudo_vacuum"))
+    assert np.array_equal(pol, T.reshape(cfg.nr, -1))
+    for k in (0, -1):
+        assert not dpol[k].any() and not tor[k].any()

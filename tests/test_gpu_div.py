@@ -201,3 +201,48 @@ def test_vorticity_source_after_split_cycle():
     for q in range(3):
         assert _relerr(res[:, cfg.ncf + q], ref[q]) <= 1e-13, q
     assert _relerr(res[:, cfg.ncf + 3], div_force(cfg.radius(), l, adv[:, 0], adv[:, 1])) <= 1e-13
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("bc_icb,bc_cmb,host", [(1, 1, False), (0, 1, True), (1, 0, False)],
+                         ids=["flux_flux", "field_flux_host", "flux_field"])
+def test_div_flux_bc_matches_oracle(bc_icb, bc_cmb, host):
+    import torch
+    from kemorin_mhd_b200.sph_trans import SphTransform
+    cfg = CFG
+    tr = SphTransform(cfg, tier=TIER_FP64)
+    n = cfg.J * cfg.nr
+    rng = np.random.default_rng(19)
+    d = np.asfortranarray(rng.standard_normal((n, 3)))
+    vi, vo = rng.standard_normal(cfg.J), rng.standard_normal(cfg.J)
+    l, _ = rj_order(cfg.ltr)
+    names = {0: "field", 1: "flux"}
+    ref = div_flux(cfg.radius(), l, d[:, 0], d[:, 1], vi, vo, names[bc_icb], names[bc_cmb])
+    if host:
+        arr = d.copy(order="F")
+        tr.div_flux_bc(arr, 0, 2, bc_icb, bc_cmb, vi, vo)
+        got = arr[:, 2]
+    else:
+        t = to_dev_fortran(d)
+        tr.div_flux_bc(t, 0, 2, bc_icb, bc_cmb, torch.from_numpy(vi).cuda(), torch.from_numpy(vo).cuda())
+        got = from_dev_fortran(t)[:, 2]
+    assert _relerr(got, ref) <= 1e-13
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("bc_icb,bc_cmb", [(1, 1), (0, 1), (1, 0)], ids=["qvac_qvac", "ins_qvac", "qvac_ins"])
+def test_rot_induction_bc_matches_oracle(bc_icb, bc_cmb):
+    from kemorin_mhd_b200.sph_trans import SphTransform
+    from oracle.sph_div import rot_uxb
+    cfg = CFG
+    tr = SphTransform(cfg, tier=TIER_FP64)
+    n = cfg.J * cfg.nr
+    d = np.asfortranarray(np.random.default_rng(20).standard_normal((n, 6)))
+    l, _ = rj_order(cfg.ltr)
+    names = {0: "insulator", 1: "pseudo_vacuum"}
+    ref = rot_uxb(cfg.radius(), l, d[:, 0], d[:, 1], d[:, 2], names[bc_icb], names[bc_cmb])
+    t = to_dev_fortran(d)
+    tr.rot_induction_bc(t, 0, 3, bc_icb, bc_cmb)
+    got = from_dev_fortran(t)
+    for q in range(3):
+        assert _relerr(got[:, 3 + q], ref[q]) <= 1e-13, q
