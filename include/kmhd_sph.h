@@ -247,6 +247,16 @@ int kmhd_sph_div_flux_bc(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t 
 int kmhd_sph_rot_induction_bc(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t col_fld, int32_t col_rot,
                               int32_t bc_icb, int32_t bc_cmb, int32_t ptr_kind);
 
+/* Current density J = curl B from the magnetic field's spectra (columns
+ * col_magne .. + 2) into col_current .. + 2: pol = T, dpol/dr = dT/dr, tor =
+ * -d2S/dr2 + l(l+1) S / r^2 with 3-point FDMs (cal_sph_nod_vect_rot2,
+ * MHD_src/sph_MHD/cal_sph_exp_rotation.f90:157-203), boundary rows per
+ * KMHD_BC_INSULATOR / KMHD_BC_PSEUDO_VACUUM: replaces const_sph_current
+ * (const_sph_rotation.f90:141-158) with sel_bc_sph_current
+ * (select_exp_magne_bc.f90:172-218).  The restart files hold B, not J. */
+int kmhd_sph_current(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t col_magne, int32_t col_current,
+                     int32_t bc_icb, int32_t bc_cmb, int32_t ptr_kind);
+
 /* Velocity boundary conditions of the momentum equation (the reference's
  * iflag_icb / iflag_cmb for the velocity): non-slip and free slip. */
 #define KMHD_BC_NON_SLIP 0
@@ -267,6 +277,14 @@ int kmhd_sph_rot_induction_bc(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int
  * centre row and the rotating inner core's torque are not provided.  Column
  * ranges must not overlap; Nr >= 3; host or device pointers. */
 int kmhd_sph_rot_force(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t col_fld, int32_t col_rot,
+                       int32_t bc_icb, int32_t bc_cmb, int32_t ptr_kind);
+
+/* Vorticity = curl u from the velocity's spectra into col_vort .. + 2, with
+ * the interior rows of kmhd_sph_current and the velocity boundary rows of
+ * kmhd_sph_rot_force (KMHD_BC_NON_SLIP / KMHD_BC_FREE_SLIP): replaces
+ * const_sph_vorticity (MHD_src/sph_MHD/const_sph_rotation.f90:111-137).  The
+ * restart files hold u, not the vorticity. */
+int kmhd_sph_vorticity(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t col_velo, int32_t col_vort,
                        int32_t bc_icb, int32_t bc_cmb, int32_t ptr_kind);
 
 /* Divergence of a momentum force (the pressure equation's source): as

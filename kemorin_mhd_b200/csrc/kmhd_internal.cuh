@@ -216,6 +216,14 @@ cudaError_t launch_div_flux(long long J, int nr, const double* S, const double* 
 struct RotBnd {
   int insulating_in, insulating_out;
   int qvac_in, qvac_out;  // pseudo-vacuum (radial field): dpol/dr = tor = 0
+  // curl of a field (vorticity, current) rather than of a force: interior
+  // rows take the 3-point second derivative of S instead of d(dS/dr)/dr
+  int d2_interior;
+  // insulating boundary of the current: the potential field's dS/dr =
+  // (l+1) S / r (inner) or -l S / r (outer) folded into the second derivative
+  // with the fixed-derivative coefficient cdr
+  int ins_s_in, ins_s_out;
+  double cdr_in, cdr_out;
   double s_in[2], t_in[3], s_out[2], t_out[3];
 };
 // Curl of a vector (kmhd_post.cu): input S, dS, T, output pol, dpol, tor (one

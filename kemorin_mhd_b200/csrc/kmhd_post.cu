@@ -55,7 +55,8 @@ __global__ void k_div_flux(long long J, int nr, const double* __restrict__ S, co
 //   -(d2S/dr2 - g3 S / r^2) with RotBnd's coefficients (non-slip:
 //   cal_sph_nod_icb_rigid_rot2 / cal_sph_nod_cmb_rigid_rot2, free slip:
 //   cal_sph_nod_icb_free_rot2 / cal_sph_nod_cmb_free_rot2).
-// coef as k_div_flux, then ar1[nr] = 1/r and gl[J] = l.
+// coef as k_div_flux, then ar1[nr] = 1/r, gl[J] = l and d2[3 nr] (second
+// derivative, offsets -1, 0, +1).
 __global__ void k_rot_vec(long long J, int nr, const double* __restrict__ S, const double* __restrict__ dS,
                           const double* __restrict__ T, double* __restrict__ pol, double* __restrict__ dpol,
                           double* __restrict__ tor, const double* __restrict__ coef, const RotBnd b) {
@@ -64,6 +65,7 @@ __global__ void k_rot_vec(long long J, int nr, const double* __restrict__ S, con
   const double* g3 = ar2 + nr;
   const double* ar1 = g3 + J;
   const double* gl = ar1 + nr;
+  const double* d2 = gl + J;  // interior 3-point second derivative
   const long long n = J * nr;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const int k = (int)(i / J);
@@ -81,7 +83,8 @@ __global__ void k_rot_vec(long long J, int nr, const double* __restrict__ S, con
         dp = (gl[j] + 1.0) * ar1[0] * t;
         tr = 0.0;
       } else {
-        const double d2s = b.s_in[0] * S[i] + b.s_in[1] * S[i + J];
+        const double s0 = b.ins_s_in ? (gl[j] + 1.0) * ar1[0] * b.cdr_in + b.s_in[0] : b.s_in[0];
+        const double d2s = s0 * S[i] + b.s_in[1] * S[i + J];
         dp = b.t_in[0] * t + b.t_in[1] * T[i + J] + b.t_in[2] * T[i + 2 * J];
         tr = -(d2s - g3j * ar2[0] * S[i]);
       }
@@ -93,14 +96,20 @@ __global__ void k_rot_vec(long long J, int nr, const double* __restrict__ S, con
         dp = -gl[j] * ar1[k] * t;
         tr = 0.0;
       } else {
-        const double d2s = b.s_out[1] * S[i - J] + b.s_out[0] * S[i];
+        const double s0 = b.ins_s_out ? b.s_out[0] - gl[j] * ar1[k] * b.cdr_out : b.s_out[0];
+        const double d2s = b.s_out[1] * S[i - J] + s0 * S[i];
         dp = b.t_out[2] * T[i - 2 * J] + b.t_out[1] * T[i - J] + b.t_out[0] * t;
         tr = -(d2s - g3j * ar2[k] * S[i]);
       }
     } else {
-      const double d1d = d1[3 * k] * dS[i - J] + d1[3 * k + 1] * dS[i] + d1[3 * k + 2] * dS[i + J];
       dp = d1[3 * k] * T[i - J] + d1[3 * k + 1] * t + d1[3 * k + 2] * T[i + J];
-      tr = -d1d + g3j * ar2[k] * S[i];
+      if (b.d2_interior) {  // cal_sph_nod_vect_rot2 (cal_sph_exp_rotation.f90:157-203)
+        const double d2s = d2[3 * k] * S[i - J] + d2[3 * k + 1] * S[i] + d2[3 * k + 2] * S[i + J];
+        tr = -d2s + g3j * ar2[k] * S[i];
+      } else {
+        const double d1d = d1[3 * k] * dS[i - J] + d1[3 * k + 1] * dS[i] + d1[3 * k + 2] * dS[i + J];
+        tr = -d1d + g3j * ar2[k] * S[i];
+      }
     }
     pol[i] = t;
     dpol[i] = dp;

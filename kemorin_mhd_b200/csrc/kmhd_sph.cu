@@ -927,7 +927,8 @@ int build_div_coef(kmhd_sph* h) {
   const Plan& p = h->plan;
   const int nr = p.nr, L = p.L;
   const std::vector<double>& r = h->radius_h;
-  std::vector<double> c(3 * (size_t)nr + 6 + nr + (size_t)p.J + nr + (size_t)p.J, 0.0);
+  std::vector<double> c(3 * (size_t)nr + 6 + nr + (size_t)p.J + nr + (size_t)p.J + 3 * (size_t)nr, 0.0);
+  double* d2c = c.data() + 3 * (size_t)nr + 6 + nr + (size_t)p.J + nr + (size_t)p.J;
   for (int k = 1; k < nr - 1; ++k) {
     const double dp = r[k + 1] - r[k], dn = r[k] - r[k - 1];
     const double t[3][3] = {{1.0, 0.0, 0.0}, {1.0, dp, 0.5 * dp * dp}, {1.0, -dn, 0.5 * dn * dn}};
@@ -936,6 +937,10 @@ int build_div_coef(kmhd_sph* h) {
     c[3 * k + 0] = inv[1][2];
     c[3 * k + 1] = inv[1][0];
     c[3 * k + 2] = inv[1][1];
+    // second derivative (fdm(2) of copy_fdm2_nod_coefs_from_mat, t_fdm_coefs.f90:146-163)
+    d2c[3 * k + 0] = inv[2][2];
+    d2c[3 * k + 1] = inv[2][0];
+    d2c[3 * k + 2] = inv[2][1];
   }
   {
     const double d1 = r[1] - r[0], d2 = r[2] - r[0];
@@ -1232,6 +1237,52 @@ int kmhd_sph_rot_force(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_fld, i
   if (!ok_in || !ok_out) return KMHD_ERR_ARG;
   if (h->plan.nr < 3) return KMHD_ERR_SIZE;
   return rot_vec(h, d_rj, ld, col_fld, col_rot, velocity_bnd(h->radius_h, bc_icb, bc_cmb), ptr_kind);
+}
+
+int kmhd_sph_vorticity(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_velo, int32_t col_vort, int32_t bc_icb,
+                       int32_t bc_cmb, int32_t ptr_kind) {
+  if (!h) return KMHD_ERR_ARG;
+  const int ok_in = bc_icb == KMHD_BC_NON_SLIP || bc_icb == KMHD_BC_FREE_SLIP;
+  const int ok_out = bc_cmb == KMHD_BC_NON_SLIP || bc_cmb == KMHD_BC_FREE_SLIP;
+  if (!ok_in || !ok_out) return KMHD_ERR_ARG;
+  if (h->plan.nr < 3) return KMHD_ERR_SIZE;
+  RotBnd b = velocity_bnd(h->radius_h, bc_icb, bc_cmb);
+  b.d2_interior = 1;
+  return rot_vec(h, d_rj, ld, col_velo, col_vort, b, ptr_kind);
+}
+
+int kmhd_sph_current(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_magne, int32_t col_current, int32_t bc_icb,
+                     int32_t bc_cmb, int32_t ptr_kind) {
+  if (!h) return KMHD_ERR_ARG;
+  const int ok_in = bc_icb == KMHD_BC_INSULATOR || bc_icb == KMHD_BC_PSEUDO_VACUUM;
+  const int ok_out = bc_cmb == KMHD_BC_INSULATOR || bc_cmb == KMHD_BC_PSEUDO_VACUUM;
+  if (!ok_in || !ok_out) return KMHD_ERR_ARG;
+  if (h->plan.nr < 3) return KMHD_ERR_SIZE;
+  // the non-slip coefficient rows (fixed dS/dr): pseudo-vacuum takes dS/dr = 0,
+  // an insulator the potential field's dS/dr, through the coefficient of the
+  // fixed derivative (cal_sph_nod_icb_ins_rot2 / cal_sph_nod_cmb_ins_rot2,
+  // cal_sph_exp_nod_icb_ins.f90, cal_sph_exp_nod_cmb_ins.f90;
+  // cal_sph_nod_icb_qvc_rot2 / cal_sph_nod_cmb_qvc_rot2)
+  RotBnd b = velocity_bnd(h->radius_h, KMHD_BC_NON_SLIP, KMHD_BC_NON_SLIP);
+  b.d2_interior = 1;
+  const std::vector<double>& r = h->radius_h;
+  const int nr = (int)r.size();
+  double inv[3][3];
+  {
+    const double dr = r[1] - r[0];
+    const double t[3][3] = {{1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {dr, 1.0, dr * dr / 2.0}};
+    inverse33(t, inv);
+    b.cdr_in = inv[2][0];  // fdm2_fix_dr_ICB(-1,3): the fixed derivative's coefficient
+  }
+  {
+    const double dn = r[nr - 1] - r[nr - 2];
+    const double t[3][3] = {{1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {1.0, -dn, dn * dn / 2.0}};
+    inverse33(t, inv);
+    b.cdr_out = inv[2][1];  // fdm2_fix_dr_CMB(1,3)
+  }
+  b.ins_s_in = bc_icb == KMHD_BC_INSULATOR;
+  b.ins_s_out = bc_cmb == KMHD_BC_INSULATOR;
+  return rot_vec(h, d_rj, ld, col_magne, col_current, b, ptr_kind);
 }
 
 int kmhd_sph_div_force(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_fld, int32_t col_div, int32_t ptr_kind) {

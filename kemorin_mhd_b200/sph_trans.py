@@ -66,7 +66,7 @@ EXPORTS = ["kmhd_sph_create", "kmhd_sph_destroy", "kmhd_sph_set_stream", "kmhd_s
            "kmhd_sph_last_kernel_timing", "kmhd_sph_get_path", "kmhd_selftest_wait_timeout",
            "kmhd_sph_div_flux", "kmhd_sph_rot_induction", "kmhd_sph_rot_force", "kmhd_sph_div_force",
            "kmhd_sph_rot_coriolis", "kmhd_sph_set_coriolis", "kmhd_sph_b_trans_pole",
-           "kmhd_sph_div_flux_bc", "kmhd_sph_rot_induction_bc"]
+           "kmhd_sph_div_flux_bc", "kmhd_sph_rot_induction_bc", "kmhd_sph_vorticity", "kmhd_sph_current"]
 
 _lib = None
 
@@ -103,6 +103,8 @@ def load_library(path: str | None = None):
     lib.kmhd_sph_b_trans_pole.argtypes = [vp, vp, i64, vp, vp, i32]
     lib.kmhd_sph_div_flux_bc.argtypes = [vp, vp, i64, i32, i32, i32, i32, vp, vp, i32]
     lib.kmhd_sph_rot_induction_bc.argtypes = [vp, vp, i64, i32, i32, i32, i32, i32]
+    lib.kmhd_sph_vorticity.argtypes = [vp, vp, i64, i32, i32, i32, i32, i32]
+    lib.kmhd_sph_current.argtypes = [vp, vp, i64, i32, i32, i32, i32, i32]
     lib.kmhd_selftest_wait_timeout.argtypes = [ctypes.c_int, ctypes.c_int]
     lib.kmhd_sph_get_tables.argtypes = [vp, i32] + [ctypes.POINTER(ctypes.c_double)] * 4
     lib.kmhd_sph_device_bytes.restype = i64
@@ -289,6 +291,24 @@ class SphTransform:
         n = self.cfg.J * self.cfg.nr
         _check(load_library().kmhd_sph_rot_induction_bc(self._h, p, ld or n, col_fld, col_rot, bc_icb, bc_cmb, kind),
                "kmhd_sph_rot_induction_bc")
+        return d_rj
+
+    def vorticity(self, d_rj, col_velo: int, col_vort: int, bc_icb: int = 0, bc_cmb: int = 0,
+                  ld: int | None = None):
+        """curl u into col_vort.. with BC_NON_SLIP / BC_FREE_SLIP per side."""
+        p, kind = _ptr(d_rj)
+        n = self.cfg.J * self.cfg.nr
+        _check(load_library().kmhd_sph_vorticity(self._h, p, ld or n, col_velo, col_vort, bc_icb, bc_cmb, kind),
+               "kmhd_sph_vorticity")
+        return d_rj
+
+    def current(self, d_rj, col_magne: int, col_current: int, bc_icb: int = 0, bc_cmb: int = 0,
+                ld: int | None = None):
+        """curl B into col_current.. with BC_INSULATOR / BC_PSEUDO_VACUUM per side."""
+        p, kind = _ptr(d_rj)
+        n = self.cfg.J * self.cfg.nr
+        _check(load_library().kmhd_sph_current(self._h, p, ld or n, col_magne, col_current, bc_icb, bc_cmb, kind),
+               "kmhd_sph_current")
         return d_rj
 
     def rot_induction(self, d_rj, col_fld: int, col_rot: int, ld: int | None = None):

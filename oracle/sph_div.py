@@ -221,3 +221,87 @@ def div_force(radius, l_of_j, S, dS):
     nr = len(radius)
     S2 = np.asarray(S).reshape(nr, -1)
     return div_flux(radius, l_of_j, S, dS, fix_in=S2[0], fix_out=S2[-1])
+
+
+def _d2_coefs(r):
+    """Interior 3-point second derivative (offsets -1, 0, +1): row 2 of the
+    inverse Taylor matrix, fdm(2) of copy_fdm2_nod_coefs_from_mat
+    (CORE_src/SPH_SPECTR_src/t_fdm_coefs.f90:146-163)."""
+    nr = len(r)
+    d2 = np.zeros((nr, 3))
+    for k in range(1, nr - 1):
+        dp, dn = r[k + 1] - r[k], r[k] - r[k - 1]
+        inv = inverse33(np.array([[1.0, 0.0, 0.0], [1.0, dp, 0.5 * dp * dp], [1.0, -dn, 0.5 * dn * dn]]))
+        d2[k] = [inv[2, 2], inv[2, 0], inv[2, 1]]
+    return d2
+
+
+def _rot_field(radius, l_of_j, S, dS, T, bnd_rows):
+    """Curl of a field (S, dS/dr, T): interior rows cal_sph_nod_vect_rot2
+    (MHD_src/sph_MHD/cal_sph_exp_rotation.f90:157-203), pol = T, dpol/dr = d1 T,
+    tor = -d2 S + g3 S / r^2; boundary rows from bnd_rows(k, S, T) -> (dpol, d2s)."""
+    r = np.asarray(radius, dtype=np.float64)
+    nr, J = len(r), len(l_of_j)
+    S = np.asarray(S).reshape(nr, J)
+    T = np.asarray(T).reshape(nr, J)
+    l = np.asarray(l_of_j).astype(np.float64)
+    g3 = l * (l + 1.0)
+    ar2 = (1.0 / r) ** 2
+    d1, _, _ = fdm_coefs(r)
+    d2 = _d2_coefs(r)
+    pol, dpol, tor = T.copy(), np.zeros((nr, J)), np.zeros((nr, J))
+    for k in range(1, nr - 1):
+        d2s = d2[k, 0] * S[k - 1] + d2[k, 1] * S[k] + d2[k, 2] * S[k + 1]
+        dpol[k] = d1[k, 0] * T[k - 1] + d1[k, 1] * T[k] + d1[k, 2] * T[k + 1]
+        tor[k] = -d2s + g3 * ar2[k] * S[k]
+    for k in (0, nr - 1):
+        dp, d2s = bnd_rows(k, S, T)
+        dpol[k] = dp
+        tor[k] = -(d2s - g3 * ar2[k] * S[k])
+    return pol.reshape(-1), dpol.reshape(-1), tor.reshape(-1)
+
+
+def vorticity(radius, l_of_j, S, dS, T, bc_icb=NON_SLIP, bc_cmb=NON_SLIP):
+    """const_sph_vorticity (MHD_src/sph_MHD/const_sph_rotation.f90:111-137):
+    interior rows of _rot_field, boundary rows of sel_bc_sph_vorticity (as
+    rot_force)."""
+    r = np.asarray(radius, dtype=np.float64)
+    s_in, t_in, s_out, t_out = velocity_bnd_coefs(r, bc_icb, bc_cmb)
+    nr = len(r)
+
+    def rows(k, S, T):
+        if k == 0:
+            return t_in[0] * T[0] + t_in[1] * T[1] + t_in[2] * T[2], s_in[0] * S[0] + s_in[1] * S[1]
+        return (t_out[2] * T[nr - 3] + t_out[1] * T[nr - 2] + t_out[0] * T[nr - 1],
+                s_out[1] * S[nr - 2] + s_out[0] * S[nr - 1])
+    return _rot_field(r, l_of_j, S, dS, T, rows)
+
+
+INSULATOR, PSEUDO_VACUUM = "insulator", "pseudo_vacuum"
+
+
+def current(radius, l_of_j, S, dS, T, bc_icb=INSULATOR, bc_cmb=INSULATOR):
+    """const_sph_current (const_sph_rotation.f90:141-158) with sel_bc_sph_current
+    (select_exp_magne_bc.f90:172-218): the non-slip coefficient rows, an
+    insulator folding the potential field's dS/dr = (l+1) S / r (inner,
+    cal_sph_nod_icb_ins_rot2) or -l S / r (outer, cal_sph_nod_cmb_ins_rot2)
+    into the second derivative through the fixed derivative's coefficient
+    (fdm2_fix_dr_ICB(-1,3), fdm2_fix_dr_CMB(1,3)); pseudo-vacuum rows keep
+    dS/dr = 0 (cal_sph_nod_icb_qvc_rot2 / cal_sph_nod_cmb_qvc_rot2)."""
+    r = np.asarray(radius, dtype=np.float64)
+    nr = len(r)
+    l = np.asarray(l_of_j).astype(np.float64)
+    s_in, t_in, s_out, t_out = velocity_bnd_coefs(r, NON_SLIP, NON_SLIP)
+    dr = r[1] - r[0]
+    cdr_in = inverse33([[1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [dr, 1.0, dr * dr / 2.0]])[2, 0]
+    dn = r[-1] - r[-2]
+    cdr_out = inverse33([[1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [1.0, -dn, dn * dn / 2.0]])[2, 1]
+
+    def rows(k, S, T):
+        if k == 0:
+            s0 = (l + 1.0) * (1.0 / r[0]) * cdr_in + s_in[0] if bc_icb == INSULATOR else s_in[0]
+            return t_in[0] * T[0] + t_in[1] * T[1] + t_in[2] * T[2], s0 * S[0] + s_in[1] * S[1]
+        s0 = s_out[0] - l * (1.0 / r[nr - 1]) * cdr_out if bc_cmb == INSULATOR else s_out[0]
+        return (t_out[2] * T[nr - 3] + t_out[1] * T[nr - 2] + t_out[0] * T[nr - 1],
+                s_out[1] * S[nr - 2] + s0 * S[nr - 1])
+    return _rot_field(r, l_of_j, S, dS, T, rows)

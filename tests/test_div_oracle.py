@@ -184,3 +184,30 @@ def test_pseudo_vacuum_rows():
     assert np.array_equal(pol, T.reshape(cfg.nr, -1))
     for k in (0, -1):
         assert not dpol[k].any() and not tor[k].any()
+
+
+def test_vorticity_and_current_exact_cases():
+    """Interior: tor = -d2S/dr2 + l(l+1) S / r^2 exactly for quadratic S; an
+    insulating outer row is exact for a quadratic S with the potential field's
+    slope dS/dr = -l S / r there (inner: (l + 1) S / r)."""
+    from oracle.sph_div import current, vorticity
+    cfg = SphConfig(15, 24, 48, 9)
+    r = cfg.radius()
+    l, _ = rj_order(cfg.ltr)
+    lf = l.astype(np.float64)
+    g3 = lf * (lf + 1.0)
+    rng = np.random.default_rng(16)
+    a, b, c = (rng.standard_normal(cfg.J) for _ in range(3))
+    S = np.outer(np.ones_like(r), a) + np.outer(r, b) + np.outer(r * r, c)
+    T = np.zeros_like(S)
+    for f in (vorticity, current):
+        tor = f(r, l, S.reshape(-1), np.zeros(S.size), T.reshape(-1))[2].reshape(cfg.nr, -1)
+        ref = -2.0 * c + g3 * S / r[:, None] ** 2
+        assert np.abs(tor[1:-1] - ref[1:-1]).max() < 1e-9 * np.abs(ref).max()
+    for side in (0, -1):
+        rb = r[side]
+        slope = (lf + 1.0) / rb if side == 0 else -lf / rb
+        S2 = np.outer(np.ones_like(r), a) + np.outer(r - rb, slope * a) + np.outer((r - rb) ** 2, c)
+        tor = current(r, l, S2.reshape(-1), np.zeros(S2.size), T.reshape(-1))[2].reshape(cfg.nr, -1)
+        ref = -(2.0 * c - g3 * S2[side] / rb ** 2)
+        assert np.abs(tor[side] - ref).max() < 1e-8 * np.abs(ref).max()

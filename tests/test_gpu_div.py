@@ -246,3 +246,37 @@ def test_rot_induction_bc_matches_oracle(bc_icb, bc_cmb):
     got = from_dev_fortran(t)
     for q in range(3):
         assert _relerr(got[:, 3 + q], ref[q]) <= 1e-13, q
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("which,bc_icb,bc_cmb,host", [("vort", 0, 0, False), ("vort", 1, 0, True),
+                                                      ("cur", 0, 0, False), ("cur", 1, 0, False),
+                                                      ("cur", 0, 1, True)],
+                         ids=["vort_nonslip", "vort_free_nonslip_host", "cur_ins", "cur_qvac_ins",
+                              "cur_ins_qvac_host"])
+def test_vorticity_current_match_oracle(which, bc_icb, bc_cmb, host):
+    from kemorin_mhd_b200.sph_trans import SphTransform
+    from oracle.sph_div import FREE_SLIP, INSULATOR, NON_SLIP, PSEUDO_VACUUM, current, vorticity
+    cfg = CFG
+    tr = SphTransform(cfg, tier=TIER_FP64)
+    n = cfg.J * cfg.nr
+    d = np.asfortranarray(np.random.default_rng(23).standard_normal((n, 6)))
+    l, _ = rj_order(cfg.ltr)
+    if which == "vort":
+        names = {0: NON_SLIP, 1: FREE_SLIP}
+        ref = vorticity(cfg.radius(), l, d[:, 0], d[:, 1], d[:, 2], names[bc_icb], names[bc_cmb])
+        call = tr.vorticity
+    else:
+        names = {0: INSULATOR, 1: PSEUDO_VACUUM}
+        ref = current(cfg.radius(), l, d[:, 0], d[:, 1], d[:, 2], names[bc_icb], names[bc_cmb])
+        call = tr.current
+    if host:
+        arr = d.copy(order="F")
+        call(arr, 0, 3, bc_icb, bc_cmb)
+        got = arr
+    else:
+        t = to_dev_fortran(d)
+        call(t, 0, 3, bc_icb, bc_cmb)
+        got = from_dev_fortran(t)
+    for q in range(3):
+        assert _relerr(got[:, 3 + q], ref[q]) <= 1e-13, q
