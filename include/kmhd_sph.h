@@ -248,7 +248,10 @@ int kmhd_sph_rot_induction_bc(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int
                               int32_t bc_icb, int32_t bc_cmb, int32_t ptr_kind);
 
 /* Current density J = curl B from the magnetic field's spectra (columns
- * col_magne .. + 2) into col_current .. + 2: pol = T, dpol/dr = dT/dr, tor =
+ * col_magne .. + 2) into col_current .. + 2 (the time loop's
+ * const_grad_bp_and_current, const_sph_radial_grad.f90:166-200, forms the same
+ * rows and also extends the potential field to radii outside the shell, which
+ * a shell-only grid does not have).  Rows: pol = T, dpol/dr = dT/dr, tor =
  * -d2S/dr2 + l(l+1) S / r^2 with 3-point FDMs (cal_sph_nod_vect_rot2,
  * MHD_src/sph_MHD/cal_sph_exp_rotation.f90:157-203), boundary rows per
  * KMHD_BC_INSULATOR / KMHD_BC_PSEUDO_VACUUM: replaces const_sph_current
@@ -281,8 +284,12 @@ int kmhd_sph_rot_force(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t co
 
 /* Vorticity = curl u from the velocity's spectra into col_vort .. + 2, with
  * the interior rows of kmhd_sph_current and the velocity boundary rows of
- * kmhd_sph_rot_force (KMHD_BC_NON_SLIP / KMHD_BC_FREE_SLIP): replaces
+ * kmhd_sph_rot_force (KMHD_BC_NON_SLIP / KMHD_BC_FREE_SLIP), as
  * const_sph_vorticity (MHD_src/sph_MHD/const_sph_rotation.f90:111-137).  The
+ * time loop's const_grad_vp_and_vorticity (const_sph_radial_grad.f90:136-162,
+ * called from cal_sol_sph_MHD_crank.f90) gives the same vorticity for a
+ * velocity that meets its boundary condition; it also rewrites the velocity's
+ * boundary values and its dS/dr column, which this call leaves alone.  The
  * restart files hold u, not the vorticity. */
 int kmhd_sph_vorticity(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t col_velo, int32_t col_vort,
                        int32_t bc_icb, int32_t bc_cmb, int32_t ptr_kind);
