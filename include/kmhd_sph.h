@@ -302,6 +302,15 @@ int kmhd_sph_vorticity(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t co
 int kmhd_sph_div_force(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t col_fld, int32_t col_div,
                        int32_t ptr_kind);
 
+/* Curl of the radial buoyancy, the toroidal source of the vorticity equation:
+ * column col_out = coef_t * T * r, or (coef_t * T + coef_c * C) * r when
+ * col_c >= 0 (thermal and compositional buoyancy).  Replaces
+ * cal_rot_radial_self_gravity (MHD_src/sph_MHD/cal_rot_buoyancies_sph_MHD.f90:46-165,
+ * called from cal_sol_sph_MHD_crank.f90) into itor%i_rot_buoyancy.  Host or
+ * device pointers. */
+int kmhd_sph_rot_buoyancy(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t col_t, double coef_t,
+                          int32_t col_c, double coef_c, int32_t col_out, int32_t ptr_kind);
+
 /* Curl of the Coriolis term for a rotation about z, formed in spectral space
  * from the velocity (columns col_velo .. col_velo + 2 = S, dS/dr, T) and the
  * vorticity (col_vort .. col_vort + 2): column col_out = poloidal and

@@ -240,6 +240,9 @@ cudaError_t launch_rot_coriolis(long long J, int nr, const double* vel, const do
 // (south) for every radius, ncb columns with stride ldv (Cartesian vectors).
 cudaError_t launch_b_trans_pole(const Plan& p, const double* d_rj, long long ld, const int* cols, double* v,
                                 long long ldv, cudaStream_t s);
+// Curl of the radial buoyancy (kmhd_post.cu); C null: one scalar.
+cudaError_t launch_rot_buoyancy(long long J, int nr, const double* T, double coef_t, const double* C, double coef_c,
+                                double* out, const double* radius, cudaStream_t s);
 // Set-up of the on-the-fly tables (cos_t, pco, dco, pst, pseed of the plan).
 cudaError_t launch_otf_tables(const Plan& p, double* cos_t, double2* pco, double2* dco, double2* pst,
                               double* pseed, const long long* pseed_off, cudaStream_t s);

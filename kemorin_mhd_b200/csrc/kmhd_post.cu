@@ -232,6 +232,19 @@ __global__ void k_b_trans_pole(Plan P, const double* __restrict__ d_rj, long lon
   }
 }
 
+// Curl of the radial buoyancy (toroidal part): out = coef_t T r, or
+// (coef_t T + coef_c C) r with a second scalar (cal_rot_buoyancy_sph_MHD /
+// cal_rot_double_buoyancy_sph_MHD, MHD_src/sph_MHD/cal_rot_buoyancies_sph_MHD.f90:106-165).
+__global__ void k_rot_buoyancy(long long J, int nr, const double* __restrict__ T, double coef_t,
+                               const double* __restrict__ C, double coef_c, double* __restrict__ out,
+                               const double* __restrict__ radius) {
+  const long long n = J * nr;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(i / J);
+    out[i] = C ? (coef_t * T[i] + coef_c * C[i]) * radius[k] : coef_t * T[i] * radius[k];
+  }
+}
+
 }  // namespace
 
 cudaError_t launch_rot_vec(long long J, int nr, const double* S, const double* dS, const double* T, double* pol,
@@ -244,6 +257,19 @@ cudaError_t launch_rot_vec(long long J, int nr, const double* S, const double* d
   const int grid = (int)(want < 8LL * nsm ? want : 8LL * nsm);
   if (grid <= 0) return cudaSuccess;
   k_rot_vec<<<grid, 256, 0, s>>>(J, nr, S, dS, T, pol, dpol, tor, coef, b);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rot_buoyancy(long long J, int nr, const double* T, double coef_t, const double* C, double coef_c,
+                                double* out, const double* radius, cudaStream_t s) {
+  const long long n = J * nr;
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const long long want = (n + 255) / 256;
+  const int grid = (int)(want < 8LL * nsm ? want : 8LL * nsm);
+  if (grid <= 0) return cudaSuccess;
+  k_rot_buoyancy<<<grid, 256, 0, s>>>(J, nr, T, coef_t, C, coef_c, out, radius);
   return cudaGetLastError();
 }
 

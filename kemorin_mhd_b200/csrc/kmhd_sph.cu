@@ -1372,6 +1372,33 @@ int kmhd_sph_b_trans_pole(kmhd_sph* h, const double* d_rj, int64_t ld, const int
   return KMHD_OK;
 }
 
+int kmhd_sph_rot_buoyancy(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_t, double coef_t, int32_t col_c,
+                          double coef_c, int32_t col_out, int32_t ptr_kind) {
+  if (!h || !d_rj) return KMHD_ERR_ARG;
+  if (check_ld(h, ld)) return KMHD_ERR_ARG;
+  if (col_t < 0 || col_out < 0 || col_out == col_t || (col_c >= 0 && col_out == col_c)) return KMHD_ERR_ARG;
+  const Plan& p = h->plan;
+  KCHECK(cudaSetDevice(h->device));
+  const size_t nrj = (size_t)p.J * p.nr;
+  int st;
+  if (ptr_kind == KMHD_PTR_HOST) {
+    // T, C and the result in the divergence staging (3 columns)
+    if (!h->div_stage && (st = dalloc(h, &h->div_stage, 3 * nrj + 2 * (size_t)p.J))) return st;
+    double* s0 = h->div_stage;
+    KCHECK(cudaMemcpyAsync(s0, d_rj + ld * col_t, sizeof(double) * nrj, cudaMemcpyHostToDevice, h->stream));
+    if (col_c >= 0)
+      KCHECK(cudaMemcpyAsync(s0 + nrj, d_rj + ld * col_c, sizeof(double) * nrj, cudaMemcpyHostToDevice, h->stream));
+    KCHECK(launch_rot_buoyancy(p.J, p.nr, s0, coef_t, col_c >= 0 ? s0 + nrj : nullptr, coef_c, s0 + 2 * nrj, h->radius,
+                               h->stream));
+    KCHECK(cudaMemcpyAsync(d_rj + ld * col_out, s0 + 2 * nrj, sizeof(double) * nrj, cudaMemcpyDeviceToHost, h->stream));
+  } else {
+    KCHECK(launch_rot_buoyancy(p.J, p.nr, d_rj + ld * col_t, coef_t, col_c >= 0 ? d_rj + ld * col_c : nullptr, coef_c,
+                               d_rj + ld * col_out, h->radius, h->stream));
+  }
+  KCHECK(cudaStreamSynchronize(h->stream));
+  return KMHD_OK;
+}
+
 int kmhd_sph_last_kernel_timing(kmhd_sph* h, double* ms5) {
   if (!h || !ms5) return KMHD_ERR_ARG;
   if (!h->kernel_timed) return KMHD_ERR_STATE;

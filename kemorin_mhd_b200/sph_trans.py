@@ -66,7 +66,8 @@ EXPORTS = ["kmhd_sph_create", "kmhd_sph_destroy", "kmhd_sph_set_stream", "kmhd_s
            "kmhd_sph_last_kernel_timing", "kmhd_sph_get_path", "kmhd_selftest_wait_timeout",
            "kmhd_sph_div_flux", "kmhd_sph_rot_induction", "kmhd_sph_rot_force", "kmhd_sph_div_force",
            "kmhd_sph_rot_coriolis", "kmhd_sph_set_coriolis", "kmhd_sph_b_trans_pole",
-           "kmhd_sph_div_flux_bc", "kmhd_sph_rot_induction_bc", "kmhd_sph_vorticity", "kmhd_sph_current"]
+           "kmhd_sph_div_flux_bc", "kmhd_sph_rot_induction_bc", "kmhd_sph_vorticity", "kmhd_sph_current",
+           "kmhd_sph_rot_buoyancy"]
 
 _lib = None
 
@@ -105,6 +106,7 @@ def load_library(path: str | None = None):
     lib.kmhd_sph_rot_induction_bc.argtypes = [vp, vp, i64, i32, i32, i32, i32, i32]
     lib.kmhd_sph_vorticity.argtypes = [vp, vp, i64, i32, i32, i32, i32, i32]
     lib.kmhd_sph_current.argtypes = [vp, vp, i64, i32, i32, i32, i32, i32]
+    lib.kmhd_sph_rot_buoyancy.argtypes = [vp, vp, i64, i32, ctypes.c_double, i32, ctypes.c_double, i32, i32]
     lib.kmhd_selftest_wait_timeout.argtypes = [ctypes.c_int, ctypes.c_int]
     lib.kmhd_sph_get_tables.argtypes = [vp, i32] + [ctypes.POINTER(ctypes.c_double)] * 4
     lib.kmhd_sph_device_bytes.restype = i64
@@ -309,6 +311,15 @@ class SphTransform:
         n = self.cfg.J * self.cfg.nr
         _check(load_library().kmhd_sph_current(self._h, p, ld or n, col_magne, col_current, bc_icb, bc_cmb, kind),
                "kmhd_sph_current")
+        return d_rj
+
+    def rot_buoyancy(self, d_rj, col_t: int, coef_t: float, col_out: int, col_c: int = -1, coef_c: float = 0.0,
+                     ld: int | None = None):
+        """Toroidal curl of the radial buoyancy: (coef_t T [+ coef_c C]) r into col_out."""
+        p, kind = _ptr(d_rj)
+        n = self.cfg.J * self.cfg.nr
+        _check(load_library().kmhd_sph_rot_buoyancy(self._h, p, ld or n, col_t, float(coef_t), col_c, float(coef_c),
+                                                    col_out, kind), "kmhd_sph_rot_buoyancy")
         return d_rj
 
     def rot_induction(self, d_rj, col_fld: int, col_rot: int, ld: int | None = None):

@@ -305,3 +305,14 @@ def current(radius, l_of_j, S, dS, T, bc_icb=INSULATOR, bc_cmb=INSULATOR):
         return (t_out[2] * T[nr - 3] + t_out[1] * T[nr - 2] + t_out[0] * T[nr - 1],
                 s_out[1] * S[nr - 2] + s0 * S[nr - 1])
     return _rot_field(r, l_of_j, S, dS, T, rows)
+
+
+def rot_buoyancy(radius, J, T, coef_t, C=None, coef_c=0.0):
+    """cal_rot_buoyancy_sph_MHD / cal_rot_double_buoyancy_sph_MHD
+    (MHD_src/sph_MHD/cal_rot_buoyancies_sph_MHD.f90:106-165): coef T r, or
+    (coef_t T + coef_c C) r."""
+    r = np.repeat(np.asarray(radius, dtype=np.float64), J)
+    T = np.asarray(T)
+    if C is None:
+        return coef_t * T * r
+    return (coef_t * T + coef_c * np.asarray(C)) * r

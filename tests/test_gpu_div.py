@@ -280,3 +280,26 @@ def test_vorticity_current_match_oracle(which, bc_icb, bc_cmb, host):
         got = from_dev_fortran(t)
     for q in range(3):
         assert _relerr(got[:, 3 + q], ref[q]) <= 1e-13, q
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("double,host", [(False, False), (True, False), (True, True)],
+                         ids=["thermal", "double", "double_host"])
+def test_rot_buoyancy_matches_oracle(double, host):
+    from kemorin_mhd_b200.sph_trans import SphTransform
+    from oracle.sph_div import rot_buoyancy
+    cfg = CFG
+    tr = SphTransform(cfg, tier=TIER_FP64)
+    n = cfg.J * cfg.nr
+    d = np.asfortranarray(np.random.default_rng(24).standard_normal((n, 3)))
+    ref = rot_buoyancy(cfg.radius(), cfg.J, d[:, 0], 2.5, d[:, 1] if double else None, -0.75)
+    kw = dict(col_c=1, coef_c=-0.75) if double else {}
+    if host:
+        arr = d.copy(order="F")
+        tr.rot_buoyancy(arr, 0, 2.5, 2, **kw)
+        got = arr[:, 2]
+    else:
+        t = to_dev_fortran(d)
+        tr.rot_buoyancy(t, 0, 2.5, 2, **kw)
+        got = from_dev_fortran(t)[:, 2]
+    assert _relerr(got, ref) <= 1e-14
