@@ -13,8 +13,53 @@
 
 using namespace kmhd::calypso;
 
+// Second mode (an output path as the third argument): the full MHD field set
+// through the spectral steps around the transform, as the reference's time
+// step orders them -- const_grad_vp_and_vorticity / const_grad_bp_and_current,
+// the cycle with the Coriolis curl, rot_momentum_eq_exp_sph,
+// cal_rot_radial_self_gravity -- on host arrays; d_fld is written to the path
+// (nnod x 47 doubles, column-major) for the test to compare with the oracle.
+static int run_full(int tier, const char* out_path) {
+  const int L = 15, nth = 24, nph = 48, nr = 6;
+  std::vector<double> radius(nr);
+  for (int k = 0; k < nr; ++k)
+    radius[k] = 0.35 / 0.65 + 0.5 * (1.0 / 0.65 - 0.35 / 0.65) * (1.0 - std::cos(M_PI * k / (nr - 1)));
+  PhysAddress ipol;
+  ipol.i_velo = 1; ipol.i_vort = 4; ipol.i_magne = 7; ipol.i_current = 10; ipol.i_temp = 13; ipol.i_light = 14;
+  ipol.i_m_advect = 15; ipol.i_lorentz = 18; ipol.i_vp_induct = 21; ipol.i_h_flux = 24; ipol.i_c_flux = 27;
+  ipol.i_k_heli = 30;
+  ipol.i_rot_inertia = 31; ipol.i_rot_Lorentz = 34; ipol.i_induction = 37; ipol.i_h_advect = 40;
+  ipol.i_c_advect = 41; ipol.i_rot_Coriolis = 42; ipol.i_rot_buoyancy = 45;
+  const int ntot = 47;
+  const long J = (long)(L + 1) * (L + 1), nnod = J * nr;
+  std::vector<double> d_fld(nnod * ntot, 0.0);
+  std::mt19937_64 g(11);
+  std::normal_distribution<double> nd;
+  for (int c : {0, 1, 2, 6, 7, 8, 12, 13})
+    for (long i = 0; i < nnod; ++i) d_fld[c * nnod + i] = nd(g);
+  try {
+    SphTransMHD tr(L, nth, nph, radius, ipol, tier);
+    SphBoundaries bc;   // non-slip, insulating, fixed (zero) temperature and composition
+    tr.init_sum_coriolis_rlm(2.0e2);
+    tr.const_grad_vp_and_vorticity(d_fld.data(), bc);
+    tr.const_grad_bp_and_current(d_fld.data(), bc);
+    tr.nonlinear_by_pseudo_sph(d_fld.data());
+    tr.rot_momentum_eq_exp_sph(d_fld.data(), bc);
+    tr.cal_rot_radial_self_gravity(d_fld.data(), 3.0, -1.5);
+  } catch (const TransformError& e) {
+    std::fprintf(stderr, "%s\n", e.what());
+    return 3;
+  }
+  FILE* f = std::fopen(out_path, "wb");
+  if (!f) return 2;
+  const size_t n = std::fwrite(d_fld.data(), sizeof(double), d_fld.size(), f);
+  std::fclose(f);
+  return n == d_fld.size() ? 0 : 2;
+}
+
 int main(int argc, char** argv) {
-  if (argc < 2) { std::fprintf(stderr, "usage: %s liboracle.so\n", argv[0]); return 2; }
+  if (argc < 2) { std::fprintf(stderr, "usage: %s liboracle.so [tier [out]]\n", argv[0]); return 2; }
+  if (argc > 3) return run_full(std::atoi(argv[2]), argv[3]);
   const int L = 15, nth = 24, nph = 48, nr = 5;
   std::vector<double> radius(nr);
   for (int k = 0; k < nr; ++k)
