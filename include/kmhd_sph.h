@@ -69,8 +69,8 @@ typedef struct kmhd_sph_desc {
   int32_t nr;           /* radial points (nidx_rj(1))                          */
   const double *radius; /* [nr] host, radius_1d_rj_r                           */
   const int32_t *idx_rj_lm; /* [2*(L+1)^2] host (l, m) per rj j, or NULL       */
-  int32_t nvector_b, nscalar_b;   /* rj -> rtp fields  (nvector_rj_2_rtp ...)  */
-  int32_t nvector_f, nscalar_f;   /* rtp -> rj fields  (nvector_rtp_2_rj ...)  */
+  int32_t nvector_b, nscalar_b;   /* rj -> rtp fields  (nvector_rj_2_rtp ...), <= 5 / 2 */
+  int32_t nvector_f, nscalar_f;   /* rtp -> rj fields  (nvector_rtp_2_rj ...), <= 5 / 2 */
   int32_t nproduct;               /* grid products for kmhd_sph_cycle          */
   const kmhd_product *products;   /* [nproduct] host                           */
   int32_t tier;                   /* enum kmhd_tier                            */
