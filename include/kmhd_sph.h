@@ -71,6 +71,7 @@ typedef struct kmhd_sph_desc {
   const int32_t *idx_rj_lm; /* [2*(L+1)^2] host (l, m) per rj j, or NULL       */
   int32_t nvector_b, nscalar_b;   /* rj -> rtp fields  (nvector_rj_2_rtp ...), <= 5 / 2 */
   int32_t nvector_f, nscalar_f;   /* rtp -> rj fields  (nvector_rtp_2_rj ...), <= 5 / 2 */
+                                  /* split tiers: at most 6 fields per direction   */
   int32_t nproduct;               /* grid products for kmhd_sph_cycle          */
   const kmhd_product *products;   /* [nproduct] host                           */
   int32_t tier;                   /* enum kmhd_tier                            */
