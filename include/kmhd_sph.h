@@ -338,7 +338,10 @@ int kmhd_sph_rot_coriolis(kmhd_sph *handle, double *d_rj, int64_t ld_rj, int32_t
  * own staged copies (no second transfer).  The two columns may not be written
  * by a forward field, nor be input columns when input and output are one
  * array (KMHD_ERR_ARG at the cycle call).  iv_velo < 0 switches it off.  The
- * tables are built here (device memory), not inside the cycle. */
+ * tables are built here (device memory), not inside the cycle.  The separable
+ * calls split it as the reference does: kmhd_sph_b_trans forms the curl from
+ * its input spectra and the next kmhd_sph_f_trans writes it into d_rj's
+ * columns col_out and col_out + 2. */
 int kmhd_sph_set_coriolis(kmhd_sph *handle, double coef_cor, int32_t iv_velo, int32_t iv_vort, int32_t col_out);
 
 /* Backward transform at the poles, for grids with pole points: v_pole is a

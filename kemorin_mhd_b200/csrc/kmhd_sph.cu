@@ -67,6 +67,7 @@ struct kmhd_sph {
   int cor_on = 0, cor_iv_velo = 0, cor_iv_vort = 0, cor_col = 0;
   double cor_coef = 0.0;
   double* cor_cyc = nullptr;  // 2 J*Nr staging columns for host-pointer cycles
+  int cor_pending = 0;        // kmhd_sph_b_trans left a Coriolis curl in cor_cyc for kmhd_sph_f_trans
   double* pole_out = nullptr;  // (2 Nr) x ncb pole values for host-pointer calls
   std::vector<double> radius_h;
   std::vector<int> cols_b_cache, cols_f_cache;
@@ -763,6 +764,18 @@ int kmhd_sph_b_trans(kmhd_sph* h, const double* d_rj, int64_t ld, const int32_t*
     grid = h->stage_grid;
   }
   if ((st = timed_begin(h))) return st;
+  if (h->cor_on) {
+    // sph_b_trans_w_coriolis: the Coriolis curl of the received spectra, kept
+    // for the next kmhd_sph_f_trans (copy_coriolis_terms_rlm)
+    const size_t nrj = (size_t)p.J * p.nr;
+    if (!h->cor_cyc && (st = dalloc(h, &h->cor_cyc, 2 * nrj))) return st;
+    const int iv = ptr_kind == KMHD_PTR_HOST ? cc[h->cor_iv_velo] : cols_b[h->cor_iv_velo];
+    const int iw = ptr_kind == KMHD_PTR_HOST ? cc[h->cor_iv_vort] : cols_b[h->cor_iv_vort];
+    if ((st = enqueue_coriolis(h, src + sld * iv, src + sld * iw, sld, h->cor_cyc, h->cor_cyc + nrj, 0, p.nr,
+                               h->stream)))
+      return st;
+    h->cor_pending = 1;
+  }
   if ((st = run_bwd_spectral(h, src, sld))) return st;
   KCHECK(cudaEventRecord(h->ev[1], h->stream));
   KCHECK(launch_fft_bwd_grid(p, grid, h->stream));
@@ -780,6 +793,10 @@ int kmhd_sph_f_trans(kmhd_sph* h, const double* frc_rtp, double* d_rj, int64_t l
   if (check_ld(h, ld)) return KMHD_ERR_ARG;
   const Plan& p = h->plan;
   if (p.ncf == 0) return KMHD_ERR_STATE;
+  if (h->cor_on && h->cor_pending)
+    for (int q = 0; q < 3; q += 2)
+      for (int f = 0; f < p.nvf + p.nsf; ++f)
+        if (h->cor_col + q >= cols_f[f] && h->cor_col + q < cols_f[f] + (f < p.nvf ? 3 : 1)) return KMHD_ERR_ARG;
   KCHECK(cudaSetDevice(h->device));
   const size_t nnod = (size_t)p.nr * p.nth * p.nph;
   const size_t nrj = (size_t)p.J * p.nr;
@@ -813,6 +830,14 @@ int kmhd_sph_f_trans(kmhd_sph* h, const double* frc_rtp, double* d_rj, int64_t l
         KCHECK(cudaMemcpyAsync(d_rj + ld * (cols_f[f] + q), out + nrj * (cc[f] + q), sizeof(double) * nrj,
                                cudaMemcpyDeviceToHost, h->stream));
     }
+  }
+  if (h->cor_on && h->cor_pending) {
+    // sph_f_trans_w_coriolis: copy_coriolis_terms_rlm into the forward output
+    const cudaMemcpyKind kind = ptr_kind == KMHD_PTR_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    for (int q = 0; q < 2; ++q)
+      KCHECK(cudaMemcpyAsync(d_rj + ld * (h->cor_col + 2 * q), h->cor_cyc + nrj * q, sizeof(double) * nrj, kind,
+                             h->stream));
+    h->cor_pending = 0;
   }
   KCHECK(cudaStreamSynchronize(h->stream));
   return finish_timing(h);

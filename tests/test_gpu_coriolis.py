@@ -187,3 +187,40 @@ def test_cycle_with_coriolis_rejects_conflicting_columns():
     out = torch.zeros((cfg.ncf + 3, cfg.J * cfg.nr), dtype=torch.float64, device="cuda")
     with pytest.raises(KmhdError):
         tr.nonlinear_cycle(d, out)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("host", [False, True], ids=["device", "host"])
+def test_separable_transforms_carry_coriolis(host):
+    """kmhd_sph_b_trans forms the registered Coriolis curl from its input and
+    the next kmhd_sph_f_trans writes it out (sph_b_trans_w_coriolis /
+    sph_f_trans_w_coriolis); equal to the standalone curl of the same input."""
+    import torch
+    from kemorin_mhd_b200.sph_trans import SphTransform
+    cfg = CFG
+    tr = SphTransform(cfg, tier=TIER_FP64)
+    d = make_d_rj(cfg, seed=47)
+    n = cfg.J * cfg.nr
+    ref_in = np.asfortranarray(np.concatenate([d, np.zeros((n, 3))], 1))
+    ref_t = to_dev_fortran(ref_in)
+    tr.rot_coriolis(ref_t, 0, 3, cfg.ncb, 5.0)
+    ref = from_dev_fortran(ref_t)
+    tr.set_coriolis(5.0, 0, 1, cfg.ncf)
+    nnod = cfg.nr * cfg.nth * cfg.nph
+    if host:
+        grid = np.zeros((nnod, cfg.ncb), order="F")
+        tr.sph_b_trans(np.asfortranarray(d), grid)
+        frc = np.zeros((nnod, cfg.ncf), order="F")
+        out = np.full((n, cfg.ncf + 3), 9.0, order="F")
+        tr.sph_f_trans(frc, out)
+        got = out
+    else:
+        grid = torch.zeros((cfg.ncb, nnod), dtype=torch.float64, device="cuda")
+        tr.sph_b_trans(to_dev_fortran(d), grid)
+        frc = torch.zeros((cfg.ncf, nnod), dtype=torch.float64, device="cuda")
+        out = torch.full((cfg.ncf + 3, n), 9.0, dtype=torch.float64, device="cuda")
+        tr.sph_f_trans(frc, out)
+        got = from_dev_fortran(out)
+    assert np.array_equal(got[:, cfg.ncf], ref[:, cfg.ncb])
+    assert np.array_equal(got[:, cfg.ncf + 2], ref[:, cfg.ncb + 2])
+    assert (got[:, cfg.ncf + 1] == 9.0).all()
