@@ -866,9 +866,11 @@ struct DFT2F_ZM<3, B, SIGN> {
 // inputs from the staged spectra.  Twiddles w^(j q) are read straight from the
 // table (j q < N here).  When N = 3 (L + 1) (PR), the middle third of the
 // inputs (L < k < N - L) is zero and the outer thirds need no range checks.
-template <int N, bool PR>
+// st: the line's records, staged (order stride 2 ncs) or, with INPLACE, the
+// rtm records themselves (order stride rsg doubles)
+template <int N, bool PR, bool INPLACE = false>
 __device__ __forceinline__ void ff_dif_first(const double* st, int nc, int nv, double2* z, int npair, int L,
-                                             const double2* __restrict__ tw) {
+                                             const double2* __restrict__ tw, long long rsg = 0) {
   constexpr int R = ff_first(N), S1 = N / R, NP = N + 1, T3 = R / 3;
   for (int it = threadIdx.x; it < npair * S1; it += blockDim.x) {
     const int pp = it / S1, j = it - pp * S1;
@@ -888,7 +890,7 @@ __device__ __forceinline__ void ff_dif_first(const double* st, int nc, int nv, d
         }
         const bool mir = r >= 2 * T3;
         const int m = mir ? N - j - r * S1 : j + r * S1;
-        const double* rec = st + (m <= L ? m : 0) * rs;
+        const double* rec = INPLACE ? st + (long long)(m <= L ? m : 0) * rsg : st + (m <= L ? m : 0) * rs;
         const double2 c0 = *reinterpret_cast<const double2*>(rec + o0);
         const double2 c1 = o1 >= 0 ? *reinterpret_cast<const double2*>(rec + o1) : make_double2(0.0, 0.0);
         if (mir) {
@@ -901,7 +903,8 @@ __device__ __forceinline__ void ff_dif_first(const double* st, int nc, int nv, d
       DFT2F_ZM<3, T3, +1>::run(x);
     } else {
 #pragma unroll
-      for (int r = 0; r < R; ++r) x[r] = spec_at_t(st, nc, nv, pp, j + r * S1, N, L);
+      for (int r = 0; r < R; ++r)
+        x[r] = INPLACE ? spec_at(st, nc, nv, pp, j + r * S1, N, L, rsg) : spec_at_t(st, nc, nv, pp, j + r * S1, N, L);
       DFT<R, +1>::run(x);
     }
     double2* zp = z + pp * NP;
@@ -1208,7 +1211,7 @@ __device__ void ff_store_records(const double2* z, const Plan& P, double* rtm, i
 // doubles past each record zero-filled, which lands the records at the
 // conflict-free stride 2 ncs that the first pass reads; completion on an
 // mbarrier with a bounded wait.  Otherwise 16-byte cp.async pieces.
-template <int N, int MVB, int MSB, int MVF, int MSF, bool PR, int PK>
+template <int N, int MVB, int MSB, int MVF, int MSF, bool PR, int PK, bool STG = true>
 __global__ void __launch_bounds__(kFftThreadsF, 1)
     k_fft_cycle_f(Plan P, int line0, int nlines, const __grid_constant__ CUtensorMap tmap, int tma, int mbox) {
   extern __shared__ double4 smraw[];
@@ -1222,6 +1225,28 @@ __global__ void __launch_bounds__(kFftThreadsF, 1)
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(st + (P.L + 1) * NCS2);
   int line = line0 + blockIdx.x;
   if (line >= nlines) return;
+  if constexpr (!STG) {
+    // only the grid fits in shared memory: the first pass reads the line's
+    // records in place (order stride nth nr ncb 2)
+    const long long rsg = (long long)P.nth * P.nr * P.ncb * 2;
+    for (; line < nlines; line += gridDim.x) {
+      const int th = line % P.nth, r = line / P.nth;
+      ff_dif_first<N, PR, true>(P.rtm_b + rtm_off(P, 0, th, r, P.ncb), P.ncb, P.nvb, z, npb, P.L, P.twid, rsg);
+      __syncthreads();
+      ff_mid_pass<N, +1>(z, npb, P.twid);
+      __syncthreads();
+      ff_fused<N, MVB, MSB, MVF, MSF, PK>(z, P);
+      __syncthreads();
+      ff_mid_pass<N, -1>(z, npf, P.twid);
+      __syncthreads();
+      ff_dit_last<N, PR>(z, npf, P.twid);
+      __syncthreads();
+      if constexpr ((3 * MVF + MSF) % 2 == 0) ff_store_records<N, MVF, MSF>(z, P, P.rtm_f, th, r);
+      else ff_store_line<N>(z, npf, P, P.rtm_f, P.ncf, P.nvf, th, r);
+      __syncthreads();
+    }
+    return;
+  }
   if (tma && threadIdx.x == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(ssa(bar)));
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -1282,10 +1307,11 @@ __global__ void __launch_bounds__(kFftThreadsF, 1)
   }
 }
 
-template <int N, int MVB, int MSB, int MVF, int MSF, bool PR, int PK>
+template <int N, int MVB, int MSB, int MVF, int MSF, bool PR, int PK, bool STG = true>
 cudaError_t run_cycle_fk(const Plan& p, cudaStream_t s) {
-  auto kern = k_fft_cycle_f<N, MVB, MSB, MVF, MSF, PR, PK>;
-  const size_t smem = smem_cycle_f(p);
+  auto kern = k_fft_cycle_f<N, MVB, MSB, MVF, MSF, PR, PK, STG>;
+  const int npair = ((p.ncb > p.ncf ? p.ncb : p.ncf) + 1) / 2;
+  const size_t smem = STG ? smem_cycle_f(p) : sizeof(double2) * (size_t)npair * (N + 1);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int dev = 0, nsm = 0, occ = 0;
@@ -1301,9 +1327,19 @@ cudaError_t run_cycle_fk(const Plan& p, cudaStream_t s) {
   CUtensorMap map;
   std::memset(&map, 0, sizeof(map));
   int mbox = 1;
-  const int tma = make_rtm_map(p, &map, &mbox) ? 1 : 0;
+  const int tma = STG && make_rtm_map(p, &map, &mbox) ? 1 : 0;
   kern<<<grid, kFftThreadsF, smem, s>>>(p, line0, nlines, map, tma, mbox);
   return cudaGetLastError();
+}
+
+// The specialised passes without staging (the first pass reads the records in
+// place), for lines whose grid fits in shared memory but not with the staged
+// spectra; generic products.
+template <int N, int MVB, int MSB, int MVF, int MSF>
+cudaError_t run_cycle_fu(const Plan& p, cudaStream_t s) {
+  const bool pr = p.nph == 3 * (p.L + 1);
+  return pr ? run_cycle_fk<N, MVB, MSB, MVF, MSF, true, 0, false>(p, s)
+            : run_cycle_fk<N, MVB, MSB, MVF, MSF, false, 0, false>(p, s);
 }
 
 // the standard MHD product list, after the vectors-first reordering
@@ -1437,6 +1473,14 @@ cudaError_t run_cycle_wide(const Plan& p, cudaStream_t s) {
 
 cudaError_t launch_fft_cycle(const Plan& p, cudaStream_t s) {
   if (smem_cycle(p) > 227 * 1024 && smem_cycle_f(p) > 227 * 1024) {
+    // the specialised passes need (N + 1)-strided pairs: at most 16 pairs more
+    if (smem_direct(p) + 16 * 16 <= 227 * 1024) {
+      // the reference's full MHD set (u, omega, B, J + T, C -> five vectors + one scalar) at its own counts
+      if (p.nph == 1536 && p.nvb == 4 && p.nsb == 2 && p.nvf == 5 && p.nsf == 1)
+        return run_cycle_fu<1536, 4, 2, 5, 1>(p, s);
+      if (p.nph == 1536) return run_cycle_fu<1536, kMaxVec, kMaxScl, kMaxVec, kMaxScl>(p, s);
+      if (p.nph == 768) return run_cycle_fu<768, kMaxVec, kMaxScl, kMaxVec, kMaxScl>(p, s);
+    }
     if (smem_direct(p) <= 227 * 1024) return run_cycle_direct<kMaxVec, kMaxScl, kMaxVec, kMaxScl>(p, s);
     if (p.nvb == 3 && p.nsb == 1 && p.nvf == 3 && p.nsf == 1) return run_cycle_wide<3, 1, 3, 1>(p, s);
     return run_cycle_wide<kMaxVec, kMaxScl, kMaxVec, kMaxScl>(p, s);
