@@ -176,9 +176,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-tier comparison run")
     ap.add_argument("--nr", type=int, default=0, help="override the radius count (small profiling cases)")
-    ap.add_argument("--fields", default="default", choices=["default", "full"],
-                    help="field set: default u,omega,B + T; full u,omega,B,J + T,C with the Lorentz force and "
-                         "the composition flux")
+    ap.add_argument("--fields", default="default", choices=["default", "dynamo", "full"],
+                    help="field set: default u,omega,B + T; dynamo u,omega,B,J + T with the Lorentz force; "
+                         "full u,omega,B,J + T,C with the Lorentz force and the composition flux")
     ap.add_argument("--p-on-the-fly", action="store_true",
                     help="FP64 tier: P_l^m generated inside the Legendre kernels (no stored tables); "
                          "also times the stored-table FP64 tier on the same input")

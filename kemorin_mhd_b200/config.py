@@ -122,17 +122,23 @@ NAMED = {"cfg1": CFG1, "cfg2": CFG2, "cfg3": CFG3, "cfg5": CFG5}
 
 # Field sets of the reference's MHD transforms (set_address_sph_trans_MHD.f90):
 # "default" = u, omega, B + T -> omega x u, u x B, u T + u.omega;
+# "dynamo" = u, omega, B, J + T -> omega x u, J x B, u x B, u T (the dynamo
+# benchmark set with the Lorentz force);
 # "full" = u, omega, B, J + T, C -> omega x u, J x B, u x B, u T, u C + u.omega.
 FIELD_SETS = {
     "default": dict(nvb=3, nsb=1, nvf=3, nsf=1,
                     products=((PROD_CROSS, 1, 0, 1.0), (PROD_CROSS, 0, 2, 1.0), (PROD_VEC_SCALAR, 0, 0, 1.0),
                               (PROD_DOT, 0, 1, 1.0))),
+    "dynamo": dict(nvb=4, nsb=1, nvf=4, nsf=0,
+                   products=((PROD_CROSS, 1, 0, 1.0), (PROD_CROSS, 3, 2, 1.0), (PROD_CROSS, 0, 2, 1.0),
+                             (PROD_VEC_SCALAR, 0, 0, 1.0))),
     "full": dict(nvb=4, nsb=2, nvf=5, nsf=1,
                  products=((PROD_CROSS, 1, 0, 1.0), (PROD_CROSS, 3, 2, 1.0), (PROD_CROSS, 0, 2, 1.0),
                            (PROD_VEC_SCALAR, 0, 0, 1.0), (PROD_VEC_SCALAR, 0, 1, 1.0), (PROD_DOT, 0, 1, 1.0))),
 }
 FIELD_NAMES = {
     "default": ("u,omega,B + T", "omega x u, u x B, u T + u.omega"),
+    "dynamo": ("u,omega,B,J + T", "omega x u, J x B, u x B, u T"),
     "full": ("u,omega,B,J + T,C", "omega x u, J x B, u x B, u T, u C + u.omega"),
 }
 

@@ -1478,6 +1478,9 @@ cudaError_t launch_fft_cycle(const Plan& p, cudaStream_t s) {
       // the reference's full MHD set (u, omega, B, J + T, C -> five vectors + one scalar) at its own counts
       if (p.nph == 1536 && p.nvb == 4 && p.nsb == 2 && p.nvf == 5 && p.nsf == 1)
         return run_cycle_fu<1536, 4, 2, 5, 1>(p, s);
+      // the dynamo benchmark set (u, omega, B, J + T -> omega x u, J x B, u x B, u T)
+      if (p.nph == 1536 && p.nvb == 4 && p.nsb == 1 && p.nvf == 4 && p.nsf == 0)
+        return run_cycle_fu<1536, 4, 1, 4, 0>(p, s);
       if (p.nph == 1536) return run_cycle_fu<1536, kMaxVec, kMaxScl, kMaxVec, kMaxScl>(p, s);
       if (p.nph == 768) return run_cycle_fu<768, kMaxVec, kMaxScl, kMaxVec, kMaxScl>(p, s);
     }

@@ -65,14 +65,16 @@ def test_six_fields_host_chunked_equals_device():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("fields", ["dynamo", "full"])
 @pytest.mark.parametrize("tier", [TIER_FP64, TIER_SPLIT_I8], ids=["fp64", "split"])
-def test_full_set_wide_grid_reads_spectra_in_place(tier):
-    """L=255 on a 1536-point phi grid with the full set: the line's 8 grid
-    pairs (197 KB) fit in shared memory but not with the staged spectra, so
-    the fused FFT reads the spectra in place (k_fft_cycle_direct)."""
+def test_wide_grid_field_sets_read_spectra_in_place(tier, fields):
+    """L=255 on a 1536-point phi grid with the dynamo and full sets: the
+    line's grid pairs (7 or 8, up to 197 KB) fit in shared memory but not with
+    the staged spectra, so the specialised FFT passes read the spectra in
+    place (instantiated at each set's own counts)."""
     import torch
     from kemorin_mhd_b200.sph_trans import SphTransform
-    cfg = SphConfig(255, 384, 1536, 3, name="L255_full_wide", **FULL)
+    cfg = SphConfig(255, 384, 1536, 3, name="L255_wide_" + fields, **(FULL if fields == "full" else DYNAMO))
     d = make_d_rj(cfg, seed=83)
     ref = Oracle(cfg, nthreads=16).cycle(d)
     tr = SphTransform(cfg, tier=tier)
