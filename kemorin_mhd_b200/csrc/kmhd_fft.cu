@@ -1211,8 +1211,10 @@ __device__ void ff_store_records(const double2* z, const Plan& P, double* rtm, i
 // doubles past each record zero-filled, which lands the records at the
 // conflict-free stride 2 ncs that the first pass reads; completion on an
 // mbarrier with a bounded wait.  Otherwise 16-byte cp.async pieces.
-template <int N, int MVB, int MSB, int MVF, int MSF, bool PR, int PK, bool STG = true>
-__global__ void __launch_bounds__(kFftThreadsF, 1)
+// NT threads: fewer threads leave more registers to each for the fused
+// products of many fields (the unstaged variants)
+template <int N, int MVB, int MSB, int MVF, int MSF, bool PR, int PK, bool STG = true, int NT = kFftThreadsF>
+__global__ void __launch_bounds__(NT, 1)
     k_fft_cycle_f(Plan P, int line0, int nlines, const __grid_constant__ CUtensorMap tmap, int tma, int mbox) {
   extern __shared__ double4 smraw[];
   constexpr int NP = N + 1;
@@ -1307,9 +1309,9 @@ __global__ void __launch_bounds__(kFftThreadsF, 1)
   }
 }
 
-template <int N, int MVB, int MSB, int MVF, int MSF, bool PR, int PK, bool STG = true>
+template <int N, int MVB, int MSB, int MVF, int MSF, bool PR, int PK, bool STG = true, int NT = kFftThreadsF>
 cudaError_t run_cycle_fk(const Plan& p, cudaStream_t s) {
-  auto kern = k_fft_cycle_f<N, MVB, MSB, MVF, MSF, PR, PK, STG>;
+  auto kern = k_fft_cycle_f<N, MVB, MSB, MVF, MSF, PR, PK, STG, NT>;
   const int npair = ((p.ncb > p.ncf ? p.ncb : p.ncf) + 1) / 2;
   const size_t smem = STG ? smem_cycle_f(p) : sizeof(double2) * (size_t)npair * (N + 1);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1317,7 +1319,7 @@ cudaError_t run_cycle_fk(const Plan& p, cudaStream_t s) {
   int dev = 0, nsm = 0, occ = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kFftThreadsF, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NT, smem);
   if (occ < 1) occ = 1;
   // lines (r, theta) of the radial window, theta fastest
   const int line0 = p.r_lo * p.nth, nlines = p.r_hi * p.nth;
@@ -1328,18 +1330,18 @@ cudaError_t run_cycle_fk(const Plan& p, cudaStream_t s) {
   std::memset(&map, 0, sizeof(map));
   int mbox = 1;
   const int tma = STG && make_rtm_map(p, &map, &mbox) ? 1 : 0;
-  kern<<<grid, kFftThreadsF, smem, s>>>(p, line0, nlines, map, tma, mbox);
+  kern<<<grid, NT, smem, s>>>(p, line0, nlines, map, tma, mbox);
   return cudaGetLastError();
 }
 
 // The specialised passes without staging (the first pass reads the records in
 // place), for lines whose grid fits in shared memory but not with the staged
 // spectra; generic products.
-template <int N, int MVB, int MSB, int MVF, int MSF>
+template <int N, int MVB, int MSB, int MVF, int MSF, int NT = kFftThreadsF>
 cudaError_t run_cycle_fu(const Plan& p, cudaStream_t s) {
   const bool pr = p.nph == 3 * (p.L + 1);
-  return pr ? run_cycle_fk<N, MVB, MSB, MVF, MSF, true, 0, false>(p, s)
-            : run_cycle_fk<N, MVB, MSB, MVF, MSF, false, 0, false>(p, s);
+  return pr ? run_cycle_fk<N, MVB, MSB, MVF, MSF, true, 0, false, NT>(p, s)
+            : run_cycle_fk<N, MVB, MSB, MVF, MSF, false, 0, false, NT>(p, s);
 }
 
 // the standard MHD product list, after the vectors-first reordering
@@ -1480,7 +1482,7 @@ cudaError_t launch_fft_cycle(const Plan& p, cudaStream_t s) {
         return run_cycle_fu<1536, 4, 2, 5, 1>(p, s);
       // the dynamo benchmark set (u, omega, B, J + T -> omega x u, J x B, u x B, u T)
       if (p.nph == 1536 && p.nvb == 4 && p.nsb == 1 && p.nvf == 4 && p.nsf == 0)
-        return run_cycle_fu<1536, 4, 1, 4, 0>(p, s);
+        return run_cycle_fu<1536, 4, 1, 4, 0, 256>(p, s);  // 256 threads: 71.8 against 78.8 ms at L=511
       if (p.nph == 1536) return run_cycle_fu<1536, kMaxVec, kMaxScl, kMaxVec, kMaxScl>(p, s);
       if (p.nph == 768) return run_cycle_fu<768, kMaxVec, kMaxScl, kMaxVec, kMaxScl>(p, s);
     }
