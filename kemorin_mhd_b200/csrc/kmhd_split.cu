@@ -350,8 +350,12 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_mr(Plan P, SliceTabs S,
   const int* dxa = S.dexp + S.deoff[m * kNT + t0];
   const int* dxb = S.dexp + S.deoff[m * kNT + t0 + 1];
   const int nx = ncolg * kst;
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) X[i] = 0.0;
-  __syncthreads();
+  // Forward with m > 0 and no theta padding, pass 1 writes every X entry
+  // (both parts of the vector types, both slots of every field)
+  if (!(FWD && m > 0 && P.nh % kTK == 0)) {
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) X[i] = 0.0;
+    __syncthreads();
+  }
   const double ar = 1.0 / P.radius[r];
 
   // ---- pass 1: derived columns
