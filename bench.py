@@ -100,44 +100,59 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_cycle_rate(cfg, seconds_target: float = 12.0, steps: int = 1, warmup: int = 0):
+def cpu_slab_radii(cfg, threads: int) -> int:
+    """Radii of the CPU sample: at least two per host thread (the oracle runs
+    OpenMP over radial blocks, as the reference's flag-11 path does) and at
+    least 16, never more than the shell."""
+    return int(min(cfg.nr, max(16, 2 * threads)))
+
+
+def cpu_cycle_rate(cfg, steps: int = 1, warmup: int = 1, budget_s: float = 150.0):
     """Times the CPU FP64 oracle (reference sym_dgemm path restated, OpenBLAS
-    DGEMM, OpenMP over radial blocks) on a radial slab; returns cycles/s scaled
-    to the full radius count, the slab size, and the thread count."""
+    DGEMM, OpenMP over radial blocks on all host threads) on a radial slab of
+    cpu_slab_radii radii spread over the shell.  Every stage is linear in Nr,
+    so cycles/s of the full shell = slab cycles/s x nr_slab / Nr.  Up to
+    `steps` cycles are timed, fewer when they would overrun `budget_s` (the
+    slab size is kept, the repeat count shrinks).  Returns (cycles/s of the
+    full shell, slab radii, threads, stage times of the last cycle, cycles
+    timed)."""
     import numpy as np
     from oracle import oracle as om
     from kemorin_mhd_b200.config import SphConfig
     from kemorin_mhd_b200.synthetic import make_d_rj
     om.use_openblas()
     threads = os.cpu_count() or 1
-    full_r = cfg.radius()
-
-    def slab(nr):
-        c = SphConfig(cfg.ltr, cfg.nth, cfg.nph, nr, cfg.nvb, cfg.nsb, cfg.nvf, cfg.nsf, cfg.products)
-        idx = np.linspace(0, cfg.nr - 1, nr).round().astype(int)
-        return c, full_r[idx]
-
-    c1, r1 = slab(2)
-    o = om.Oracle(c1, nthreads=threads, radius=r1)
-    d = make_d_rj(c1)
-    o.cycle(d)
-    t0 = time.perf_counter()
-    o.cycle(d)
-    t_per_radius = (time.perf_counter() - t0) / c1.nr
-    nr = int(max(2, min(cfg.nr, round(seconds_target / max(t_per_radius, 1e-6) / max(1, steps)))))
-    c, r = slab(nr)
-    o = om.Oracle(c, nthreads=threads, radius=r)
+    nr = cpu_slab_radii(cfg, threads)
+    idx = np.linspace(0, cfg.nr - 1, nr).round().astype(int)
+    c = SphConfig(cfg.ltr, cfg.nth, cfg.nph, nr, cfg.nvb, cfg.nsb, cfg.nvf, cfg.nsf, cfg.products)
+    o = om.Oracle(c, nthreads=threads, radius=cfg.radius()[idx])
     d = make_d_rj(c)
-    for _ in range(warmup):
+    t_start = time.perf_counter()
+    for _ in range(max(0, warmup)):
         o.cycle(d)
     times = []
     for _ in range(max(1, steps)):
         t0 = time.perf_counter()
         o.cycle(d)
         times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start + times[-1] > budget_s:
+            break
     t = statistics.median(times)
     rate = 1.0 / (t * cfg.nr / nr)
-    return rate, nr, threads, o.last_timing()
+    return rate, nr, threads, o.last_timing(), len(times)
+
+
+def bench_config(cfg, fields_bwd, fields_fwd, ws):
+    """The `config` object of both arms' JSON lines."""
+    return {"workload": cfg.name, "L": cfg.ltr, "Nr": cfg.nr, "Ntheta": cfg.nth, "Nphi": cfg.nph,
+            "fields_bwd": fields_bwd, "fields_fwd": fields_fwd,
+            "parallelism": f"radial-instance x{ws} (no collective)",
+            "l2": "inputs larger than L2 (d_rj 5.4 GB, rtm 16 GB per direction)"}
+
+
+def cpu_sample_text(nr, cfg, timed):
+    return (f"radial slab of {nr}/{cfg.nr} radii spread over the shell, {timed} cycle(s) timed (median), "
+            f"scaled x{cfg.nr / nr:.2f} to the full shell (every stage is linear in Nr)")
 
 
 def run_reference(args, cfg):
@@ -145,18 +160,17 @@ def run_reference(args, cfg):
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
-    rate, nr, threads, stages = cpu_cycle_rate(cfg, seconds_target=max(4.0, 20.0 / max(1, args.steps)),
-                                              steps=args.steps, warmup=min(args.warmup, 1))
+    rate, nr, threads, stages, timed = cpu_cycle_rate(cfg, steps=args.steps, warmup=min(args.warmup, 1))
+    fb, ff = FIELD_NAMES[args.fields]
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / rate,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded spectra N(0,1)(l+1)^-2 sin(pi(r-ri)/(ro-ri)))",
-        "config": {"workload": cfg.name, "L": cfg.ltr, "Nr": cfg.nr, "Ntheta": cfg.nth,
-                   "Nphi": cfg.nph, "fields_bwd": FIELD_NAMES[args.fields][0],
-                   "fields_fwd": FIELD_NAMES[args.fields][1]},
+        "data": "synthetic (seeded spectra N(0,1)(l+1)^-2 sin(pi(r-ri)/(ro-ri)), Chebyshev radii)",
+        "config": bench_config(cfg, fb, ff, ws),
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"radial slab of {nr}/{cfg.nr} radii per step, scaled x{cfg.nr / nr:.2f} (cost is linear in Nr)",
+                         "sample": cpu_sample_text(nr, cfg, timed), "slab_radii": nr,
+                         "extrapolation_factor": cfg.nr / nr, "cycles_timed": timed,
                          "stages_ms": stages},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -175,6 +189,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-tier comparison run")
+    ap.add_argument("--no-tiers", action="store_true", help="split tier: skip the fp32acc comparison run")
     ap.add_argument("--nr", type=int, default=0, help="override the radius count (small profiling cases)")
     ap.add_argument("--fields", default="default", choices=["default", "dynamo", "full"],
                     help="field set: default u,omega,B + T; dynamo u,omega,B,J + T with the Lorentz force; "
@@ -296,11 +311,34 @@ def main():
         f1.record(stream)
         torch.cuda.synchronize()
         ms64 = max_over_ranks(f0.elapsed_time(f1) / n64)
+        k64 = ref64.kernel_timing()
         den = out64.abs().amax(dim=1)
         err = ((d_out - out64).abs().amax(dim=1) / den).tolist()
-        extra = {"fp64_gpu": {"value": ws * 1e3 / ms64, "unit": UNIT, "ms_per_step": ms64},
+        extra = {"fp64_gpu": {"value": ws * 1e3 / ms64, "unit": UNIT, "ms_per_step": ms64, "kernels_ms": k64,
+                              "roofline": fp64_rooflines(cfg, k64, ctypes_probe(lib, local))},
                  "speedup_vs_fp64_gpu": ms64 / ms_step,
                  "rel_err_vs_fp64_per_field": err, "rel_err_max": max(err)}
+        if tier == "split" and not args.no_tiers:
+            # the third tier on the same input: fp32acc (4 slices, 10 products, bound 1e-6)
+            t32 = make("fp32acc")
+            t32.set_stream(stream.cuda_stream)
+            out32 = torch.zeros_like(d_out)
+            for _ in range(2):
+                t32.nonlinear_cycle(d_in, out32)
+            torch.cuda.synchronize()
+            f0.record(stream)
+            for _ in range(n64):
+                t32.nonlinear_cycle(d_in, out32)
+            f1.record(stream)
+            torch.cuda.synchronize()
+            ms32 = max_over_ranks(f0.elapsed_time(f1) / n64)
+            err32 = ((out32 - out64).abs().amax(dim=1) / den).tolist()
+            extra["fp32acc_gpu"] = {"value": ws * 1e3 / ms32, "unit": UNIT, "ms_per_step": ms32,
+                                    "kernels_ms": t32.kernel_timing(), "speedup_vs_fp64_gpu": ms64 / ms32,
+                                    "rel_err_vs_fp64_per_field": err32, "rel_err_max": max(err32)}
+            t32.close()
+            del out32
+        ref64.close()
         del ref64, out64
     if args.p_on_the_fly:
         # the stored-table FP64 tier on the same input (one handle at a time:
@@ -358,6 +396,10 @@ def main():
                 "executed_int8_tops": execd / (dur * 1e-3) / 1e12,
                 "executed_frac": execd / (dur * 1e-3) / 1e12 / pk,
                 "overhead_factor": execd / flops}
+        p8 = ctypes_probe_i8(lib, local)
+        if p8:
+            roof["int8_probe_tops"] = p8
+            roof["executed_frac_of_int8_probe"] = roof["executed_int8_tops"] / p8
     roof["frac"] = roof["achieved"] / roof["peak"] if roof["peak"] else None
     roof["traffic"] = read_traffic(roof["kernel"], cfg.name)
     roof["algorithmic_flops_per_launch"] = flops
@@ -397,11 +439,10 @@ def main():
 
     cpu = None
     if rank == 0 and not args.no_cpu:
-        rate, nr, threads, stages = cpu_cycle_rate(cfg)
+        rate, nr, threads, stages, timed = cpu_cycle_rate(cfg, steps=1, warmup=1)
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"one cycle of a radial slab of {nr}/{cfg.nr} radii, scaled x{cfg.nr / nr:.2f} "
-                         "(every stage is linear in Nr)",
-               "stages_ms": stages}
+               "sample": cpu_sample_text(nr, cfg, timed), "slab_radii": nr,
+               "extrapolation_factor": cfg.nr / nr, "stages_ms": stages}
 
     launches = {"fp64": 4, "split": 6, "fp32acc": 6}[tier]
     line = {
@@ -409,10 +450,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": DTYPES[tier], "tier": tier,
         "data": "synthetic (seeded spectra N(0,1)(l+1)^-2 sin(pi(r-ri)/(ro-ri)), Chebyshev radii)",
-        "config": {"workload": cfg.name, "L": cfg.ltr, "Nr": cfg.nr, "Ntheta": cfg.nth, "Nphi": cfg.nph,
-                   "fields_bwd": fields_bwd, "fields_fwd": fields_fwd,
-                   "parallelism": f"radial-instance x{ws} (no collective)",
-                   "l2": "inputs larger than L2 (d_rj 5.4 GB, rtm 16 GB per direction)"},
+        "config": bench_config(cfg, fields_bwd, fields_fwd, ws),
         "stages_ms": stage, "kernels_ms": kern, "roofline": roof, "roofline_fft": roof_fft,
         "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": launches * args.steps, "clocks": clk,
@@ -523,6 +561,36 @@ def ctypes_probe(lib, dev):
     f.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     v = ctypes.c_double()
     return v.value if f(dev, ctypes.byref(v)) == 0 else None
+
+
+def ctypes_probe_i8(lib, dev):
+    """INT8 tensor-pipe rate measured in-process: back-to-back tcgen05 kind::i8
+    MMAs of 128 x 256 x 32 from shared memory on every SM (TOP/s)."""
+    import ctypes
+    try:
+        f = lib.kmhd_probe_i8_mma
+    except AttributeError:
+        return None
+    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    v = ctypes.c_double()
+    return v.value if f(dev, 256, 100000, 64, ctypes.byref(v)) == 0 else None
+
+
+def fp64_rooflines(cfg, kern, probe_tflops):
+    """FP64-tier Legendre GEMMs (DMMA) against the FP64 tensor pipe measured
+    in-process by the DMMA chain probe: useful flops per launch
+    2*Nh*J*Nr*(5nv+ns) of each direction over its CUDA-event duration."""
+    out = {}
+    for key, name, nv, ns in (("gemm_bwd", "k_leg_bwd_f64", cfg.nvb, cfg.nsb),
+                              ("gemm_fwd", "k_leg_fwd_f64", cfg.nvf, cfg.nsf)):
+        fl = 2.0 * cfg.nh * cfg.J * cfg.nr * (5 * nv + ns)
+        dur = kern.get(key, 0.0)
+        ach = fl / (dur * 1e-3) / 1e12 if dur > 0 else None
+        out[name] = {"bound": "tensor", "unit": "TFLOP/s", "achieved": ach, "peak": probe_tflops,
+                     "frac": ach / probe_tflops if (ach and probe_tflops) else None, "ms_per_launch": dur,
+                     "algorithmic_flops_per_launch": fl,
+                     "peak_source": "FP64 tensor pipe measured in-process (DMMA chain probe)"}
+    return out
 
 
 def read_traffic(kernel, workload):

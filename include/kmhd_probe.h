@@ -20,16 +20,9 @@ int kmhd_selftest_i8_mma(int lbo, int sbo, const signed char *A, const signed ch
 
 /* INT8 tensor-pipe rate (TOP/s) of back-to-back tcgen05 kind::i8 MMAs of shape
  * 128 x n x 32 from shared memory, one CTA per SM, commit + wait every `group`
- * instructions. */
+ * instructions: the measured INT8 peak that the benchmark divides the split
+ * GEMM's executed rate by. */
 int kmhd_probe_i8_mma(int device, int n, int iters, int group, double *tops);
-
-/* As kmhd_selftest_i8_mma for a 128B-swizzled K-major layout:
- * D(128x64) = A(128x128) * B(64x128)^T, int8 row-major host inputs. */
-int kmhd_selftest_i8_mma_sw128(const signed char *A, const signed char *B, int *D);
-
-/* INT8 tensor-pipe rate for operand layout 0 (no swizzle, 8x16-byte core
- * matrices) or 1 (128-byte swizzle), N = n, cycling nacc accumulators. */
-int kmhd_probe_i8_mma2(int device, int layout, int n, int nacc, int iters, double *tops);
 
 #ifdef __cplusplus
 }

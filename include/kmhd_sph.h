@@ -41,7 +41,7 @@ enum kmhd_status {
 enum kmhd_tier {
   KMHD_TIER_FP64 = 0,      /* FP64 Legendre GEMMs (DMMA), bit-faithful method   */
   KMHD_TIER_SPLIT_I8 = 1,  /* INT8-slice split products on tcgen05, <=1e-12     */
-  KMHD_TIER_FP32ACC = 2    /* 3-slice INT8 split products on tcgen05, <=1e-6    */
+  KMHD_TIER_FP32ACC = 2    /* 4-slice INT8 split, 10 products on tcgen05, <=1e-6 */
 };
 
 enum kmhd_product_kind {
@@ -89,7 +89,7 @@ typedef struct kmhd_sph kmhd_sph;
 /* kmhd_sph_desc.flags, FP64 tier only: no stored P / dP tables; the Legendre
  * kernels generate P_l^m and dP_l^m/dtheta by the fixed-order recurrence as
  * they go, from O(L^2) coefficients, O(L Ntheta) start values and seeds every
- * 64 degrees (about 20x less memory than the O(L^2 Ntheta) tables).  Values
+ * 32 degrees (about 20x less memory than the O(L^2 Ntheta) tables).  Values
  * differ from the stored tables in the last bits only.  The reference stores
  * the tables (schmidt_poly_on_rtm_grid.f90:145-197). */
 #define KMHD_FLAG_P_ON_THE_FLY 2
@@ -184,10 +184,12 @@ int kmhd_sph_get_tables(kmhd_sph *handle, int32_t m, double *colat, double *weig
  * stay on the host); stream is a cudaStream_t (NULL = default stream) and the
  * call returns after it has been synchronised.  Returns KMHD_ERR_SIZE when the
  * problem needs more than the 32 MiB (about L = 31, Ntheta = 48, Nphi = 96,
- * Nr = 33 with four fields each way fits).  The first call on a device looks
- * up the array's device address, so make it before any stream capture.  All
- * calls share the one array: calls that overlap on the GPU (other host
- * threads, other streams) race and corrupt each other's results.
+ * Nr = 33 with four fields each way fits).  desc->flags must be 0
+ * (KMHD_ERR_ARG otherwise).  Every call looks up the array's address on
+ * desc->device, makes that device current for the call and makes the caller's
+ * device current again before it returns.  All calls share the one array:
+ * calls that overlap on the GPU (other host threads, other streams) race and
+ * corrupt each other's results.
  * This entry point has no counterpart in the reference. */
 int kmhd_sph_cycle_noalloc(const kmhd_sph_desc *desc, const double *d_rj_in, int64_t ld_in,
                            const int32_t *cols_b, double *d_rj_out, int64_t ld_out,

@@ -13,7 +13,6 @@
 
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include <vector>
 
 #include "kmhd_internal.cuh"
@@ -27,23 +26,31 @@ namespace {
 constexpr size_t kNoAllocBytes = size_t(32) << 20;
 static __device__ __align__(256) unsigned char g_noalloc_ws[kNoAllocBytes];
 
-constexpr int kNoAllocMaxDevices = 64;
-std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
-
-// Device address of g_noalloc_ws on the current device (host code only sees a
-// host-side stand-in under that name).  Looked up once per device.
-cudaError_t noalloc_base(int dev, unsigned char** out) {
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_ws);
-    if (e != cudaSuccess) return e;
-    g_noalloc_ptr[dev] = p;
-  }
-  *out = static_cast<unsigned char*>(g_noalloc_ptr[dev]);
+// Device address of g_noalloc_ws in the current device's context (host code
+// only sees a host-side stand-in under that name).  Looked up on every call,
+// with that device current: a cudaDeviceReset by the caller loads the module
+// again, possibly at another address, so no address is kept between calls.
+cudaError_t noalloc_base(unsigned char** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_ws);
+  if (e != cudaSuccess) return e;
+  *out = static_cast<unsigned char*>(p);
   return cudaSuccess;
 }
+
+// Makes `dev` current for the scope and restores the caller's device after.
+struct DeviceScope {
+  int prev = -1;
+  bool ok = false;
+  explicit DeviceScope(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) return;
+    ok = prev == dev || cudaSetDevice(dev) == cudaSuccess;
+  }
+  ~DeviceScope() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
 
 // Bump allocator over the work area: offsets are 256-byte aligned.  With a
 // null base it only measures.
@@ -74,6 +81,7 @@ bool na_factor(int n, std::vector<int>& f) {
 int na_validate(const kmhd_sph_desc* d) {
   if (!d) return KMHD_ERR_ARG;
   if (d->tier != KMHD_TIER_FP64) return KMHD_ERR_ARG;
+  if (d->flags != 0) return KMHD_ERR_ARG;  // no autotuning, no on-the-fly tables here
   if (d->ltr < 1 || d->nth < 2 || d->nr < 1 || d->nph < 4) return KMHD_ERR_SIZE;
   if (d->nph <= 2 * d->ltr + 1) return KMHD_ERR_SIZE;
   if (!d->radius) return KMHD_ERR_ARG;
@@ -278,15 +286,15 @@ extern "C" int kmhd_sph_cycle_noalloc(const kmhd_sph_desc* desc, const double* d
   if ((st = na_tables(desc, p, H)) != KMHD_OK) return st;
 
   int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || desc->device < 0 || desc->device >= ndev ||
-      desc->device >= kNoAllocMaxDevices)
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || desc->device < 0 || desc->device >= ndev)
     return KMHD_ERR_DEVICE;
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, desc->device) != cudaSuccess) return KMHD_ERR_CUDA;
   if (prop.major != 10) return KMHD_ERR_DEVICE;
-  if (cudaSetDevice(desc->device) != cudaSuccess) return KMHD_ERR_CUDA;
+  const DeviceScope scope(desc->device);  // the caller's device is current again on return
+  if (!scope.ok) return KMHD_ERR_CUDA;
   unsigned char* base = nullptr;
-  if (noalloc_base(desc->device, &base) != cudaSuccess) return KMHD_ERR_CUDA;
+  if (noalloc_base(&base) != cudaSuccess) return KMHD_ERR_CUDA;
   na_layout(p, H, base, b);
 
   const cudaStream_t s = static_cast<cudaStream_t>(stream);

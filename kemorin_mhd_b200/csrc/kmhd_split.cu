@@ -18,8 +18,8 @@
 //                        asym = [dP_e | (m/sin) P_o] . [b_e ; c_o]-type columns
 //   backward r, scalars: sym = P_e . a_e,  asym = P_o . a_o
 //   forward comp 1, scalars: P_p . X,  comp 2/3: [dP_p | m P_p] . [W ; U]-type columns
-// The backward sym and asym halves are computed by the two CTAs of a cluster and
-// combined (N = sym + asym, S = sym - asym) through distributed shared memory.
+// One CTA computes both the backward sym and asym tiles of an output tile and
+// combines them (N = sym + asym, S = sym - asym) through its own shared memory.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -1622,158 +1622,3 @@ extern "C" int kmhd_probe_i8_mma(int device, int n, int iters, int group, double
   return KMHD_OK;
 }
 
-// ---------------------------------------------------------------------------
-// Layout study: SWIZZLE_128B K-major operands (128-byte rows, 16-byte chunk c
-// of row r stored at chunk c ^ (r & 7), 8-row atoms of 1024 bytes), k-steps of
-// 32 int8 advance the descriptor start address by 32 bytes.
-namespace kmhd {
-namespace {
-__host__ __device__ __forceinline__ int sw128_off(int row, int k) {
-  return row * 128 + ((((k >> 4) & 7) ^ (row & 7)) << 4) + (k & 15);
-}
-__device__ __forceinline__ uint64_t smem_desc_sw128(const void* p) {
-  const uint64_t a = (sptr(p) >> 4) & 0x3FFF;
-  return a | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) | (2ull << 61);
-}
-
-// D(128 x 64) = A(128 x 128) B(64 x 128)^T with SWIZZLE_128B tiles (4 k-steps)
-__global__ void __launch_bounds__(128, 1) k_selftest_mma_sw(const signed char* A, const signed char* B, int* D, int* err) {
-  __shared__ __align__(1024) unsigned char sa[128 * 128];
-  __shared__ __align__(1024) unsigned char sb[64 * 128];
-  __shared__ unsigned long long bar;
-  __shared__ unsigned slot;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  for (int i = tid; i < 128 * 128; i += blockDim.x) sa[sw128_off(i / 128, i % 128)] = (unsigned char)A[i];
-  for (int i = tid; i < 64 * 128; i += blockDim.x) sb[sw128_off(i / 128, i % 128)] = (unsigned char)B[i];
-  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-  if (tid == 0) {
-    mbar_init(&bar, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-  }
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;\n" ::"r"(sptr(&slot)));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const unsigned tmem = slot;
-  if (tid == 0) {
-    const unsigned idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(64 >> 3) << 17) | ((unsigned)(128 >> 4) << 24);
-    const uint64_t ad = smem_desc_sw128(sa), bd = smem_desc_sw128(sb);
-    for (int ks = 0; ks < 4; ++ks) mma_i8(tmem, ad + (uint64_t)(ks * 2), bd + (uint64_t)(ks * 2), idesc, ks > 0 ? 1u : 0u);
-    mma_commit(&bar);
-  }
-  __syncwarp();
-  if (!mbar_wait(&bar, 0)) atomicExch(err, KMHD_ERR_TIMEOUT);
-  tc_fence_after();
-  for (int cb = 0; cb < 4; ++cb) {
-    int v[16];
-    tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)(cb * 16), v);
-    tmem_wait_ld();
-    for (int c = 0; c < 16; ++c) D[(warp * 32 + lane) * 64 + cb * 16 + c] = v[c];
-  }
-  tc_fence_before();
-  __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;\n" ::"r"(tmem));
-}
-
-// rate probe: layout 0 = SWIZZLE_NONE core matrices, 1 = SWIZZLE_128B; nacc accumulators cycled
-__global__ void __launch_bounds__(128, 1) k_probe_mma2(int layout, int n, int nacc, int iters, int* err) {
-  extern __shared__ __align__(1024) unsigned char smp[];
-  unsigned char* sa = smp;                 // 16 KB
-  unsigned char* sb = smp + 128 * 128;     // up to 32 KB
-  __shared__ unsigned long long bar;
-  __shared__ unsigned slot;
-  for (int i = threadIdx.x; i < (128 + 256) * 128; i += blockDim.x) smp[i] = (unsigned char)(i * 7);
-  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-  if (threadIdx.x == 0) {
-    mbar_init(&bar, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-  }
-  if (threadIdx.x < 32) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;\n" ::"r"(sptr(&slot)));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const unsigned tmem = slot;
-  if (threadIdx.x == 0) {
-    const unsigned idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(n >> 3) << 17) | ((unsigned)(128 >> 4) << 24);
-    const uint64_t ad = layout ? smem_desc_sw128(sa) : smem_desc(sa, 128, 256);
-    const uint64_t bd = layout ? smem_desc_sw128(sb) : smem_desc(sb, 128, 256);
-    for (int it = 0; it < iters; ++it) {
-      const int ks = it & 3;
-      const uint64_t koff = layout ? (uint64_t)(ks * 2) : 0;
-      mma_i8(tmem + (unsigned)((it % nacc) * n), ad + koff, bd + koff, idesc, it >= nacc ? 1u : 0u);
-    }
-    mma_commit(&bar);
-    if (!mbar_wait(&bar, 0)) atomicExch(err, KMHD_ERR_TIMEOUT);
-  }
-  tc_fence_before();
-  __syncthreads();
-  if (threadIdx.x < 32) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;\n" ::"r"(tmem));
-}
-}  // namespace
-}  // namespace kmhd
-
-extern "C" int kmhd_selftest_i8_mma_sw128(const signed char* A, const signed char* B, int* D) {
-  using namespace kmhd;
-  signed char *dA = nullptr, *dB = nullptr;
-  int *dD = nullptr, *err = nullptr;
-  int st = KMHD_OK;
-  if (cudaMalloc(&dA, 128 * 128) || cudaMalloc(&dB, 64 * 128) || cudaMalloc(&dD, sizeof(int) * 128 * 64) ||
-      cudaMalloc(&err, sizeof(int)))
-    st = KMHD_ERR_NOMEM;
-  if (!st) {
-    cudaMemcpy(dA, A, 128 * 128, cudaMemcpyHostToDevice);
-    cudaMemcpy(dB, B, 64 * 128, cudaMemcpyHostToDevice);
-    cudaMemset(err, 0, sizeof(int));
-    k_selftest_mma_sw<<<1, 128>>>(dA, dB, dD, err);
-    int h = 0;
-    if (cudaDeviceSynchronize() != cudaSuccess) st = KMHD_ERR_CUDA;
-    else {
-      cudaMemcpy(D, dD, sizeof(int) * 128 * 64, cudaMemcpyDeviceToHost);
-      cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost);
-      st = h;
-    }
-  }
-  cudaFree(dA);
-  cudaFree(dB);
-  cudaFree(dD);
-  cudaFree(err);
-  return st;
-}
-
-extern "C" int kmhd_probe_i8_mma2(int device, int layout, int n, int nacc, int iters, double* tops) {
-  using namespace kmhd;
-  if (!tops || n < 16 || n > 256 || n % 16 || nacc < 1 || nacc * n > 512) return KMHD_ERR_ARG;
-  if (cudaSetDevice(device) != cudaSuccess) return KMHD_ERR_DEVICE;
-  int nsm = 0;
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-  int* err = nullptr;
-  if (cudaMalloc(&err, sizeof(int)) != cudaSuccess) return KMHD_ERR_NOMEM;
-  cudaMemset(err, 0, sizeof(int));
-  const int smem = (128 + 256) * 128 + 1024;
-  cudaFuncSetAttribute(k_probe_mma2, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  k_probe_mma2<<<nsm, 128, smem>>>(layout, n, nacc, 64, err);
-  cudaEventRecord(e0);
-  k_probe_mma2<<<nsm, 128, smem>>>(layout, n, nacc, iters, err);
-  cudaEventRecord(e1);
-  cudaError_t ce = cudaEventSynchronize(e1);
-  float ms = 0.f;
-  cudaEventElapsedTime(&ms, e0, e1);
-  int h = 0;
-  cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  cudaFree(err);
-  if (ce != cudaSuccess) return KMHD_ERR_CUDA;
-  if (h) return h;
-  *tops = 2.0 * 128 * n * 32 * (double)iters * nsm / (ms * 1e-3) / 1e12;
-  return KMHD_OK;
-}

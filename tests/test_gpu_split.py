@@ -132,3 +132,49 @@ def test_split_vs_fp64_L1023():
         tr.close()
     err = col_relerr(outs[1], outs[0])
     assert err.max() <= TOL[TIER_SPLIT_I8], err
+
+
+# The benchmark's angular grids with their own default field set (u, omega, B
+# + T backward; omega x u, u x B, u T + u.omega forward): cfg3's L=511,
+# Ntheta=768, Nphi=1536 and cfg2's L=255, Ntheta=384, Nphi=768, on a few
+# radii so the CPU oracle finishes in seconds.  Every tier against the oracle,
+# per field, at its stated bound.
+BENCH_GRIDS = [
+    SphConfig(511, 768, 1536, 3, name="L511_Nr3"),
+    SphConfig(255, 384, 768, 5, name="L255_Nr5"),
+]
+
+
+@pytest.fixture(scope="module")
+def bench_oracle_outputs():
+    cache = {}
+
+    def get(cfg, what, seed):
+        key = (cfg.name, what, seed)
+        if key not in cache:
+            orc = Oracle(cfg, nthreads=8)
+            if what == "cycle":
+                cache[key] = orc.cycle(make_d_rj(cfg, seed=seed))
+            else:
+                cache[key] = orc.b_trans(make_d_rj(cfg, seed=seed))
+        return cache[key]
+    return get
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tier", [TIER_SPLIT_I8, TIER_FP32ACC], ids=["split", "fp32acc"])
+@pytest.mark.parametrize("cfg", BENCH_GRIDS, ids=lambda c: c.name)
+def test_split_tiers_at_benchmark_grids(cfg, tier, bench_oracle_outputs):
+    import torch
+    from kemorin_mhd_b200.sph_trans import SphTransform
+    tr = SphTransform(cfg, tier=tier)
+    d = make_d_rj(cfg, seed=31)
+    out = torch.zeros((cfg.ncf, cfg.J * cfg.nr), dtype=torch.float64, device="cuda")
+    tr.nonlinear_cycle(to_dev_fortran(d), out)
+    err = col_relerr(from_dev_fortran(out), bench_oracle_outputs(cfg, "cycle", 31))
+    fld = torch.empty((cfg.ncb, cfg.nr * cfg.nth * cfg.nph), dtype=torch.float64, device="cuda")
+    tr.sph_b_trans(to_dev_fortran(d), fld)
+    err_b = col_relerr(from_dev_fortran(fld), bench_oracle_outputs(cfg, "b_trans", 31))
+    tr.close()
+    assert err.max() <= TOL[tier], err
+    assert err_b.max() <= TOL[tier], err_b

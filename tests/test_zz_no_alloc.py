@@ -77,6 +77,10 @@ def test_noalloc_rejects_without_touching_the_gpu():
     ok = _Args(CFG_A)
     assert lib.kmhd_sph_cycle_noalloc(ctypes.byref(ok.desc), dummy, n - 1, ok.cols_b, dummy, n,
                                       ok.cols_f, None) == 1  # leading dimension too small
+    flagged = _Args(CFG_A)
+    flagged.desc.flags = 2  # on-the-fly tables are a handle option, not offered here
+    assert lib.kmhd_sph_cycle_noalloc(ctypes.byref(flagged.desc), dummy, n, flagged.cols_b, dummy, n,
+                                      flagged.cols_f, None) == 1
 
 
 @pytest.mark.gpu
@@ -89,6 +93,7 @@ def test_noalloc_matches_cycle_two_calls():
     for call in range(2):
         out = torch.zeros((CFG_A.ncf, CFG_A.J * CFG_A.nr), dtype=torch.float64, device="cuda")
         assert _noalloc(lib, CFG_A, d_in, out) == 0
+        assert torch.cuda.current_device() == 0  # the caller's device is current again
         err = col_relerr(from_dev_fortran(out), ref)
         assert err.max() <= TOL, (call, err)
 
