@@ -318,6 +318,11 @@ def main():
                               "roofline": fp64_rooflines(cfg, k64, ctypes_probe(lib, local))},
                  "speedup_vs_fp64_gpu": ms64 / ms_step,
                  "rel_err_vs_fp64_per_field": err, "rel_err_max": max(err)}
+        # release the FP64 handle (about 50 GB at L=511, Nr=257) before the next
+        # tier's handle is made; its output stays for the error fields
+        ref64.close()
+        del ref64
+        torch.cuda.synchronize()
         if tier == "split" and not args.no_tiers:
             # the third tier on the same input: fp32acc (4 slices, 10 products, bound 1e-6)
             t32 = make("fp32acc")
@@ -338,8 +343,7 @@ def main():
                                     "rel_err_vs_fp64_per_field": err32, "rel_err_max": max(err32)}
             t32.close()
             del out32
-        ref64.close()
-        del ref64, out64
+        del out64
     if args.p_on_the_fly:
         # the stored-table FP64 tier on the same input (one handle at a time:
         # at L=1023 each holds ~80 GB)
