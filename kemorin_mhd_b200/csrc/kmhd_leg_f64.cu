@@ -376,8 +376,11 @@ struct FwdGeo {
 // OTF: the A tiles (P / dP of the block's 64 degrees at 16 latitudes) are
 // generated by warp 0 one latitude chunk ahead, each latitude's recurrence
 // starting from the seeds at the block's two 32-degree halves.
+// Two CTAs per SM while the accumulators fit in 128 registers (up to ten
+// components); one CTA with the whole register file for more (four or five
+// vectors: 42-52 accumulators per lane), which would otherwise spill.
 template <int NV, int NS, bool OTF>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, 3 * NV + NS > 10 ? 1 : 2)
 k_leg_fwd_f64(Plan p, double* __restrict__ d_rj, long long ld, const int* __restrict__ cols) {
   using G = FwdGeo<NV, NS>;
   extern __shared__ double sm[];
@@ -406,19 +409,28 @@ k_leg_fwd_f64(Plan p, double* __restrict__ d_rj, long long ld, const int* __rest
 
   constexpr int kItems = (kKC * kRB * (3 * NV + NS) + kThreads - 1) / kThreads;
   double2 pfN[kItems], pfS[kItems];
+  // item it = tid + q kThreads of a chunk is (latitude row, radius u, component
+  // c), the same in every chunk: decomposed once (nc is not a compile-time
+  // constant, so the divisions stay out of the chunk loop), packed as
+  // c | u << 8 | row << 12, or -1 past the chunk's items
+  int item[kItems];
+#pragma unroll
+  for (int q = 0; q < kItems; ++q) {
+    const int it = tid + q * kThreads;
+    const int rest = it / nc;
+    item[q] = it < kKC * kRB * nc ? (it - rest * nc) | (rest % kRB) << 8 | (rest / kRB) << 12 : -1;
+  }
   // global loads of one chunk's rtm_f values into registers (overlaps the MMAs)
   auto prefetch = [&](int ch) {
     const int th0 = ch * kKC;
 #pragma unroll
     for (int q = 0; q < kItems; ++q) {
-      const int it = tid + q * kThreads;
       pfN[q] = make_double2(0.0, 0.0);
       pfS[q] = make_double2(0.0, 0.0);
-      if (it < kKC * kRB * nc) {
-        const int c = it % nc, rest = it / nc, u = rest % kRB, row = rest / kRB;
-        const int i = th0 + row, r = kRB * rb + u;
+      if (item[q] >= 0) {
+        const int i = th0 + (item[q] >> 12), r = kRB * rb + ((item[q] >> 8) & 15);
         if (i < p.nh && r < p.nr) {
-          const int ro = rec_off(c, NV);
+          const int ro = rec_off(item[q] & 255, NV);
           pfN[q] = *reinterpret_cast<const double2*>(p.rtm_f + rtm_off(p, m, i, r, nc) + ro);
           if (i < p.nth / 2)
             pfS[q] = *reinterpret_cast<const double2*>(p.rtm_f + rtm_off(p, m, p.nth - 1 - i, r, nc) + ro);
@@ -509,12 +521,8 @@ k_leg_fwd_f64(Plan p, double* __restrict__ d_rj, long long ld, const int* __rest
     // B: sym/asym with weights from the prefetched registers
 #pragma unroll
     for (int q = 0; q < kItems; ++q) {
-      const int it = tid + q * kThreads;
-      if (it >= kKC * kRB * nc) continue;
-      const int c = it % nc;
-      const int rest = it / nc;
-      const int u = rest % kRB;
-      const int row = rest / kRB;
+      if (item[q] < 0) continue;
+      const int c = item[q] & 255, u = (item[q] >> 8) & 15, row = item[q] >> 12;
       const int i = th0 + row;
       const int r = kRB * rb + u;
       double2 sy = make_double2(0.0, 0.0), as = sy, syn = sy, asn = sy;
