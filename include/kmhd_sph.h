@@ -82,9 +82,17 @@ typedef struct kmhd_sph_desc {
 
 typedef struct kmhd_sph kmhd_sph;
 
-/* kmhd_sph_desc.flags: for the split tiers, time the FP64 DMMA path against
- * the split path on the first kmhd_sph_batch_cycle call and keep the faster
- * (both meet the tier's error bound).  The reference has no counterpart. */
+/* kmhd_sph_desc.flags: for the split tiers, on the first kmhd_sph_batch_cycle
+ * call run three candidates on the call's own data -- the FP64 DMMA path, the
+ * split path with the tier's full slice-product count (26 split, 10 fp32acc)
+ * and the split path with the highest digit-pair group dropped (21, 6) --
+ * compare the split outputs with the FP64 path's (max-norm relative error per
+ * output column) and keep the fastest candidate whose error is at most a
+ * quarter of the tier's bound (1e-12, 1e-6).  kmhd_sph_get_tuning reports the
+ * choice, the times and the errors.  The reference times its Legendre variants
+ * at start-up (select_legendre_transform,
+ * MHD_src/sph_MHD/init_sphrical_transform_MHD.f90:201-345), without an error
+ * check. */
 #define KMHD_FLAG_AUTOTUNE 1
 /* kmhd_sph_desc.flags, FP64 tier only: no stored P / dP tables; the Legendre
  * kernels generate P_l^m and dP_l^m/dtheta by the fixed-order recurrence as
@@ -361,6 +369,20 @@ int kmhd_sph_b_trans_pole(kmhd_sph *handle, const double *d_rj, int64_t ld_rj, c
 /* Legendre path the handle runs: 1 = the tier's split path, 0 = FP64 DMMA
  * (FP64 tier, or a split-tier handle the autotuner moved to FP64). */
 int kmhd_sph_get_path(const kmhd_sph *handle, int32_t *path);
+
+/* Legendre path (as kmhd_sph_get_path), slice products per GEMM of the split
+ * path (26 or 21 split, 10 or 6 fp32acc, 0 for the FP64 tier), and after an
+ * autotuned batch call the candidates' cycle times (ms3: FP64 path, full and
+ * reduced product count) and errors against the FP64 path (err3; 0 for the
+ * FP64 candidate); zeros before tuning.  Any pointer may be NULL.  Extends the
+ * reference's start-up choice of a Legendre variant (init_sphrical_transform_MHD.f90:201-345). */
+int kmhd_sph_get_tuning(const kmhd_sph *handle, int32_t *path, int32_t *products, float *ms3, double *err3);
+
+/* Pins the slice products per GEMM of a split-tier handle: 26 or 21 (split),
+ * 10 or 6 (fp32acc); KMHD_ERR_ARG otherwise.  21 (6) drops the digit pairs of
+ * the highest group: about 20% (40%) fewer tensor-core products, an error
+ * near 256 times larger.  No counterpart in the reference. */
+int kmhd_sph_set_products(kmhd_sph *handle, int32_t products);
 
 /* Device bytes held by the handle. */
 int64_t kmhd_sph_device_bytes(const kmhd_sph *handle);

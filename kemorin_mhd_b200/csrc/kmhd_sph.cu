@@ -27,8 +27,9 @@ struct BatchGraph {
   std::vector<cudaEvent_t> join;
   // split-path instances of one tier (6 or 4 slices) share one grouped GEMM
   // launch per direction, on the group's stream
-  SplitGroup* group[2] = {nullptr, nullptr};
-  cudaStream_t gs[2] = {nullptr, nullptr};
+  // kinds: (6 slices, 26 products), (6, 21), (4, 10), (4, 6)
+  SplitGroup* group[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaStream_t gs[4] = {nullptr, nullptr, nullptr, nullptr};
   std::vector<cudaEvent_t> ev;  // phase events of the grouped instances
 };
 
@@ -76,8 +77,12 @@ struct kmhd_sph {
   // split-precision state
   SplitState* split = nullptr;
   bool use_split = true;   // split tiers: run the split path (false: the FP64 DMMA path)
-  bool autotune = false;   // choose use_split by timing on the first batch call
+  bool autotune = false;   // choose the Legendre path (and product count) on the first batch call
   bool tuned = false;
+  // autotuner record: times (ms) and errors against the FP64 path of the
+  // candidates FP64, split with the full product count, split with one group fewer
+  float tune_ms[3] = {0, 0, 0};
+  double tune_err[3] = {0, 0, 0};
   // batched cycles whose first handle this is: captured graph and its signature
   struct BatchGraph* batch = nullptr;
   // host-pointer cycles: radial chunks (bounds, empty = no chunking) whose
@@ -220,6 +225,25 @@ int kmhd_sph_get_path(const kmhd_sph* h, int32_t* path) {
   return KMHD_OK;
 }
 
+int kmhd_sph_get_tuning(const kmhd_sph* h, int32_t* path, int32_t* products, float* ms3, double* err3) {
+  if (!h) return KMHD_ERR_ARG;
+  if (path) *path = (h->split && h->use_split) ? 1 : 0;
+  if (products) *products = h->split ? split_products(split_ns(h->split), split_terms(h->split)) : 0;
+  for (int c = 0; c < 3; ++c) {
+    if (ms3) ms3[c] = h->tuned ? h->tune_ms[c] : 0.0f;
+    if (err3) err3[c] = h->tuned ? h->tune_err[c] : 0.0;
+  }
+  return KMHD_OK;
+}
+
+int kmhd_sph_set_products(kmhd_sph* h, int32_t products) {
+  if (!h || !h->split) return KMHD_ERR_ARG;
+  const int ns = split_ns(h->split), full = ns == 6 ? 6 : 3;
+  for (int T = full - 1; T <= full; ++T)
+    if (split_products(ns, T) == products) return split_set_terms(h->split, T);
+  return KMHD_ERR_ARG;
+}
+
 int kmhd_sph_destroy(kmhd_sph* h) {
   if (!h) return KMHD_ERR_ARG;
   cudaSetDevice(h->device);
@@ -230,7 +254,7 @@ int kmhd_sph_destroy(kmhd_sph* h) {
     if (h->batch->fork) cudaEventDestroy(h->batch->fork);
     for (cudaEvent_t e : h->batch->join) cudaEventDestroy(e);
     for (cudaEvent_t e : h->batch->ev) cudaEventDestroy(e);
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < 4; ++k) {
       split_group_destroy(h->batch->group[k]);
       if (h->batch->gs[k]) cudaStreamDestroy(h->batch->gs[k]);
     }
@@ -1488,21 +1512,114 @@ int kmhd_sph_batch_cycle(kmhd_sph** hs, int32_t n, const double* const* d_rj_in,
 // faster one (both meet the tier's error bound).
 namespace {
 
+// Per output column c: bits of max |out - ref| and max |ref| (non-negative
+// doubles order like their bit patterns).
+__global__ void k_col_err(const double* __restrict__ out, long long ld, const int* __restrict__ col,
+                          const double* __restrict__ ref, long long rows, unsigned long long* res) {
+  const int c = blockIdx.y;
+  const double* o = out + ld * col[c];
+  const double* f = ref + rows * c;
+  double d = 0.0, a = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < rows; i += (long long)gridDim.x * blockDim.x) {
+    d = fmax(d, fabs(o[i] - f[i]));
+    a = fmax(a, fabs(f[i]));
+  }
+  for (int k = 16; k > 0; k >>= 1) {
+    d = fmax(d, __shfl_xor_sync(0xffffffffu, d, k));
+    a = fmax(a, __shfl_xor_sync(0xffffffffu, a, k));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(res + 2 * c, (unsigned long long)__double_as_longlong(d));
+    atomicMax(res + 2 * c + 1, (unsigned long long)__double_as_longlong(a));
+  }
+}
+
+// Candidates of a split-tier handle: 0 the FP64 DMMA path, 1 the split path
+// with the tier's full slice-product count (26 / 10), 2 with the highest
+// digit-pair group dropped (21 / 6).  Each runs twice on the call's own data
+// (the first round warms up); the split candidates' outputs are compared with
+// the FP64 path's (max-norm relative error per output column, the measure of
+// the tier's bound), and the fastest candidate whose error stays within a
+// quarter of the tier's bound (1e-12 split, 1e-6 fp32acc) is kept.  The
+// reference times its Legendre variants at start-up the same way, without the
+// error check (select_legendre_transform,
+// MHD_src/sph_MHD/init_sphrical_transform_MHD.f90:201-345).
 int autotune_path(kmhd_sph* h, const double* in, int64_t ld_in, double* out, int64_t ld_out) {
-  float ms[2] = {0, 0};
-  for (int rep = 0; rep < 2; ++rep) {  // first round warms up
-    for (int path = 0; path < 2; ++path) {
-      h->use_split = path == 1;
-      KCHECK(cudaEventRecord(h->ev[0], h->stream));
-      const int st = enqueue_cycle(h, in, ld_in, out, ld_out);
-      if (st) return st;
-      KCHECK(cudaEventRecord(h->ev[3], h->stream));
-      KCHECK(cudaEventSynchronize(h->ev[3]));
-      KCHECK(cudaEventElapsedTime(&ms[path], h->ev[0], h->ev[3]));
+  const Plan& p = h->plan;
+  const int full = split_ns(h->split) == 6 ? 6 : 3;
+  const double bound = 0.25 * (h->desc.tier == KMHD_TIER_SPLIT_I8 ? 1e-12 : 1e-6);
+  // written output columns: three per forward vector, one per scalar
+  std::vector<int> cols;
+  for (int f = 0; f < p.nvf + p.nsf; ++f)
+    for (int q = 0; q < (f < p.nvf ? 3 : 1); ++q) cols.push_back(h->cols_f_cache[f] + q);
+  const int nc = (int)cols.size();
+  const long long rows = p.J * (long long)p.nr;
+  double* ref = nullptr;
+  int* col_d = nullptr;
+  unsigned long long* res = nullptr;
+  int st = KMHD_OK;
+  auto fail = [&](int e) {
+    cudaFree(ref);
+    cudaFree(col_d);
+    cudaFree(res);
+    h->use_split = true;
+    split_set_terms(h->split, full);
+    return e;
+  };
+  if (cudaMalloc(&ref, sizeof(double) * rows * nc) != cudaSuccess || cudaMalloc(&col_d, sizeof(int) * nc) != cudaSuccess ||
+      cudaMalloc(&res, sizeof(unsigned long long) * 2 * nc) != cudaSuccess)
+    return fail(KMHD_ERR_NOMEM);
+  if (cudaMemcpyAsync(col_d, cols.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
+    return fail(KMHD_ERR_CUDA);
+  float ms[3] = {0, 0, 0};
+  double err[3] = {0, 0, 0};
+  for (int rep = 0; rep < 2; ++rep) {
+    for (int c = 0; c < 3; ++c) {
+      h->use_split = c > 0;
+      split_set_terms(h->split, c == 2 ? full - 1 : full);
+      if (cudaEventRecord(h->ev[0], h->stream) != cudaSuccess) return fail(KMHD_ERR_CUDA);
+      if ((st = enqueue_cycle(h, in, ld_in, out, ld_out))) return fail(st);
+      if (cudaEventRecord(h->ev[3], h->stream) != cudaSuccess || cudaEventSynchronize(h->ev[3]) != cudaSuccess ||
+          cudaEventElapsedTime(&ms[c], h->ev[0], h->ev[3]) != cudaSuccess)
+        return fail(KMHD_ERR_CUDA);
+      if ((st = check_dev_err(h))) return fail(st);
+      if (rep == 0) continue;
+      if (c == 0) {
+        for (int k = 0; k < nc; ++k)
+          if (cudaMemcpyAsync(ref + rows * k, out + ld_out * cols[k], sizeof(double) * rows, cudaMemcpyDeviceToDevice,
+                              h->stream) != cudaSuccess)
+            return fail(KMHD_ERR_CUDA);
+        continue;
+      }
+      std::vector<unsigned long long> r(2 * nc);
+      if (cudaMemsetAsync(res, 0, sizeof(unsigned long long) * 2 * nc, h->stream) != cudaSuccess) return fail(KMHD_ERR_CUDA);
+      k_col_err<<<dim3(64, nc), 256, 0, h->stream>>>(out, ld_out, col_d, ref, rows, res);
+      if (cudaGetLastError() != cudaSuccess ||
+          cudaMemcpyAsync(r.data(), res, sizeof(unsigned long long) * 2 * nc, cudaMemcpyDeviceToHost, h->stream) !=
+              cudaSuccess ||
+          cudaStreamSynchronize(h->stream) != cudaSuccess)
+        return fail(KMHD_ERR_CUDA);
+      for (int k = 0; k < nc; ++k) {
+        double d, a;
+        std::memcpy(&d, &r[2 * k], sizeof(d));
+        std::memcpy(&a, &r[2 * k + 1], sizeof(a));
+        if (a > 0.0) err[c] = std::max(err[c], d / a);
+      }
     }
   }
-  h->use_split = ms[1] < ms[0];
+  int best = 0;
+  for (int c = 1; c < 3; ++c)
+    if (err[c] <= bound && ms[c] < ms[best]) best = c;
+  h->use_split = best > 0;
+  split_set_terms(h->split, best == 2 ? full - 1 : full);
+  for (int c = 0; c < 3; ++c) {
+    h->tune_ms[c] = ms[c];
+    h->tune_err[c] = err[c];
+  }
   h->tuned = true;
+  cudaFree(ref);
+  cudaFree(col_d);
+  cudaFree(res);
   return KMHD_OK;
 }
 
@@ -1560,6 +1677,7 @@ int batch_cycle_impl(kmhd_sph** hs, int32_t n, const double* const* d_rj_in, con
       sig.push_back(d_rj_in[i]);
       sig.push_back(d_rj_out[i]);
       sig.push_back(hs[i]->use_split ? hs[i] : nullptr);
+      sig.push_back(reinterpret_cast<const void*>((intptr_t)(hs[i]->split ? split_terms(hs[i]->split) : 0)));
       sig.push_back(hs[i]->stream);
       sig_ld.push_back(ld_in[i]);
       sig_ld.push_back(ld_out[i]);
@@ -1586,11 +1704,16 @@ int batch_cycle_impl(kmhd_sph** hs, int32_t n, const double* const* d_rj_in, con
         KCHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         bg->join.push_back(e);
       }
-      // split-path instances by tier: grouped GEMMs (built before the capture)
-      std::vector<int> grp[2];
+      // split-path instances by tier and product count: grouped GEMMs (built
+      // before the capture); kind 0/1: 6 slices, 26/21 products, 2/3: 4 slices, 10/6
+      std::vector<int> grp[4];
       for (int i = 0; i < n; ++i)
-        if (hs[i]->split && hs[i]->use_split) grp[split_ns(hs[i]->split) == 6 ? 0 : 1].push_back(i);
-      for (int k = 0; k < 2; ++k) {
+        if (hs[i]->split && hs[i]->use_split) {
+          const bool six = split_ns(hs[i]->split) == 6;
+          const int full = six ? 6 : 3;
+          grp[(six ? 0 : 2) + (split_terms(hs[i]->split) == full ? 0 : 1)].push_back(i);
+        }
+      for (int k = 0; k < 4; ++k) {
         split_group_destroy(bg->group[k]);
         bg->group[k] = nullptr;
         if (grp[k].size() < 2) {
@@ -1615,9 +1738,9 @@ int batch_cycle_impl(kmhd_sph** hs, int32_t n, const double* const* d_rj_in, con
         if (!bg->gs[k]) KCHECK(cudaStreamCreateWithFlags(&bg->gs[k], cudaStreamNonBlocking));
       }
       std::vector<char> grouped(n, 0);
-      for (int k = 0; k < 2; ++k)
+      for (int k = 0; k < 4; ++k)
         for (int i : grp[k]) grouped[i] = 1;
-      while (bg->ev.size() < (size_t)(2 * n + 4)) {
+      while (bg->ev.size() < (size_t)(2 * n + 8)) {
         cudaEvent_t e;
         KCHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         bg->ev.push_back(e);
@@ -1640,7 +1763,7 @@ int batch_cycle_impl(kmhd_sph** hs, int32_t n, const double* const* d_rj_in, con
       }
       // grouped instances: slicers, FFT and the FP64 dipole modes on the
       // instance streams, one grouped GEMM per direction on the group stream
-      for (int k = 0; k < 2 && cst == KMHD_OK; ++k) {
+      for (int k = 0; k < 4 && cst == KMHD_OK; ++k) {
         if (grp[k].empty()) continue;
         cudaStream_t g = bg->gs[k];
         cudaEvent_t eg0 = bg->ev[2 * n + 2 * k], eg1 = bg->ev[2 * n + 2 * k + 1];

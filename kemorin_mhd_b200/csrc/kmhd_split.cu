@@ -1072,9 +1072,11 @@ cudaError_t launch_gemm(const GemmArgs& a, cudaStream_t st) {
   return launch_gemm<NS, TG, false>(l, a.nwork / 2, st);
 }
 
+// Instantiations: the split tier keeps the digit pairs a + b <= 6 (26
+// products) or <= 5 (21), the fp32acc tier a + b <= 3 (10) or <= 2 (6).
 cudaError_t run_gemm(const SplitState* s, const GemmArgs& a, cudaStream_t st) {
-  if (s->ns == 6) return launch_gemm<6, 6>(a, st);
-  return launch_gemm<4, 3>(a, st);
+  if (s->ns == 6) return s->T == 6 ? launch_gemm<6, 6>(a, st) : launch_gemm<6, 5>(a, st);
+  return s->T == 3 ? launch_gemm<4, 3>(a, st) : launch_gemm<4, 2>(a, st);
 }
 
 }  // namespace
@@ -1342,13 +1344,30 @@ int split_fwd(SplitState* s, const Plan& p, double* d_rj, long long ld, const in
 }
 
 int split_ns(const SplitState* s) { return s ? s->ns : 0; }
+int split_terms(const SplitState* s) { return s ? s->T : 0; }
+
+int split_products(int ns, int T) {
+  int n = 0;
+  for (int a = 0; a < ns; ++a)
+    for (int b = 0; b < ns; ++b) n += a + b <= T;
+  return n;
+}
+
+int split_set_terms(SplitState* s, int T) {
+  if (!s) return KMHD_ERR_ARG;
+  const int full = s->ns == 6 ? 6 : 3;
+  if (T != full && T != full - 1) return KMHD_ERR_ARG;
+  s->T = T;
+  s->S.T = T;
+  return KMHD_OK;
+}
 
 // ---------------------------------------------------------------------------
 // Grouped GEMM of several instances of one tier: per direction one device
 // array of the instances' arguments and one list of (instance, pair unit),
 // largest instance first; one persistent launch runs them all.
 struct SplitGroup {
-  int ns = 0, n = 0;
+  int ns = 0, T = 0, n = 0;
   GemmArgs* inst[2] = {nullptr, nullptr};  // [bwd, fwd]
   int2* unit[2] = {nullptr, nullptr};
   int nunit[2] = {0, 0};
@@ -1370,6 +1389,7 @@ int split_group_create(SplitGroup** out, SplitState* const* ss, const Plan* plan
   if (n < 1) return KMHD_ERR_ARG;
   SplitGroup* g = new SplitGroup();
   g->ns = ss[0]->ns;
+  g->T = ss[0]->T;
   g->n = n;
   g->err = ss[0]->err;
   for (int d = 0; d < 2; ++d) {
@@ -1377,7 +1397,7 @@ int split_group_create(SplitGroup** out, SplitState* const* ss, const Plan* plan
     std::vector<GemmArgs> args(n);
     std::vector<int> order(n);
     for (int i = 0; i < n; ++i) {
-      if (ss[i]->ns != g->ns) { split_group_destroy(g); return KMHD_ERR_ARG; }
+      if (ss[i]->ns != g->ns || ss[i]->T != g->T) { split_group_destroy(g); return KMHD_ERR_ARG; }
       Plan p = plans[i];
       p.r_lo = 0;
       p.r_hi = p.nr;
@@ -1416,7 +1436,9 @@ int split_group_gemm(SplitGroup* g, bool fwd, cudaStream_t st) {
   l.inst = g->inst[d];
   l.gunit = g->unit[d];
   l.gunits = g->nunit[d];
-  const cudaError_t e = g->ns == 6 ? launch_gemm<6, 6, true>(l, l.gunits, st) : launch_gemm<4, 3, true>(l, l.gunits, st);
+  cudaError_t e;
+  if (g->ns == 6) e = g->T == 6 ? launch_gemm<6, 6, true>(l, l.gunits, st) : launch_gemm<6, 5, true>(l, l.gunits, st);
+  else e = g->T == 3 ? launch_gemm<4, 3, true>(l, l.gunits, st) : launch_gemm<4, 2, true>(l, l.gunits, st);
   return e == cudaSuccess ? KMHD_OK : KMHD_ERR_CUDA;
 }
 

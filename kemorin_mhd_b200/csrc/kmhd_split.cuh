@@ -20,6 +20,11 @@ int split_fwd(SplitState* s, const Plan& p, double* d_rj, long long ld, const in
 int split_slicer(SplitState* s, const Plan& p, bool fwd, const double* d_rj, long long ld, const int* cols,
                  cudaStream_t st);
 int split_ns(const SplitState* s);
+// Highest digit-pair group T kept by the GEMMs (slice products a + b <= T of
+// the ns x ns digit pairs): the tier's full T (6 split, 3 fp32acc) or one less.
+int split_terms(const SplitState* s);
+int split_set_terms(SplitState* s, int T);
+int split_products(int ns, int T);
 // Grouped GEMM over n instances of one split tier (one persistent launch per
 // direction over every instance's pair units; d_rj_out / ld_out / cols_f are
 // the forward outputs, device pointers).  The arguments are copied to the

@@ -67,7 +67,7 @@ EXPORTS = ["kmhd_sph_create", "kmhd_sph_destroy", "kmhd_sph_set_stream", "kmhd_s
            "kmhd_sph_div_flux", "kmhd_sph_rot_induction", "kmhd_sph_rot_force", "kmhd_sph_div_force",
            "kmhd_sph_rot_coriolis", "kmhd_sph_set_coriolis", "kmhd_sph_b_trans_pole",
            "kmhd_sph_div_flux_bc", "kmhd_sph_rot_induction_bc", "kmhd_sph_vorticity", "kmhd_sph_current",
-           "kmhd_sph_rot_buoyancy"]
+           "kmhd_sph_rot_buoyancy", "kmhd_sph_get_tuning", "kmhd_sph_set_products"]
 
 _lib = None
 
@@ -95,6 +95,9 @@ def load_library(path: str | None = None):
     lib.kmhd_sph_last_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     lib.kmhd_sph_last_kernel_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     lib.kmhd_sph_get_path.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
+    lib.kmhd_sph_get_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
+                                        ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double)]
+    lib.kmhd_sph_set_products.argtypes = [vp, i32]
     lib.kmhd_sph_div_flux.argtypes = [vp, vp, i64, i32, i32, vp, vp, i32]
     lib.kmhd_sph_rot_induction.argtypes = [vp, vp, i64, i32, i32, i32]
     lib.kmhd_sph_rot_force.argtypes = [vp, vp, i64, i32, i32, i32, i32, i32]
@@ -211,6 +214,19 @@ class SphTransform:
         v = ctypes.c_int32()
         _check(load_library().kmhd_sph_get_path(self._h, ctypes.byref(v)), "get_path")
         return v.value == 1
+
+    def tuning(self) -> dict:
+        """Legendre path, slice products per GEMM and, after an autotuned batch
+        call, the candidates' times (ms) and errors against the FP64 path."""
+        path, prod = ctypes.c_int32(), ctypes.c_int32()
+        ms, err = (ctypes.c_float * 3)(), (ctypes.c_double * 3)()
+        _check(load_library().kmhd_sph_get_tuning(self._h, ctypes.byref(path), ctypes.byref(prod), ms, err),
+               "get_tuning")
+        return dict(path=path.value, products=prod.value, ms=list(ms), err=list(err))
+
+    def set_products(self, products: int):
+        """Pins the split path's slice products per GEMM (26/21 split, 10/6 fp32acc)."""
+        _check(load_library().kmhd_sph_set_products(self._h, int(products)), "set_products")
 
     def kernel_timing(self):
         """Per-launch ms of the last cycle (CUDA events on the handle's stream)."""
