@@ -178,6 +178,102 @@ def run_reference(args, cfg):
     return 0
 
 
+def run_slabs(args, cfg, fields_bwd, fields_fwd):
+    """One instance spread over the N ranks by radius (kemorin_mhd_b200/slabs.py):
+    rank i holds its owned radii plus one halo radius on each side; every step
+    first refreshes the input halo from the neighbouring ranks (NCCL send/recv,
+    one radius row per backward column and neighbour) and then runs its local
+    cycle.  Strong scaling: `value` is the whole shell's cycles/s (one cycle of
+    the instance per step, time = max over ranks).  With --check every rank
+    also runs the whole shell on its GPU once (untimed) and compares its owned
+    radii bit for bit."""
+    import datetime
+    import torch
+    from kemorin_mhd_b200.slabs import SlabTransform, exchange_halo, radial_slab
+    from kemorin_mhd_b200.synthetic import make_d_rj_torch
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    tier = "split" if args.tier == "auto" else args.tier
+    slab = radial_slab(cfg.nr, ws, rank)
+    J = cfg.J
+    st = SlabTransform(cfg, slab, tier=TIERS[tier])
+    stream = torch.cuda.current_stream()
+    st.tr.set_stream(stream.cuda_stream)
+    full = make_d_rj_torch(cfg, seed=1234)
+    d_in = full[:, slab.lo * J:slab.hi * J].contiguous()
+    d_out = torch.zeros((cfg.ncf, J * slab.nr_local), dtype=torch.float64, device="cuda")
+    cols = list(range(cfg.ncb))
+
+    def step():
+        if dist is not None:
+            exchange_halo(slab, J, d_in, cols)
+        st.tr.nonlinear_cycle(d_in, d_out)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    ms_step = float(ms.item()) / args.steps
+    check = None
+    if args.check:
+        st_out = d_out[:, slab.owned_rows(J)].clone()
+        st.close()
+        from kemorin_mhd_b200 import sph_trans
+        whole = sph_trans.SphTransform(cfg, tier=TIERS[tier], device=local)
+        w_out = torch.zeros((cfg.ncf, J * cfg.nr), dtype=torch.float64, device="cuda")
+        whole.nonlinear_cycle(full, w_out)
+        torch.cuda.synchronize()
+        same = torch.tensor([1.0 if torch.equal(st_out, w_out[:, slab.r0 * J:slab.r1 * J]) else 0.0],
+                            dtype=torch.float64, device="cuda")
+        if dist is not None:
+            dist.all_reduce(same, op=dist.ReduceOp.MIN)
+        check = bool(same.item() == 1.0)
+        whole.close()
+    else:
+        st.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": 1e3 / ms_step, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": DTYPES[tier], "tier": tier,
+            "data": "synthetic (seeded spectra N(0,1)(l+1)^-2 sin(pi(r-ri)/(ro-ri)), Chebyshev radii)",
+            "config": dict(bench_config(cfg, fields_bwd, fields_fwd, ws),
+                           parallelism=f"radial slabs x{ws} (one instance; NCCL halo send/recv of one "
+                                       "radius per backward column and neighbour each step)"),
+            "slab_radii_rank0": [slab.r0, slab.r1], "bit_exact_vs_whole_shell": check,
+            "gpu_launches": {"fp64": 4, "split": 6, "fp32acc": 6}[tier] * args.steps,
+            "clocks": clk, "cpu_baseline": None,
+            "e2e": None,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -194,6 +290,9 @@ def main():
     ap.add_argument("--fields", default="default", choices=["default", "dynamo", "full"],
                     help="field set: default u,omega,B + T; dynamo u,omega,B,J + T with the Lorentz force; "
                          "full u,omega,B,J + T,C with the Lorentz force and the composition flux")
+    ap.add_argument("--slabs", action="store_true",
+                    help="one instance over the N ranks by radius (strong scaling) instead of one instance per rank")
+    ap.add_argument("--check", action="store_true", help="--slabs: compare every rank's radii with the whole shell")
     ap.add_argument("--p-on-the-fly", action="store_true",
                     help="FP64 tier: P_l^m generated inside the Legendre kernels (no stored tables); "
                          "also times the stored-table FP64 tier on the same input")
@@ -211,6 +310,8 @@ def main():
     fields_bwd, fields_fwd = FIELD_NAMES[args.fields]
     if args.impl == "reference":
         return run_reference(args, cfg)
+    if args.slabs:
+        return run_slabs(args, cfg, fields_bwd, fields_fwd)
 
     import numpy as np
     import torch
