@@ -366,6 +366,20 @@ int kmhd_sph_set_coriolis(kmhd_sph *handle, double coef_cor, int32_t iv_velo, in
 int kmhd_sph_b_trans_pole(kmhd_sph *handle, const double *d_rj, int64_t ld_rj, const int32_t *cols_b, double *v_pole,
                           int32_t ptr_kind);
 
+/* Backward transform at the centre of a full-sphere grid (the r = 0 node of a
+ * mesh with a centre point): v_center[0 .. ncomp_b) holds that node's
+ * components in the order of v_pole; for every backward vector, from the
+ * poloidal column S at the innermost radius r_1 = radius[0]:
+ * v[3f] = -2 S(1,-1) / r_1^2, v[3f+1] = -2 S(1,+1) / r_1^2, v[3f+2] =
+ * 2 S(1,0) / r_1^2.  Scalar entries are not written (the reference leaves
+ * them unchanged).  Replaces schmidt_b_trans_center_vect / _scalar
+ * (PARALLEL_src/SPH_SHELL_src/schmidt_b_trans_at_center.f90:45-119), called
+ * by pole_backward_transforms for iflag_MESH_w_center
+ * (pole_sph_transform.f90:148-157).  Host or device pointers (both arrays
+ * the same kind). */
+int kmhd_sph_b_trans_center(kmhd_sph *handle, const double *d_rj, int64_t ld_rj, const int32_t *cols_b,
+                            double *v_center, int32_t ptr_kind);
+
 /* Legendre path the handle runs: 1 = the tier's split path, 0 = FP64 DMMA
  * (FP64 tier, or a split-tier handle the autotuner moved to FP64). */
 int kmhd_sph_get_path(const kmhd_sph *handle, int32_t *path);

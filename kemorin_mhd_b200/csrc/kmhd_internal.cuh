@@ -238,6 +238,8 @@ cudaError_t launch_rot_coriolis(long long J, int nr, const double* vel, const do
                                 double coef_cor, cudaStream_t s);
 // Backward transform at the poles (kmhd_post.cu): v rows r (north) and nr + r
 // (south) for every radius, ncb columns with stride ldv (Cartesian vectors).
+cudaError_t launch_b_trans_center(const Plan& p, const double* d_rj, long long ld, const int* cols, double* v,
+                                  cudaStream_t s);
 cudaError_t launch_b_trans_pole(const Plan& p, const double* d_rj, long long ld, const int* cols, double* v,
                                 long long ldv, cudaStream_t s);
 // Curl of the radial buoyancy (kmhd_post.cu); C null: one scalar.

@@ -232,6 +232,29 @@ __global__ void k_b_trans_pole(Plan P, const double* __restrict__ d_rj, long lon
   }
 }
 
+// Backward transform at the centre of a full-sphere grid (the node at r = 0
+// of a mesh with a centre point): schmidt_b_trans_center_vect
+// (PARALLEL_src/SPH_SHELL_src/schmidt_b_trans_at_center.f90:64-119).  From
+// the poloidal column S of the innermost radius r_1 = radius[0]: component 3
+// = 2 S(1, 0) / r_1^2, component 1 = -2 S(1, -1) / r_1^2, component 2 =
+// -2 S(1, +1) / r_1^2 (orders -1 / +1 as the code assigns them; its header
+// comment names the opposite pairing).  Scalars are left as they are
+// (schmidt_b_trans_center_scalar assigns a value to itself).  Thread f: vector f.
+__global__ void k_b_trans_center(Plan P, const double* __restrict__ d_rj, long long ld, const int* __restrict__ cols,
+                                 double* __restrict__ v) {
+  const int f = threadIdx.x;
+  if (f >= P.nvb || P.L < 1) return;
+  const int L = P.L;
+  const double* S = d_rj + ld * cols[f];  // radius index 0: rows 0 .. J - 1
+  const double ar = 1.0 / P.radius[0];
+  const long long j0 = P.jmap[(0LL * 2 + 0) * (L + 1) + 1];
+  const long long jp = P.jmap[(1LL * 2 + 0) * (L + 1) + 1];
+  const long long jm = P.jmap[(1LL * 2 + 1) * (L + 1) + 1];
+  v[3 * f + 0] = -2.0 * S[jm] * ar * ar;
+  v[3 * f + 1] = -2.0 * S[jp] * ar * ar;
+  v[3 * f + 2] = 2.0 * S[j0] * ar * ar;
+}
+
 // Curl of the radial buoyancy (toroidal part): out = coef_t T r, or
 // (coef_t T + coef_c C) r with a second scalar (cal_rot_buoyancy_sph_MHD /
 // cal_rot_double_buoyancy_sph_MHD, MHD_src/sph_MHD/cal_rot_buoyancies_sph_MHD.f90:106-165).
@@ -278,6 +301,13 @@ cudaError_t launch_b_trans_pole(const Plan& p, const double* d_rj, long long ld,
   if (p.nr <= 0 || p.nvb + p.nsb == 0) return cudaSuccess;
   const int warps = p.nvb + p.nsb < 8 ? p.nvb + p.nsb : 8;
   k_b_trans_pole<<<p.nr, 32 * warps, 0, s>>>(p, d_rj, ld, cols, v, ldv);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_b_trans_center(const Plan& p, const double* d_rj, long long ld, const int* cols, double* v,
+                                  cudaStream_t s) {
+  if (p.nvb <= 0) return cudaSuccess;
+  k_b_trans_center<<<1, 32 * ((p.nvb + 31) / 32), 0, s>>>(p, d_rj, ld, cols, v);
   return cudaGetLastError();
 }
 

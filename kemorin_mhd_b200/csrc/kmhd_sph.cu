@@ -1421,6 +1421,34 @@ int kmhd_sph_b_trans_pole(kmhd_sph* h, const double* d_rj, int64_t ld, const int
   return KMHD_OK;
 }
 
+int kmhd_sph_b_trans_center(kmhd_sph* h, const double* d_rj, int64_t ld, const int32_t* cols_b, double* v_center,
+                            int32_t ptr_kind) {
+  if (!h || !d_rj || !v_center || !cols_b) return KMHD_ERR_ARG;
+  if (check_ld(h, ld)) return KMHD_ERR_ARG;
+  const Plan& p = h->plan;
+  if (p.nvb + p.nsb == 0) return KMHD_ERR_STATE;
+  if (p.nvb == 0) return KMHD_OK;  // scalars are left as they are
+  KCHECK(cudaSetDevice(h->device));
+  int st;
+  const double* src = d_rj;
+  int64_t sld = ld;
+  std::vector<int> cc;
+  double* out = v_center;
+  if (ptr_kind == KMHD_PTR_HOST) {
+    if ((st = stage_host_in(h, d_rj, ld, cols_b, p.nvb, p.nsb, &src, &sld, cc))) return st;
+    if ((st = sync_cols(h, cc.data(), p.nvb + p.nsb, h->cols_b_cache, h->cols_b_d))) return st;
+    if (!h->pole_out && (st = dalloc(h, &h->pole_out, 2 * (size_t)p.nr * p.ncb))) return st;
+    out = h->pole_out;
+  } else if ((st = sync_cols(h, cols_b, p.nvb + p.nsb, h->cols_b_cache, h->cols_b_d))) {
+    return st;
+  }
+  KCHECK(launch_b_trans_center(p, src, sld, h->cols_b_d, out, h->stream));
+  if (ptr_kind == KMHD_PTR_HOST)
+    KCHECK(cudaMemcpyAsync(v_center, out, sizeof(double) * 3 * p.nvb, cudaMemcpyDeviceToHost, h->stream));
+  KCHECK(cudaStreamSynchronize(h->stream));
+  return KMHD_OK;
+}
+
 int kmhd_sph_rot_buoyancy(kmhd_sph* h, double* d_rj, int64_t ld, int32_t col_t, double coef_t, int32_t col_c,
                           double coef_c, int32_t col_out, int32_t ptr_kind) {
   if (!h || !d_rj) return KMHD_ERR_ARG;

@@ -67,7 +67,7 @@ EXPORTS = ["kmhd_sph_create", "kmhd_sph_destroy", "kmhd_sph_set_stream", "kmhd_s
            "kmhd_sph_div_flux", "kmhd_sph_rot_induction", "kmhd_sph_rot_force", "kmhd_sph_div_force",
            "kmhd_sph_rot_coriolis", "kmhd_sph_set_coriolis", "kmhd_sph_b_trans_pole",
            "kmhd_sph_div_flux_bc", "kmhd_sph_rot_induction_bc", "kmhd_sph_vorticity", "kmhd_sph_current",
-           "kmhd_sph_rot_buoyancy", "kmhd_sph_get_tuning", "kmhd_sph_set_products"]
+           "kmhd_sph_rot_buoyancy", "kmhd_sph_get_tuning", "kmhd_sph_set_products", "kmhd_sph_b_trans_center"]
 
 _lib = None
 
@@ -105,6 +105,7 @@ def load_library(path: str | None = None):
     lib.kmhd_sph_rot_coriolis.argtypes = [vp, vp, i64, i32, i32, i32, ctypes.c_double, i32]
     lib.kmhd_sph_set_coriolis.argtypes = [vp, ctypes.c_double, i32, i32, i32]
     lib.kmhd_sph_b_trans_pole.argtypes = [vp, vp, i64, vp, vp, i32]
+    lib.kmhd_sph_b_trans_center.argtypes = [vp, vp, i64, vp, vp, i32]
     lib.kmhd_sph_div_flux_bc.argtypes = [vp, vp, i64, i32, i32, i32, i32, vp, vp, i32]
     lib.kmhd_sph_rot_induction_bc.argtypes = [vp, vp, i64, i32, i32, i32, i32, i32]
     lib.kmhd_sph_vorticity.argtypes = [vp, vp, i64, i32, i32, i32, i32, i32]
@@ -386,6 +387,19 @@ class SphTransform:
         n = self.cfg.J * self.cfg.nr
         _check(load_library().kmhd_sph_b_trans_pole(self._h, p, ld or n, cb, q, kind), "kmhd_sph_b_trans_pole")
         return v_pole
+
+    def b_trans_center(self, d_rj, v_center, cols_b=None, ld: int | None = None):
+        """Values at the centre node of a full-sphere grid: v_center (ncomp_b;
+        torch CUDA tensor or numpy array); vector entries are written, scalar
+        entries left as they are."""
+        p, kind = _ptr(d_rj)
+        q, kind2 = _ptr(v_center)
+        if kind != kind2:
+            raise ValueError("d_rj and v_center must both be host or both be device arrays")
+        cb = self._cols_b if cols_b is None else _i32(cols_b)
+        n = self.cfg.J * self.cfg.nr
+        _check(load_library().kmhd_sph_b_trans_center(self._h, p, ld or n, cb, q, kind), "kmhd_sph_b_trans_center")
+        return v_center
 
     def set_coriolis(self, coef_cor: float, iv_velo: int = 0, iv_vort: int = 1, col_out: int = -1):
         """Every following cycle also writes the curl of the Coriolis term of

@@ -19,6 +19,12 @@ P_l^0(-1) = (-1)^l, dP_l^1/dtheta = sqrt(l(l+1)/2) at the north pole and
 - sqrt((l-1)(l+2)) P_l^2) / 2 with P_l^2 = 0 at the poles); g3 = g_sph_rlm(j,3)
 = l(l+1), 1/2 at l = 0.
 
+The centre node of a full-sphere grid (b_trans_center) follows
+schmidt_b_trans_center_vect / _scalar (schmidt_b_trans_at_center.f90:45-119):
+from the innermost radius r_1, vector components (1, 2, 3) =
+(-2 S(1,-1), -2 S(1,+1), 2 S(1,0)) / r_1^2 -- the pairing of the code, whose
+header comment names the opposite one -- and scalar entries unchanged.
+
 Parity unpinned against the reference's own outputs (no Fortran compiler in
 this image); the tests pin the sign conventions by the uniform fields x, y, z
 (poloidal l = 1 fields with S = r^2/2) and the pole values by quadrature.
@@ -75,4 +81,19 @@ def b_trans_pole(radius, L, l_of_j, m_of_j, d_rj, nvb, nsb):
                 sn = sn + row(c, l, 0) * pn
                 ss = ss + row(c, l, 0) * ps
             v[k, c], v[nr + k, c] = sn, ss
+    return v
+
+
+def b_trans_center(radius, l_of_j, m_of_j, d_rj, nvb, nsb, v_in=None):
+    """The centre node's components (3 nvb + nsb) from the innermost radius of
+    d_rj (J*nr x ncomp); scalar entries are copied from v_in (zeros if None)."""
+    r1 = float(np.asarray(radius, dtype=np.float64)[0])
+    idx = {(int(a), int(b)): j for j, (a, b) in enumerate(zip(l_of_j, m_of_j))}
+    dr = np.asarray(d_rj, dtype=np.float64)
+    v = np.zeros(3 * nvb + nsb) if v_in is None else np.array(v_in, dtype=np.float64)
+    for nd in range(nvb):
+        c = 3 * nd
+        v[c] = -2.0 * dr[idx[(1, -1)], c] * (1.0 / r1) * (1.0 / r1)
+        v[c + 1] = -2.0 * dr[idx[(1, 1)], c] * (1.0 / r1) * (1.0 / r1)
+        v[c + 2] = 2.0 * dr[idx[(1, 0)], c] * (1.0 / r1) * (1.0 / r1)
     return v

@@ -39,3 +39,34 @@ def test_pole_values_match_oracle(host, tier):
         tr.b_trans_pole(to_dev_fortran(wide), out, cols_b=cols)
         got = from_dev_fortran(out)
     assert col_relerr(got, ref).max() <= 1e-13
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("host", [False, True], ids=["device", "host"])
+def test_center_values_match_oracle(host):
+    """Centre node of a full-sphere grid (kmhd_sph_b_trans_center) against the
+    oracle of schmidt_b_trans_center_vect: vector entries bit-identical,
+    scalar entries untouched, fields in permuted columns."""
+    import torch
+    from kemorin_mhd_b200.sph_trans import SphTransform
+    from oracle.sph_pole import b_trans_center
+    cfg = CFG
+    tr = SphTransform(cfg, tier=TIER_FP64)
+    d = make_d_rj(cfg, seed=17)
+    l, m = rj_order(cfg.ltr)
+    v0 = np.full(cfg.ncb, 5.25)
+    ref = b_trans_center(cfg.radius(), l, m, d, cfg.nvb, cfg.nsb, v_in=v0)
+    wide = np.zeros((d.shape[0], 12), order="F")
+    wide[:, 0] = d[:, 9]
+    wide[:, 1:4] = d[:, 6:9]
+    wide[:, 5:8] = d[:, 0:3]
+    wide[:, 8:11] = d[:, 3:6]
+    cols = [5, 8, 1, 0]
+    if host:
+        got = v0.copy()
+        tr.b_trans_center(wide, got, cols_b=cols)
+    else:
+        out = torch.from_numpy(v0.copy()).cuda()
+        tr.b_trans_center(to_dev_fortran(wide), out, cols_b=cols)
+        got = out.cpu().numpy()
+    assert np.array_equal(got, ref), (got, ref)

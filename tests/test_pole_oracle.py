@@ -46,3 +46,25 @@ def test_uniform_fields_at_the_poles():
     expect = np.concatenate([np.eye(3).reshape(-1), [1.0]])
     for row in range(2 * nr):
         assert np.abs(v[row] - expect).max() < 1e-14, (row, v[row])
+
+
+def test_center_oracle_uniform_z_and_scalars_untouched():
+    """Centre node (b_trans_center): the uniform field z (S(1,0) = r^2 / 2)
+    gives (0, 0, 1); orders -1 / +1 feed components 1 / 2 with the factor -2
+    as schmidt_b_trans_center_vect assigns them; scalar entries keep v_in."""
+    from oracle.sph_pole import b_trans_center
+    L, nr = 4, 3
+    radius = np.array([0.2, 0.6, 1.0])
+    l, m = rj_order(L)
+    J = len(l)
+    d = np.zeros((J * nr, 4))
+    jz = int(np.flatnonzero((l == 1) & (m == 0))[0])
+    for k in range(nr):
+        d[k * J + jz, 0] = radius[k] ** 2 / 2
+    v = b_trans_center(radius, l, m, d, 1, 1, v_in=[9.0, 9.0, 9.0, 7.5])
+    assert np.allclose(v, [0.0, 0.0, 1.0, 7.5], rtol=0, atol=1e-15)
+    jm, jp = (int(np.flatnonzero((l == 1) & (m == s))[0]) for s in (-1, 1))
+    d2 = np.zeros_like(d)
+    d2[jm, 0], d2[jp, 0] = 0.02, -0.04
+    v2 = b_trans_center(radius, l, m, d2, 1, 1)
+    assert np.allclose(v2[:3], [-2 * 0.02 / 0.04, 2 * 0.04 / 0.04, 0.0], rtol=1e-15, atol=0)
