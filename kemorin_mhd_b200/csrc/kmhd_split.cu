@@ -120,6 +120,11 @@ __device__ __forceinline__ double pow2(int e) {
   return __longlong_as_double((long long)(e + 1023) << 52);
 }
 
+// 32-byte global load (sm_100 256-bit ld.global, read-only path); p must be 32-byte aligned
+__device__ __forceinline__ void ld_global_v4(const double* p, double& a, double& b, double& c, double& d) {
+  asm volatile("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];\n" : "=d"(a), "=d"(b), "=d"(c), "=d"(d) : "l"(p));
+}
+
 // frexp-style exponent: smallest e with |x| < 2^e (x > 0)
 __device__ __forceinline__ int exp_above(double x) {
   int e;
@@ -363,6 +368,9 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_mr(Plan P, SliceTabs S,
     const int rec = 2 * P.ncf;
     const long long strideTh = rec;  // records of one (m, r) are contiguous over theta
     const double* base = P.rtm_f + rtm_off(P, m, 0, r, P.ncf) + (vgrp ? 4 * v : 4 * nv);
+    // 256-bit loads need 32-byte aligned records (an even forward component count)
+    const bool v4 = ((reinterpret_cast<uintptr_t>(P.rtm_f) | (uintptr_t)(16 * P.ncf)) & 31) == 0;
+    double2 nxt = make_double2(0.0, 0.0), sxt = nxt;  // second field of a 256-bit load
     for (int th = threadIdx.x; th < P.nh; th += blockDim.x) {
       const bool hasS = th < P.nth / 2;
       const double w = __ldg(P.weight + th);
@@ -370,15 +378,22 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_mr(Plan P, SliceTabs S,
       const double* ps = base + (long long)(P.nth - 1 - th) * strideTh;
       const double sa = pow2(-__ldg(dxa + th)), sb = pow2(-__ldg(dxb + th));
       if (vgrp) {
-        // words (theta slot 0, theta slot 1, phi slot 0, phi slot 1)
-        const double2 n01 = __ldg(reinterpret_cast<const double2*>(pn));
-        const double2 n23 = __ldg(reinterpret_cast<const double2*>(pn + 2));
-        double2 s01 = make_double2(0.0, 0.0), s23 = s01;
-        if (hasS) {
-          s01 = __ldg(reinterpret_cast<const double2*>(ps));
-          s23 = __ldg(reinterpret_cast<const double2*>(ps + 2));
+        // words (theta slot 0, theta slot 1, phi slot 0, phi slot 1): one
+        // 32-byte sector per row, one 256-bit load when the records are aligned
+        double nn[4], ss[4] = {0.0, 0.0, 0.0, 0.0};
+        if (v4) {
+          ld_global_v4(pn, nn[0], nn[1], nn[2], nn[3]);
+          if (hasS) ld_global_v4(ps, ss[0], ss[1], ss[2], ss[3]);
+        } else {
+          const double2 n01 = __ldg(reinterpret_cast<const double2*>(pn));
+          const double2 n23 = __ldg(reinterpret_cast<const double2*>(pn + 2));
+          nn[0] = n01.x; nn[1] = n01.y; nn[2] = n23.x; nn[3] = n23.y;
+          if (hasS) {
+            const double2 s01 = __ldg(reinterpret_cast<const double2*>(ps));
+            const double2 s23 = __ldg(reinterpret_cast<const double2*>(ps + 2));
+            ss[0] = s01.x; ss[1] = s01.y; ss[2] = s23.x; ss[3] = s23.y;
+          }
         }
-        const double nn[4] = {n01.x, n01.y, n23.x, n23.y}, ss[4] = {s01.x, s01.y, s23.x, s23.y};
         double sy[4], as[4];
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
@@ -409,8 +424,23 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_mr(Plan P, SliceTabs S,
         }
       } else {
         for (int f = 0; f < nF; ++f) {
-          const double2 nn = __ldg(reinterpret_cast<const double2*>(pn + 2 * f));
-          const double2 ss = hasS ? __ldg(reinterpret_cast<const double2*>(ps + 2 * f)) : make_double2(0.0, 0.0);
+          double2 nn, ss = make_double2(0.0, 0.0);
+          if (v4 && f + 1 < nF && !(f & 1)) {
+            // fields f, f + 1 in one 32-byte sector
+            double4 a, b = make_double4(0.0, 0.0, 0.0, 0.0);
+            ld_global_v4(pn + 2 * f, a.x, a.y, a.z, a.w);
+            if (hasS) ld_global_v4(ps + 2 * f, b.x, b.y, b.z, b.w);
+            nn = make_double2(a.x, a.y);
+            ss = make_double2(b.x, b.y);
+            nxt = make_double2(a.z, a.w);
+            sxt = make_double2(b.z, b.w);
+          } else if (v4 && (f & 1)) {
+            nn = nxt;
+            ss = sxt;
+          } else {
+            nn = __ldg(reinterpret_cast<const double2*>(pn + 2 * f));
+            if (hasS) ss = __ldg(reinterpret_cast<const double2*>(ps + 2 * f));
+          }
           X[(4 * f + 0) * kst + th] = (nn.x + ss.x) * w * sa;
           X[(4 * f + 2) * kst + th] = hasS ? (nn.x - ss.x) * w * sb : 0.0;
           if (m > 0) {
