@@ -501,10 +501,6 @@ def main():
                 "executed_int8_tops": execd / (dur * 1e-3) / 1e12,
                 "executed_frac": execd / (dur * 1e-3) / 1e12 / pk,
                 "overhead_factor": execd / flops}
-        p8 = ctypes_probe_i8(lib, local)
-        if p8:
-            roof["int8_probe_tops"] = p8
-            roof["executed_frac_of_int8_probe"] = roof["executed_int8_tops"] / p8
     roof["frac"] = roof["achieved"] / roof["peak"] if roof["peak"] else None
     roof["traffic"] = read_traffic(roof["kernel"], cfg.name)
     roof["algorithmic_flops_per_launch"] = flops
@@ -666,19 +662,6 @@ def ctypes_probe(lib, dev):
     f.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     v = ctypes.c_double()
     return v.value if f(dev, ctypes.byref(v)) == 0 else None
-
-
-def ctypes_probe_i8(lib, dev):
-    """INT8 tensor-pipe rate measured in-process: back-to-back tcgen05 kind::i8
-    MMAs of 128 x 256 x 32 from shared memory on every SM (TOP/s)."""
-    import ctypes
-    try:
-        f = lib.kmhd_probe_i8_mma
-    except AttributeError:
-        return None
-    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
-    v = ctypes.c_double()
-    return v.value if f(dev, 256, 100000, 64, ctypes.byref(v)) == 0 else None
 
 
 def fp64_rooflines(cfg, kern, probe_tflops):

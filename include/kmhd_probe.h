@@ -18,12 +18,6 @@ int kmhd_probe_fp64_tflops(int device, double *tflops);
  * tensor-core operand layout used by the split-precision tiers. */
 int kmhd_selftest_i8_mma(int lbo, int sbo, const signed char *A, const signed char *B, int *D);
 
-/* INT8 tensor-pipe rate (TOP/s) of back-to-back tcgen05 kind::i8 MMAs of shape
- * 128 x n x 32 from shared memory, one CTA per SM, commit + wait every `group`
- * instructions: the measured INT8 peak that the benchmark divides the split
- * GEMM's executed rate by. */
-int kmhd_probe_i8_mma(int device, int n, int iters, int group, double *tops);
-
 #ifdef __cplusplus
 }
 #endif

@@ -1592,85 +1592,4 @@ extern "C" int kmhd_selftest_i8_mma(int lbo, int sbo, const signed char* A, cons
   return st;
 }
 
-// ---------------------------------------------------------------------------
-// Tensor-pipe probe: kind::i8 MMAs (M = 128, N = n, K = 32) from one shared
-// tile, issued back to back by one thread, with a commit/wait every `group`
-// instructions; one CTA per SM.  Measures the achievable INT8 MMA rate for the
-// operand layout used above.
-namespace kmhd {
-namespace {
-__global__ void __launch_bounds__(128, 1) k_probe_mma(int n, int iters, int group, int* err) {
-  extern __shared__ __align__(1024) unsigned char smp[];
-  unsigned char* sa = smp;
-  unsigned char* sb = smp + kTM * kTK;
-  __shared__ unsigned long long bar;
-  __shared__ unsigned slot;
-  for (int i = threadIdx.x; i < (kTM + 256) * kTK; i += blockDim.x) smp[i] = (unsigned char)(i * 7);
-  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-  if (threadIdx.x == 0) {
-    mbar_init(&bar, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-  }
-  if (threadIdx.x < 32) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;\n" ::"r"(sptr(&slot)));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const unsigned tmem = slot;
-  if (threadIdx.x == 0) {
-    const unsigned idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(n >> 3) << 17) | ((unsigned)(kTM >> 4) << 24);
-    const uint64_t ad = smem_desc(sa, 128, 256), bd = smem_desc(sb, 128, 256);
-    unsigned phase = 0;
-    for (int it = 0; it < iters; ++it) {
-      mma_i8(tmem + (unsigned)((it & 1) * 256 % (512 - n + 1)), ad, bd, idesc, it > 1 ? 1u : 0u);
-      if ((it + 1) % group == 0) {
-        mma_commit(&bar);
-        if (!mbar_wait(&bar, phase)) { atomicExch(err, KMHD_ERR_TIMEOUT); break; }
-        phase ^= 1u;
-      }
-    }
-    mma_commit(&bar);
-    if (!mbar_wait(&bar, phase)) atomicExch(err, KMHD_ERR_TIMEOUT);
-  }
-  tc_fence_before();
-  __syncthreads();
-  if (threadIdx.x < 32) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;\n" ::"r"(tmem));
-}
-}  // namespace
-}  // namespace kmhd
-
-extern "C" int kmhd_probe_i8_mma(int device, int n, int iters, int group, double* tops) {
-  using namespace kmhd;
-  if (!tops || n < 16 || n > 256 || n % 16) return KMHD_ERR_ARG;
-  if (cudaSetDevice(device) != cudaSuccess) return KMHD_ERR_DEVICE;
-  int nsm = 0;
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-  int* err = nullptr;
-  if (cudaMalloc(&err, sizeof(int)) != cudaSuccess) return KMHD_ERR_NOMEM;
-  cudaMemset(err, 0, sizeof(int));
-  const size_t smem = (kTM + 256) * kTK + 1024;
-  cudaFuncSetAttribute(k_probe_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, 120 * 1024);
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  k_probe_mma<<<nsm, 128, 120 * 1024>>>(n, 64, group, err);
-  cudaEventRecord(e0);
-  k_probe_mma<<<nsm, 128, 120 * 1024>>>(n, iters, group, err);
-  cudaEventRecord(e1);
-  cudaError_t ce = cudaEventSynchronize(e1);
-  float ms = 0.f;
-  cudaEventElapsedTime(&ms, e0, e1);
-  int h = 0;
-  cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  cudaFree(err);
-  (void)smem;
-  if (ce != cudaSuccess) return KMHD_ERR_CUDA;
-  if (h) return h;
-  *tops = 2.0 * kTM * n * kTK * (double)iters * nsm / (ms * 1e-3) / 1e12;
-  return KMHD_OK;
-}
 
