@@ -100,6 +100,11 @@ __device__ __forceinline__ void tmem_ld16(unsigned taddr, int* v) {
         "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
       : "r"(taddr));
 }
+__device__ __forceinline__ void tmem_ld8(unsigned taddr, int* v) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "r"(taddr));
+}
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
 
 // ---------------------------------------------------------------------------
@@ -605,7 +610,7 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_mr(Plan P, SliceTabs S,
 //   warp 0 (one lane): issues the tcgen05.mma slice products into TMEM
 //   warp 1 (one lane): streams pre-laid-out slice tiles with bulk copies into a
 //                      stage ring, running ahead across tiles
-//   warps 2..9:        epilogue (TMEM -> FP64 recombination -> output), two per TMEM lane quadrant
+//   warps 2..17:       epilogue (TMEM -> FP64 recombination -> output), four per TMEM lane quadrant
 // One tile = (m, type, m-tile, n-tile).  The work lists pair the two parity
 // tiles (types 0/1, 2/3, 4/5 or 6/7) of one output tile; one CTA runs them back
 // to back and keeps the first in shared memory.  Backward it then emits the
@@ -627,9 +632,11 @@ struct GemmArgs {
   int* err;        // device error word
 };
 
-constexpr int kGemmWarps = 10;     // MMA issuer, bulk-copy producer, 8 epilogue warps
-constexpr int kEpiThreads = 256;
-constexpr int kHalf = kTN / 2;     // columns recombined by one epilogue warp
+constexpr int kEpiWarps = 16;                // four per TMEM lane quadrant
+constexpr int kGemmWarps = 2 + kEpiWarps;    // MMA issuer, bulk-copy producer, epilogue
+constexpr int kEpiThreads = 32 * kEpiWarps;
+constexpr int kCols = kTN * 4 / kEpiWarps;   // columns recombined by one epilogue warp
+constexpr int kLd = 8;                       // columns per TMEM load
 constexpr int kRing = 4;           // stage ring depth
 constexpr int kXS = kTN + 2;       // stash row stride (doubles): 16-byte rows, conflict-free v2 accesses
 
@@ -808,11 +815,11 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
       if (!ok) atomicExch(L.a.err, KMHD_ERR_TIMEOUT);
     }
   } else {
-    // ---- epilogue warps 2..9: TMEM lane quadrant = warp % 4, two warps per
-    // quadrant, each recombining one 32-column half of the tile
+    // ---- epilogue warps 2..17: TMEM lane quadrant = warp % 4, four warps per
+    // quadrant, each recombining one 16-column quarter of the tile
     const int quad = warp & 3;
-    const int half = (warp - 2) >> 2;
-    const int cbase = kHalf * half;
+    const int part = (warp - 2) >> 2;
+    const int cbase = kCols * part;
     const int row = quad * 32 + lane;
     const double wscale = pow2(8 * (2 * NS - 2 - TG));
     int it = 0;
@@ -831,21 +838,21 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
         const int grow = w.mt * kTM + row;
         const int eA = (grow < g.rows) ? S.aexp[S.aeoff[w.m * kNT + w.t] + grow] : 0;
         // column exponents: lane i holds column cbase + i, broadcast by shuffles
-        const int eBl = __ldg(S.bexp + S.beoff[w.m * kNT + w.t] + w.nt * kTN + cbase + lane);
+        const int eBl = lane < kCols ? __ldg(S.bexp + S.beoff[w.m * kNT + w.t] + w.nt * kTN + cbase + lane) : 0;
         if (ok && !mbar_wait(done, (unsigned)(it & 1))) ok = false;
         ok = __all_sync(0xffffffffu, ok);
         tc_fence_after();
-        double val[kHalf];  // columns cbase .. cbase + 31
+        double val[kCols];  // columns cbase .. cbase + kCols - 1
         if (nk > 0 && ok) {
 #pragma unroll
-          for (int cb = 0; cb < kHalf / 16; ++cb) {
-            int acc[TG + 1][16];
+          for (int cb = 0; cb < kCols / kLd; ++cb) {
+            int acc[TG + 1][kLd];
 #pragma unroll
             for (int gi = 0; gi <= TG; ++gi)
-              tmem_ld16(tmem + ((unsigned)(quad * 32) << 16) + (unsigned)(gi * kTN + cbase + cb * 16), acc[gi]);
+              tmem_ld8(tmem + ((unsigned)(quad * 32) << 16) + (unsigned)(gi * kTN + cbase + cb * kLd), acc[gi]);
             tmem_wait_ld();
 #pragma unroll
-            for (int c = 0; c < 16; ++c) {
+            for (int c = 0; c < kLd; ++c) {
               // sum_g acc[g] 256^(TG-g): the four lowest groups combine exactly in
               // int64 (< 2^51), the higher ones exactly in FP64 (< 2^43); one rounding
               constexpr int G0 = TG >= 3 ? TG - 3 : 0;
@@ -859,13 +866,13 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
                 for (int gi = 1; gi < G0; ++gi) hi = fma(hi, 256.0, i2d(acc[gi][c]));
                 v = fma(hi, pow2(8 * (TG - G0 + 1)), v);
               }
-              const int eB = __shfl_sync(0xffffffffu, eBl, cb * 16 + c);
-              val[cb * 16 + c] = v * (wscale * pow2(eA + eB));
+              const int eB = __shfl_sync(0xffffffffu, eBl, cb * kLd + c);
+              val[cb * kLd + c] = v * (wscale * pow2(eA + eB));
             }
           }
         } else {
 #pragma unroll
-          for (int c = 0; c < kHalf; ++c) val[c] = 0.0;
+          for (int c = 0; c < kCols; ++c) val[c] = 0.0;
         }
         tc_fence_before();
         asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(sptr(tfree)) : "memory");
@@ -874,7 +881,7 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
           // first tile of the pair: keep this thread's half row in shared memory
           double* sr = stash + row * kXS + cbase;
 #pragma unroll
-          for (int c = 0; c < kHalf; c += 2) *reinterpret_cast<double2*>(sr + c) = make_double2(val[c], val[c + 1]);
+          for (int c = 0; c < kCols; c += 2) *reinterpret_cast<double2*>(sr + c) = make_double2(val[c], val[c + 1]);
         } else if (!bwd) {
           // forward pair: row i carries degree l0 = m + 2 (128 mt + i) in the even
           // tile (stash) and l0 + 1 in the odd tile (val).  Scatter both into d_rj
@@ -894,7 +901,7 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
             // column c = 8 (block - 8 nt) + 2 (f % 4) + slot, block = (f / 4) nrR + r
             const double g60 = g6_of(l0, w.m), g61 = g6_of(l1, w.m);
 #pragma unroll
-            for (int rr = 0; rr < kHalf / 8; ++rr) {
+            for (int rr = 0; rr < kCols / 8; ++rr) {
               const int rg = w.nt * (kTN / 8) + cbase / 8 + rr;
               const int fg = rg / S.nrR, r = rg - fg * S.nrR;
               if (r >= P.nr) continue;
@@ -921,7 +928,7 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
           } else {
             // column c = 4 (r + nrT v) + q, q = 2 (component - 1) + slot
 #pragma unroll
-            for (int c4 = 0; c4 < kHalf / 4; ++c4) {
+            for (int c4 = 0; c4 < kCols / 4; ++c4) {
               const int rv = w.nt * (kTN / 4) + cbase / 4 + c4;
               const int r = rv % S.nrT, v = rv / S.nrT;
               if (v >= P.nvf) break;
@@ -961,7 +968,7 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
             if (w.t <= 1) {
               // column c = 4 (r + nrT v) + q: one vector's (theta c, theta s, phi c, phi s)
 #pragma unroll
-              for (int c = 0; c < kHalf; c += 4) {
+              for (int c = 0; c < kCols; c += 4) {
                 const int col = w.nt * kTN + cbase + c;
                 const int r = (col >> 2) % S.nrT, vv = (col >> 2) / S.nrT;
                 if (vv >= P.nvb || r >= P.nr) continue;
@@ -993,7 +1000,7 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
               // radial components and scalars, record words 4 nvb + 2 f
               const int nF = P.nvb + P.nsb;
 #pragma unroll
-              for (int rr = 0; rr < kHalf / 8; ++rr) {
+              for (int rr = 0; rr < kCols / 8; ++rr) {
                 const int rg = w.nt * (kTN / 8) + cbase / 8 + rr;
                 const int fg = rg / S.nrR, r = rg - fg * S.nrR;
                 if (r >= P.nr || 4 * fg >= nF) continue;
