@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "kmhd_split.cuh"
@@ -679,10 +680,17 @@ struct MmaSched {
   }
 };
 
-// exact int32 -> double on the FP64 pipe (2^52 + 2^31 magic)
-__device__ __forceinline__ double i2d(int x) {
-  return __hiloint2double(0x43300000, (unsigned)x ^ 0x80000000u) - 4503601774854144.0;
+// d = a * b + c with a 32 x 32 -> 64-bit signed product (one wide integer multiply-add)
+__device__ __forceinline__ long long mad_wide(int a, int b, long long c) {
+  long long d;
+  asm("mad.wide.s32 %0, %1, %2, %3;\n" : "=l"(d) : "r"(a), "r"(b), "l"(c));
+  return d;
 }
+// Integers x with |x| < 2^51 are carried as the bit pattern of the double
+// 1.5 2^52 + x (that double's mantissa is 2^51 + x, its ulp 1): kBias + x read
+// as a double, minus 1.5 2^52, is x exactly.
+constexpr long long kBias = 0x4338000000000000LL;
+constexpr double kBiasD = 6755399441055744.0;  // 1.5 2^52
 template <int NS>
 __host__ __device__ constexpr size_t gemm_stage_bytes() { return (size_t)NS * (kTM + kTN) * kTK; }
 
@@ -821,7 +829,7 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
     const int part = (warp - 2) >> 2;
     const int cbase = kCols * part;
     const int row = quad * 32 + lane;
-    const double wscale = pow2(8 * (2 * NS - 2 - TG));
+    constexpr int kW = 8 * (2 * NS - 2 - TG);  // weight exponent of the lowest kept group
     int it = 0;
     bool ok = true;
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
@@ -839,37 +847,50 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
         const int eA = (grow < g.rows) ? S.aexp[S.aeoff[w.m * kNT + w.t] + grow] : 0;
         // column exponents: lane i holds column cbase + i, broadcast by shuffles
         const int eBl = lane < kCols ? __ldg(S.bexp + S.beoff[w.m * kNT + w.t] + w.nt * kTN + cbase + lane) : 0;
+        // value scale 2^(ea + eB): built from its exponent bits when every
+        // exponent of this warp's block is in the normal range (warp-uniform test)
+        const int ea = eA + kW;
+        const bool fast = __reduce_min_sync(0xffffffffu, ea) + __reduce_min_sync(0xffffffffu, lane < kCols ? eBl : 0x3fffffff) >= -1022 &&
+                          __reduce_max_sync(0xffffffffu, ea) + __reduce_max_sync(0xffffffffu, lane < kCols ? eBl : -0x3fffffff) <= 1023;
         if (ok && !mbar_wait(done, (unsigned)(it & 1))) ok = false;
         ok = __all_sync(0xffffffffu, ok);
         tc_fence_after();
         double val[kCols];  // columns cbase .. cbase + kCols - 1
         if (nk > 0 && ok) {
+          auto drain = [&](auto fastc) {
+            constexpr bool F = decltype(fastc)::value;
 #pragma unroll
-          for (int cb = 0; cb < kCols / kLd; ++cb) {
-            int acc[TG + 1][kLd];
+            for (int cb = 0; cb < kCols / kLd; ++cb) {
+              int acc[TG + 1][kLd];
 #pragma unroll
-            for (int gi = 0; gi <= TG; ++gi)
-              tmem_ld8(tmem + ((unsigned)(quad * 32) << 16) + (unsigned)(gi * kTN + cbase + cb * kLd), acc[gi]);
-            tmem_wait_ld();
+              for (int gi = 0; gi <= TG; ++gi)
+                tmem_ld8(tmem + ((unsigned)(quad * 32) << 16) + (unsigned)(gi * kTN + cbase + cb * kLd), acc[gi]);
+              tmem_wait_ld();
 #pragma unroll
-            for (int c = 0; c < kLd; ++c) {
-              // sum_g acc[g] 256^(TG-g): the four lowest groups combine exactly in
-              // int64 (< 2^51), the higher ones exactly in FP64 (< 2^43); one rounding
-              constexpr int G0 = TG >= 3 ? TG - 3 : 0;
-              long long lo = acc[G0][c];
+              for (int c = 0; c < kLd; ++c) {
+                // sum_g acc[g] 256^(TG-g): the (up to) four lowest groups combine
+                // exactly in int64 (|lo| < 2^51), the higher ones likewise
+                // (|hi| < 2^43), both by wide multiply-adds onto the bias; one
+                // rounding where hi 256^(TG-G0+1) + lo is formed
+                constexpr int G0 = TG >= 3 ? TG - 3 : 0;
+                long long lo = mad_wide(acc[TG][c], 1, kBias);
 #pragma unroll
-              for (int gi = G0 + 1; gi <= TG; ++gi) lo = lo * 256 + acc[gi][c];
-              double v = (double)lo;
-              if constexpr (G0 > 0) {
-                double hi = i2d(acc[0][c]);
+                for (int gi = TG - 1; gi >= G0; --gi) lo = mad_wide(acc[gi][c], 1 << (8 * (TG - gi)), lo);
+                double v = __longlong_as_double(lo) - kBiasD;
+                if constexpr (G0 > 0) {
+                  long long hi = mad_wide(acc[G0 - 1][c], 1, kBias);
 #pragma unroll
-                for (int gi = 1; gi < G0; ++gi) hi = fma(hi, 256.0, i2d(acc[gi][c]));
-                v = fma(hi, pow2(8 * (TG - G0 + 1)), v);
+                  for (int gi = G0 - 2; gi >= 0; --gi) hi = mad_wide(acc[gi][c], 1 << (8 * (G0 - 1 - gi)), hi);
+                  v = fma(__longlong_as_double(hi) - kBiasD, pow2(8 * (TG - G0 + 1)), v);
+                }
+                const int eB = __shfl_sync(0xffffffffu, eBl, cb * kLd + c);
+                const double sc = F ? __longlong_as_double((long long)(ea + eB + 1023) << 52) : pow2(ea + eB);
+                val[cb * kLd + c] = v * sc;
               }
-              const int eB = __shfl_sync(0xffffffffu, eBl, cb * kLd + c);
-              val[cb * kLd + c] = v * (wscale * pow2(eA + eB));
             }
-          }
+          };
+          if (fast) drain(std::true_type{});
+          else drain(std::false_type{});
         } else {
 #pragma unroll
           for (int c = 0; c < kCols; ++c) val[c] = 0.0;
