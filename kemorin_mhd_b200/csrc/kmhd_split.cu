@@ -635,7 +635,6 @@ struct GemmArgs {
 
 constexpr int kEpiWarps = 16;                // four per TMEM lane quadrant
 constexpr int kGemmWarps = 2 + kEpiWarps;    // MMA issuer, bulk-copy producer, epilogue
-constexpr int kEpiThreads = 32 * kEpiWarps;
 constexpr int kCols = kTN * 4 / kEpiWarps;   // columns recombined by one epilogue warp
 constexpr int kLd = 8;                       // columns per TMEM load
 constexpr int kRing = 4;           // stage ring depth
@@ -745,7 +744,7 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
       mbar_init(&empty[q], 1);
     }
     mbar_init(done, 1);
-    mbar_init(tfree, kEpiThreads);
+    mbar_init(tfree, kEpiWarps);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 0) {
@@ -895,8 +894,10 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
 #pragma unroll
           for (int c = 0; c < kCols; ++c) val[c] = 0.0;
         }
+        // TMEM drained: one arrival per warp, after every lane's loads completed
         tc_fence_before();
-        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(sptr(tfree)) : "memory");
+        __syncwarp();
+        if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(sptr(tfree)) : "memory");
 
         if (h == 0) {
           // first tile of the pair: keep this thread's half row in shared memory
