@@ -211,6 +211,13 @@ struct SliceTabs {
   int ncolT[kNT];        // valid columns per type
   int npadT[kNT];        // padded columns per type
   int nrT, nrR;          // radius paddings (theta/phi and F2: 16; r and F1: 8)
+  // Forward tiles: byte kc of the 64-byte block bnz[64 (foff[m kNT + t] +
+  // n-tile) ..] is set to 1 by the forward slicer when any digit of K chunk kc
+  // of that tile is nonzero (at most 64 chunks tracked; types 4..7 only).  A
+  // chunk whose B digits are all zero adds nothing to the tile's products, so
+  // the GEMM skips it.
+  unsigned char* bnz;
+  const long long* foff;
 };
 
 // Column equilibration exponents: dexp = -(smallest e with max_rows |A[:,k]| < 2^e)
@@ -555,9 +562,12 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_mr(Plan P, SliceTabs S,
     const int nkc = geo.kpad / kTK;
     const int nt = gcol / kTN, blk = (gcol % kTN) >> 3, rbase = gcol & 7;
     signed char* base = S.B + S.boff[m * kNT + t];
+    unsigned char* live = nullptr;  // forward: the tile's live-chunk flags
+    if constexpr (FWD) live = S.bnz + 64 * (S.foff[m * kNT + t] + nt);
     for (int kc = ((warp - item0) % nw + nw) % nw; kc < nkc; kc += nw) {
       const int k = kc * kTK + kq;
       signed char* dst0 = base + (long long)(nt * nkc + kc) * NS * (kTN * kTK) + blk * 256;
+      uint32_t anynz = 0u;  // forward: OR of this lane's digit words
       for (int q = q4; q < (eight ? 8 : 4); q += 4) {
         // local column of block row rbase + q
         int c = -1;
@@ -575,6 +585,8 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_mr(Plan P, SliceTabs S,
           for (int s2 = 0; s2 < NS; ++s2) wd[s2] = 0u;
         }
         if constexpr (FWD) {
+#pragma unroll
+          for (int s2 = 0; s2 < NS; ++s2) anynz |= wd[s2];
           const int o = (kq >> 4) * 192 + (rbase + q) * 16 + (kq & 15);
 #pragma unroll
           for (int s2 = 0; s2 < NS; ++s2) *reinterpret_cast<uint32_t*>(wb + s2 * kSlab + o) = wd[s2];
@@ -585,6 +597,8 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_mr(Plan P, SliceTabs S,
         }
       }
       if constexpr (FWD) {
+        // live-chunk flag of the tile: every writer stores the same 1
+        if (__any_sync(0xffffffffu, anynz != 0u) && lane == 0 && kc < 64) live[kc] = 1;
         __syncwarp();
         if (eight) {
           for (int u = lane; u < NS * 16; u += 32) {
@@ -708,6 +722,27 @@ struct GemmLaunch {
   int gunits;
 };
 
+// Live K chunks of a work tile: forward tiles of at most 64 chunks read the
+// forward slicer's bits, every other tile takes all chunks.
+__device__ __forceinline__ unsigned long long chunk_mask(const SliceTabs& S, const Work& w, int nk, bool bwd) {
+  if (bwd || nk <= 0 || nk > 64) return ~0ull;
+  const uint4* f = reinterpret_cast<const uint4*>(S.bnz + 64 * (S.foff[w.m * kNT + w.t] + w.nt));
+  unsigned long long mk = 0ull;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    if (16 * i >= nk) break;
+    const uint4 q = __ldg(f + i);
+    const unsigned x[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      // flag bytes (0 or 1) of chunks 16 i + 4 j .. + 3 -> four bits
+      const unsigned b = (x[j] & 1u) | ((x[j] >> 7) & 2u) | ((x[j] >> 14) & 4u) | ((x[j] >> 21) & 8u);
+      mk |= (unsigned long long)b << (16 * i + 4 * j);
+    }
+  }
+  return mk;
+}
+
 template <int NS, int TG, bool GROUPED>
 __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_constant__ GemmLaunch L) {
   extern __shared__ __align__(1024) unsigned char sm[];
@@ -775,12 +810,15 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
           const int nk = nk_of(A.P, w);
           const signed char* Ag = S.A + S.aoff[w.m * kNT + w.t] + (long long)w.mt * nk * A_BYTES;
           const signed char* Bg = S.B + S.boff[w.m * kNT + w.t] + (long long)w.nt * nk * B_BYTES;
-          for (int kc = 0; kc < nk; ++kc, ++gc) {
+          const unsigned long long live = chunk_mask(S, w, nk, bwd);
+          for (int kc = 0; kc < nk; ++kc) {
+            if (!((live >> (kc & 63)) & 1ull)) continue;  // all-zero B digits: nothing to add
             const int st = (int)(gc % kRing);
             if (gc >= kRing && !mbar_wait(&empty[st], (unsigned)(((gc / kRing) - 1) & 1))) { ok = false; break; }
             mbar_expect_tx(&full[st], STAGE);
             bulk_g2s(sm + st * STAGE, Ag + (long long)kc * A_BYTES, A_BYTES, &full[st]);
             bulk_g2s(sm + st * STAGE + A_BYTES, Bg + (long long)kc * B_BYTES, B_BYTES, &full[st]);
+            ++gc;
           }
         }
       }
@@ -799,9 +837,12 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
         for (int h = 0; h < per; ++h, ++it) {
           const Work w = A.work[base + h];
           const int nk = nk_of(A.P, w);
+          const unsigned long long live = chunk_mask(A.S, w, nk, bwd);
           if (it > 0 && ok && !mbar_wait(tfree, (unsigned)((it - 1) & 1))) ok = false;
           tc_fence_after();
-          for (int kc = 0; kc < nk && ok; ++kc, ++gc) {
+          int issued = 0;  // the first issued chunk initialises the accumulators
+          for (int kc = 0; kc < nk && ok; ++kc) {
+            if (!((live >> (kc & 63)) & 1ull)) continue;
             const int st = (int)(gc % kRing);
             if (!mbar_wait(&full[st], (unsigned)((gc / kRing) & 1))) { ok = false; break; }
             tc_fence_after();
@@ -810,11 +851,13 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
             const uint64_t b0 = smem_desc(sm + st * STAGE + A_BYTES, 128, 256);
 #pragma unroll
             for (int q = 0; q < sch.n; ++q) {
-              const unsigned acc = (kc > 0 || !sch.init[q]) ? 1u : 0u;
+              const unsigned acc = (issued > 0 || !sch.init[q]) ? 1u : 0u;
               mma_i8(tmem + (unsigned)((sch.a[q] + sch.b[q]) * kTN), a0 + (uint64_t)(sch.a[q] * (kTM * kTK / 16)),
                      b0 + (uint64_t)(sch.b[q] * (kTN * kTK / 16)), make_idesc(kTN * sch.nb[q]), acc);
             }
             mma_commit(&empty[st]);
+            ++gc;
+            ++issued;
           }
           mma_commit(done);
         }
@@ -846,6 +889,7 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
         const int eA = (grow < g.rows) ? S.aexp[S.aeoff[w.m * kNT + w.t] + grow] : 0;
         // column exponents: lane i holds column cbase + i, broadcast by shuffles
         const int eBl = lane < kCols ? __ldg(S.bexp + S.beoff[w.m * kNT + w.t] + w.nt * kTN + cbase + lane) : 0;
+        const bool anylive = chunk_mask(S, w, nk, bwd) != 0ull;  // else no MMA wrote the accumulators
         // value scale 2^(ea + eB): built from its exponent bits when every
         // exponent of this warp's block is in the normal range (warp-uniform test)
         const int ea = eA + kW;
@@ -855,7 +899,7 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
         ok = __all_sync(0xffffffffu, ok);
         tc_fence_after();
         double val[kCols];  // columns cbase .. cbase + kCols - 1
-        if (nk > 0 && ok) {
+        if (nk > 0 && ok && anylive) {
           auto drain = [&](auto fastc) {
             constexpr bool F = decltype(fastc)::value;
 #pragma unroll
@@ -1075,7 +1119,8 @@ struct SplitState {
   SliceTabs S;
   std::vector<void*> allocs;
   int64_t bytes = 0;
-  std::vector<long long> aoff, aeoff, deoff, boff, beoff;
+  std::vector<long long> aoff, aeoff, deoff, boff, beoff, foff;
+  long long nbnz = 0;  // 64-byte tile blocks of S.bnz
   Work* work_b = nullptr;  // backward work (parity tile pairs)
   Work* work_f = nullptr;  // forward work
   int nwork_b = 0, nwork_f = 0;
@@ -1177,7 +1222,8 @@ int split_create(SplitState** out, const Plan& p, int tier, int nslice, cudaStre
   s->deoff.resize((L + 1) * kNT);
   s->boff.resize((L + 1) * kNT);
   s->beoff.resize((L + 1) * kNT);
-  long long ao = 0, aeo = 0, deo = 0, bo = 0, beo = 0;
+  s->foff.resize((L + 1) * kNT);
+  long long ao = 0, aeo = 0, deo = 0, bo = 0, beo = 0, fo = 0;
   std::vector<Work> wb, wf;
   for (int m = 0; m <= L; ++m)
     for (int t = 0; t < kNT; ++t) {
@@ -1188,6 +1234,8 @@ int split_create(SplitState** out, const Plan& p, int tier, int nslice, cudaStre
       s->deoff[i] = deo;
       s->boff[i] = bo;
       s->beoff[i] = beo;
+      s->foff[i] = fo;
+      if (t >= 4) fo += S.npadT[t] / kTN;
       ao += (long long)g.rpad * g.kpad * s->ns;
       aeo += g.rpad;
       deo += g.kpad;
@@ -1223,13 +1271,15 @@ int split_create(SplitState** out, const Plan& p, int tier, int nslice, cudaStre
     }
   }
   int st_ = KMHD_OK;
-  long long *aoff_d, *aeoff_d, *deoff_d, *boff_d, *beoff_d;
+  long long *aoff_d, *aeoff_d, *deoff_d, *boff_d, *beoff_d, *foff_d;
+  s->nbnz = fo;
   if (p.err) s->err = p.err;  // the instance's error word
   if ((st_ = salloc(s, &S.A, (size_t)ao)) || (st_ = salloc(s, &S.aexp, (size_t)aeo)) ||
       (st_ = salloc(s, &S.dexp, (size_t)deo)) || (st_ = salloc(s, &S.B, (size_t)bo)) ||
       (st_ = salloc(s, &S.bexp, (size_t)beo)) || (st_ = salloc(s, &aoff_d, s->aoff.size())) ||
       (st_ = salloc(s, &aeoff_d, s->aeoff.size())) || (st_ = salloc(s, &deoff_d, s->deoff.size())) ||
       (st_ = salloc(s, &boff_d, s->boff.size())) || (st_ = salloc(s, &beoff_d, s->beoff.size())) ||
+      (st_ = salloc(s, &foff_d, s->foff.size())) || (st_ = salloc(s, &S.bnz, (size_t)fo * 64)) ||
       (st_ = salloc(s, &s->work_b, wb.size())) || (st_ = salloc(s, &s->work_f, wf.size())) ||
       (!p.err && (st_ = salloc(s, &s->err, 1)))) {
     split_destroy(s);
@@ -1240,6 +1290,7 @@ int split_create(SplitState** out, const Plan& p, int tier, int nslice, cudaStre
   S.deoff = deoff_d;
   S.boff = boff_d;
   S.beoff = beoff_d;
+  S.foff = foff_d;
   s->nwork_b = (int)wb.size();
   s->nwork_f = (int)wf.size();
   s->wb_h = wb;
@@ -1250,6 +1301,8 @@ int split_create(SplitState** out, const Plan& p, int tier, int nslice, cudaStre
       up(deoff_d, s->deoff.data(), sizeof(long long) * s->deoff.size()) ||
       up(boff_d, s->boff.data(), sizeof(long long) * s->boff.size()) ||
       up(beoff_d, s->beoff.data(), sizeof(long long) * s->beoff.size()) ||
+      up(foff_d, s->foff.data(), sizeof(long long) * s->foff.size()) ||
+      cudaMemsetAsync(S.bnz, 0, 64 * (size_t)(fo > 0 ? fo : 1), st) ||
       (wb.size() && up(s->work_b, wb.data(), sizeof(Work) * wb.size())) ||
       (wf.size() && up(s->work_f, wf.data(), sizeof(Work) * wf.size())) ||
       cudaMemsetAsync(s->err, 0, sizeof(int), st) || cudaMemsetAsync(S.B, 0, (size_t)bo, st) ||
@@ -1359,6 +1412,10 @@ int split_slicer(SplitState* s, const Plan& p, bool fwd, const double* d_rj, lon
   auto kern = fwd ? (s->ns == 6 ? k_slice_mr<true, 6> : k_slice_mr<true, 4>)
                   : (s->ns == 6 ? k_slice_mr<false, 6> : k_slice_mr<false, 4>);
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return KMHD_ERR_CUDA;
+  // the forward slicer sets the live-chunk bits of the tiles it cuts
+  if (fwd && p.r_hi > p.r_lo && s->nbnz > 0 &&
+      cudaMemsetAsync(S.bnz, 0, 64 * (size_t)s->nbnz, st) != cudaSuccess)
     return KMHD_ERR_CUDA;
   if (p.r_hi > p.r_lo)
     kern<<<dim3((fwd ? p.nvf : p.nvb) + 1, p.r_hi - p.r_lo, p.L + 1), kSliceThreads, smem, st>>>(p, S, d_rj, ld, cols);
