@@ -966,10 +966,12 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
           if (w.t == 5) {
             // column c = 8 (block - 8 nt) + 2 (f % 4) + slot, block = (f / 4) nrR + r
             const double g60 = g6_of(l0, w.m), g61 = g6_of(l1, w.m);
+            // nrR is a multiple of 8, so the tile's 8-column blocks share one field group
+            const int rg0 = w.nt * (kTN / 8) + cbase / 8;
+            const int fg = rg0 / S.nrR, r0 = rg0 - fg * S.nrR;
 #pragma unroll
             for (int rr = 0; rr < kCols / 8; ++rr) {
-              const int rg = w.nt * (kTN / 8) + cbase / 8 + rr;
-              const int fg = rg / S.nrR, r = rg - fg * S.nrR;
+              const int r = r0 + rr;
               if (r >= P.nr) continue;
               const double r1 = P.radius[r];
               const long long jr = P.J * (long long)r;
@@ -992,11 +994,13 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
               }
             }
           } else {
-            // column c = 4 (r + nrT v) + q, q = 2 (component - 1) + slot
+            // column c = 4 (r + nrT v) + q, q = 2 (component - 1) + slot; nrT is a
+            // multiple of 16, so the tile's columns belong to one vector
+            const int rv0 = w.nt * (kTN / 4) + cbase / 4;
+            const int v = rv0 / S.nrT, r0 = rv0 - v * S.nrT;
 #pragma unroll
             for (int c4 = 0; c4 < kCols / 4; ++c4) {
-              const int rv = w.nt * (kTN / 4) + cbase / 4 + c4;
-              const int r = rv % S.nrT, v = rv / S.nrT;
+              const int r = r0 + c4;
               if (v >= P.nvf) break;
               if (r >= P.nr) continue;
               const double rr1 = P.radius[r];
@@ -1032,11 +1036,13 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
             double* baseN = P.rtm_b + rtm_off(P, w.m, th, 0, P.ncb);
             double* baseS = P.rtm_b + rtm_off(P, w.m, P.nth - 1 - th, 0, P.ncb);
             if (w.t <= 1) {
-              // column c = 4 (r + nrT v) + q: one vector's (theta c, theta s, phi c, phi s)
+              // column c = 4 (r + nrT v) + q: one vector's (theta c, theta s, phi c, phi s);
+              // nrT is a multiple of 16, so the tile's columns belong to one vector
+              const int g0 = (w.nt * kTN + cbase) >> 2;
+              const int vv = g0 / S.nrT, r0 = g0 - vv * S.nrT;
 #pragma unroll
               for (int c = 0; c < kCols; c += 4) {
-                const int col = w.nt * kTN + cbase + c;
-                const int r = (col >> 2) % S.nrT, vv = (col >> 2) / S.nrT;
+                const int r = r0 + (c >> 2);
                 if (vv >= P.nvb || r >= P.nr) continue;
                 const double2 a01 = *reinterpret_cast<const double2*>(sr + c);
                 const double2 a23 = *reinterpret_cast<const double2*>(sr + c + 2);
@@ -1065,10 +1071,12 @@ __global__ void __launch_bounds__(kGemmWarps * 32, 1) k_split_gemm(const __grid_
               // column c = 8 (block - 8 nt) + 2 (f % 4) + slot, block = (f / 4) nrR + r:
               // radial components and scalars, record words 4 nvb + 2 f
               const int nF = P.nvb + P.nsb;
+              // nrR is a multiple of 8, so the tile's 8-column blocks share one field group
+              const int rg0 = w.nt * (kTN / 8) + cbase / 8;
+              const int fg = rg0 / S.nrR, r0 = rg0 - fg * S.nrR;
 #pragma unroll
               for (int rr = 0; rr < kCols / 8; ++rr) {
-                const int rg = w.nt * (kTN / 8) + cbase / 8 + rr;
-                const int fg = rg / S.nrR, r = rg - fg * S.nrR;
+                const int r = r0 + rr;
                 if (r >= P.nr || 4 * fg >= nF) continue;
                 double* dN = baseN + (long long)r * rec + 4 * P.nvb + 8 * fg;
                 double* dS = baseS + (long long)r * rec + 4 * P.nvb + 8 * fg;
