@@ -263,8 +263,9 @@ __global__ void k_a_slices(Plan P, SliceTabs S, int t) {
 // quantity q (8 columns), for each field f < 4: types 2/3 slots (4 columns);
 // forward: types 4/5 (field f, slot) and types 6/7 (vector v, quantity q).
 constexpr int kGrpCols = 24;  // derived columns of one slicer field group (at most 6 fields x 2 slots x 2 types)
-// slicer CTA size (measured at L = 511: 256 threads 14.2 ms, 384 18.6 ms,
-// 512 15.0 ms for the forward slicer)
+// slicer CTA size (measured at L = 511 for the forward slicer: 256 threads
+// 14.2 ms, 384 18.6 ms, 512 15.0 ms; in a later build 256 13.6 ms, 192
+// 14.3 ms, 320 17.4 ms)
 constexpr int kSliceThreads = 256;
 constexpr int kSlab = 320;    // per-slice staging bytes of one 256-byte tile block (k halves 192 apart)
 
