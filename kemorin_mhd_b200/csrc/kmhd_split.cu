@@ -385,6 +385,16 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_mr(Plan P, SliceTabs S,
     // 256-bit loads need 32-byte aligned records (an even forward component count)
     const bool v4 = ((reinterpret_cast<uintptr_t>(P.rtm_f) | (uintptr_t)(16 * P.ncf)) & 31) == 0;
     double2 nxt = make_double2(0.0, 0.0), sxt = nxt;  // second field of a 256-bit load
+    // vector groups: the sectors of the thread's second row are loaded before
+    // the first row is processed (twice the loads in flight)
+    const int th2 = threadIdx.x + blockDim.x;
+    const bool pre = vgrp && v4 && th2 < P.nh;
+    double pn2[4] = {0.0, 0.0, 0.0, 0.0}, ps2[4] = {0.0, 0.0, 0.0, 0.0};
+    if (pre) {
+      ld_global_v4(base + th2 * strideTh, pn2[0], pn2[1], pn2[2], pn2[3]);
+      if (th2 < P.nth / 2)
+        ld_global_v4(base + (long long)(P.nth - 1 - th2) * strideTh, ps2[0], ps2[1], ps2[2], ps2[3]);
+    }
     for (int th = threadIdx.x; th < P.nh; th += blockDim.x) {
       const bool hasS = th < P.nth / 2;
       const double w = __ldg(P.weight + th);
@@ -395,7 +405,13 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_mr(Plan P, SliceTabs S,
         // words (theta slot 0, theta slot 1, phi slot 0, phi slot 1): one
         // 32-byte sector per row, one 256-bit load when the records are aligned
         double nn[4], ss[4] = {0.0, 0.0, 0.0, 0.0};
-        if (v4) {
+        if (pre && th == th2) {
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            nn[c] = pn2[c];
+            ss[c] = ps2[c];
+          }
+        } else if (v4) {
           ld_global_v4(pn, nn[0], nn[1], nn[2], nn[3]);
           if (hasS) ld_global_v4(ps, ss[0], ss[1], ss[2], ss[3]);
         } else {
