@@ -385,10 +385,11 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_mr(Plan P, SliceTabs S,
     // 256-bit loads need 32-byte aligned records (an even forward component count)
     const bool v4 = ((reinterpret_cast<uintptr_t>(P.rtm_f) | (uintptr_t)(16 * P.ncf)) & 31) == 0;
     double2 nxt = make_double2(0.0, 0.0), sxt = nxt;  // second field of a 256-bit load
-    // vector groups: the sectors of the thread's second row are loaded before
-    // the first row is processed (twice the loads in flight)
+    // the thread's second row is loaded (vector groups) or its first sector
+    // pair (radial / scalar group: fields 0 and 1) before the first row is
+    // processed: twice the loads in flight
     const int th2 = threadIdx.x + blockDim.x;
-    const bool pre = vgrp && v4 && th2 < P.nh;
+    const bool pre = v4 && th2 < P.nh && (vgrp || nF >= 2);
     double pn2[4] = {0.0, 0.0, 0.0, 0.0}, ps2[4] = {0.0, 0.0, 0.0, 0.0};
     if (pre) {
       ld_global_v4(base + th2 * strideTh, pn2[0], pn2[1], pn2[2], pn2[3]);
@@ -458,8 +459,13 @@ __global__ void __launch_bounds__(kSliceThreads) k_slice_mr(Plan P, SliceTabs S,
           if (v4 && f + 1 < nF && !(f & 1)) {
             // fields f, f + 1 in one 32-byte sector
             double4 a, b = make_double4(0.0, 0.0, 0.0, 0.0);
-            ld_global_v4(pn + 2 * f, a.x, a.y, a.z, a.w);
-            if (hasS) ld_global_v4(ps + 2 * f, b.x, b.y, b.z, b.w);
+            if (pre && th == th2 && f == 0) {
+              a = make_double4(pn2[0], pn2[1], pn2[2], pn2[3]);
+              b = make_double4(ps2[0], ps2[1], ps2[2], ps2[3]);
+            } else {
+              ld_global_v4(pn + 2 * f, a.x, a.y, a.z, a.w);
+              if (hasS) ld_global_v4(ps + 2 * f, b.x, b.y, b.z, b.w);
+            }
             nn = make_double2(a.x, a.y);
             ss = make_double2(b.x, b.y);
             nxt = make_double2(a.z, a.w);
